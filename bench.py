@@ -1,0 +1,362 @@
+"""Benchmark of the SHORE L1 volume fit (voxels/s).
+
+Workload: the brain-sized synthetic volume (96 x 114 x 96 grid, ellipsoidal
+mask of 299,432 voxels, CS-DSI table with N = 259, radial order 6 -> K = 72,
+zeta 700), L1 FISTA with a fixed alpha = 0.01 at the reference defaults
+(max_iter 1000, tol 1e-6), FP64.  One step = one whole-volume fit.
+
+* value   voxels/s with the volume already resident in HBM (device entry
+          point), CUDA events on the fit stream, max over ranks.
+* e2e     the same fit through the reference-facing C ABI with host buffers:
+          pinned host volume -> device, fit, coefficient volume -> host, every
+          step (host clock around the blocking call).
+* roofline  the dominant kernel (FP64 FISTA on DMMA tensor cores): algorithmic
+          FLOPs = executed voxel-iterations x (2K^2 + 8K) per launch over the
+          kernel's event-timed duration, against the FP64 DMMA peak measured
+          live by libcsdpeak (no FP64 figure exists in MEASURED_PEAKS.json).
+* cpu_baseline  the CPU FP64 oracle (a restatement of the reference's rayon
+          path: the Rust reference cannot be built without cargo) on all host
+          threads, on a bounded sample of the same voxels.
+
+``--impl reference`` times that CPU path alone, as the reference arm.
+Multi-GPU (torchrun): every rank fits its own copy of the volume (independent
+subjects; weak scaling, no collective in the data path).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SHORE L1-fit voxels/s (FP64, radial order 6, fixed alpha 0.01)"
+WORKLOAD = "brain300k"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU sample")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", choices=["brain300k", "grid64k"], default="brain300k",
+                    help="brain300k: the benchmark volume; grid64k: 40^3 fully masked (profiling case)")
+    return ap.parse_args()
+
+
+def fit_kwargs():
+    return dict(alpha_mode="fixed", alpha=0.01, max_iter=1000, tol=1e-6, radial_order=6, zeta=700.0)
+
+
+def load_phantom():
+    from cs_dmri_b200.phantom import config_phantom
+    return config_phantom(WORKLOAD)
+
+
+def select_workload(name: str) -> None:
+    global WORKLOAD
+    WORKLOAD = name
+
+
+# ------------------------------------------------------------------ CPU leg
+
+def cpu_sample_rate(ph, target_s: float, threads: int = 0):
+    """Voxels/s of the CPU FP64 oracle on a bounded sample of the volume."""
+    import numpy as np
+    from oracle import oracle as O
+
+    ids = np.flatnonzero(ph.mask.ravel())
+    n = ph.data.shape[-1]
+    flat = ph.data.reshape(-1, n)
+    kw = fit_kwargs()
+
+    def run(count):
+        sub = flat[ids[:count]].reshape(count, 1, 1, n)
+        m = np.ones((count, 1, 1), bool)
+        t = time.perf_counter()
+        O.shore_fit(sub, ph.bvals, ph.bvecs, m, big_delta=ph.big_delta, small_delta=ph.small_delta,
+                    n_threads=threads, return_coef64=False, **kw)
+        return time.perf_counter() - t
+
+    cores = threads or O.cpu_count()
+    probe = max(64, 8 * cores)
+    t = run(probe)
+    count = int(min(len(ids), max(probe, probe * target_s / max(t, 1e-3))))
+    t = run(count)
+    return count / t, count, cores, t
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                mhz.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, p[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+# ------------------------------------------------------------------ helpers
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def traffic_from_profile():
+    """Per-launch DRAM bytes of the FISTA kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "k_fista_fp64_brain300k.md"
+    if not p.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+def fp64_peak_tflops(device: int):
+    import ctypes
+    lib = ctypes.CDLL(str(ROOT / "cs_dmri_b200" / "libcsdpeak.so"))
+    a, b = ctypes.c_double(), ctypes.c_double()
+    vals = []
+    for _ in range(3):
+        if lib.csd_peak_fp64(device, ctypes.byref(a), ctypes.byref(b)) != 0:
+            return None, None
+        vals.append((a.value, b.value))
+    return max(v[0] for v in vals), max(v[1] for v in vals)
+
+
+# ------------------------------------------------------------------ arms
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    ph = load_phantom()
+    from oracle import oracle as O
+    O.build()
+    vals = []
+    cores = O.cpu_count()
+    count = 0
+    for i in range(args.warmup + args.steps):
+        rate, count, cores, t = cpu_sample_rate(ph, args.cpu_seconds / 2, threads=0)
+        if i >= args.warmup:
+            vals.append(rate)
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * ph.n_voxels / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded CS-DSI multi-tensor phantom, S0 1000, SNR 25)",
+        "config": {"workload": WORKLOAD, "voxels": ph.n_voxels, "N": 259, "K": 72, "alpha": 0.01,
+                   "solver": "FISTA fixed alpha"},
+        "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": cores, "kind": "port",
+                         "sample": f"{count} of the {ph.n_voxels} masked voxels per step (CPU FP64 oracle, "
+                                   "all host threads; the Rust reference needs cargo, absent here)"},
+        "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup(args)
+    device = local if world > 1 else 0
+    torch.cuda.set_device(device)
+    from cs_dmri_b200 import _abi, shore_fit, shore_fit_device
+
+    ph = load_phantom()
+    kw = fit_kwargs()
+    X, Y, Z, N = ph.data.shape
+    K = 72
+    d_data = torch.from_numpy(ph.data).to(f"cuda:{device}")
+    d_mask = torch.from_numpy(ph.mask).to(f"cuda:{device}")
+    coeffs = torch.empty((X, Y, Z, K), dtype=torch.float32, device=f"cuda:{device}")
+    stream = torch.cuda.Stream(device=device)
+
+    def device_step():
+        c, res = shore_fit_device(d_data, d_mask, ph.bvals, ph.bvecs, coefficients=coeffs, stream=stream,
+                                  device=device, big_delta=ph.big_delta, small_delta=ph.small_delta, **kw)
+        return res
+
+    # ---- value: inputs resident in HBM (1.09 GB volume > 126 MB L2 per step)
+    for _ in range(args.warmup):
+        device_step()
+    torch.cuda.synchronize(device)
+    barrier(world)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    kernel_ms, solve_flops, launches, iters = [], [], 0, []
+    with ClockSampler(device) as clocks:
+        torch.cuda.synchronize(device)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            res = device_step()
+            tm = _abi.last_timing(device)
+            kernel_ms.append(tm.ms_solve_kernel)
+            iters.append(res.total_iterations)
+            launches += tm.launches
+        ev1.record(stream)
+        torch.cuda.synchronize(device)
+    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms, world, torch.device("cuda", device))
+    V = int(ph.mask.sum())
+    value = world * V * args.steps / (ms / 1e3)
+
+    # ---- e2e: host buffers through the C ABI (pinned host volume)
+    pinned = torch.empty(ph.data.shape, dtype=torch.float32, pin_memory=True)
+    pinned.numpy()[...] = ph.data
+    host_data = pinned.numpy()
+    e2e_t = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize(device)
+        barrier(world)
+        t = time.perf_counter()
+        out = shore_fit(host_data, ph.bvals, ph.bvecs, ph.mask, big_delta=ph.big_delta,
+                        small_delta=ph.small_delta, device=device, **kw)
+        dt = time.perf_counter() - t
+        if i >= args.warmup:
+            e2e_t.append(dt)
+    e2e_s = max_over_ranks(sum(e2e_t), world, torch.device("cuda", device))
+    e2e_value = world * V * args.steps / e2e_s
+    h2d = ph.data.nbytes + ph.mask.nbytes
+    d2h = out["coefficients"].nbytes
+
+    # ---- roofline of the FISTA kernel
+    flops_per_iter = 2 * K * K + 8 * K
+    k_ms = statistics.median(kernel_ms)
+    it_launch = statistics.median(iters)
+    achieved = it_launch * flops_per_iter / (k_ms * 1e-3) / 1e12
+    dmma_peak, dfma_peak = fp64_peak_tflops(device)
+    traffic = traffic_from_profile()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, count, cores, t = cpu_sample_rate(ph, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "voxels/s", "cores": cores, "kind": "port",
+               "sample": f"{count} of the {V} masked voxels ({t:.1f} s, CPU FP64 oracle on all host threads)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded CS-DSI multi-tensor phantom, S0 1000, SNR 25)",
+            "config": {"workload": WORKLOAD, "voxels": V, "grid": [X, Y, Z], "N": N, "K": K, "alpha": 0.01,
+                       "solver": "FISTA fixed alpha, FP64 (reference stopping rule)",
+                       "l2": "inputs larger than L2 (1.09 GB volume per step)",
+                       "parallelism": f"{world} independent volume(s), one per GPU"},
+            "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": dmma_peak, "unit": "TFLOP/s",
+                         "frac": (achieved / dmma_peak) if dmma_peak else None, "traffic": traffic,
+                         "kernel": "k_fista_fp64<9>", "kernel_ms": k_ms,
+                         "flops_per_launch": it_launch * flops_per_iter,
+                         "peak_source": "FP64 DMMA microbenchmark measured in this run (libcsdpeak); "
+                                        f"scalar DFMA measured {dfma_peak:.1f} TFLOP/s" if dmma_peak else None},
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "iterations_per_voxel": it_launch / V,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    select_workload(args.workload)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

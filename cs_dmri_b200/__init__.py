@@ -1,0 +1,15 @@
+"""B200-native 3D-SHORE fit with the interface of cs_dmri's SHORE path.
+
+``ShoreModel(gtab).fit(data, mask)`` and ``shore_fit(...)`` mirror
+``cs_dmri.ShoreModel`` and ``cs_dmri._cs_dmri.shore_fit``; every per-voxel
+computation runs in libcsdshore.so (hand-written CUDA for sm_100a) behind the
+C ABI declared in include/csd_shore.h.
+"""
+
+from ._core import affine_rotation, design_matrix, shore_fit, shore_fit_device
+from .gradients import GradientTable, as_gradient_table, read_bvals_bvecs
+from .shore import ShoreFit, ShoreModel
+
+__all__ = ["ShoreModel", "ShoreFit", "GradientTable", "as_gradient_table", "read_bvals_bvecs",
+           "shore_fit", "shore_fit_device", "design_matrix", "affine_rotation"]
+__version__ = "0.1.0"

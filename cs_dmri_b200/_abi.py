@@ -1,0 +1,197 @@
+"""ctypes mirror of include/csd_shore.h and the loader of libcsdshore.so.
+
+The CUDA library is the only implementation of the fit: if it is missing or
+cannot be loaded this module raises, it never substitutes another code path.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libcsdshore.so"
+
+# enum csd_status / csd_regularization / csd_alpha_mode / csd_precision
+OK, ERR_INVALID, ERR_FIT_REFUSED, ERR_NUMERICAL, ERR_CUDA, ERR_TIMEOUT = range(6)
+REG_L1, REG_L2, REG_NONNEG = 1, 2, 3
+ALPHA_FIXED, ALPHA_RATIO, ALPHA_PATH_BIC, ALPHA_L2_ANCHORED = range(4)
+PRECISION_FP64 = 0
+
+
+class Gtab(C.Structure):
+    _fields_ = [
+        ("bvals", C.POINTER(C.c_double)),
+        ("bvecs", C.POINTER(C.c_double)),
+        ("n", C.c_int32),
+        ("big_delta", C.c_double),
+        ("small_delta", C.c_double),
+        ("b0_threshold", C.c_double),
+    ]
+
+
+class Spec(C.Structure):
+    _fields_ = [
+        ("radial_order", C.c_int32),
+        ("zeta", C.c_double),
+        ("regularization", C.c_int32),
+        ("alpha_mode", C.c_int32),
+        ("alpha", C.c_double),
+        ("alpha_ratio", C.c_double),
+        ("path_n_alphas", C.c_int32),
+        ("path_eps", C.c_double),
+        ("slack", C.c_double),
+        ("max_iter", C.c_int32),
+        ("tol", C.c_double),
+        ("non_negative", C.c_int32),
+        ("lambda_n", C.c_double),
+        ("lambda_l", C.c_double),
+        ("nonneg_max_iter", C.c_int32),
+        ("nonneg_tol", C.c_double),
+        ("nonneg_epsilon", C.c_double),
+        ("diagnostics", C.c_int32),
+        ("allow_single_shell", C.c_int32),
+        ("precision", C.c_int32),
+    ]
+
+
+class FitResult(C.Structure):
+    _fields_ = [
+        ("coefficients", C.c_void_p),
+        ("r2", C.c_void_p),
+        ("residual_l2", C.c_void_p),
+        ("iterations", C.c_void_p),
+        ("regularization_kind", C.c_void_p),
+        ("alpha", C.c_void_p),
+        ("bic", C.c_void_p),
+        ("rss_l2", C.c_void_p),
+        ("coef64", C.c_void_p),
+        ("converged", C.c_void_p),
+        ("n_coeffs", C.c_int32),
+        ("n_voxels", C.c_int64),
+        ("has_alpha_distribution", C.c_int32),
+        ("alpha_distribution", C.c_double * 3),
+        ("representative_alpha", C.c_double),
+        ("big_delta_seconds", C.c_double),
+        ("small_delta_seconds", C.c_double),
+        ("tau_seconds", C.c_double),
+        ("delta_source", C.c_int32),
+        ("n_shells", C.c_int32),
+        ("dwi_shells", C.c_double * 32),
+        ("lmax", C.c_int32),
+        ("n_constraint_dirs", C.c_int32),
+        ("total_iterations", C.c_uint64),
+        ("warnings", C.c_char * 2048),
+    ]
+
+
+class Timing(C.Structure):
+    _fields_ = [
+        ("ms_setup", C.c_float),
+        ("ms_rhs", C.c_float),
+        ("ms_solve", C.c_float),
+        ("ms_epilogue", C.c_float),
+        ("ms_total", C.c_float),
+        ("launches", C.c_int32),
+        ("ms_solve_kernel", C.c_float),
+    ]
+
+
+# Every symbol include/csd_shore.h declares, for load checks.
+EXPORTS = (
+    "csd_version",
+    "csd_abi_version",
+    "csd_default_spec",
+    "csd_shore_n_coeffs",
+    "csd_create",
+    "csd_destroy",
+    "csd_shore_fit_volume",
+    "csd_shore_fit_volume_device",
+    "csd_shore_design_matrix",
+    "csd_last_timing",
+)
+
+_lib = None
+_lock = threading.Lock()
+
+
+def _declare(lib: C.CDLL) -> C.CDLL:
+    lib.csd_version.restype = C.c_char_p
+    lib.csd_version.argtypes = []
+    lib.csd_abi_version.restype = C.c_int
+    lib.csd_abi_version.argtypes = []
+    lib.csd_default_spec.restype = None
+    lib.csd_default_spec.argtypes = [C.POINTER(Spec)]
+    lib.csd_shore_n_coeffs.restype = C.c_int
+    lib.csd_shore_n_coeffs.argtypes = [C.c_int32]
+    lib.csd_create.restype = C.c_int
+    lib.csd_create.argtypes = [C.POINTER(C.c_void_p), C.c_int32, C.c_char_p, C.c_size_t]
+    lib.csd_destroy.restype = None
+    lib.csd_destroy.argtypes = [C.c_void_p]
+    fit_args = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64,
+                C.POINTER(Gtab), C.POINTER(Spec), C.POINTER(FitResult)]
+    lib.csd_shore_fit_volume.restype = C.c_int
+    lib.csd_shore_fit_volume.argtypes = fit_args + [C.c_char_p, C.c_size_t]
+    lib.csd_shore_fit_volume_device.restype = C.c_int
+    lib.csd_shore_fit_volume_device.argtypes = fit_args + [C.c_void_p, C.c_char_p, C.c_size_t]
+    lib.csd_shore_design_matrix.restype = C.c_int
+    lib.csd_shore_design_matrix.argtypes = [C.c_void_p, C.POINTER(Gtab), C.c_int32, C.c_double,
+                                            C.c_void_p, C.c_char_p, C.c_size_t]
+    lib.csd_last_timing.restype = C.c_int
+    lib.csd_last_timing.argtypes = [C.c_void_p, C.POINTER(Timing)]
+    return lib
+
+
+def load() -> C.CDLL:
+    """Load libcsdshore.so (raises if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                raise RuntimeError(
+                    f"{LIB_PATH.name} is not built; run `python -m cs_dmri_b200.build` "
+                    "(the fit has no implementation other than the CUDA library)")
+            _lib = _declare(C.CDLL(str(LIB_PATH)))
+    return _lib
+
+
+class CsdError(ValueError):
+    """Raised for a non-zero status; ValueError like the reference's map_err
+    (python/src/lib.rs:33-35)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+def check(code: int, err) -> None:
+    if code != OK:
+        raise CsdError(code, err.value.decode("utf-8", "replace"))
+
+
+_handles: dict[int, C.c_void_p] = {}
+
+
+def handle(device: int = 0) -> C.c_void_p:
+    """Process-wide handle of `device` (created on first use)."""
+    lib = load()
+    with _lock:
+        h = _handles.get(device)
+        if h is None:
+            h = C.c_void_p()
+            err = C.create_string_buffer(1024)
+            check(lib.csd_create(C.byref(h), device, err, len(err)), err)
+            _handles[device] = h
+    return h
+
+
+def default_spec() -> Spec:
+    s = Spec()
+    load().csd_default_spec(C.byref(s))
+    return s
+
+
+def last_timing(device: int = 0) -> Timing:
+    t = Timing()
+    load().csd_last_timing(handle(device), C.byref(t))
+    return t

@@ -1,0 +1,1026 @@
+// csd_shore.cu - host runtime and C ABI of the B200 SHORE volume fit.
+//
+// Replaces cs_dmri's fit_shore (src/fit.rs:687-805) and the three
+// fit_volume_* drivers (src/fit.rs:74-527) at volume granularity.  The host
+// side validates the specification exactly as the reference does (shell
+// guard, alpha-strategy checks, radial order), then queues the device
+// pipeline on one stream:
+//
+//   setup (cached per gradient table): design M, Gram G, Lipschitz L,
+//         Tikhonov factor, packed DMMA tiles, M^T
+//   compaction of the mask -> masked voxel list (x-y-z order)
+//   b = M^T s for every masked voxel
+//   solve: FISTA (fixed / ratio / path strategies) or Tikhonov
+//   epilogue: residual, R^2, BIC, maps, scatter to (X, Y, Z, K)
+//
+// Every per-voxel computation runs on the GPU; the host only handles the
+// gradient table (shells, TORTOISE deltas) and the one-number read-backs
+// (masked voxel count, factorisation status, executed iteration total).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/csd_shore.h"
+#include "device_math.cuh"
+#include "path_kernels.cuh"
+#include "setup_kernels.cuh"
+#include "solve_kernels.cuh"
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kTortoiseGmax = 80e-3;  // src/qspace.rs:262
+constexpr double kGyro = 267.51532e6;    // src/qspace.rs:265
+constexpr double kShellTolerance = 50.0; // src/fit.rs:618
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+#define CSD_CUDA(call)                                                                         \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) throw Error{CSD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+
+#define CSD_LAUNCH()                                                                          \
+  do {                                                                                         \
+    cudaError_t e_ = cudaGetLastError();                                                       \
+    if (e_ != cudaSuccess) throw Error{CSD_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)}; \
+    ++h->launches;                                                                             \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  void ensure(size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (bytes <= cap) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    CSD_CUDA(cudaMalloc(&p, bytes));
+    cap = bytes;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+uint64_t fnv1a(uint64_t h, const void* data, size_t n) {
+  const unsigned char* b = static_cast<const unsigned char*>(data);
+  for (size_t i = 0; i < n; ++i) {
+    h ^= b[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+// Gradient table on the host (src/qspace.rs:90-227, python/src/lib.rs:89-105).
+struct HostGtab {
+  std::vector<double> bvals, bvecs;
+  double big = 0, small = 0, b0 = 50.0, tau = 0;
+  int delta_source = 0;
+  std::vector<double> shells;  // mean b of the non-zero shells, ascending
+};
+
+void tortoise_deltas(const std::vector<double>& bvals, double gmax, double* big, double* small) {
+  double max_b = 0.0;
+  for (double b : bvals) max_b = std::max(max_b, b);
+  if (max_b <= 0.0) {
+    const double small_ms = std::pow(1.0, 1.0 / 3.0);
+    *big = 3.0 * small_ms * 1e-3;
+    *small = small_ms * 1e-3;
+    return;
+  }
+  const double temp = max_b / kGyro / kGyro / gmax / gmax / 2.0 * 1e6;
+  const double small_ms = std::pow(temp, 1.0 / 3.0) * 1000.0;
+  *big = small_ms * 3.0 * 1e-3;
+  *small = small_ms * 1e-3;
+}
+
+// Non-zero shells: a gradient joins the first shell within the tolerance,
+// whose b is the running mean; shells sorted by b (src/qspace.rs:171-197).
+std::vector<double> dwi_shells(const std::vector<double>& bvals, double b0_threshold) {
+  std::vector<double> b;
+  std::vector<size_t> cnt;
+  for (double v : bvals) {
+    if (v <= b0_threshold) continue;
+    size_t s = 0;
+    for (; s < b.size(); ++s)
+      if (std::fabs(b[s] - v) <= kShellTolerance) break;
+    if (s < b.size()) {
+      const double n = static_cast<double>(cnt[s]);
+      b[s] = (b[s] * n + v) / (n + 1.0);
+      cnt[s] += 1;
+    } else {
+      b.push_back(v);
+      cnt.push_back(1);
+    }
+  }
+  std::stable_sort(b.begin(), b.end());
+  return b;
+}
+
+HostGtab make_gtab(const csd_gtab* g) {
+  HostGtab t;
+  t.bvals.assign(g->bvals, g->bvals + g->n);
+  t.bvecs.assign(g->bvecs, g->bvecs + 3 * static_cast<size_t>(g->n));
+  if (!std::isnan(g->big_delta) && !std::isnan(g->small_delta)) {
+    t.big = g->big_delta;
+    t.small = g->small_delta;
+    t.delta_source = 0;
+  } else {
+    tortoise_deltas(t.bvals, kTortoiseGmax, &t.big, &t.small);
+    t.delta_source = 1;
+  }
+  t.b0 = g->b0_threshold;
+  t.tau = t.big - t.small / 3.0;
+  t.shells = dwi_shells(t.bvals, t.b0);
+  return t;
+}
+
+int n_coeffs(int radial_order) {
+  int k = 0;
+  for (int n = 0; n <= radial_order; ++n)
+    for (int l = 0; l <= n; l += 2) k += 2 * l + 1;
+  return k;
+}
+
+// Solve-kernel tile count for K coefficients (rows padded to 8).
+int mt_for(int K) { return (K + 7) / 8; }
+
+}  // namespace
+
+struct csd_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  int launches = 0;
+  cudaEvent_t ev[8] = {};
+  csd_fit_timing timing{};
+
+  // setup cache
+  uint64_t setup_key = 0;
+  bool setup_valid = false;
+  bool chol_valid = false;
+  uint64_t chol_key = 0;
+  int N = 0, K = 0, Kp = 0;
+  double lipschitz = 0.0, lambda_max = 0.0;
+  DevBuf bvals, bvecs, M, Mt, G, A, gfrag, scal, ok;
+
+  // per-fit buffers
+  DevBuf data, mask, coeffs, r2, resid, iters_map, kind_map, alpha_map, bic_map, rss_map;
+  DevBuf blk, total, vox, B, X, iters, conv, queue, itotal, resid_v, nnz_v;
+  DevBuf amax, zero, alpha_v, Xsel, Xfb, Xl2, rss_l2, list, active, pbest, psel, pact, palpha_sel,
+      pit_sel, pconv_sel, palpha_fb, pit_fb, pconv_fb, pcode;
+};
+
+namespace {
+
+void set_err(char* err, size_t len, const std::string& msg) {
+  if (err && len > 0) std::snprintf(err, len, "%s", msg.c_str());
+}
+
+// Build (or reuse) the per-gradient-table device setup.
+void ensure_setup(csd_handle* h, const HostGtab& g, int radial_order, double zeta, bool need_chol,
+                  double lambda_n, double lambda_l) {
+  const int N = static_cast<int>(g.bvals.size());
+  const int K = n_coeffs(radial_order);
+  const int Kp = 8 * mt_for(K);
+  uint64_t key = 1469598103934665603ull;
+  key = fnv1a(key, g.bvals.data(), g.bvals.size() * sizeof(double));
+  key = fnv1a(key, g.bvecs.data(), g.bvecs.size() * sizeof(double));
+  const double sc[4] = {g.tau, g.b0, zeta, static_cast<double>(radial_order)};
+  key = fnv1a(key, sc, sizeof sc);
+  cudaStream_t st = h->stream;
+  if (!(h->setup_valid && h->setup_key == key)) {
+    h->setup_valid = false;
+    h->chol_valid = false;
+    h->N = N;
+    h->K = K;
+    h->Kp = Kp;
+    h->bvals.ensure(sizeof(double) * N);
+    h->bvecs.ensure(sizeof(double) * 3 * N);
+    CSD_CUDA(cudaMemcpyAsync(h->bvals.p, g.bvals.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st));
+    CSD_CUDA(cudaMemcpyAsync(h->bvecs.p, g.bvecs.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+    h->M.ensure(sizeof(double) * N * K);
+    h->Mt.ensure(sizeof(double) * static_cast<size_t>(Kp) * N);
+    h->G.ensure(sizeof(double) * Kp * Kp);
+    h->A.ensure(sizeof(double) * Kp * Kp);
+    const int MT = Kp / 8, KT = Kp / 4;
+    h->gfrag.ensure(sizeof(double) * MT * KT * 32);
+    h->scal.ensure(sizeof(double) * 4);
+    h->ok.ensure(sizeof(int) * 4);
+    // 4 pi^2 tau in the reference's evaluation order (src/qspace.rs:384-385).
+    const double qdenom = 4.0 * kPi * kPi * g.tau;
+    const long long nk = static_cast<long long>(N) * K;
+    csd::k_design<<<static_cast<unsigned>((nk + 255) / 256), 256, 0, st>>>(
+        h->bvals.as<double>(), h->bvecs.as<double>(), N, K, radial_order, zeta, qdenom, g.b0,
+        h->M.as<double>());
+    CSD_LAUNCH();
+    csd::k_gram<<<(Kp * Kp + 255) / 256, 256, 0, st>>>(h->M.as<double>(), N, K, Kp, radial_order,
+                                                      0.0, 0.0, h->G.as<double>(), nullptr);
+    CSD_LAUNCH();
+    const size_t lsm = sizeof(double) * (static_cast<size_t>(Kp) * Kp + 2 * Kp);
+    CSD_CUDA(cudaFuncSetAttribute(csd::k_lipschitz, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(lsm)));
+    csd::k_lipschitz<<<1, 256, lsm, st>>>(h->G.as<double>(), Kp, N, 200000, h->scal.as<double>(),
+                                          h->scal.as<double>() + 1);
+    CSD_LAUNCH();
+    csd::k_pack_gfrag<<<(MT * KT * 32 + 255) / 256, 256, 0, st>>>(h->G.as<double>(), Kp,
+                                                                   h->gfrag.as<double>());
+    CSD_LAUNCH();
+    csd::k_transpose_design<<<(Kp * N + 255) / 256, 256, 0, st>>>(h->M.as<double>(), N, K, Kp,
+                                                                  h->Mt.as<double>());
+    CSD_LAUNCH();
+    double sc2[2];
+    CSD_CUDA(cudaMemcpyAsync(sc2, h->scal.p, sizeof sc2, cudaMemcpyDeviceToHost, st));
+    CSD_CUDA(cudaStreamSynchronize(st));
+    h->lipschitz = sc2[0];
+    h->lambda_max = sc2[1];
+    h->setup_key = key;
+    h->setup_valid = true;
+  }
+  if (need_chol) {
+    uint64_t ck = fnv1a(key, &lambda_n, sizeof lambda_n);
+    ck = fnv1a(ck, &lambda_l, sizeof lambda_l);
+    if (!(h->chol_valid && h->chol_key == ck)) {
+      csd::k_gram<<<(Kp * Kp + 255) / 256, 256, 0, st>>>(h->M.as<double>(), N, K, Kp, radial_order,
+                                                        lambda_n, lambda_l, h->G.as<double>(),
+                                                        h->A.as<double>());
+      CSD_LAUNCH();
+      const size_t csm = sizeof(double) * static_cast<size_t>(K) * K;
+      CSD_CUDA(cudaFuncSetAttribute(csd::k_cholesky, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(csm)));
+      csd::k_cholesky<<<1, 256, csm, st>>>(h->A.as<double>(), K, Kp, h->ok.as<int>());
+      CSD_LAUNCH();
+      int okv = 0;
+      CSD_CUDA(cudaMemcpyAsync(&okv, h->ok.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CSD_CUDA(cudaStreamSynchronize(st));
+      if (!okv) throw Error{CSD_ERR_NUMERICAL, "normal-equations matrix should be PD"};
+      h->chol_key = ck;
+      h->chol_valid = true;
+    }
+  }
+}
+
+// Masked voxel list; returns V.
+int64_t compact(csd_handle* h, const uint8_t* d_flags, int64_t n, DevBuf& out) {
+  cudaStream_t st = h->stream;
+  const int nblk = static_cast<int>((n + csd::kCompactBlock - 1) / csd::kCompactBlock);
+  h->blk.ensure(sizeof(int) * std::max(nblk, 1));
+  h->total.ensure(sizeof(long long));
+  out.ensure(sizeof(int64_t) * std::max<int64_t>(n, 1));
+  if (nblk == 0) return 0;
+  csd::k_mask_count<<<nblk, 256, 0, st>>>(d_flags, n, h->blk.as<int>());
+  CSD_LAUNCH();
+  csd::k_scan_blocks<<<1, 1024, 0, st>>>(h->blk.as<int>(), nblk, h->total.as<long long>());
+  CSD_LAUNCH();
+  csd::k_mask_compact<<<nblk, csd::kCompactBlock / 4, 0, st>>>(d_flags, n, h->blk.as<int>(),
+                                                              out.as<int64_t>());
+  CSD_LAUNCH();
+  long long total = 0;
+  CSD_CUDA(cudaMemcpyAsync(&total, h->total.p, sizeof total, cudaMemcpyDeviceToHost, st));
+  CSD_CUDA(cudaStreamSynchronize(st));
+  return static_cast<int64_t>(total);
+}
+
+inline unsigned grid1(int64_t n, int bs = 256) { return static_cast<unsigned>((n + bs - 1) / bs); }
+
+template <int MT>
+void launch_fista_t(csd_handle* h, const csd::FistaParams& p) {
+  constexpr int KP = 8 * MT, KT = 2 * MT;
+  const size_t smem = sizeof(double) * (static_cast<size_t>(MT) * KT * 32 + 8 * KP * 8);
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_fista_fp64<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  int per_sm = 0;
+  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_fista_fp64<MT>, 256, smem));
+  per_sm = std::max(per_sm, 1);
+  const int64_t warps_needed = (p.n_work + 7) / 8;
+  int64_t blocks = std::min<int64_t>(static_cast<int64_t>(h->num_sms) * per_sm, (warps_needed + 7) / 8);
+  blocks = std::max<int64_t>(blocks, 1);
+  csd::k_fista_fp64<MT><<<static_cast<unsigned>(blocks), 256, smem, h->stream>>>(p);
+  CSD_LAUNCH();
+}
+
+void launch_fista(csd_handle* h, int MT, const csd::FistaParams& p) {
+  if (p.max_iter <= 0) {
+    // An empty iteration loop: the warm start (or zero) is the result, with
+    // 0 iterations and not converged (fista.rs:126-140 with max_iter = 0).
+    csd::k_fista_noop<<<grid1(p.n_work * (h->Kp + 1)), 256, 0, h->stream>>>(p, h->Kp);
+    CSD_LAUNCH();
+    return;
+  }
+  switch (MT) {
+    case 1: launch_fista_t<1>(h, p); break;
+    case 4: launch_fista_t<4>(h, p); break;
+    case 9: launch_fista_t<9>(h, p); break;
+    default:
+      throw Error{CSD_ERR_INVALID, "FISTA kernel is built for radial orders 2, 4 and 6 (K <= 72); got K = " +
+                                       std::to_string(h->K)};
+  }
+}
+
+template <int KP>
+void launch_rhs_t(csd_handle* h, const float* d_data, int64_t V) {
+  const size_t smem = sizeof(double) * (32 * KP + 64 * 33);
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_rhs<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  csd::k_rhs<KP><<<static_cast<unsigned>((V + 63) / 64), 256, smem, h->stream>>>(
+      d_data, h->vox.as<int64_t>(), V, h->N, h->M.as<double>(), h->K, h->B.as<double>());
+  CSD_LAUNCH();
+}
+
+void launch_rhs(csd_handle* h, const float* d_data, int64_t V) {
+  switch (h->Kp) {
+    case 8: launch_rhs_t<8>(h, d_data, V); break;
+    case 32: launch_rhs_t<32>(h, d_data, V); break;
+    case 72: launch_rhs_t<72>(h, d_data, V); break;
+    case 152: launch_rhs_t<152>(h, d_data, V); break;
+    default: throw Error{CSD_ERR_INVALID, "unsupported coefficient count " + std::to_string(h->K)};
+  }
+}
+
+void launch_tikhonov(csd_handle* h, const double* B, double* X, int64_t V) {
+  const int K = h->K;
+  const size_t smem = sizeof(double) * static_cast<size_t>(K) * (K + 1);
+  const int rpl = (K + 31) / 32;
+  const int blocks = std::max(1, static_cast<int>(std::min<int64_t>((V + 7) / 8, h->num_sms * 8)));
+  auto go = [&](auto kern) {
+    CSD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    kern<<<blocks, 256, smem, h->stream>>>(h->A.as<double>(), K, h->Kp, B, X, V);
+    CSD_LAUNCH();
+  };
+  switch (rpl) {
+    case 1: go(csd::k_tikhonov<1>); break;
+    case 2: go(csd::k_tikhonov<2>); break;
+    case 3: go(csd::k_tikhonov<3>); break;
+    case 4: go(csd::k_tikhonov<4>); break;
+    case 5: go(csd::k_tikhonov<5>); break;
+    default: throw Error{CSD_ERR_INVALID, "Tikhonov kernel supports K <= 160"};
+  }
+}
+
+void launch_epilogue(csd_handle* h, const csd::EpilogueParams& p) {
+  const size_t smem = sizeof(double) * 8 * static_cast<size_t>(h->Kp) * 8;
+  const int64_t groups = (p.n_work + 7) / 8;
+  const int blocks = std::max(1, static_cast<int>(std::min<int64_t>((groups + 7) / 8, h->num_sms * 16)));
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_epilogue, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  csd::k_epilogue<<<blocks, 256, smem, h->stream>>>(p);
+  CSD_LAUNCH();
+}
+
+// Device outputs of one fit (all device pointers; maps nullable).
+struct DevOut {
+  float* coeffs;
+  float *r2, *resid, *alpha, *bic, *rss_l2;
+  uint32_t* iters;
+  uint8_t* kind;
+};
+
+struct FitInfo {
+  int64_t V = 0;
+  uint64_t total_iterations = 0;
+  bool has_dist = false;
+  double dist[3] = {0, 0, 0};
+  double representative_alpha = 0.0;
+  const double* Xfinal = nullptr;  // device V x Kp
+  const uint8_t* conv_final = nullptr;
+  std::string warnings;
+};
+
+// Validation shared by both entry points (src/fit.rs:555-591, 691-730;
+// python/src/models.rs:112-144).
+double validate(const csd_shore_spec* s, const HostGtab& g, std::string& warnings) {
+  if (s->radial_order <= 0 || s->radial_order % 2 != 0)
+    throw Error{CSD_ERR_INVALID,
+                "radial_order must be a positive even number, got " + std::to_string(s->radial_order)};
+  if (s->precision != CSD_PRECISION_FP64) throw Error{CSD_ERR_INVALID, "unknown precision"};
+  if (s->max_iter < 0) throw Error{CSD_ERR_INVALID, "max_iter must be >= 0"};
+  double path_eps = s->path_eps;
+  if (s->regularization == CSD_REG_L1) {
+    const int mode = s->alpha_mode;
+    if (mode < CSD_ALPHA_FIXED || mode > CSD_ALPHA_L2_ANCHORED)
+      throw Error{CSD_ERR_INVALID, "alpha_mode must be fixed, alpha-ratio, path-bic or l2-anchored"};
+    if (mode == CSD_ALPHA_RATIO && !(s->alpha_ratio > 0.0 && s->alpha_ratio < 1.0)) {
+      char b[128];
+      std::snprintf(b, sizeof b, "--alpha-ratio must lie in (0, 1), got %g", s->alpha_ratio);
+      throw Error{CSD_ERR_INVALID, b};
+    }
+    if (mode == CSD_ALPHA_PATH_BIC || mode == CSD_ALPHA_L2_ANCHORED) {
+      if (s->path_n_alphas < 2)
+        throw Error{CSD_ERR_INVALID, "--path-n-alphas must be \xe2\x89\xa5 2, got " + std::to_string(s->path_n_alphas)};
+      if (!(path_eps > 0.0)) path_eps = (mode == CSD_ALPHA_PATH_BIC) ? 1e-3 : 1e-4;
+      if (!(path_eps > 0.0 && path_eps < 1.0)) {
+        char b[128];
+        std::snprintf(b, sizeof b, "--path-eps must lie in (0, 1), got %g", path_eps);
+        throw Error{CSD_ERR_INVALID, b};
+      }
+      if (mode == CSD_ALPHA_L2_ANCHORED && s->slack < 0.0) {
+        char b[128];
+        std::snprintf(b, sizeof b, "--slack must be \xe2\x89\xa5 0, got %g", s->slack);
+        throw Error{CSD_ERR_INVALID, b};
+      }
+    }
+  } else if (s->regularization != CSD_REG_L2 && s->regularization != CSD_REG_NONNEG) {
+    throw Error{CSD_ERR_INVALID, "regularization must be l1, l2 or nonneg"};
+  }
+  if (g.shells.empty())
+    throw Error{CSD_ERR_FIT_REFUSED,
+                "3D-SHORE needs diffusion-weighted data; every volume is at or below the b=0 threshold"};
+  if (g.shells.size() < 2) {
+    char what[96];
+    std::snprintf(what, sizeof what, "a single shell (b = %.0f s/mm\xc2\xb2)", g.shells[0]);
+    if (!s->allow_single_shell)
+      throw Error{CSD_ERR_FIT_REFUSED,
+                  std::string("3D-SHORE needs diffusion-weighted data on at least 2 b-value shells; this "
+                              "series has ") +
+                      what +
+                      ". With a single shell the radial decay of the signal is not determined by the "
+                      "data: a fit would match the measurements, but its propagator-derived scalars "
+                      "(RTOP, RTAP, RTPP, MSD, QIV) and the signals it predicts at other b-values would "
+                      "reflect the regularization rather than the data. To fit anyway for orientation "
+                      "information only, allow single-shell data (--allow-single-shell, or "
+                      "allow_single_shell=True in Python)."};
+    warnings += std::string("the data have ") + what +
+                ": only the orientation information of this fit is meaningful, and "
+                "propagator-derived scalars are not computed\n";
+  }
+  const int K = n_coeffs(s->radial_order);
+  const int N = static_cast<int>(g.bvals.size());
+  if (N < K && s->regularization != CSD_REG_L1) {
+    warnings += std::to_string(N) + " measurements for " + std::to_string(K) +
+                " coefficients (radial order " + std::to_string(s->radial_order) +
+                "): without L1 regularization the fit is underdetermined and its fit statistics are "
+                "not meaningful; use a lower radial order or L1\n";
+  }
+  return path_eps;
+}
+
+void record(csd_handle* h, int i) { CSD_CUDA(cudaEventRecord(h->ev[i], h->stream)); }
+
+// The whole-volume fit on device buffers.
+FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64_t nvol,
+                const HostGtab& g, const csd_shore_spec* spec, double path_eps, const DevOut& out) {
+  FitInfo info;
+  cudaStream_t st = h->stream;
+  h->launches = 0;
+  const bool is_l1 = spec->regularization == CSD_REG_L1;
+  const int mode = spec->alpha_mode;
+  if (spec->regularization == CSD_REG_NONNEG)
+    throw Error{CSD_ERR_INVALID, "regularization 'nonneg' (amplitude ICLS) is not available in this build"};
+  const bool need_chol = spec->regularization == CSD_REG_L2 || (is_l1 && mode == CSD_ALPHA_L2_ANCHORED);
+
+  record(h, 0);
+  ensure_setup(h, g, spec->radial_order, spec->zeta, need_chol, spec->lambda_n, spec->lambda_l);
+  const int N = h->N, K = h->K, Kp = h->Kp;
+  record(h, 1);
+
+  // Zero the output volumes (coefficients and maps are 0 outside the mask).
+  CSD_CUDA(cudaMemsetAsync(out.coeffs, 0, sizeof(float) * static_cast<size_t>(nvol) * K, st));
+  if (spec->diagnostics) {
+    if (out.r2) CSD_CUDA(cudaMemsetAsync(out.r2, 0, sizeof(float) * nvol, st));
+    if (out.resid) CSD_CUDA(cudaMemsetAsync(out.resid, 0, sizeof(float) * nvol, st));
+    if (out.iters) CSD_CUDA(cudaMemsetAsync(out.iters, 0, sizeof(uint32_t) * nvol, st));
+    if (out.kind) CSD_CUDA(cudaMemsetAsync(out.kind, 0, nvol, st));
+    if (out.alpha && is_l1) CSD_CUDA(cudaMemsetAsync(out.alpha, 0, sizeof(float) * nvol, st));
+    if (out.bic && is_l1) CSD_CUDA(cudaMemsetAsync(out.bic, 0, sizeof(float) * nvol, st));
+    if (out.rss_l2 && is_l1 && mode == CSD_ALPHA_L2_ANCHORED)
+      CSD_CUDA(cudaMemsetAsync(out.rss_l2, 0, sizeof(float) * nvol, st));
+  }
+
+  const int64_t V = compact(h, d_mask, nvol, h->vox);
+  info.V = V;
+  if (V == 0) {
+    record(h, 2);
+    record(h, 3);
+    record(h, 4);
+    record(h, 5);
+    return info;
+  }
+  h->B.ensure(sizeof(double) * V * Kp);
+  h->X.ensure(sizeof(double) * V * Kp);
+  h->iters.ensure(sizeof(uint32_t) * V);
+  h->conv.ensure(V);
+  h->queue.ensure(sizeof(unsigned long long));
+  h->itotal.ensure(sizeof(unsigned long long));
+  h->resid_v.ensure(sizeof(double) * V);
+  h->nnz_v.ensure(sizeof(int) * V);
+  CSD_CUDA(cudaMemsetAsync(h->itotal.p, 0, sizeof(unsigned long long), st));
+
+  launch_rhs(h, d_data, V);
+  record(h, 2);
+
+  csd::EpilogueParams ep{};
+  ep.data = d_data;
+  ep.vox = h->vox.as<int64_t>();
+  ep.V = V;
+  ep.N = N;
+  ep.K = K;
+  ep.Kp = Kp;
+  ep.Mt = h->Mt.as<double>();
+  ep.n_work = V;
+
+  const int MT = Kp / 8;
+  csd::FistaParams fp{};
+  fp.gfrag = h->gfrag.as<double>();
+  fp.B = h->B.as<double>();
+  fp.X = h->X.as<double>();
+  fp.iters = h->iters.as<uint32_t>();
+  fp.conv = h->conv.as<uint8_t>();
+  fp.V = V;
+  fp.n_inv = 1.0 / static_cast<double>(N);
+  fp.step = 1.0 / h->lipschitz;
+  fp.tol = spec->tol;
+  fp.max_iter = spec->max_iter;
+  fp.non_negative = spec->non_negative;
+  fp.queue = h->queue.as<unsigned long long>();
+  fp.iter_total = h->itotal.as<unsigned long long>();
+  fp.n_work = V;
+
+  const double* Xfinal = h->X.as<double>();
+  const uint32_t* it_final = h->iters.as<uint32_t>();
+  const uint8_t* conv_final = h->conv.as<uint8_t>();
+  const double* alpha_final = nullptr;
+  const uint8_t* zero_final = nullptr;
+  uint8_t kind = 1;
+  double alpha_const = 0.0;
+
+  if (spec->regularization == CSD_REG_L2) {
+    kind = 2;
+    record(h, 6);
+    launch_tikhonov(h, h->B.as<double>(), h->X.as<double>(), V);
+    record(h, 7);
+    it_final = nullptr;
+    CSD_CUDA(cudaMemsetAsync(h->conv.p, 1, V, st));
+    info.total_iterations = static_cast<uint64_t>(V);
+  } else {
+    // L1 (src/fit.rs:741-774)
+    kind = 1;
+    if (mode == CSD_ALPHA_FIXED) {
+      alpha_const = spec->alpha;
+      fp.thr = fp.step * spec->alpha;
+      fp.alpha_v = nullptr;
+      fp.warm = nullptr;
+      CSD_CUDA(cudaMemsetAsync(h->queue.p, 0, sizeof(unsigned long long), st));
+      record(h, 6);
+      launch_fista(h, MT, fp);
+      record(h, 7);
+      info.representative_alpha = spec->alpha;
+    } else {
+      h->amax.ensure(sizeof(double) * V);
+      h->zero.ensure(V);
+      h->alpha_v.ensure(sizeof(double) * V);
+      csd::k_alpha_max<<<grid1(V), 256, 0, st>>>(h->B.as<double>(), V, K, Kp, N, h->amax.as<double>(),
+                                                 h->zero.as<uint8_t>());
+      CSD_LAUNCH();
+      zero_final = h->zero.as<uint8_t>();
+      if (mode == CSD_ALPHA_RATIO) {
+        csd::k_alpha_ratio<<<grid1(V), 256, 0, st>>>(h->amax.as<double>(), V, spec->alpha_ratio,
+                                                     h->alpha_v.as<double>());
+        CSD_LAUNCH();
+        fp.alpha_v = h->alpha_v.as<double>();
+        fp.warm = nullptr;
+        // zero voxels are fitted with alpha 0 on a zero right-hand side and
+        // then overwritten with the zero result below
+        CSD_CUDA(cudaMemsetAsync(h->queue.p, 0, sizeof(unsigned long long), st));
+        record(h, 6);
+        launch_fista(h, MT, fp);
+        record(h, 7);
+        csd::k_zero_voxels<<<grid1(V), 256, 0, st>>>(V, h->zero.as<uint8_t>(), h->alpha_v.as<double>(),
+                                                     h->iters.as<uint32_t>(), h->conv.as<uint8_t>());
+        CSD_LAUNCH();
+        alpha_final = h->alpha_v.as<double>();
+      } else {
+        // Path strategies (src/solver/alpha.rs:249-318).
+        const int P = spec->path_n_alphas;
+        h->Xsel.ensure(sizeof(double) * V * Kp);
+        h->Xfb.ensure(sizeof(double) * V * Kp);
+        h->list.ensure(sizeof(int64_t) * V);
+        h->active.ensure(V);
+        h->pbest.ensure(sizeof(double) * V);
+        h->psel.ensure(V);
+        h->palpha_sel.ensure(sizeof(double) * V);
+        h->pit_sel.ensure(sizeof(uint32_t) * V);
+        h->pconv_sel.ensure(V);
+        h->palpha_fb.ensure(sizeof(double) * V);
+        h->pit_fb.ensure(sizeof(uint32_t) * V);
+        h->pconv_fb.ensure(V);
+        h->pcode.ensure(V);
+        CSD_CUDA(cudaMemsetAsync(h->Xsel.p, 0, sizeof(double) * V * Kp, st));
+        CSD_CUDA(cudaMemsetAsync(h->psel.p, 0, V, st));
+        CSD_CUDA(cudaMemsetAsync(h->palpha_sel.p, 0, sizeof(double) * V, st));
+        CSD_CUDA(cudaMemsetAsync(h->pit_sel.p, 0, sizeof(uint32_t) * V, st));
+        CSD_CUDA(cudaMemsetAsync(h->pconv_sel.p, 1, V, st));
+        {
+          // best metric starts at +inf
+          csd::k_fill_f64<<<grid1(V), 256, 0, st>>>(h->pbest.as<double>(), V, INFINITY);
+          CSD_LAUNCH();
+        }
+        csd::PathState ps{};
+        ps.best = h->pbest.as<double>();
+        ps.selected = h->psel.as<uint8_t>();
+        ps.active = h->active.as<uint8_t>();
+        ps.alpha_sel = h->palpha_sel.as<double>();
+        ps.it_sel = h->pit_sel.as<uint32_t>();
+        ps.conv_sel = h->pconv_sel.as<uint8_t>();
+        ps.alpha_fb = h->palpha_fb.as<double>();
+        ps.it_fb = h->pit_fb.as<uint32_t>();
+        ps.conv_fb = h->pconv_fb.as<uint8_t>();
+        ps.copy_code = h->pcode.as<int8_t>();
+        csd::k_init_active<<<grid1(V), 256, 0, st>>>(V, h->zero.as<uint8_t>(), h->active.as<uint8_t>());
+        CSD_LAUNCH();
+        const double* rss_l2 = nullptr;
+        if (mode == CSD_ALPHA_L2_ANCHORED) {
+          // Tikhonov reference RSS per voxel (src/fit.rs:436-438).
+          h->Xl2.ensure(sizeof(double) * V * Kp);
+          h->rss_l2.ensure(sizeof(double) * V);
+          launch_tikhonov(h, h->B.as<double>(), h->Xl2.as<double>(), V);
+          csd::EpilogueParams rp = ep;
+          rp.X = h->Xl2.as<double>();
+          rp.scatter = false;
+          rp.resid_out = h->resid_v.as<double>();
+          launch_epilogue(h, rp);
+          csd::k_square<<<grid1(V), 256, 0, st>>>(h->resid_v.as<double>(), h->rss_l2.as<double>(), V);
+          CSD_LAUNCH();
+          rss_l2 = h->rss_l2.as<double>();
+        }
+        record(h, 6);
+        int64_t n_work = 0;
+        for (int i = 0; i < P; ++i) {
+          n_work = compact(h, h->active.as<uint8_t>(), V, h->list);
+          if (n_work == 0) break;
+          csd::k_path_alpha<<<grid1(n_work), 256, 0, st>>>(h->amax.as<double>(), h->list.as<int64_t>(),
+                                                           n_work, i, P, path_eps, h->alpha_v.as<double>());
+          CSD_LAUNCH();
+          fp.alpha_v = h->alpha_v.as<double>();
+          fp.warm = (i == 0) ? nullptr : h->X.as<double>();
+          fp.list = h->list.as<int64_t>();
+          fp.n_work = n_work;
+          CSD_CUDA(cudaMemsetAsync(h->queue.p, 0, sizeof(unsigned long long), st));
+          launch_fista(h, MT, fp);
+          csd::EpilogueParams rp = ep;
+          rp.X = h->X.as<double>();
+          rp.scatter = false;
+          rp.resid_out = h->resid_v.as<double>();
+          rp.nnz_out = h->nnz_v.as<int>();
+          rp.list = h->list.as<int64_t>();
+          rp.n_work = n_work;
+          launch_epilogue(h, rp);
+          csd::k_path_update<<<grid1(n_work), 256, 0, st>>>(
+              mode, h->list.as<int64_t>(), n_work, N, h->resid_v.as<double>(), h->nnz_v.as<int>(),
+              h->alpha_v.as<double>(), h->iters.as<uint32_t>(), h->conv.as<uint8_t>(), rss_l2,
+              spec->slack, ps);
+          CSD_LAUNCH();
+          csd::k_path_copy<<<grid1(n_work * Kp), 256, 0, st>>>(h->list.as<int64_t>(), n_work, Kp,
+                                                               h->pcode.as<int8_t>(), h->X.as<double>(),
+                                                               h->Xsel.as<double>(), h->Xfb.as<double>());
+          CSD_LAUNCH();
+        }
+        if (mode == CSD_ALPHA_L2_ANCHORED) {
+          csd::k_path_finalize<<<grid1(V * Kp), 256, 0, st>>>(V, Kp, h->zero.as<uint8_t>(), ps,
+                                                               h->Xfb.as<double>(), h->Xsel.as<double>());
+          CSD_LAUNCH();
+        }
+        record(h, 7);
+        Xfinal = h->Xsel.as<double>();
+        it_final = h->pit_sel.as<uint32_t>();
+        conv_final = h->pconv_sel.as<uint8_t>();
+        alpha_final = h->palpha_sel.as<double>();
+        csd::k_zero_voxels<<<grid1(V), 256, 0, st>>>(V, h->zero.as<uint8_t>(), h->palpha_sel.as<double>(),
+                                                     h->pit_sel.as<uint32_t>(), h->pconv_sel.as<uint8_t>());
+        CSD_LAUNCH();
+      }
+    }
+  }
+
+  // Epilogue: residuals, maps, scatter.
+  csd::EpilogueParams fpo = ep;
+  fpo.X = Xfinal;
+  fpo.iters = it_final;
+  fpo.coeffs = out.coeffs;
+  fpo.scatter = true;
+  fpo.kind = kind;
+  fpo.alpha = alpha_const;
+  fpo.alpha_v = alpha_final;
+  fpo.zero_v = zero_final;
+  if (spec->diagnostics) {
+    fpo.r2 = out.r2;
+    fpo.resid = out.resid;
+    fpo.iter_map = out.iters;
+    fpo.kind_map = out.kind;
+    if (is_l1) {
+      fpo.alpha_map = out.alpha;
+      fpo.bic_map = out.bic;
+    }
+  }
+  if (is_l1 && mode == CSD_ALPHA_L2_ANCHORED && spec->diagnostics && out.rss_l2) {
+    csd::k_scatter_f64_to_f32<<<grid1(V), 256, 0, st>>>(h->rss_l2.as<double>(), h->vox.as<int64_t>(), V,
+                                                        out.rss_l2);
+    CSD_LAUNCH();
+  }
+  launch_epilogue(h, fpo);
+  record(h, 3);
+
+  // executed iteration total and the alpha distribution
+  unsigned long long itot = 0;
+  if (spec->regularization != CSD_REG_L2) {
+    CSD_CUDA(cudaMemcpyAsync(&itot, h->itotal.p, sizeof itot, cudaMemcpyDeviceToHost, st));
+  }
+  CSD_CUDA(cudaStreamSynchronize(st));
+  if (spec->regularization != CSD_REG_L2) info.total_iterations = itot;
+  if (is_l1 && mode != CSD_ALPHA_FIXED) {
+    // median / p10 / p90 by nearest rank (src/fit.rs:334-352)
+    std::vector<double> a(V);
+    CSD_CUDA(cudaMemcpy(a.data(), alpha_final, sizeof(double) * V, cudaMemcpyDeviceToHost));
+    std::sort(a.begin(), a.end());
+    auto pct = [&](double q) {
+      size_t i = static_cast<size_t>(std::round(static_cast<double>(a.size() - 1) * q));
+      return a[std::min(i, a.size() - 1)];
+    };
+    info.has_dist = true;
+    info.dist[0] = pct(0.5);
+    info.dist[1] = pct(0.10);
+    info.dist[2] = pct(0.90);
+    info.representative_alpha = info.dist[0];
+  }
+  info.Xfinal = Xfinal;
+  info.conv_final = conv_final;
+  float ms = 0;
+  h->timing.ms_setup = (cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]) == cudaSuccess) ? ms : 0.f;
+  h->timing.ms_rhs = (cudaEventElapsedTime(&ms, h->ev[1], h->ev[2]) == cudaSuccess) ? ms : 0.f;
+  h->timing.ms_solve = (cudaEventElapsedTime(&ms, h->ev[2], h->ev[7]) == cudaSuccess) ? ms : 0.f;
+  h->timing.ms_solve_kernel = (cudaEventElapsedTime(&ms, h->ev[6], h->ev[7]) == cudaSuccess) ? ms : 0.f;
+  h->timing.ms_epilogue = (cudaEventElapsedTime(&ms, h->ev[7], h->ev[3]) == cudaSuccess) ? ms : 0.f;
+  h->timing.ms_total = (cudaEventElapsedTime(&ms, h->ev[0], h->ev[3]) == cudaSuccess) ? ms : 0.f;
+  h->timing.launches = h->launches;
+  return info;
+}
+
+void fill_scalars(const HostGtab& g, const FitInfo& info, const csd_shore_spec* spec, csd_fit_result* out) {
+  out->n_coeffs = n_coeffs(spec->radial_order);
+  out->n_voxels = info.V;
+  out->has_alpha_distribution = info.has_dist ? 1 : 0;
+  for (int i = 0; i < 3; ++i) out->alpha_distribution[i] = info.dist[i];
+  out->representative_alpha = info.representative_alpha;
+  out->big_delta_seconds = g.big;
+  out->small_delta_seconds = g.small;
+  out->tau_seconds = g.tau;
+  out->delta_source = g.delta_source;
+  out->n_shells = static_cast<int32_t>(std::min<size_t>(g.shells.size(), 32));
+  for (int i = 0; i < out->n_shells; ++i) out->dwi_shells[i] = g.shells[i];
+  out->lmax = 0;
+  out->n_constraint_dirs = 0;
+  out->total_iterations = info.total_iterations;
+}
+
+}  // namespace
+
+// ======================================================================
+// C ABI
+// ======================================================================
+
+extern "C" {
+
+const char* csd_version(void) { return "cs_dmri_b200 0.1.0 (sm_100a)"; }
+int csd_abi_version(void) { return CSD_ABI_VERSION; }
+
+void csd_default_spec(csd_shore_spec* s) {
+  s->radial_order = 6;
+  s->zeta = 700.0;
+  s->regularization = CSD_REG_L1;
+  s->alpha_mode = CSD_ALPHA_L2_ANCHORED;
+  s->alpha = 1.0;
+  s->alpha_ratio = 1e-3;
+  s->path_n_alphas = 20;
+  s->path_eps = 0.0;
+  s->slack = 0.05;
+  s->max_iter = 1000;
+  s->tol = 1e-6;
+  s->non_negative = 0;
+  s->lambda_n = 1e-8;
+  s->lambda_l = 1e-8;
+  s->nonneg_max_iter = 200;
+  s->nonneg_tol = 1e-9;
+  s->nonneg_epsilon = 1e-10;
+  s->diagnostics = 0;
+  s->allow_single_shell = 0;
+  s->precision = CSD_PRECISION_FP64;
+}
+
+int csd_shore_n_coeffs(int32_t radial_order) { return radial_order < 0 ? 0 : n_coeffs(radial_order); }
+
+int csd_create(csd_handle** out, int32_t device, char* err, size_t err_len) {
+  if (!out) {
+    set_err(err, err_len, "null handle pointer");
+    return CSD_ERR_INVALID;
+  }
+  *out = nullptr;
+  csd_handle* h = new csd_handle();
+  try {
+    int count = 0;
+    CSD_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count)
+      throw Error{CSD_ERR_INVALID, "CUDA device " + std::to_string(device) + " not present (" +
+                                       std::to_string(count) + " visible)"};
+    CSD_CUDA(cudaSetDevice(device));
+    h->device = device;
+    cudaDeviceProp prop{};
+    CSD_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+      throw Error{CSD_ERR_CUDA, std::string("this library is built for sm_100a (B200); device is ") +
+                                    prop.name};
+    h->num_sms = prop.multiProcessorCount;
+    CSD_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    for (auto& e : h->ev) CSD_CUDA(cudaEventCreate(&e));
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    delete h;
+    return e.code;
+  }
+  *out = h;
+  return CSD_OK;
+}
+
+void csd_destroy(csd_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  DevBuf* bufs[] = {&h->bvals, &h->bvecs, &h->M, &h->Mt, &h->G, &h->A, &h->gfrag, &h->scal, &h->ok,
+                    &h->data, &h->mask, &h->coeffs, &h->r2, &h->resid, &h->iters_map, &h->kind_map,
+                    &h->alpha_map, &h->bic_map, &h->rss_map, &h->blk, &h->total, &h->vox, &h->B, &h->X,
+                    &h->iters, &h->conv, &h->queue, &h->itotal, &h->resid_v, &h->nnz_v, &h->amax,
+                    &h->zero, &h->alpha_v, &h->Xsel, &h->Xfb, &h->Xl2, &h->rss_l2, &h->list, &h->active,
+                    &h->pbest, &h->psel, &h->pact, &h->palpha_sel, &h->pit_sel, &h->pconv_sel,
+                    &h->palpha_fb, &h->pit_fb, &h->pconv_fb, &h->pcode};
+  for (DevBuf* b : bufs) b->release();
+  for (auto& e : h->ev)
+    if (e) cudaEventDestroy(e);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+static int check_common(csd_handle* h, const void* data, const void* mask, int64_t X, int64_t Y, int64_t Z,
+                        const csd_gtab* gtab, const csd_shore_spec* spec, csd_fit_result* out) {
+  if (!h || !data || !mask || !gtab || !spec || !out || !out->coefficients) return 1;
+  if (X < 0 || Y < 0 || Z < 0 || gtab->n <= 0 || !gtab->bvals || !gtab->bvecs) return 1;
+  return 0;
+}
+
+int csd_shore_fit_volume_device(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64_t X,
+                                int64_t Y, int64_t Z, const csd_gtab* gtab, const csd_shore_spec* spec,
+                                csd_fit_result* out, void* stream, char* err, size_t err_len) {
+  if (check_common(h, d_data, d_mask, X, Y, Z, gtab, spec, out)) {
+    set_err(err, err_len, "invalid argument: null pointer or bad shape");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    CSD_CUDA(cudaSetDevice(h->device));
+    HostGtab g = make_gtab(gtab);
+    std::string warnings;
+    const double path_eps = validate(spec, g, warnings);
+    // Queue the whole fit on the caller's stream when one is given.
+    struct StreamSwap {
+      csd_handle* h;
+      cudaStream_t saved;
+      ~StreamSwap() { h->stream = saved; }
+    } swap{h, h->stream};
+    if (stream) h->stream = static_cast<cudaStream_t>(stream);
+    DevOut d{out->coefficients, out->r2,  out->residual_l2, out->alpha, out->bic, out->rss_l2,
+             out->iterations,   out->regularization_kind};
+    FitInfo info = run_fit(h, d_data, d_mask, X * Y * Z, g, spec, path_eps, d);
+    const int K = n_coeffs(spec->radial_order);
+    if (out->coef64 && info.V > 0)
+      CSD_CUDA(cudaMemcpy2DAsync(out->coef64, sizeof(double) * K, info.Xfinal, sizeof(double) * h->Kp,
+                                 sizeof(double) * K, info.V, cudaMemcpyDeviceToDevice, h->stream));
+    if (out->converged && info.V > 0)
+      CSD_CUDA(cudaMemcpyAsync(out->converged, info.conv_final, info.V, cudaMemcpyDeviceToDevice, h->stream));
+    CSD_CUDA(cudaStreamSynchronize(h->stream));
+    fill_scalars(g, info, spec, out);
+    std::snprintf(out->warnings, sizeof out->warnings, "%s", warnings.c_str());
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}
+
+int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, int64_t X, int64_t Y,
+                         int64_t Z, const csd_gtab* gtab, const csd_shore_spec* spec, csd_fit_result* out,
+                         char* err, size_t err_len) {
+  if (check_common(h, data, mask, X, Y, Z, gtab, spec, out)) {
+    set_err(err, err_len, "invalid argument: null pointer or bad shape");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    CSD_CUDA(cudaSetDevice(h->device));
+    HostGtab g = make_gtab(gtab);
+    std::string warnings;
+    const double path_eps = validate(spec, g, warnings);
+    const int64_t nvol = X * Y * Z;
+    const int N = gtab->n;
+    const int K = n_coeffs(spec->radial_order);
+    cudaStream_t st = h->stream;
+    h->data.ensure(sizeof(float) * static_cast<size_t>(nvol) * N);
+    h->mask.ensure(static_cast<size_t>(nvol));
+    h->coeffs.ensure(sizeof(float) * static_cast<size_t>(nvol) * K);
+    CSD_CUDA(cudaMemcpyAsync(h->data.p, data, sizeof(float) * static_cast<size_t>(nvol) * N,
+                             cudaMemcpyHostToDevice, st));
+    CSD_CUDA(cudaMemcpyAsync(h->mask.p, mask, static_cast<size_t>(nvol), cudaMemcpyHostToDevice, st));
+    const bool diag = spec->diagnostics != 0;
+    auto map_f = [&](DevBuf& b, void* host) -> float* {
+      if (!diag || !host) return nullptr;
+      b.ensure(sizeof(float) * nvol);
+      return b.as<float>();
+    };
+    DevOut d{};
+    d.coeffs = h->coeffs.as<float>();
+    d.r2 = map_f(h->r2, out->r2);
+    d.resid = map_f(h->resid, out->residual_l2);
+    d.alpha = map_f(h->alpha_map, out->alpha);
+    d.bic = map_f(h->bic_map, out->bic);
+    d.rss_l2 = map_f(h->rss_map, out->rss_l2);
+    if (diag && out->iterations) {
+      h->iters_map.ensure(sizeof(uint32_t) * nvol);
+      d.iters = h->iters_map.as<uint32_t>();
+    }
+    if (diag && out->regularization_kind) {
+      h->kind_map.ensure(nvol);
+      d.kind = h->kind_map.as<uint8_t>();
+    }
+    FitInfo info = run_fit(h, h->data.as<float>(), h->mask.as<uint8_t>(), nvol, g, spec, path_eps, d);
+    CSD_CUDA(cudaMemcpyAsync(out->coefficients, d.coeffs, sizeof(float) * static_cast<size_t>(nvol) * K,
+                             cudaMemcpyDeviceToHost, st));
+    const bool is_l1 = spec->regularization == CSD_REG_L1;
+    if (diag) {
+      if (d.r2) CSD_CUDA(cudaMemcpyAsync(out->r2, d.r2, sizeof(float) * nvol, cudaMemcpyDeviceToHost, st));
+      if (d.resid)
+        CSD_CUDA(cudaMemcpyAsync(out->residual_l2, d.resid, sizeof(float) * nvol, cudaMemcpyDeviceToHost, st));
+      if (d.iters)
+        CSD_CUDA(cudaMemcpyAsync(out->iterations, d.iters, sizeof(uint32_t) * nvol, cudaMemcpyDeviceToHost, st));
+      if (d.kind)
+        CSD_CUDA(cudaMemcpyAsync(out->regularization_kind, d.kind, nvol, cudaMemcpyDeviceToHost, st));
+      if (d.alpha && is_l1)
+        CSD_CUDA(cudaMemcpyAsync(out->alpha, d.alpha, sizeof(float) * nvol, cudaMemcpyDeviceToHost, st));
+      if (d.bic && is_l1)
+        CSD_CUDA(cudaMemcpyAsync(out->bic, d.bic, sizeof(float) * nvol, cudaMemcpyDeviceToHost, st));
+      if (d.rss_l2 && is_l1 && spec->alpha_mode == CSD_ALPHA_L2_ANCHORED)
+        CSD_CUDA(cudaMemcpyAsync(out->rss_l2, d.rss_l2, sizeof(float) * nvol, cudaMemcpyDeviceToHost, st));
+    }
+    if (out->coef64 && info.V > 0)
+      CSD_CUDA(cudaMemcpy2DAsync(out->coef64, sizeof(double) * K, info.Xfinal, sizeof(double) * h->Kp,
+                                 sizeof(double) * K, info.V, cudaMemcpyDeviceToHost, st));
+    if (out->converged && info.V > 0)
+      CSD_CUDA(cudaMemcpyAsync(out->converged, info.conv_final, info.V, cudaMemcpyDeviceToHost, st));
+    CSD_CUDA(cudaStreamSynchronize(st));
+    fill_scalars(g, info, spec, out);
+    std::snprintf(out->warnings, sizeof out->warnings, "%s", warnings.c_str());
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}
+
+int csd_shore_design_matrix(csd_handle* h, const csd_gtab* gtab, int32_t radial_order, double zeta,
+                            double* out, char* err, size_t err_len) {
+  if (!h || !gtab || !out || gtab->n <= 0 || radial_order < 0) {
+    set_err(err, err_len, "invalid argument");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    CSD_CUDA(cudaSetDevice(h->device));
+    HostGtab g = make_gtab(gtab);
+    ensure_setup(h, g, radial_order, zeta, false, 0.0, 0.0);
+    CSD_CUDA(cudaMemcpyAsync(out, h->M.p, sizeof(double) * h->N * h->K, cudaMemcpyDeviceToHost, h->stream));
+    CSD_CUDA(cudaStreamSynchronize(h->stream));
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}
+
+int csd_last_timing(const csd_handle* h, csd_fit_timing* out) {
+  if (!h || !out) return CSD_ERR_INVALID;
+  *out = h->timing;
+  return CSD_OK;
+}
+
+}  // extern "C"

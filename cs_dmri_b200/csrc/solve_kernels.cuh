@@ -1,0 +1,627 @@
+// solve_kernels.cuh - the per-voxel kernels of the SHORE volume fit.
+//
+//   k_mask_count / k_scan_blocks / k_mask_compact
+//       masked voxel list in canonical x-y-z order (src/voxel_loop.rs:28-42)
+//   k_rhs         b_v = M^T s_v for every masked voxel (the A^T s of every
+//                 solver: fista.rs:142-144 in Gram form, tikhonov.rs:343,
+//                 alpha.rs:51)
+//   k_fista_fp64  warm-startable FISTA iterations (src/solver/fista.rs:121-194)
+//                 in Gram form on FP64 DMMA tensor cores, 8 voxels per warp,
+//                 slots refilled from a device work queue as voxels converge
+//   k_tikhonov    L L^T c = b by forward/back substitution
+//                 (src/solver/tikhonov.rs:342-357)
+//   k_epilogue    residual ||s - M c||, R^2, BIC, diagnostic maps and the
+//                 scatter into the (X, Y, Z, K) coefficient volume
+//                 (src/fit.rs:115-155, 264-318)
+#pragma once
+
+#include <cstdint>
+
+namespace csd {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// ------------------------------------------------------------ compaction
+
+constexpr int kCompactBlock = 1024;
+
+__global__ void k_mask_count(const uint8_t* __restrict__ mask, int64_t n,
+                             int* __restrict__ block_counts) {
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kCompactBlock;
+  int c = 0;
+  for (int i = threadIdx.x; i < kCompactBlock; i += blockDim.x) {
+    const int64_t g = base + i;
+    c += (g < n && mask[g] != 0) ? 1 : 0;
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+  __shared__ int red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int w = 0; w < (blockDim.x + 31) / 32; ++w) s += red[w];
+    block_counts[blockIdx.x] = s;
+  }
+}
+
+// Exclusive scan of the per-block counts, one CTA; total written to *total.
+__global__ void k_scan_blocks(int* __restrict__ counts, int nblocks, long long* __restrict__ total) {
+  __shared__ long long carry;
+  __shared__ long long warp_sums[32];
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nblocks; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    long long v = (i < nblocks) ? counts[i] : 0;
+    // inclusive warp scan
+    long long x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(kFull, x, o);
+      if ((threadIdx.x & 31) >= o) x += y;
+    }
+    if ((threadIdx.x & 31) == 31) warp_sums[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      long long w = (threadIdx.x < blockDim.x / 32) ? warp_sums[threadIdx.x] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(kFull, w, o);
+        if (threadIdx.x >= o) w += y;
+      }
+      warp_sums[threadIdx.x] = w;
+    }
+    __syncthreads();
+    const long long warp_prefix = (threadIdx.x >= 32) ? warp_sums[(threadIdx.x >> 5) - 1] : 0;
+    const long long excl = carry + warp_prefix + x - v;
+    if (i < nblocks) counts[i] = static_cast<int>(excl);
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void k_mask_compact(const uint8_t* __restrict__ mask, int64_t n,
+                               const int* __restrict__ block_offsets, int64_t* __restrict__ vox) {
+  // blockDim.x == kCompactBlock / 4; each thread scans 4 consecutive voxels.
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kCompactBlock;
+  const int t = threadIdx.x;
+  int flags[4];
+  int c = 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int64_t g = base + 4 * t + j;
+    flags[j] = (g < n && mask[g] != 0) ? 1 : 0;
+    c += flags[j];
+  }
+  int x = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, x, o);
+    if ((t & 31) >= o) x += y;
+  }
+  __shared__ int ws[32];
+  if ((t & 31) == 31) ws[t >> 5] = x;
+  __syncthreads();
+  if (t < 32) {
+    int w = (t < blockDim.x / 32) ? ws[t] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, w, o);
+      if (t >= o) w += y;
+    }
+    ws[t] = w;
+  }
+  __syncthreads();
+  int pos = block_offsets[blockIdx.x] + ((t >= 32) ? ws[(t >> 5) - 1] : 0) + x - c;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (flags[j]) vox[pos++] = base + 4 * t + j;
+  }
+}
+
+// ---------------------------------------------------------------- A^T s
+
+// b_v[k] = sum_i M[i, k] * s_v[i] for a tile of 64 voxels x Kp columns,
+// sweeping N in chunks of 32 rows staged in shared memory.  Thread (tv, tk)
+// owns voxel tv and the contiguous columns [tk*NC, tk*NC + NC); its M reads
+// are warp-uniform 16-byte broadcasts and the signal tile is padded against
+// bank conflicts.  Rows are accumulated in index order, as M^T s is.
+template <int KP>
+__global__ void __launch_bounds__(256) k_rhs(const float* __restrict__ data,
+                                             const int64_t* __restrict__ vox, int64_t V, int N,
+                                             const double* __restrict__ M, int K,
+                                             double* __restrict__ B) {
+  constexpr int TV = 64, TR = 32, NC = KP / 4, SLD = TR + 1;
+  extern __shared__ __align__(16) double rsm[];
+  double* sM = rsm;              // TR x KP
+  double* sS = rsm + TR * KP;    // TV x SLD
+  const int tid = threadIdx.x;
+  const int tv = tid & 63, tk = tid >> 6;
+  const int64_t v0 = static_cast<int64_t>(blockIdx.x) * TV;
+  double acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) acc[c] = 0.0;
+  for (int r0 = 0; r0 < N; r0 += TR) {
+    for (int e = tid; e < TV * TR; e += 256) {
+      const int lv = e / TR, lr = e % TR;
+      const int64_t v = v0 + lv;
+      const int r = r0 + lr;
+      double sv = 0.0;
+      if (v < V && r < N) sv = static_cast<double>(data[vox[v] * N + r]);
+      sS[lv * SLD + lr] = sv;
+    }
+    for (int e = tid; e < TR * KP; e += 256) {
+      const int lr = e / KP, k = e % KP;
+      const int r = r0 + lr;
+      sM[lr * KP + k] = (r < N && k < K) ? M[static_cast<size_t>(r) * K + k] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int lr = 0; lr < TR; ++lr) {
+      const double sv = sS[tv * SLD + lr];
+      const double2* mrow = reinterpret_cast<const double2*>(sM + lr * KP + tk * NC);
+#pragma unroll
+      for (int c = 0; c < NC / 2; ++c) {
+        const double2 m2 = mrow[c];
+        acc[2 * c] = fma(m2.x, sv, acc[2 * c]);
+        acc[2 * c + 1] = fma(m2.y, sv, acc[2 * c + 1]);
+      }
+    }
+    __syncthreads();
+  }
+  const int64_t v = v0 + tv;
+  if (v < V) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) B[v * KP + tk * NC + c] = acc[c];
+  }
+}
+
+// ------------------------------------------------------------------ FISTA
+
+// D(8x8) += A(8x4, row) * B(4x8, col) in FP64 on the tensor cores.
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+struct FistaParams {
+  const double* gfrag;         // packed Gram tiles, MT*KT*32
+  const double* B;             // V x Kp
+  double* X;                   // V x Kp out
+  const double* warm;          // V x Kp warm start, or nullptr
+  uint32_t* iters;             // V
+  uint8_t* conv;               // V
+  int64_t V;
+  double n_inv;                // 1 / n_samples
+  double step;                 // 1 / L
+  double thr;                  // step * alpha (when alpha_v is null)
+  const double* alpha_v;       // per-voxel alpha (V), or nullptr
+  double tol;
+  int max_iter;
+  int non_negative;
+  unsigned long long* queue;   // next unassigned position in the work list
+  const int64_t* list;         // work list of voxel positions, or nullptr (= 0..V-1)
+  int64_t n_work;              // length of the work list
+  unsigned long long* iter_total;  // executed iterations, summed (nullable)
+};
+
+// One warp fits 8 voxels at a time (the 8 columns of an m8n8k4 tile).  Lane
+// l holds rows 8*mt + l/4 of voxel columns 2*(l%4) + {0,1} for every row tile
+// mt: the DMMA accumulator layout, so the elementwise FISTA update, the
+// per-voxel norms (a 3-step xor shuffle over the 8 lanes of a column) and the
+// per-voxel state all stay in registers.  y goes through a per-warp shared
+// buffer once per iteration to become the next B operand.  G's tiles are
+// staged once per CTA in shared memory.  A voxel leaves its slot when its
+// relative change drops below tol or it reaches max_iter, exactly the
+// reference's per-voxel stopping rule, and the slot is refilled from the
+// queue, so no lane waits for the slowest voxel of a fixed batch.
+template <int MT>
+__global__ void __launch_bounds__(256) k_fista_fp64(FistaParams p) {
+  constexpr int KP = 8 * MT, KT = 2 * MT;
+  extern __shared__ __align__(16) double smem[];
+  double* sG = smem;                                   // MT*KT*32
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* ybuf = sG + MT * KT * 32 + warp * (KP * 8);  // KP x 8, row-major [k][voxel]
+  for (int i = threadIdx.x; i < MT * KT * 32; i += blockDim.x) sG[i] = p.gfrag[i];
+  __syncthreads();
+
+  const int g = lane >> 2;     // row within a tile / B-fragment column
+  const int q = lane & 3;      // column pair / B-fragment row
+
+  double x[MT][2], y[MT][2], b[MT][2];
+  int64_t vid[2] = {-1, -1};
+  int it[2] = {0, 0};
+  double t[2] = {1.0, 1.0};
+  double thr[2] = {p.thr, p.thr};
+  bool need[2] = {true, true};
+  bool exhausted = false;
+  unsigned long long executed = 0;  // voxel-iterations run by this warp
+
+  while (true) {
+    // ---- refill finished or empty slots from the queue (warp-aggregated)
+    {
+      const unsigned n0 = __ballot_sync(kFull, lane < 4 && need[0]);
+      const unsigned n1 = __ballot_sync(kFull, lane < 4 && need[1]);
+      unsigned colmask = 0;
+#pragma unroll
+      for (int l = 0; l < 4; ++l)
+        colmask |= (((n0 >> l) & 1u) << (2 * l)) | (((n1 >> l) & 1u) << (2 * l + 1));
+      const int nneed = __popc(colmask);
+      if (nneed > 0) {
+        // `base` is warp-uniform; V_END marks "nothing left to hand out".
+        const unsigned long long V_END = static_cast<unsigned long long>(p.n_work);
+        unsigned long long base = V_END;
+        if (!exhausted) {
+          if (lane == 0) base = atomicAdd(p.queue, static_cast<unsigned long long>(nneed));
+          base = __shfl_sync(kFull, base, 0);
+          if (base + nneed >= V_END) exhausted = true;
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          if (!need[j]) continue;
+          const int col = 2 * q + j;
+          const unsigned long long cand = base + __popc(colmask & ((1u << col) - 1u));
+          const int64_t nv = (cand < V_END)
+                                 ? (p.list ? p.list[cand] : static_cast<int64_t>(cand))
+                                 : -1;
+          vid[j] = nv;
+          it[j] = 0;
+          t[j] = 1.0;
+          thr[j] = (p.alpha_v && nv >= 0) ? __dmul_rn(p.step, p.alpha_v[nv]) : p.thr;
+          need[j] = false;
+#pragma unroll
+          for (int mt = 0; mt < MT; ++mt) {
+            const int row = 8 * mt + g;
+            if (nv >= 0) {
+              b[mt][j] = p.B[nv * KP + row];
+              x[mt][j] = p.warm ? p.warm[nv * KP + row] : 0.0;
+            } else {
+              b[mt][j] = 0.0;
+              x[mt][j] = 0.0;
+            }
+            y[mt][j] = x[mt][j];
+          }
+        }
+      }
+    }
+    const bool any_active = __any_sync(kFull, vid[0] >= 0 || vid[1] >= 0);
+    if (!any_active) break;
+    executed += (g == 0) ? ((vid[0] >= 0) + (vid[1] >= 0)) : 0;
+
+    // ---- y -> shared, as the B operand [k][voxel]
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+      const int row = 8 * mt + g;
+      *reinterpret_cast<double2*>(&ybuf[row * 8 + 2 * q]) = make_double2(y[mt][0], y[mt][1]);
+    }
+    __syncwarp();
+
+    // ---- acc = G y on the FP64 tensor cores
+    double acc[MT][2];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) acc[mt][0] = acc[mt][1] = 0.0;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+      const double bf = ybuf[(4 * kt + q) * 8 + g];
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) {
+        const double af = sG[(mt * KT + kt) * 32 + lane];
+        dmma_m8n8k4(acc[mt][0], acc[mt][1], af, bf);
+      }
+    }
+    __syncwarp();
+
+    // ---- proximal gradient step and momentum (fista.rs:141-173)
+    double tn[2], mom[2], dx2[2] = {0.0, 0.0}, xn2[2] = {0.0, 0.0};
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      tn[j] = 0.5 * (1.0 + sqrt(1.0 + 4.0 * t[j] * t[j]));
+      mom[j] = (t[j] - 1.0) / tn[j];
+    }
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const double grad = __dmul_rn(__dsub_rn(acc[mt][j], b[mt][j]), p.n_inv);
+        const double cand = __dsub_rn(y[mt][j], __dmul_rn(p.step, grad));
+        double sv;
+        if (cand > thr[j])
+          sv = __dsub_rn(cand, thr[j]);
+        else if (cand < -thr[j])
+          sv = __dadd_rn(cand, thr[j]);
+        else
+          sv = 0.0;
+        const double xn = p.non_negative ? fmax(sv, 0.0) : sv;
+        const double d = __dsub_rn(xn, x[mt][j]);
+        y[mt][j] = __dadd_rn(xn, __dmul_rn(mom[j], d));
+        dx2[j] = __dadd_rn(dx2[j], __dmul_rn(d, d));
+        xn2[j] = __dadd_rn(xn2[j], __dmul_rn(xn, xn));
+        x[mt][j] = xn;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+#pragma unroll
+      for (int o = 4; o < 32; o <<= 1) {
+        dx2[j] += __shfl_xor_sync(kFull, dx2[j], o);
+        xn2[j] += __shfl_xor_sync(kFull, xn2[j], o);
+      }
+    }
+
+    // ---- per-voxel stopping rule (fista.rs:166-179) and write-out
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      if (vid[j] < 0) continue;
+      const double rel = sqrt(dx2[j]) / fmax(sqrt(xn2[j]), 1e-12);
+      t[j] = tn[j];
+      it[j] += 1;
+      const bool converged = rel < p.tol;
+      if (converged || it[j] >= p.max_iter) {
+        const int64_t v = vid[j];
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) p.X[v * KP + 8 * mt + g] = x[mt][j];
+        if (g == 0) {
+          p.iters[v] = static_cast<uint32_t>(it[j]);
+          p.conv[v] = converged ? 1 : 0;
+        }
+        need[j] = true;
+      }
+    }
+  }
+  if (p.iter_total) {
+    for (int o = 16; o > 0; o >>= 1) executed += __shfl_xor_sync(kFull, executed, o);
+    if (lane == 0) atomicAdd(p.iter_total, executed);
+  }
+}
+
+// max_iter == 0: every voxel of the work list keeps its starting point.
+__global__ void k_fista_noop(FistaParams p, int Kp) {
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= p.n_work * (Kp + 1)) return;
+  const int64_t w = e / (Kp + 1);
+  const int k = static_cast<int>(e % (Kp + 1));
+  const int64_t v = p.list ? p.list[w] : w;
+  if (k < Kp) {
+    p.X[v * Kp + k] = p.warm ? p.warm[v * Kp + k] : 0.0;
+  } else {
+    p.iters[v] = 0;
+    p.conv[v] = 0;
+  }
+}
+
+// --------------------------------------------------------------- Tikhonov
+
+// c = (L L^T)^{-1} b, one warp per voxel.  Lane l owns rows l, l + 32, ...;
+// forward then backward substitution in the column (axpy) order, so every
+// entry accumulates its terms in index order as a sequential solve does.
+// L is staged in shared memory with a padded row stride.
+template <int RPL>  // rows per lane = ceil(K / 32)
+__global__ void __launch_bounds__(256) k_tikhonov(const double* __restrict__ Lg, int K, int Kp,
+                                                  const double* __restrict__ B,
+                                                  double* __restrict__ X, int64_t V) {
+  extern __shared__ double sL[];  // K x (K + 1)
+  const int ld = K + 1;
+  for (int i = threadIdx.x; i < K * K; i += blockDim.x) sL[(i / K) * ld + (i % K)] = Lg[(i / K) * Kp + (i % K)];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t warps_total = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t v = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); v < V;
+       v += warps_total) {
+    double r[RPL];
+#pragma unroll
+    for (int c = 0; c < RPL; ++c) {
+      const int row = lane + 32 * c;
+      r[c] = (row < K) ? B[v * Kp + row] : 0.0;
+    }
+    // forward: L y = b
+    for (int i = 0; i < K; ++i) {
+      const int owner = i & 31, oc = i >> 5;
+      double yi = 0.0;
+#pragma unroll
+      for (int c = 0; c < RPL; ++c)
+        if (c == oc && lane == owner) yi = __ddiv_rn(r[c], sL[i * ld + i]);
+      yi = __shfl_sync(kFull, yi, owner);
+#pragma unroll
+      for (int c = 0; c < RPL; ++c) {
+        const int row = lane + 32 * c;
+        if (row > i && row < K) r[c] = __dsub_rn(r[c], __dmul_rn(sL[row * ld + i], yi));
+        if (row == i) r[c] = yi;
+      }
+    }
+    // backward: L^T x = y
+    for (int i = K - 1; i >= 0; --i) {
+      const int owner = i & 31, oc = i >> 5;
+      double xi = 0.0;
+#pragma unroll
+      for (int c = 0; c < RPL; ++c)
+        if (c == oc && lane == owner) xi = __ddiv_rn(r[c], sL[i * ld + i]);
+      xi = __shfl_sync(kFull, xi, owner);
+#pragma unroll
+      for (int c = 0; c < RPL; ++c) {
+        const int row = lane + 32 * c;
+        if (row < i) r[c] = __dsub_rn(r[c], __dmul_rn(sL[i * ld + row], xi));
+        if (row == i) r[c] = xi;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < RPL; ++c) {
+      const int row = lane + 32 * c;
+      if (row < Kp) X[v * Kp + row] = (row < K) ? r[c] : 0.0;
+    }
+  }
+}
+
+// --------------------------------------------------------------- epilogue
+
+struct EpilogueParams {
+  const float* data;
+  const int64_t* vox;
+  int64_t V;
+  int N, K, Kp;
+  const double* Mt;         // Kp x N row-major (transposed design, zero rows past K)
+  const double* X;          // V x Kp
+  const uint32_t* iters;    // V, or nullptr (then iteration count 1)
+  float* coeffs;            // X*Y*Z*K volume (pre-zeroed)
+  double* coef64;           // V x K, or nullptr
+  float* r2;                // maps (nullable)
+  float* resid;
+  uint32_t* iter_map;
+  uint8_t* kind_map;
+  float* alpha_map;
+  float* bic_map;
+  uint8_t kind;
+  double alpha;             // alpha written to the alpha map (Fixed)
+  const double* alpha_v;    // per-voxel alpha (V), overrides `alpha` if set
+  const uint8_t* zero_v;    // per-voxel "alpha_max == 0" flag (V), or nullptr:
+                            // such voxels report residual 0 and BIC 0
+                            // (VoxelAlphaResult::zero, src/solver/alpha.rs:179-188)
+  double* resid_out;        // V, or nullptr: residual_l2 per voxel (FP64)
+  int* nnz_out;             // V, or nullptr: exactly non-zero coefficients
+  const int64_t* list;      // subset of positions to process, or nullptr (= all V)
+  int64_t n_work;           // length of `list` (or V)
+  bool scatter;             // write coefficients and maps (false: residuals only)
+};
+
+// Eight voxels per warp: lane l computes rows i = l, l+32, ... of
+// r_v = s_v - M c_v for all eight voxels at once, so each coalesced load of a
+// column of M^T feeds eight FMAs.  Then residual_l2 = ||r||, R^2 = 1 - RSS /
+// sum (s - mean)^2 with the mean taken first (src/fit.rs:115-128), BIC with
+// the count of exactly non-zero coefficients (src/solver/alpha.rs:99-103,
+// 217-219), and the scatter of coefficients and map entries.
+__global__ void __launch_bounds__(256) k_epilogue(EpilogueParams p) {
+  extern __shared__ __align__(16) double sx[];  // per warp: Kp x 8, [k][voxel]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* xs = sx + warp * (p.Kp * 8);
+  const int64_t groups = (p.n_work + 7) / 8;
+  const int64_t warps_total = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t gi = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp; gi < groups;
+       gi += warps_total) {
+    const int64_t w0 = gi * 8;
+    const int nv = static_cast<int>((p.n_work - w0) < 8 ? (p.n_work - w0) : 8);
+    int64_t vv[8], li[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      vv[j] = (j < nv) ? (p.list ? p.list[w0 + j] : w0 + j) : 0;
+      li[j] = (j < nv) ? p.vox[vv[j]] : 0;
+    }
+    for (int e = lane; e < p.Kp * 8; e += 32) {
+      const int k = e >> 3, j = e & 7;
+      xs[e] = (j < nv) ? p.X[vv[j] * p.Kp + k] : 0.0;
+    }
+    __syncwarp();
+    double rss[8], ssum[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) rss[j] = ssum[j] = 0.0;
+    for (int i = lane; i < p.N; i += 32) {
+      double acc[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[j] = 0.0;
+      for (int k = 0; k < p.K; ++k) {
+        const double m = __ldg(p.Mt + static_cast<size_t>(k) * p.N + i);
+        const double2* xk = reinterpret_cast<const double2*>(xs + k * 8);
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const double2 xv = xk[h];
+          acc[2 * h] = fma(m, xv.x, acc[2 * h]);
+          acc[2 * h + 1] = fma(m, xv.y, acc[2 * h + 1]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (j < nv) {
+          const double si = static_cast<double>(p.data[li[j] * p.N + i]);
+          const double r = si - acc[j];
+          rss[j] = fma(r, r, rss[j]);
+          ssum[j] += si;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      for (int o = 16; o > 0; o >>= 1) {
+        rss[j] += __shfl_xor_sync(kFull, rss[j], o);
+        ssum[j] += __shfl_xor_sync(kFull, ssum[j], o);
+      }
+    double sst[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) sst[j] = 0.0;
+    for (int i = lane; i < p.N; i += 32) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (j < nv) {
+          const double d = static_cast<double>(p.data[li[j] * p.N + i]) - ssum[j] / static_cast<double>(p.N);
+          sst[j] = fma(d, d, sst[j]);
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      for (int o = 16; o > 0; o >>= 1) sst[j] += __shfl_xor_sync(kFull, sst[j], o);
+    for (int j = 0; j < nv; ++j) {
+      const int64_t v = vv[j];
+      int nnz = 0;
+      for (int k = lane; k < p.K; k += 32) {
+        const double c = xs[k * 8 + j];
+        nnz += (c != 0.0) ? 1 : 0;
+        if (p.scatter) {
+          p.coeffs[li[j] * p.K + k] = static_cast<float>(c);
+          if (p.coef64) p.coef64[v * p.K + k] = c;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) nnz += __shfl_xor_sync(kFull, nnz, o);
+      if (lane == 0) {
+        const bool zero = p.zero_v && p.zero_v[v];
+        const double resid = zero ? 0.0 : sqrt(rss[j]);
+        const double ss_res = resid * resid;
+        const double r2 = sst[j] > 0.0 ? 1.0 - ss_res / sst[j] : 0.0;
+        const double a = p.alpha_v ? p.alpha_v[v] : p.alpha;
+        if (p.resid_out) p.resid_out[v] = resid;
+        if (p.nnz_out) p.nnz_out[v] = nnz;
+        if (p.scatter) {
+          if (p.r2) p.r2[li[j]] = static_cast<float>(r2);
+          if (p.resid) p.resid[li[j]] = static_cast<float>(resid);
+          if (p.iter_map) p.iter_map[li[j]] = p.iters ? p.iters[v] : 1u;
+          if (p.kind_map) p.kind_map[li[j]] = p.kind;
+          if (p.alpha_map) p.alpha_map[li[j]] = static_cast<float>(a);
+          if (p.bic_map) {
+            const double n = static_cast<double>(p.N);
+            const double rc = fmax(ss_res, 2.2250738585072014e-308);
+            p.bic_map[li[j]] =
+                zero ? 0.0f
+                     : static_cast<float>(n * log(rc / n) + log(n) * static_cast<double>(nnz));
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------- utility
+
+// M^T, padded to Kp rows (rows past K are zero), row-major Kp x N.
+__global__ void k_transpose_design(const double* __restrict__ M, int N, int K, int Kp,
+                                   double* __restrict__ Mt) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= Kp * N) return;
+  const int k = idx / N, i = idx % N;
+  Mt[idx] = (k < K) ? M[static_cast<size_t>(i) * K + k] : 0.0;
+}
+
+__global__ void k_fill_f64(double* __restrict__ a, int64_t n, double v) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
+__global__ void k_square(const double* __restrict__ a, double* __restrict__ b, int64_t n) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = a[i] * a[i];
+}
+
+// map[vox[v]] = (float) a[v]
+__global__ void k_scatter_f64_to_f32(const double* __restrict__ a, const int64_t* __restrict__ vox,
+                                     int64_t V, float* __restrict__ map) {
+  const int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v < V) map[vox[v]] = static_cast<float>(a[v]);
+}
+
+}  // namespace csd

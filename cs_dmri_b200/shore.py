@@ -1,0 +1,139 @@
+"""3D-SHORE model and fit objects with the reference's Python interface
+(``cs_dmri.ShoreModel`` / ``cs_dmri.ShoreFit``, python/cs_dmri/shore.py:25-299),
+fitted by the CUDA library."""
+
+from __future__ import annotations
+
+import warnings
+
+import numpy as np
+
+from . import _core
+from .gradients import as_gradient_table
+
+__all__ = ["ShoreModel", "ShoreFit"]
+
+_REGULARIZATIONS = ("l1", "l2", "nonneg")
+_ALPHA_MODES = ("l2-anchored", "path-bic", "alpha-ratio", "fixed")
+_FRAMES = ("auto", "world", "image")
+
+
+def _fit_frame(bvec_frame: str, affine):
+    """("world" | "image", R) with R rotating image-axis vectors into the fit
+    frame (python/cs_dmri/_frame.py:13-31)."""
+    if bvec_frame not in _FRAMES:
+        raise ValueError(f"bvec_frame must be one of {_FRAMES}, got {bvec_frame!r}")
+    if bvec_frame == "auto":
+        bvec_frame = "world" if affine is not None else "image"
+    if bvec_frame == "world":
+        if affine is None:
+            raise ValueError("bvec_frame='world' needs an affine (fit a DWI, or pass affine=)")
+        return "world", _core.affine_rotation(np.asarray(affine, dtype=np.float64))
+    return "image", np.eye(3)
+
+
+def _rotate(vectors, R):
+    return np.ascontiguousarray(np.asarray(vectors, dtype=np.float64) @ R.T)
+
+
+class ShoreModel:
+    """3D-SHORE model (Merlet & Deriche 2013; Ozarslan et al. 2013).
+
+    Same parameters and defaults as ``cs_dmri.ShoreModel``: ``radial_order``
+    (even; 6 gives 72 coefficients), ``zeta`` (700), ``regularization`` in
+    ``{"l1", "l2", "nonneg"}``, ``alpha_mode`` in ``{"l2-anchored",
+    "path-bic", "alpha-ratio", "fixed"}``, the L1 path settings, the Tikhonov
+    weights ``lambda_n`` / ``lambda_l``, the amplitude-ICLS settings,
+    ``bvec_frame`` and ``allow_single_shell``.  ``device`` picks the GPU.
+    """
+
+    def __init__(self, gtab, *, radial_order: int = 6, zeta: float = 700.0, regularization: str = "l1",
+                 alpha_mode: str = "l2-anchored", alpha: float = 1.0, alpha_ratio: float = 1e-3,
+                 path_n_alphas: int = 20, path_eps: float | None = None, slack: float = 0.05,
+                 max_iter: int = 1000, tol: float = 1e-6, non_negative: bool = False,
+                 lambda_n: float = 1e-8, lambda_l: float = 1e-8, nonneg_max_iter: int = 200,
+                 nonneg_tol: float = 1e-9, nonneg_epsilon: float = 1e-10, bvec_frame: str = "auto",
+                 allow_single_shell: bool = False, device: int = 0):
+        if regularization not in _REGULARIZATIONS:
+            raise ValueError(f"regularization must be one of {_REGULARIZATIONS}, got {regularization!r}")
+        if alpha_mode not in _ALPHA_MODES:
+            raise ValueError(f"alpha_mode must be one of {_ALPHA_MODES}, got {alpha_mode!r}")
+        self.gtab = as_gradient_table(gtab)
+        self.radial_order = radial_order
+        self.zeta = zeta
+        self.regularization = regularization
+        self.bvec_frame = bvec_frame
+        self.device = device
+        self._solver = dict(
+            alpha_mode=alpha_mode, alpha=alpha, alpha_ratio=alpha_ratio, path_n_alphas=path_n_alphas,
+            path_eps=path_eps, slack=slack, max_iter=max_iter, tol=tol, non_negative=non_negative,
+            lambda_n=lambda_n, lambda_l=lambda_l, nonneg_max_iter=nonneg_max_iter, nonneg_tol=nonneg_tol,
+            nonneg_epsilon=nonneg_epsilon, allow_single_shell=allow_single_shell)
+
+    def fit(self, data, mask=None, *, affine=None, diagnostics: bool = True,
+            n_threads: int | None = None) -> "ShoreFit":
+        """Fit every voxel in ``mask`` ((X, Y, Z) bool; required for arrays)."""
+        vol = np.asarray(data, dtype=np.float32)
+        if vol.ndim != 4:
+            raise ValueError(f"expected a 4-D (X, Y, Z, N) array, got shape {vol.shape}")
+        if mask is None:
+            raise ValueError("a mask is required")
+        m = np.asarray(mask)
+        if m.dtype != bool:
+            m = m > 0
+        if m.shape != vol.shape[:3]:
+            raise ValueError(f"mask shape {m.shape} does not match data spatial shape {vol.shape[:3]}")
+        affine = None if affine is None else np.asarray(affine, dtype=np.float64)
+        frame, R = _fit_frame(self.bvec_frame, affine)
+        out = _core.shore_fit(
+            vol, self.gtab.bvals, _rotate(self.gtab.bvecs, R), m,
+            big_delta=self.gtab.big_delta, small_delta=self.gtab.small_delta,
+            b0_threshold=self.gtab.b0_threshold,
+            bvec_frame="world-ras" if frame == "world" else "image-axis",
+            radial_order=self.radial_order, zeta=self.zeta, regularization=self.regularization,
+            diagnostics=diagnostics, n_threads=n_threads, device=self.device, **self._solver)
+        for message in out.pop("warnings", ()):
+            warnings.warn(message, stacklevel=2)
+        return ShoreFit(out, model=self, mask=m, affine=affine, frame=frame, rotation=R)
+
+
+class ShoreFit:
+    """Result of :meth:`ShoreModel.fit`: ``coefficients`` (X, Y, Z, K) float32,
+    the diagnostic maps (``r2, rmse, residual_l2, iterations,
+    regularization_kind``, and ``alpha, bic, rss_l2`` where the solver has
+    them), ``sidecar`` and ``frame``."""
+
+    def __init__(self, arrays: dict, *, model=None, mask=None, affine=None, frame="image", rotation=None):
+        self.coefficients = arrays["coefficients"]
+        self.sidecar = arrays["sidecar"]
+        self.alpha_distribution = arrays.get("alpha_distribution")
+        for k in ("r2", "rmse", "residual_l2", "iterations", "regularization_kind", "alpha", "bic", "rss_l2"):
+            setattr(self, k, arrays.get(k))
+        self.model = model
+        self.mask = mask if mask is not None else np.any(self.coefficients != 0, axis=-1)
+        self.affine = affine
+        self.frame = frame
+        self._rotation = np.eye(3) if rotation is None else rotation
+        basis = self.sidecar["basis"]
+        self.radial_order = int(basis["radial_order"])
+        self.zeta = float(basis["zeta"])
+
+    @property
+    def dwi_shells(self):
+        shells = self.sidecar.get("dwi_shells")
+        return None if shells is None else [float(b) for b in shells]
+
+    @property
+    def single_shell(self) -> bool:
+        return self.dwi_shells is not None and len(self.dwi_shells) < 2
+
+    @property
+    def sparsity(self) -> np.ndarray:
+        """Fraction of non-zero coefficients per voxel (L1 sparsity)."""
+        out = np.zeros(self.coefficients.shape[:3], np.float32)
+        out[self.mask] = (self.coefficients[self.mask] != 0).mean(-1)
+        return out
+
+    def __repr__(self) -> str:
+        r2 = "" if self.r2 is None else f", mean R² {float(self.r2[self.mask].mean()):.3f}"
+        return f"ShoreFit(radial_order={self.radial_order}, {int(self.mask.sum())} voxels{r2}, frame={self.frame})"

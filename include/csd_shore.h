@@ -1,0 +1,221 @@
+/*
+ * csd_shore.h - C ABI of the B200 3D-SHORE volume fit (libcsdshore.so).
+ *
+ * This is the drop-in boundary for cs_dmri's masked-voxel SHORE fit.  The
+ * reference binds the same operation three ways:
+ *
+ *   Rust library : fit_shore(&DwiData, &ShoreFitSpec, on_voxel)
+ *                  -> Result<ShoreFitOutput>            (src/fit.rs:687)
+ *   PyO3         : _cs_dmri.shore_fit(data, bvals, bvecs, mask, **kw)
+ *                                                       (python/src/models.rs:70-198)
+ *   per voxel    : trait Solver { fn fit(&Problem) }    (src/solver/mod.rs:49-51)
+ *
+ * A per-voxel call is far too fine for a GPU, so the boundary sits at the
+ * volume level (fit_shore / fit_volume_*), and every entry point below
+ * replaces one of the reference's volume-level interfaces.  All buffers are
+ * owned by the caller; the handle owns device memory, streams and the
+ * per-gradient-table setup cache.  Nothing here takes or returns a torch type.
+ *
+ * Layouts follow the reference exactly (src/io/dwi.rs:22-40, src/fit.rs:89):
+ *   data          float32 (X, Y, Z, N), C order: a voxel's N samples contiguous
+ *   mask          uint8   (X, Y, Z), non-zero = fit this voxel
+ *   coefficients  float32 (X, Y, Z, K), C order, zeros outside the mask
+ *   diagnostic maps (X, Y, Z) float32 / uint32 / uint8
+ * Coefficient order is the BrainSuite SHORE order (n, l even <= n, m)
+ * (src/basis/shore.rs:29-44): K = 72 at radial order 6, 145 at order 8.
+ *
+ * Status codes mirror CsDmriError (src/lib.rs:62-81):
+ *   0 ok, 1 invalid argument / dimension mismatch (CsDmriError::Dimension,
+ *   ::Other), 2 fit refused (CsDmriError::Fit, shell guard src/fit.rs:691-717),
+ *   3 numerical (a normal matrix that is not positive definite; the reference
+ *   panics at src/solver/tikhonov.rs:326), 4 CUDA error, 5 timeout (a bounded
+ *   device wait gave up).  A message is written to `err` (NUL-terminated,
+ *   truncated to err_len).  Per-voxel non-convergence is not an error: it is
+ *   reported through the iterations map and the converged flags.
+ */
+#ifndef CSD_SHORE_H
+#define CSD_SHORE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CSD_ABI_VERSION 1
+
+enum csd_status {
+  CSD_OK = 0,
+  CSD_ERR_INVALID = 1,
+  CSD_ERR_FIT_REFUSED = 2,
+  CSD_ERR_NUMERICAL = 3,
+  CSD_ERR_CUDA = 4,
+  CSD_ERR_TIMEOUT = 5
+};
+
+/* ShoreRegularization (src/fit.rs:595-610); values match the reference's
+ * regularization_kind map (1 = L1, 2 = L2, 3 = amplitude ICLS). */
+enum csd_regularization {
+  CSD_REG_L1 = 1,
+  CSD_REG_L2 = 2,
+  CSD_REG_NONNEG = 3
+};
+
+/* AlphaMode (src/fit.rs:545-550). */
+enum csd_alpha_mode {
+  CSD_ALPHA_FIXED = 0,
+  CSD_ALPHA_RATIO = 1,
+  CSD_ALPHA_PATH_BIC = 2,
+  CSD_ALPHA_L2_ANCHORED = 3
+};
+
+/* Arithmetic of the FISTA iterations.  FP64 is the reference-faithful path:
+ * the same iteration, step 1/L and stopping rule as src/solver/fista.rs:70-143
+ * evaluated in IEEE double. */
+enum csd_precision {
+  CSD_PRECISION_FP64 = 0
+};
+
+/* Gradient table (src/qspace.rs:90-130).  big_delta / small_delta in seconds;
+ * pass NaN for either to use the TORTOISE estimate at gmax 0.08 T/m
+ * (src/qspace.rs:213-227), as the Python binding does (python/src/lib.rs:89). */
+typedef struct csd_gtab {
+  const double* bvals;      /* N */
+  const double* bvecs;      /* N x 3, row-major */
+  int32_t n;
+  double big_delta;
+  double small_delta;
+  double b0_threshold;      /* default 50 s/mm^2 */
+} csd_gtab;
+
+/* ShoreFitSpec (src/fit.rs:634-669) flattened, with the kwargs of
+ * _cs_dmri.shore_fit (python/src/models.rs:70-76).  csd_default_spec() fills
+ * the reference defaults. */
+typedef struct csd_shore_spec {
+  int32_t radial_order;     /* positive, even (models.rs:142-144); default 6 */
+  double zeta;              /* default 700 */
+  int32_t regularization;   /* csd_regularization; default L1 */
+  int32_t alpha_mode;       /* csd_alpha_mode; default L2_ANCHORED */
+  double alpha;             /* Fixed alpha and FISTA seed alpha; default 1.0 */
+  double alpha_ratio;       /* default 1e-3 */
+  int32_t path_n_alphas;    /* default 20 */
+  double path_eps;          /* <= 0: mode default (1e-3 path-bic, 1e-4 l2-anchored) */
+  double slack;             /* default 0.05 */
+  int32_t max_iter;         /* FISTA, default 1000 */
+  double tol;               /* FISTA, default 1e-6 */
+  int32_t non_negative;     /* FISTA coefficient projection, default 0 */
+  double lambda_n;          /* Tikhonov radial weight, default 1e-8 */
+  double lambda_l;          /* Tikhonov angular weight, default 1e-8 */
+  int32_t nonneg_max_iter;  /* ICLS, default 200 */
+  double nonneg_tol;        /* ICLS, default 1e-9 */
+  double nonneg_epsilon;    /* ICLS, default 1e-10 */
+  int32_t diagnostics;      /* fill the diagnostic maps; default 0 */
+  int32_t allow_single_shell; /* default 0 */
+  int32_t precision;        /* csd_precision; default FP64 */
+} csd_shore_spec;
+
+/* Outputs of one volume fit: ShoreFitOutput (src/fit.rs:672-683) plus the
+ * diagnostics maps of VolumeDiagnostics (src/fit.rs:31-43).  Pointers are
+ * caller-owned; the optional ones may be NULL.  The maps are written only when
+ * spec.diagnostics is set; alpha/bic are written for L1 and rss_l2 for the
+ * L2-anchored strategy, exactly where the reference returns Some(..). */
+typedef struct csd_fit_result {
+  /* required */
+  float* coefficients;          /* X*Y*Z*K */
+  /* optional maps (X*Y*Z) */
+  float* r2;
+  float* residual_l2;
+  uint32_t* iterations;
+  uint8_t* regularization_kind;
+  float* alpha;
+  float* bic;
+  float* rss_l2;
+  /* optional: FP64 coefficients of the masked voxels, V x K, in the
+   * canonical x-y-z mask order (src/voxel_loop.rs:28-42), for parity checks */
+  double* coef64;
+  /* optional: per masked voxel 1 = converged (V entries, mask order) */
+  uint8_t* converged;
+
+  /* scalar results, written by the call */
+  int32_t n_coeffs;
+  int64_t n_voxels;
+  int32_t has_alpha_distribution;
+  double alpha_distribution[3]; /* median, p10, p90 (src/fit.rs:334-352) */
+  double representative_alpha;
+  double big_delta_seconds;
+  double small_delta_seconds;
+  double tau_seconds;
+  int32_t delta_source;         /* 0 user supplied, 1 TORTOISE estimate */
+  int32_t n_shells;
+  double dwi_shells[32];        /* mean b of the non-zero shells, ascending */
+  int32_t lmax;                 /* amplitude-ICLS constraint order */
+  int32_t n_constraint_dirs;    /* amplitude-ICLS sphere size */
+  uint64_t total_iterations;    /* sum of solver iterations over the mask */
+  char warnings[2048];          /* '\n'-separated, as ShoreFitOutput::warnings */
+} csd_fit_result;
+
+/* Opaque handle: device memory, streams, cached per-table setup. */
+typedef struct csd_handle csd_handle;
+
+/* Library / ABI identification. */
+const char* csd_version(void);
+int csd_abi_version(void);
+
+/* Fill `spec` with ShoreFitSpec::default() and the PyO3 kwarg defaults
+ * (src/fit.rs:647-669, python/src/models.rs:70-76). */
+void csd_default_spec(csd_shore_spec* spec);
+
+/* Number of SHORE coefficients at `radial_order` (ShoreBasis::new,
+ * src/basis/shore.rs:29-44). */
+int csd_shore_n_coeffs(int32_t radial_order);
+
+/* Create / destroy a handle bound to CUDA device `device`. */
+int csd_create(csd_handle** out, int32_t device, char* err, size_t err_len);
+void csd_destroy(csd_handle* h);
+
+/* Whole-volume fit from HOST buffers (replaces fit_shore, src/fit.rs:687, and
+ * _cs_dmri.shore_fit, python/src/models.rs:77).  Host-to-device copies of the
+ * data and the device-to-host copies of every output happen inside the call.
+ * Blocking. */
+int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask,
+                         int64_t X, int64_t Y, int64_t Z, const csd_gtab* gtab,
+                         const csd_shore_spec* spec, csd_fit_result* out,
+                         char* err, size_t err_len);
+
+/* Same fit, with `data`, `mask` and every output pointer of `out` in DEVICE
+ * memory of the handle's device (e.g. torch tensors' data_ptr()).  Work is
+ * queued on `stream` (a cudaStream_t; NULL = the handle's stream); the call
+ * returns after the stream has finished, so outputs are ready on return.
+ * Replaces the same interface as csd_shore_fit_volume. */
+int csd_shore_fit_volume_device(csd_handle* h, const float* d_data, const uint8_t* d_mask,
+                                int64_t X, int64_t Y, int64_t Z, const csd_gtab* gtab,
+                                const csd_shore_spec* spec, csd_fit_result* out,
+                                void* stream, char* err, size_t err_len);
+
+/* Design matrix M (N x K, row-major, FP64) of the SHORE basis for `gtab`,
+ * built on the device (replaces ShoreBasis::design_matrix,
+ * src/basis/shore.rs:122-178).  `out` is a host buffer of N*K doubles. */
+int csd_shore_design_matrix(csd_handle* h, const csd_gtab* gtab, int32_t radial_order,
+                            double zeta, double* out, char* err, size_t err_len);
+
+/* Per-handle counters of the last fit, for measurement: kernel-only device
+ * time of each stage in milliseconds (CUDA events on the fit stream) and the
+ * number of kernel launches the fit issued. */
+typedef struct csd_fit_timing {
+  float ms_setup;       /* design, Gram, factorizations, Lipschitz */
+  float ms_rhs;         /* A^T s over the mask */
+  float ms_solve;       /* FISTA / Tikhonov / ICLS iterations */
+  float ms_epilogue;    /* residual, R^2, scatter */
+  float ms_total;       /* device time from first to last kernel */
+  int32_t launches;     /* kernels launched by the fit */
+  float ms_solve_kernel;/* duration of the dominant solve kernel alone */
+} csd_fit_timing;
+
+int csd_last_timing(const csd_handle* h, csd_fit_timing* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CSD_SHORE_H */

@@ -1,0 +1,294 @@
+"""ctypes wrapper of the CPU FP64 oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, as the checker.  It shares the argument structs
+of the product's C ABI (include/csd_shore.h) so both are driven identically.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+
+_lib = None
+
+
+def build(force: bool = False) -> Path:
+    srcs = [HERE / "shore_oracle.cpp", HERE / "shore_oracle.h", HERE.parent / "include" / "csd_shore.h"]
+    if force or not LIB.exists() or any(s.stat().st_mtime > LIB.stat().st_mtime for s in srcs):
+        subprocess.run(["make", "-C", str(HERE), "-B" if force else "all"], check=True,
+                       capture_output=True, text=True)
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        d, i32, p = C.c_double, C.c_int32, C.c_void_p
+        sig = {
+            "oracle_factorial": (d, [C.c_uint32]),
+            "oracle_gamma": (d, [d]),
+            "oracle_assoc_legendre": (d, [C.c_uint32, C.c_uint32, d]),
+            "oracle_gen_laguerre": (d, [C.c_uint32, d, d]),
+            "oracle_hyp2f1": (d, [d, d, d, d]),
+            "oracle_qvals": (C.c_int, [p, p, p, p, p]),
+            "oracle_shells": (C.c_int, [p, i32, d, d, p, p]),
+            "oracle_tortoise_deltas": (None, [p, i32, d, p, p]),
+            "oracle_n_coeffs": (C.c_int, [i32]),
+            "oracle_shore_indices": (None, [i32, p, p, p]),
+            "oracle_kappa": (d, [d, C.c_uint32, C.c_uint32]),
+            "oracle_shore_radial": (d, [C.c_uint32, C.c_uint32, d, d]),
+            "oracle_brainsuite_sh_block": (None, [C.c_uint32, d, d, p]),
+            "oracle_design_matrix": (C.c_int, [p, i32, d, p]),
+            "oracle_regularization": (None, [i32, p, p]),
+            "oracle_radial_factor": (d, [C.c_uint32, C.c_uint32, d]),
+            "oracle_brainsuite_to_tournier": (None, [C.c_uint32, i32, p, p]),
+            "oracle_shore_to_tournier": (C.c_int, [i32, d, i32, p]),
+            "oracle_odf8_hemisphere": (C.c_int, [p]),
+            "oracle_sh2amp_cart": (None, [p, i32, i32, p]),
+            "oracle_sigma_max": (d, [p, i32, i32]),
+            "oracle_fista_fit": (C.c_int, [p, i32, i32, p, d, i32, d, i32, p, p, p, p, p]),
+            "oracle_tikhonov_fit": (C.c_int, [p, i32, i32, p, p, d, d, p, p, p]),
+            "oracle_icls_solve": (C.c_int, [p, i32, i32, p, i32, p, i32, d, d, p, p, p, p, p]),
+            "oracle_alpha_max": (d, [p, i32, i32, p]),
+            "oracle_log_path": (C.c_int, [d, i32, d, p]),
+            "oracle_bic": (d, [i32, d, i32]),
+            "oracle_shore_fit_volume": (C.c_int, [p, p, C.c_int64, C.c_int64, C.c_int64, p, p, p, i32, p,
+                                                  C.c_size_t]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+# ------------------------------------------------------------ math / basis
+
+def factorial(n): return lib().oracle_factorial(n)
+def gamma(x): return lib().oracle_gamma(x)
+def assoc_legendre(l, m, x): return lib().oracle_assoc_legendre(l, m, x)
+def gen_laguerre(n, a, x): return lib().oracle_gen_laguerre(n, a, x)
+def hyp2f1(a, b, c, z): return lib().oracle_hyp2f1(a, b, c, z)
+def kappa(zeta, n, l): return lib().oracle_kappa(zeta, n, l)
+def shore_radial(n, l, q, zeta): return lib().oracle_shore_radial(n, l, q, zeta)
+def radial_factor(n, l, zeta): return lib().oracle_radial_factor(n, l, zeta)
+def n_coeffs(order): return lib().oracle_n_coeffs(order)
+def bic(n, rss, k): return lib().oracle_bic(n, rss, k)
+
+
+def _gtab(bvals, bvecs, big_delta=None, small_delta=None, b0_threshold=50.0):
+    from cs_dmri_b200._core import build_gtab
+    return build_gtab(bvals, bvecs, b0_threshold, big_delta, small_delta)
+
+
+def shore_indices(order):
+    k = n_coeffs(order)
+    n, l, m = (np.zeros(k, np.int32) for _ in range(3))
+    lib().oracle_shore_indices(order, _p(n), _p(l), _p(m))
+    return np.stack([n, l, m], 1)
+
+
+def brainsuite_sh_block(l, theta, phi):
+    out = np.zeros(2 * l + 1)
+    lib().oracle_brainsuite_sh_block(l, theta, phi, _p(out))
+    return out
+
+
+def qvals(bvals, bvecs, big_delta=None, small_delta=None, b0_threshold=50.0):
+    g, keep = _gtab(bvals, bvecs, big_delta, small_delta, b0_threshold)
+    q = np.zeros(g.n)
+    big, small, src = C.c_double(), C.c_double(), C.c_int32()
+    lib().oracle_qvals(C.addressof(g), _p(q), C.addressof(big), C.addressof(small), C.addressof(src))
+    return q, big.value, small.value, src.value
+
+
+def shells(bvals, b0_threshold=50.0, tolerance=50.0):
+    b = _f64(bvals)
+    sb = np.zeros(len(b) + 1)
+    of = np.zeros(len(b), np.int32)
+    n = lib().oracle_shells(_p(b), len(b), b0_threshold, tolerance, _p(sb), _p(of))
+    return sb[:n], of
+
+
+def tortoise_deltas(bvals, gmax=80e-3):
+    b = _f64(bvals)
+    big, small = C.c_double(), C.c_double()
+    lib().oracle_tortoise_deltas(_p(b), len(b), gmax, C.addressof(big), C.addressof(small))
+    return big.value, small.value
+
+
+def design_matrix(bvals, bvecs, order=6, zeta=700.0, big_delta=None, small_delta=None, b0_threshold=50.0):
+    g, keep = _gtab(bvals, bvecs, big_delta, small_delta, b0_threshold)
+    out = np.zeros((g.n, n_coeffs(order)))
+    lib().oracle_design_matrix(C.addressof(g), order, zeta, _p(out))
+    return out
+
+
+def regularization(order):
+    k = n_coeffs(order)
+    a, b = np.zeros(k), np.zeros(k)
+    lib().oracle_regularization(order, _p(a), _p(b))
+    return a, b
+
+
+def brainsuite_to_tournier(l, k):
+    idx, sign = C.c_int32(), C.c_double()
+    lib().oracle_brainsuite_to_tournier(l, k, C.addressof(idx), C.addressof(sign))
+    return idx.value, sign.value
+
+
+def shore_to_tournier(order, zeta, lmax):
+    nsh = (lmax + 1) * (lmax + 2) // 2
+    out = np.zeros((nsh, n_coeffs(order)))
+    lib().oracle_shore_to_tournier(order, zeta, lmax, _p(out))
+    return out
+
+
+def odf8_hemisphere():
+    out = np.zeros((700, 3))
+    n = lib().oracle_odf8_hemisphere(_p(out))
+    return out[:n].copy()
+
+
+def sh2amp_cart(dirs, lmax):
+    d = _f64(dirs)
+    out = np.zeros((len(d), (lmax + 1) * (lmax + 2) // 2))
+    lib().oracle_sh2amp_cart(_p(d), len(d), lmax, _p(out))
+    return out
+
+
+# ----------------------------------------------------------------- solvers
+
+def sigma_max(M):
+    M = _f64(M)
+    return lib().oracle_sigma_max(_p(M), M.shape[0], M.shape[1])
+
+
+def fista_fit(M, s, alpha, max_iter=1000, tol=1e-6, non_negative=False, warm=None):
+    M, s = _f64(M), _f64(s)
+    m, n = M.shape
+    c = np.zeros(n)
+    it, conv, res = C.c_int32(), C.c_int32(), C.c_double()
+    w = None if warm is None else _f64(warm)
+    lib().oracle_fista_fit(_p(M), m, n, _p(s), alpha, max_iter, tol, int(non_negative),
+                           None if w is None else _p(w), _p(c), C.addressof(it), C.addressof(conv),
+                           C.addressof(res))
+    return c, it.value, bool(conv.value), res.value
+
+
+def tikhonov_fit(M, s, n_diag, l_diag, lambda_n, lambda_l):
+    M, s, nd, ld = _f64(M), _f64(s), _f64(n_diag), _f64(l_diag)
+    m, n = M.shape
+    c = np.zeros(n)
+    res = C.c_double()
+    code = lib().oracle_tikhonov_fit(_p(M), m, n, _p(nd), _p(ld), lambda_n, lambda_l, _p(s), _p(c),
+                                     C.addressof(res))
+    if code != 0:
+        raise ValueError("normal-equations matrix should be PD")
+    return c, res.value
+
+
+def icls_solve(H, Cm, b, max_iter=200, tol=1e-10, epsilon=1e-10):
+    H, Cm, b = _f64(H), _f64(np.atleast_2d(Cm)), _f64(b)
+    m, n = H.shape
+    x = np.zeros(n)
+    it, act, conv, inf = (C.c_int32() for _ in range(4))
+    code = lib().oracle_icls_solve(_p(H), m, n, _p(Cm), Cm.shape[0], _p(b), max_iter, tol, epsilon, _p(x),
+                                   C.addressof(it), C.addressof(act), C.addressof(conv), C.addressof(inf))
+    if code != 0:
+        raise ValueError("H^T H + eps I must be positive definite")
+    return x, dict(iterations=it.value, final_active=act.value, converged=bool(conv.value),
+                   infeasible=bool(inf.value))
+
+
+def alpha_max(M, s):
+    M, s = _f64(M), _f64(s)
+    return lib().oracle_alpha_max(_p(M), M.shape[0], M.shape[1], _p(s))
+
+
+def log_path(amax, n, eps):
+    out = np.zeros(n)
+    if lib().oracle_log_path(amax, n, eps, _p(out)) != 0:
+        raise ValueError("log_path needs n >= 2, alpha_max > 0, 0 < eps < 1")
+    return out
+
+
+# ------------------------------------------------------------------ volume
+
+def shore_fit(data, bvals, bvecs, mask, *, n_threads: int = 0, big_delta=None, small_delta=None,
+              b0_threshold=50.0, bvec_frame="image-axis", return_coef64=True, **kw) -> dict:
+    """Whole-volume oracle fit with the keyword interface of shore_fit."""
+    from cs_dmri_b200 import _abi
+    from cs_dmri_b200._core import build_spec, sidecar
+
+    spec = build_spec(**kw)
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    g, keep = _gtab(bvals, bvecs, big_delta, small_delta, b0_threshold)
+    m8 = np.ascontiguousarray(np.asarray(mask).astype(bool)).view(np.uint8)
+    X, Y, Z = data.shape[:3]
+    K = n_coeffs(spec.radial_order) if spec.radial_order >= 0 else 0
+    coeffs = np.zeros((X, Y, Z, K), np.float32)
+    res = _abi.FitResult()
+    res.coefficients = coeffs.ctypes.data
+    diag = bool(kw.get("diagnostics", False))
+    maps = {}
+    if diag:
+        maps = {"r2": np.zeros((X, Y, Z), np.float32), "residual_l2": np.zeros((X, Y, Z), np.float32),
+                "iterations": np.zeros((X, Y, Z), np.uint32),
+                "regularization_kind": np.zeros((X, Y, Z), np.uint8)}
+        if kw.get("regularization", "l1") == "l1":
+            maps["alpha"] = np.zeros((X, Y, Z), np.float32)
+            maps["bic"] = np.zeros((X, Y, Z), np.float32)
+            if kw.get("alpha_mode", "l2-anchored") == "l2-anchored":
+                maps["rss_l2"] = np.zeros((X, Y, Z), np.float32)
+        for k, a in maps.items():
+            setattr(res, k, a.ctypes.data)
+    nmask = int(m8.sum())
+    c64 = np.zeros((nmask, max(K, 0)))
+    conv = np.zeros(nmask, np.uint8)
+    if return_coef64:
+        res.coef64 = c64.ctypes.data
+        res.converged = conv.ctypes.data
+    err = C.create_string_buffer(4096)
+    code = lib().oracle_shore_fit_volume(_p(data), _p(m8), X, Y, Z, C.addressof(g), C.addressof(spec),
+                                         C.addressof(res), int(n_threads), err, len(err))
+    if code != 0:
+        raise ValueError(err.value.decode())
+    kwf = dict(kw)
+    out = {"coefficients": coeffs,
+           "warnings": [w for w in res.warnings.decode().split("\n") if w],
+           "sidecar": sidecar(res, kwf, bvec_frame),
+           "alpha_distribution": tuple(res.alpha_distribution) if res.has_alpha_distribution else None,
+           "total_iterations": int(res.total_iterations), "n_voxels": int(res.n_voxels)}
+    if diag:
+        out["rmse"] = (maps["residual_l2"] / np.float32(math.sqrt(len(np.ravel(bvals))))).astype(np.float32)
+        out.update(maps)
+    if return_coef64:
+        out["coef64"] = c64
+        out["converged"] = conv.astype(bool)
+    return out
+
+
+def cpu_count() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)

@@ -1,0 +1,215 @@
+"""Parity of the CUDA library with the CPU oracle on identical seeded inputs.
+
+Tolerances.  The FP64 path runs the reference's iteration (fista.rs:121-194)
+in Gram form on FP64 tensor cores, so iterates differ from the oracle only by
+rounding; the stopping rule ||dx|| < tol ||x|| can then end a voxel's loop
+one iteration earlier or later, which moves its coefficients by about
+tol * ||x||.  Coefficient parity is therefore stated as relative L2 <= 1e-5
+per voxel (the bound the specification sets for the FP64 path), with
+iteration counts equal up to that one-step slack.  Tikhonov is a direct solve:
+its agreement is bounded by cond(A) * eps, so it is checked at 1e-8 for
+lambda = 0.05 and through the reference's normal-equation residual at the
+default lambda = 1e-8.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ph():
+    from cs_dmri_b200.phantom import make_phantom
+    p = make_phantom((8, 8, 4), seed=7)
+    p.data[0, 0, 0, :] = 0.0        # an all-zero voxel (alpha_max == 0 path)
+    return p
+
+
+def both(ph, oracle, mask=None, **kw):
+    from cs_dmri_b200 import shore_fit
+    mask = ph.mask if mask is None else mask
+    common = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, diagnostics=True)
+    common.update(kw)
+    gpu = shore_fit(ph.data, ph.bvals, ph.bvecs, mask, return_coef64=True, **common)
+    ref = oracle.shore_fit(ph.data, ph.bvals, ph.bvecs, mask, **common)
+    return gpu, ref
+
+
+def rel_rows(a, b):
+    return np.linalg.norm(a - b, axis=1) / np.maximum(np.linalg.norm(b, axis=1), 1e-300)
+
+
+def test_design_matrix_matches_oracle(ph, oracle):
+    from cs_dmri_b200 import design_matrix
+    for order in (2, 4, 6, 8):
+        g = design_matrix(ph.bvals, ph.bvecs, order, 700.0, big_delta=ph.big_delta, small_delta=ph.small_delta)
+        o = oracle.design_matrix(ph.bvals, ph.bvecs, order, 700.0, big_delta=ph.big_delta,
+                                 small_delta=ph.small_delta)
+        assert g.shape == o.shape
+        assert np.abs(g - o).max() <= 1e-13 * np.abs(o).max()
+
+
+def test_fixed_alpha_l1_parity(ph, oracle):
+    gpu, ref = both(ph, oracle, alpha_mode="fixed", alpha=0.01)
+    assert gpu["n_voxels"] == ref["n_voxels"] == ph.n_voxels
+    r = rel_rows(gpu["coef64"], ref["coef64"])
+    r = r[np.linalg.norm(ref["coef64"], axis=1) > 0]
+    assert r.max() <= 1e-5, r.max()
+    it_g = gpu["iterations"][ph.mask].astype(int)
+    it_o = ref["iterations"][ph.mask].astype(int)
+    assert np.abs(it_g - it_o).max() <= 1
+    assert np.mean(it_g == it_o) >= 0.9
+    assert np.array_equal(gpu["converged"], ref["converged"]) or np.mean(gpu["converged"] == ref["converged"]) > 0.99
+    np.testing.assert_allclose(gpu["residual_l2"], ref["residual_l2"], rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(gpu["r2"], ref["r2"], rtol=1e-5, atol=1e-6)
+    assert np.array_equal(gpu["alpha"], ref["alpha"])
+    np.testing.assert_allclose(gpu["bic"], ref["bic"], rtol=1e-5, atol=1e-3)
+    assert np.array_equal(gpu["regularization_kind"], ref["regularization_kind"])
+    # float32 coefficient volume is the rounded FP64 result, zeros outside the mask
+    np.testing.assert_allclose(gpu["coefficients"], ref["coefficients"], rtol=1e-4, atol=1e-3)
+    assert gpu["sidecar"] == ref["sidecar"]
+
+
+@pytest.mark.parametrize("lam", [0.05])
+def test_tikhonov_parity(ph, oracle, lam):
+    gpu, ref = both(ph, oracle, regularization="l2", lambda_n=lam, lambda_l=lam)
+    r = rel_rows(gpu["coef64"], ref["coef64"])
+    r = r[np.linalg.norm(ref["coef64"], axis=1) > 0]
+    assert r.max() <= 1e-8, r.max()
+    assert np.all(gpu["iterations"][ph.mask] == 1) and np.all(gpu["regularization_kind"][ph.mask] == 2)
+    np.testing.assert_allclose(gpu["residual_l2"], ref["residual_l2"], rtol=1e-7)
+    assert gpu["sidecar"] == ref["sidecar"]
+
+
+def test_tikhonov_default_lambda_normal_equations(ph, oracle):
+    """src/solver/tikhonov.rs at lambda = 1e-8: normal-equation residual, as
+    tests/optimization_kkt.rs:189-215 checks it (< 1e-9)."""
+    gpu, _ = both(ph, oracle, regularization="l2")
+    M = oracle.design_matrix(ph.bvals, ph.bvecs, 6, 700.0, big_delta=ph.big_delta, small_delta=ph.small_delta)
+    nd, ld = oracle.regularization(6)
+    S = ph.data.reshape(-1, ph.data.shape[-1])[ph.mask.ravel()].astype(np.float64)
+    for c, s in zip(gpu["coef64"][1:], S[1:]):
+        lhs = M.T @ M @ c + 1e-8 * nd * c + 1e-8 * ld * c
+        rhs = M.T @ s
+        assert np.linalg.norm(lhs - rhs) / np.linalg.norm(rhs) < 1e-9
+
+
+def test_alpha_ratio_parity(ph, oracle):
+    gpu, ref = both(ph, oracle, alpha_mode="alpha-ratio", alpha_ratio=0.05)
+    r = rel_rows(gpu["coef64"], ref["coef64"])
+    nz = np.linalg.norm(ref["coef64"], axis=1) > 0
+    assert r[nz].max() <= 1e-5
+    np.testing.assert_allclose(gpu["alpha"], ref["alpha"], rtol=1e-12)
+    assert gpu["alpha"][0, 0, 0] == 0.0 and gpu["iterations"][0, 0, 0] == 0
+    assert gpu["bic"][0, 0, 0] == 0.0 and np.all(gpu["coefficients"][0, 0, 0] == 0)
+    assert gpu["alpha_distribution"] == pytest.approx(ref["alpha_distribution"], rel=1e-12)
+
+
+@pytest.mark.parametrize("mode", ["path-bic", "l2-anchored"])
+def test_path_strategy_parity(ph, oracle, mode):
+    gpu, ref = both(ph, oracle, alpha_mode=mode)
+    same = np.isclose(gpu["alpha"][ph.mask], ref["alpha"][ph.mask], rtol=1e-9, atol=0)
+    assert same.mean() >= 0.98, same.mean()
+    r = rel_rows(gpu["coef64"], ref["coef64"])
+    nz = np.linalg.norm(ref["coef64"], axis=1) > 0
+    assert r[same & nz].max() <= 1e-5
+    assert gpu["alpha"][0, 0, 0] == 0.0 and gpu["iterations"][0, 0, 0] == 0
+    if mode == "l2-anchored":
+        np.testing.assert_allclose(gpu["rss_l2"], ref["rss_l2"], rtol=1e-6)
+    assert gpu["alpha_distribution"] == pytest.approx(ref["alpha_distribution"], rel=1e-9)
+    assert gpu["sidecar"]["solver"]["alpha_strategy"] == ref["sidecar"]["solver"]["alpha_strategy"]
+
+
+def test_empty_mask(ph, oracle):
+    gpu, ref = both(ph, oracle, mask=np.zeros(ph.mask.shape, bool), alpha_mode="fixed", alpha=0.01)
+    assert gpu["n_voxels"] == 0 and np.all(gpu["coefficients"] == 0)
+
+
+def test_partial_mask_zeros_outside(ph, oracle):
+    m = np.zeros(ph.mask.shape, bool)
+    m[2:5, 1:7, 1:3] = True
+    gpu, ref = both(ph, oracle, mask=m, alpha_mode="fixed", alpha=0.01)
+    assert np.all(gpu["coefficients"][~m] == 0) and np.all(gpu["r2"][~m] == 0)
+    assert rel_rows(gpu["coef64"], ref["coef64"]).max() <= 1e-5
+
+
+def test_nan_voxel_matches_reference_semantics(ph, oracle):
+    """A NaN sample makes every soft-threshold comparison false, so the
+    reference's prox falls through to 0.0 (src/solver/fista.rs:151-157): the
+    voxel converges to zero coefficients at iteration 1.  Other voxels are
+    unaffected."""
+    data = ph.data.copy()
+    data[1, 1, 1, 5] = np.nan
+    from cs_dmri_b200 import shore_fit
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, alpha_mode="fixed", alpha=0.01,
+              diagnostics=True, max_iter=50)
+    out = shore_fit(data, ph.bvals, ph.bvecs, ph.mask, **kw)
+    ref = oracle.shore_fit(data, ph.bvals, ph.bvecs, ph.mask, **kw)
+    bad = np.zeros(ph.mask.shape, bool)
+    bad[1, 1, 1] = True
+    assert np.all(np.isfinite(out["coefficients"][~bad]))
+    assert out["iterations"][1, 1, 1] == ref["iterations"][1, 1, 1] == 1
+    assert np.all(out["coefficients"][1, 1, 1] == 0) and np.all(ref["coefficients"][1, 1, 1] == 0)
+    np.testing.assert_array_equal(np.isnan(out["residual_l2"]), np.isnan(ref["residual_l2"]))
+
+
+def test_max_iter_zero_returns_start(ph, oracle):
+    from cs_dmri_b200 import shore_fit
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, alpha_mode="fixed", alpha=0.01,
+              diagnostics=True, max_iter=0)
+    out = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, return_coef64=True, **kw)
+    ref = oracle.shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, **kw)
+    assert np.all(out["coef64"] == 0) and np.all(ref["coef64"] == 0)
+    assert np.all(out["iterations"] == 0) and not out["converged"].any() and not ref["converged"].any()
+
+
+def test_single_shell_refused_and_allowed(oracle):
+    from cs_dmri_b200 import shore_fit
+    z = np.linspace(-1, 1, 40)
+    r = np.sqrt(1 - z * z)
+    phi = 2.399963 * np.arange(40)
+    bvecs = np.vstack([[0, 0, 1], [0, 0, 1], np.stack([r * np.cos(phi), r * np.sin(phi), z], 1)])
+    bvals = np.concatenate([[0, 0], np.full(40, 1000.0)])
+    data = np.broadcast_to(np.exp(-bvals * 8e-4).astype(np.float32), (2, 2, 1, 42)).copy()
+    mask = np.ones((2, 2, 1), bool)
+    with pytest.raises(ValueError, match="at least 2 b-value shells"):
+        shore_fit(data, bvals, bvecs, mask, big_delta=0.04, small_delta=0.01, regularization="l2")
+    out = shore_fit(data, bvals, bvecs, mask, big_delta=0.04, small_delta=0.01, regularization="l2",
+                    allow_single_shell=True)
+    assert any("only the orientation information" in w for w in out["warnings"])
+    with pytest.raises(ValueError, match="b=0 threshold"):
+        shore_fit(data, np.zeros(42), bvecs, mask, regularization="l2", allow_single_shell=True)
+
+
+def test_argument_errors(ph):
+    from cs_dmri_b200 import shore_fit
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta)
+    with pytest.raises(ValueError, match="positive even"):
+        shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, radial_order=5, **kw)
+    with pytest.raises(ValueError, match="path-n-alphas"):
+        shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, path_n_alphas=1, **kw)
+    with pytest.raises(ValueError, match="path-eps"):
+        shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, path_eps=2.0, **kw)
+    with pytest.raises(ValueError, match="alpha-ratio"):
+        shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, alpha_mode="alpha-ratio", alpha_ratio=1.5, **kw)
+    with pytest.raises(ValueError, match="slack"):
+        shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, slack=-1.0, **kw)
+    with pytest.raises(ValueError, match="volumes"):
+        shore_fit(ph.data[..., :-1], ph.bvals, ph.bvecs, ph.mask, **kw)
+
+
+def test_shore_model_interface(ph, oracle):
+    from cs_dmri_b200 import GradientTable, ShoreModel
+    gt = GradientTable(ph.bvals, ph.bvecs, big_delta=ph.big_delta, small_delta=ph.small_delta)
+    fit = ShoreModel(gt, regularization="l2", lambda_n=0.05, lambda_l=0.05).fit(ph.data, ph.mask)
+    ref = oracle.shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, big_delta=ph.big_delta,
+                           small_delta=ph.small_delta, regularization="l2", lambda_n=0.05, lambda_l=0.05,
+                           diagnostics=True)
+    assert fit.coefficients.shape == ph.data.shape[:3] + (72,)
+    assert fit.frame == "image" and fit.r2 is not None
+    np.testing.assert_allclose(fit.r2, ref["r2"], rtol=1e-6, atol=1e-7)
+    np.testing.assert_allclose(fit.rmse, ref["rmse"], rtol=1e-6)
+    assert fit.sidecar["solver"]["kind"] == "tikhonov" and not fit.single_shell
+    sp = fit.sparsity[ph.mask]
+    assert sp[0] == 0.0 and sp[1:].min() > 0.9 and "256 voxels" in repr(fit)
