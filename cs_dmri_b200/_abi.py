@@ -109,6 +109,7 @@ EXPORTS = (
     "csd_shore_fit_volume_device",
     "csd_shore_design_matrix",
     "csd_last_timing",
+    "csd_shore_fista_batch_noalloc",
 )
 
 _lib = None
@@ -139,6 +140,9 @@ def _declare(lib: C.CDLL) -> C.CDLL:
                                             C.c_void_p, C.c_char_p, C.c_size_t]
     lib.csd_last_timing.restype = C.c_int
     lib.csd_last_timing.argtypes = [C.c_void_p, C.POINTER(Timing)]
+    lib.csd_shore_fista_batch_noalloc.restype = C.c_int
+    lib.csd_shore_fista_batch_noalloc.argtypes = [C.POINTER(Gtab), C.POINTER(Spec), C.c_void_p, C.c_int64,
+                                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]
     return lib
 
 

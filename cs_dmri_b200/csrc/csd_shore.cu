@@ -24,6 +24,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1024,3 +1025,235 @@ int csd_last_timing(const csd_handle* h, csd_fit_timing* out) {
 }
 
 }  // extern "C"
+
+// ======================================================================
+// Allocation-free batch fit
+// ======================================================================
+//
+// Some callers cannot let a library call cudaMalloc: applications that hand
+// all device memory to their own pool allocator up front (a framework's
+// caching allocator, an inference server with a fixed memory budget), and
+// latency-critical pipelines for which cudaMalloc / cudaFree are unacceptable
+// because cudaFree synchronises the whole device and either may fail once
+// the pool owns the memory.  csd_shore_fista_batch_noalloc serves them: it
+// runs the fixed-alpha FISTA fit of a batch of voxels with every piece of
+// scratch (design matrix, Gram tiles, right-hand sides, iterates, work
+// queue) placed in one statically sized device array that the library
+// reserves when it is loaded.  The caller still provides the inputs and
+// outputs in device memory.
+//
+// Limits: at most kNoAllocMaxVoxels voxels and kNoAllocMaxMeasurements
+// measurements per call, radial order <= 6 (K <= 72).  The array is about
+// 10.3 MB and every GPU that loads the library holds it until the process
+// exits.  All calls share it and it keeps the last call's contents: each
+// call rebuilds what it reads and clears the work-queue counter, but two
+// calls that overlap on the GPU (different streams or threads) race on it.
+
+namespace {
+
+constexpr int64_t kNoAllocMaxVoxels = 8192;
+constexpr int kNoAllocMaxMeasurements = 1024;
+constexpr int kNoAllocMaxKp = 72;
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+constexpr size_t kNaBvals = 0;
+constexpr size_t kNaBvecs = align256(kNaBvals + sizeof(double) * kNoAllocMaxMeasurements);
+constexpr size_t kNaM = align256(kNaBvecs + sizeof(double) * 3 * kNoAllocMaxMeasurements);
+constexpr size_t kNaG = align256(kNaM + sizeof(double) * kNoAllocMaxMeasurements * kNoAllocMaxKp);
+constexpr size_t kNaGfrag = align256(kNaG + sizeof(double) * kNoAllocMaxKp * kNoAllocMaxKp);
+constexpr size_t kNaScal = align256(kNaGfrag + sizeof(double) * kNoAllocMaxKp * kNoAllocMaxKp);
+constexpr size_t kNaVox = align256(kNaScal + sizeof(double) * 4);
+constexpr size_t kNaB = align256(kNaVox + sizeof(int64_t) * kNoAllocMaxVoxels);
+constexpr size_t kNaX = align256(kNaB + sizeof(double) * kNoAllocMaxVoxels * kNoAllocMaxKp);
+constexpr size_t kNaIters = align256(kNaX + sizeof(double) * kNoAllocMaxVoxels * kNoAllocMaxKp);
+constexpr size_t kNaConv = align256(kNaIters + sizeof(uint32_t) * kNoAllocMaxVoxels);
+constexpr size_t kNaQueue = align256(kNaConv + kNoAllocMaxVoxels);
+constexpr size_t kNoAllocBytes = align256(kNaQueue + sizeof(unsigned long long));
+
+__global__ void k_noalloc_iota(int64_t* vox, int64_t V) {
+  const int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v < V) vox[v] = v;
+}
+
+__global__ void k_noalloc_to_f32(const double* X, int64_t V, int K, int Kp, float* out) {
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= V * K) return;
+  out[e] = static_cast<float>(X[(e / K) * Kp + (e % K)]);
+}
+
+}  // namespace
+
+// The scratch of csd_shore_fista_batch_noalloc.  Host code must not use this
+// name as an address: its device address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_addr[256] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device (with that device current) and cached.
+unsigned char* noalloc_scratch(int device) {
+  if (device < 0 || device >= 256) throw Error{CSD_ERR_INVALID, "device index out of range"};
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      throw Error{CSD_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e)};
+    g_noalloc_addr[device] = static_cast<unsigned char*>(p);
+  }
+  return g_noalloc_addr[device];
+}
+
+template <int MT>
+void noalloc_fista(const csd::FistaParams& p, int num_sms, cudaStream_t st) {
+  constexpr int KP = 8 * MT, KT = 2 * MT;
+  const size_t smem = sizeof(double) * (static_cast<size_t>(MT) * KT * 32 + 8 * KP * 8);
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_fista_fp64<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  int per_sm = 0;
+  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_fista_fp64<MT>, 256, smem));
+  per_sm = std::max(per_sm, 1);
+  const int64_t warps_needed = (p.n_work + 7) / 8;
+  int64_t blocks = std::min<int64_t>(static_cast<int64_t>(num_sms) * per_sm, (warps_needed + 7) / 8);
+  blocks = std::max<int64_t>(blocks, 1);
+  csd::k_fista_fp64<MT><<<static_cast<unsigned>(blocks), 256, smem, st>>>(p);
+  CSD_CUDA(cudaGetLastError());
+}
+
+template <int KP>
+void noalloc_rhs(const float* d, const int64_t* vox, int64_t V, int N, const double* M, int K, double* B,
+                 cudaStream_t st) {
+  const size_t smem = sizeof(double) * (32 * KP + 64 * 33);
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_rhs<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  csd::k_rhs<KP><<<static_cast<unsigned>((V + 63) / 64), 256, smem, st>>>(d, vox, V, N, M, K, B);
+  CSD_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+extern "C" int csd_shore_fista_batch_noalloc(const csd_gtab* gtab, const csd_shore_spec* spec,
+                                             const float* d_signals, int64_t n_voxels, float* d_coeffs,
+                                             uint32_t* d_iterations, void* stream, char* err,
+                                             size_t err_len) {
+  if (!gtab || !spec || !gtab->bvals || !gtab->bvecs || gtab->n <= 0 || n_voxels < 0 ||
+      (n_voxels > 0 && (!d_signals || !d_coeffs))) {
+    set_err(err, err_len, "invalid argument: null pointer or bad size");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    if (spec->regularization != CSD_REG_L1 || spec->alpha_mode != CSD_ALPHA_FIXED)
+      throw Error{CSD_ERR_INVALID, "the allocation-free batch fit supports L1 with a fixed alpha only"};
+    if (spec->radial_order > 6)
+      throw Error{CSD_ERR_INVALID, "the allocation-free batch fit supports radial order <= 6 (K <= 72), got " +
+                                       std::to_string(spec->radial_order)};
+    if (gtab->n > kNoAllocMaxMeasurements)
+      throw Error{CSD_ERR_INVALID, "the allocation-free batch fit takes at most " +
+                                       std::to_string(kNoAllocMaxMeasurements) + " measurements, got " +
+                                       std::to_string(gtab->n)};
+    if (n_voxels > kNoAllocMaxVoxels)
+      throw Error{CSD_ERR_INVALID, "the allocation-free batch fit takes at most " +
+                                       std::to_string(kNoAllocMaxVoxels) + " voxels per call, got " +
+                                       std::to_string(n_voxels)};
+    HostGtab g = make_gtab(gtab);
+    std::string warnings;
+    validate(spec, g, warnings);
+    int device = 0;
+    CSD_CUDA(cudaGetDevice(&device));
+    int num_sms = 0;
+    CSD_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+    unsigned char* s = noalloc_scratch(device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int N = g.bvals.empty() ? 0 : static_cast<int>(g.bvals.size());
+    const int K = n_coeffs(spec->radial_order);
+    const int Kp = 8 * mt_for(K);
+    const int MT = Kp / 8, KT = Kp / 4;
+    double* bvals = reinterpret_cast<double*>(s + kNaBvals);
+    double* bvecs = reinterpret_cast<double*>(s + kNaBvecs);
+    double* M = reinterpret_cast<double*>(s + kNaM);
+    double* G = reinterpret_cast<double*>(s + kNaG);
+    double* gfrag = reinterpret_cast<double*>(s + kNaGfrag);
+    double* scal = reinterpret_cast<double*>(s + kNaScal);
+    int64_t* vox = reinterpret_cast<int64_t*>(s + kNaVox);
+    double* B = reinterpret_cast<double*>(s + kNaB);
+    double* X = reinterpret_cast<double*>(s + kNaX);
+    uint32_t* iters = reinterpret_cast<uint32_t*>(s + kNaIters);
+    uint8_t* conv = reinterpret_cast<uint8_t*>(s + kNaConv);
+    unsigned long long* queue = reinterpret_cast<unsigned long long*>(s + kNaQueue);
+
+    // Setup of this gradient table (rebuilt on every call).
+    CSD_CUDA(cudaMemcpyAsync(bvals, g.bvals.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st));
+    CSD_CUDA(cudaMemcpyAsync(bvecs, g.bvecs.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+    const double qdenom = 4.0 * kPi * kPi * g.tau;
+    const long long nk = static_cast<long long>(N) * K;
+    csd::k_design<<<static_cast<unsigned>((nk + 255) / 256), 256, 0, st>>>(bvals, bvecs, N, K, spec->radial_order,
+                                                                           spec->zeta, qdenom, g.b0, M);
+    CSD_CUDA(cudaGetLastError());
+    csd::k_gram<<<(Kp * Kp + 255) / 256, 256, 0, st>>>(M, N, K, Kp, spec->radial_order, 0.0, 0.0, G, nullptr);
+    CSD_CUDA(cudaGetLastError());
+    const size_t lsm = sizeof(double) * (static_cast<size_t>(Kp) * Kp + 2 * Kp);
+    CSD_CUDA(cudaFuncSetAttribute(csd::k_lipschitz, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(lsm)));
+    csd::k_lipschitz<<<1, 256, lsm, st>>>(G, Kp, N, 200000, scal, scal + 1);
+    CSD_CUDA(cudaGetLastError());
+    csd::k_pack_gfrag<<<(MT * KT * 32 + 255) / 256, 256, 0, st>>>(G, Kp, gfrag);
+    CSD_CUDA(cudaGetLastError());
+    double lipschitz = 0.0;
+    CSD_CUDA(cudaMemcpyAsync(&lipschitz, scal, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CSD_CUDA(cudaStreamSynchronize(st));
+    if (n_voxels == 0) return CSD_OK;
+
+    // b = M^T s, then the FISTA iterations (the same kernels as the volume fit).
+    k_noalloc_iota<<<grid1(n_voxels), 256, 0, st>>>(vox, n_voxels);
+    CSD_CUDA(cudaGetLastError());
+    switch (Kp) {
+      case 8: noalloc_rhs<8>(d_signals, vox, n_voxels, N, M, K, B, st); break;
+      case 32: noalloc_rhs<32>(d_signals, vox, n_voxels, N, M, K, B, st); break;
+      case 72: noalloc_rhs<72>(d_signals, vox, n_voxels, N, M, K, B, st); break;
+      default: throw Error{CSD_ERR_INVALID, "unsupported coefficient count"};
+    }
+    CSD_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st));
+    csd::FistaParams fp{};
+    fp.gfrag = gfrag;
+    fp.B = B;
+    fp.X = X;
+    fp.warm = nullptr;
+    fp.iters = iters;
+    fp.conv = conv;
+    fp.V = n_voxels;
+    fp.n_inv = 1.0 / static_cast<double>(N);
+    fp.step = 1.0 / lipschitz;
+    fp.thr = fp.step * spec->alpha;
+    fp.alpha_v = nullptr;
+    fp.tol = spec->tol;
+    fp.max_iter = spec->max_iter;
+    fp.non_negative = spec->non_negative;
+    fp.queue = queue;
+    fp.list = nullptr;
+    fp.n_work = n_voxels;
+    fp.iter_total = nullptr;
+    if (spec->max_iter <= 0) {
+      csd::k_fista_noop<<<grid1(n_voxels * (Kp + 1)), 256, 0, st>>>(fp, Kp);
+      CSD_CUDA(cudaGetLastError());
+    } else {
+      switch (MT) {
+        case 1: noalloc_fista<1>(fp, num_sms, st); break;
+        case 4: noalloc_fista<4>(fp, num_sms, st); break;
+        case 9: noalloc_fista<9>(fp, num_sms, st); break;
+        default: throw Error{CSD_ERR_INVALID, "unsupported coefficient count"};
+      }
+    }
+    k_noalloc_to_f32<<<grid1(n_voxels * K), 256, 0, st>>>(X, n_voxels, K, Kp, d_coeffs);
+    CSD_CUDA(cudaGetLastError());
+    if (d_iterations)
+      CSD_CUDA(cudaMemcpyAsync(d_iterations, iters, sizeof(uint32_t) * n_voxels, cudaMemcpyDeviceToDevice, st));
+    CSD_CUDA(cudaStreamSynchronize(st));
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}

@@ -214,6 +214,33 @@ typedef struct csd_fit_timing {
 
 int csd_last_timing(const csd_handle* h, csd_fit_timing* out);
 
+/* Allocation-free fixed-alpha FISTA fit of a batch of voxels.
+ *
+ * No counterpart in the reference: it exists for callers that cannot let a
+ * library call cudaMalloc - applications whose device memory is owned by
+ * their own pool allocator (a framework's caching allocator, a server with a
+ * fixed memory budget) and latency-critical pipelines that cannot afford the
+ * device-wide synchronisation of cudaFree or an allocation failure mid-run.
+ * It allocates nothing: all scratch lives in one static device array of about
+ * 10.3 MB that the library reserves on every GPU that loads it, until exit.
+ *
+ * Inputs and outputs are caller-owned DEVICE memory on the current device:
+ * `d_signals` float32 (n_voxels, N) row-major, `d_coeffs` float32
+ * (n_voxels, K), `d_iterations` uint32 (n_voxels) or NULL.  `spec` must ask
+ * for L1 with a fixed alpha; the result is the same as csd_shore_fit_volume's
+ * for those voxels.  Limits: n_voxels <= 8192, N <= 1024, radial order <= 6;
+ * larger requests return CSD_ERR_INVALID with a message.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.  All
+ * calls share the one array and it keeps the last call's contents (each call
+ * rebuilds what it reads and zeroes its work counter): calls that overlap on
+ * the GPU race.  Work is queued on `stream` (a cudaStream_t, NULL = the
+ * legacy default stream) and the call returns after that stream finishes. */
+int csd_shore_fista_batch_noalloc(const csd_gtab* gtab, const csd_shore_spec* spec,
+                                  const float* d_signals, int64_t n_voxels, float* d_coeffs,
+                                  uint32_t* d_iterations, void* stream, char* err,
+                                  size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif
