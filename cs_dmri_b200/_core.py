@@ -151,12 +151,17 @@ def shore_fit(data, bvals, bvecs, mask, *, big_delta=None, small_delta=None, b0_
               alpha_mode="l2-anchored", alpha=1.0, alpha_ratio=1e-3, path_n_alphas=20, path_eps=None,
               slack=0.05, max_iter=1000, tol=1e-6, non_negative=False, lambda_n=1e-8, lambda_l=1e-8,
               nonneg_max_iter=200, nonneg_tol=1e-9, nonneg_epsilon=1e-10, diagnostics=False,
-              allow_single_shell=False, n_threads=None, device: int = 0, return_coef64: bool = False) -> dict:
+              allow_single_shell=False, n_threads=None, device: int = 0, return_coef64: bool = False,
+              coefficients_out=None) -> dict:
     """SHORE fit of every masked voxel on the GPU (``_cs_dmri.shore_fit``).
 
     ``n_threads`` is accepted for signature compatibility and ignored: the fit
     runs on CUDA device ``device``.  ``return_coef64=True`` adds ``coef64``
     (V, K) float64 and ``converged`` (V,) for the masked voxels in x-y-z order.
+    ``coefficients_out`` may supply the (X, Y, Z, K) float32 C-contiguous output
+    array (for example in page-locked memory, which makes the copy back
+    faster); every element is overwritten.  A page-locked ``data`` volume is
+    read in place, masked voxels only.
     """
     if bvec_frame not in ("image-axis", "world-ras"):
         raise ValueError(f"bvec_frame must be 'image-axis' or 'world-ras', got {bvec_frame!r}")
@@ -179,7 +184,13 @@ def shore_fit(data, bvals, bvecs, mask, *, big_delta=None, small_delta=None, b0_
     m8 = np.ascontiguousarray(m.astype(bool).view(np.uint8) if m.dtype == bool else (m != 0).astype(np.uint8))
     X, Y, Z = data.shape[:3]
     K = _abi.load().csd_shore_n_coeffs(int(radial_order))
-    coeffs = np.zeros((X, Y, Z, max(K, 0)), dtype=np.float32)
+    if coefficients_out is not None:
+        coeffs = coefficients_out
+        if (coeffs.shape != (X, Y, Z, K) or coeffs.dtype != np.float32 or not coeffs.flags.c_contiguous
+                or not coeffs.flags.writeable):
+            raise ValueError(f"coefficients_out must be a writable C-contiguous float32 array of shape {(X, Y, Z, K)}")
+    else:
+        coeffs = np.empty((X, Y, Z, max(K, 0)), dtype=np.float32)  # every element is written
     res = _abi.FitResult()
     res.coefficients = coeffs.ctypes.data
     maps = {}

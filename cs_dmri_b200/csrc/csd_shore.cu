@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -182,11 +183,24 @@ struct csd_handle {
   uint64_t chol_key = 0;
   int N = 0, K = 0, Kp = 0;
   double lipschitz = 0.0, lambda_max = 0.0;
-  DevBuf bvals, bvecs, M, Mt, G, A, gfrag, scal, ok;
+  DevBuf bvals, bvecs, M, Mt, G, A, gfrag, mfrag, mtfrag, scal, ok;
+  int Np = 0;               // N padded to a multiple of 8
+  bool dmma_rhs = false;    // M^T tiles fit in shared memory
+  bool dmma_resid = false;  // M tiles fit in shared memory
+  int smem_optin = 0;
+  bool dmma_rhs_possible(int n, int k) const {
+    const int kp = 8 * ((k + 7) / 8);
+    const int np = 8 * ((n + 7) / 8);
+    const size_t bytes = sizeof(double) * static_cast<size_t>(np) * kp + sizeof(float) * 8 * 8 * (np + 4);
+    return (kp == 8 || kp == 32 || kp == 72) && bytes <= static_cast<size_t>(smem_optin);
+  }
+  DevBuf mom;      // Nesterov momentum table (t_k - 1) / t_{k+1}
+  int mom_len = 0;
 
   // per-fit buffers
   DevBuf data, mask, coeffs, r2, resid, iters_map, kind_map, alpha_map, bic_map, rss_map;
-  DevBuf blk, total, vox, B, X, iters, conv, queue, itotal, resid_v, nnz_v;
+  DevBuf blk, total, vox, B, X, iters, conv, queue, itotal, resid_v, sst_v, nnz_v, sig;
+  const float* sig_compact = nullptr;  // compact masked signals of the current fit, if any
   DevBuf amax, zero, alpha_v, Xsel, Xfb, Xl2, rss_l2, list, active, pbest, psel, pact, palpha_sel,
       pit_sel, pconv_sel, palpha_fb, pit_fb, pconv_fb, pcode;
 };
@@ -246,9 +260,29 @@ void ensure_setup(csd_handle* h, const HostGtab& g, int radial_order, double zet
     csd::k_pack_gfrag<<<(MT * KT * 32 + 255) / 256, 256, 0, st>>>(h->G.as<double>(), Kp,
                                                                    h->gfrag.as<double>());
     CSD_LAUNCH();
+
     csd::k_transpose_design<<<(Kp * N + 255) / 256, 256, 0, st>>>(h->M.as<double>(), N, K, Kp,
                                                                   h->Mt.as<double>());
     CSD_LAUNCH();
+    // DMMA operand tiles of M (residual pass) and M^T (right-hand sides),
+    // used when they fit in one CTA's shared memory next to the warp buffers.
+    const int Np = 8 * ((N + 7) / 8);
+    h->Np = Np;
+    const size_t resid_smem = sizeof(double) * (static_cast<size_t>(Np) * Kp + 8 * static_cast<size_t>(Kp) * 8);
+    const size_t rhs_smem = sizeof(double) * static_cast<size_t>(Np) * Kp + sizeof(float) * 8 * 8 * (Np + 4);
+    const bool small_k = (Kp == 8 || Kp == 32 || Kp == 72);
+    h->dmma_resid = small_k && resid_smem <= static_cast<size_t>(h->smem_optin);
+    h->dmma_rhs = small_k && rhs_smem <= static_cast<size_t>(h->smem_optin);
+    if (h->dmma_resid || h->dmma_rhs) {
+      h->mfrag.ensure(sizeof(double) * static_cast<size_t>(Np) * Kp);
+      h->mtfrag.ensure(sizeof(double) * static_cast<size_t>(Np) * Kp);
+      csd::k_pack_afrag<<<(Np * Kp + 255) / 256, 256, 0, st>>>(h->M.as<double>(), N, K, K, 0, Np, Kp,
+                                                              h->mfrag.as<double>());
+      CSD_LAUNCH();
+      csd::k_pack_afrag<<<(Np * Kp + 255) / 256, 256, 0, st>>>(h->M.as<double>(), N, K, K, 1, Kp, Np,
+                                                              h->mtfrag.as<double>());
+      CSD_LAUNCH();
+    }
     double sc2[2];
     CSD_CUDA(cudaMemcpyAsync(sc2, h->scal.p, sizeof sc2, cudaMemcpyDeviceToHost, st));
     CSD_CUDA(cudaStreamSynchronize(st));
@@ -303,6 +337,28 @@ int64_t compact(csd_handle* h, const uint8_t* d_flags, int64_t n, DevBuf& out) {
 
 inline unsigned grid1(int64_t n, int bs = 256) { return static_cast<unsigned>((n + bs - 1) / bs); }
 
+// Momentum of FISTA iteration k, (t_k - 1) / t_{k+1} with t_0 = 1 and
+// t_{k+1} = (1 + sqrt(1 + 4 t_k^2)) / 2 (src/solver/fista.rs:161-163).  It
+// depends on k only; the table is built once per max_iter with the same IEEE
+// operations the reference performs inside its loop.
+void ensure_mom(csd_handle* h, int max_iter) {
+  if (max_iter <= 0 || (h->mom_len >= max_iter && h->mom.p)) return;
+  std::vector<double> m(static_cast<size_t>(max_iter));
+  volatile double t = 1.0;
+  for (int k = 0; k < max_iter; ++k) {
+    const double tk = t;
+    const double four_tt = 4.0 * tk * tk;
+    const double root = std::sqrt(1.0 + four_tt);
+    const double tn = 0.5 * (1.0 + root);
+    m[k] = (tk - 1.0) / tn;
+    t = tn;
+  }
+  h->mom.ensure(sizeof(double) * m.size());
+  CSD_CUDA(cudaMemcpyAsync(h->mom.p, m.data(), sizeof(double) * m.size(), cudaMemcpyHostToDevice, h->stream));
+  CSD_CUDA(cudaStreamSynchronize(h->stream));
+  h->mom_len = max_iter;
+}
+
 template <int MT>
 void launch_fista_t(csd_handle* h, const csd::FistaParams& p) {
   constexpr int KP = 8 * MT, KT = 2 * MT;
@@ -319,6 +375,34 @@ void launch_fista_t(csd_handle* h, const csd::FistaParams& p) {
   CSD_LAUNCH();
 }
 
+template <int MT, int WARPS>
+void launch_fista_v3_t(csd_handle* h, const csd::FistaParams& p) {
+  constexpr int KP = 8 * MT;
+  const size_t smem = sizeof(double) * (2 * static_cast<size_t>(MT) * MT * 32 + WARPS * 2 * KP * 8);  // Gram tiles + y, b
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_fista_v3<MT, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  int per_sm = 0;
+  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_fista_v3<MT, WARPS>, 32 * WARPS, smem));
+  per_sm = std::max(per_sm, 1);
+  const int64_t warps_needed = (p.n_work + 7) / 8;
+  int64_t blocks = std::min<int64_t>(static_cast<int64_t>(h->num_sms) * per_sm, (warps_needed + WARPS - 1) / WARPS);
+  blocks = std::max<int64_t>(blocks, 1);
+  csd::FistaParams q = p;
+  q.gfrag = h->gfrag.as<double>();
+  q.mom = h->mom.as<double>();
+  csd::k_fista_v3<MT, WARPS><<<static_cast<unsigned>(blocks), 32 * WARPS, smem, h->stream>>>(q);
+  CSD_LAUNCH();
+}
+
+// FISTA kernel variant: 0 = k_fista_fp64 (registers hold x, y, b); 3 / 4 =
+// k_fista_v3 with 12 / 16 warps per CTA.  CSD_FISTA_VARIANT overrides the
+// default.
+int fista_variant() {
+  const char* e = std::getenv("CSD_FISTA_VARIANT");
+  if (e && *e) return std::atoi(e);
+  return 4;
+}
+
 void launch_fista(csd_handle* h, int MT, const csd::FistaParams& p) {
   if (p.max_iter <= 0) {
     // An empty iteration loop: the warm start (or zero) is the result, with
@@ -326,6 +410,18 @@ void launch_fista(csd_handle* h, int MT, const csd::FistaParams& p) {
     csd::k_fista_noop<<<grid1(p.n_work * (h->Kp + 1)), 256, 0, h->stream>>>(p, h->Kp);
     CSD_LAUNCH();
     return;
+  }
+  const int variant = fista_variant();
+  if (variant == 3 || variant == 4) {
+    switch (MT * 8 + variant) {
+      case 1 * 8 + 3: launch_fista_v3_t<1, 12>(h, p); return;
+      case 1 * 8 + 4: launch_fista_v3_t<1, 16>(h, p); return;
+      case 4 * 8 + 3: launch_fista_v3_t<4, 12>(h, p); return;
+      case 4 * 8 + 4: launch_fista_v3_t<4, 16>(h, p); return;
+      case 9 * 8 + 3: launch_fista_v3_t<9, 12>(h, p); return;
+      case 9 * 8 + 4: launch_fista_v3_t<9, 16>(h, p); return;
+      default: break;
+    }
   }
   switch (MT) {
     case 1: launch_fista_t<1>(h, p); break;
@@ -347,7 +443,27 @@ void launch_rhs_t(csd_handle* h, const float* d_data, int64_t V) {
   CSD_LAUNCH();
 }
 
-void launch_rhs(csd_handle* h, const float* d_data, int64_t V) {
+template <int KP>
+void launch_rhs_dmma_t(csd_handle* h, const float* d_data, int64_t V, float* sig_out) {
+  const size_t smem = sizeof(double) * static_cast<size_t>(h->Np) * KP + sizeof(float) * 8 * 8 * (h->Np + 4);
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_rhs_dmma<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  const int64_t groups = (V + 7) / 8;
+  const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(h->num_sms, (groups + 7) / 8)));
+  csd::k_rhs_dmma<KP><<<blocks, 256, smem, h->stream>>>(d_data, h->vox.as<int64_t>(), V, h->N, h->Np,
+                                                        h->mtfrag.as<double>(), h->B.as<double>(), sig_out);
+  CSD_LAUNCH();
+}
+
+void launch_rhs(csd_handle* h, const float* d_data, int64_t V, float* sig_out = nullptr) {
+  if (h->dmma_rhs) {
+    switch (h->Kp) {
+      case 8: launch_rhs_dmma_t<8>(h, d_data, V, sig_out); return;
+      case 32: launch_rhs_dmma_t<32>(h, d_data, V, sig_out); return;
+      case 72: launch_rhs_dmma_t<72>(h, d_data, V, sig_out); return;
+      default: break;
+    }
+  }
   switch (h->Kp) {
     case 8: launch_rhs_t<8>(h, d_data, V); break;
     case 32: launch_rhs_t<32>(h, d_data, V); break;
@@ -377,13 +493,83 @@ void launch_tikhonov(csd_handle* h, const double* B, double* X, int64_t V) {
   }
 }
 
-void launch_epilogue(csd_handle* h, const csd::EpilogueParams& p) {
+void launch_epilogue_ffma(csd_handle* h, const csd::EpilogueParams& p) {
   const size_t smem = sizeof(double) * 8 * static_cast<size_t>(h->Kp) * 8;
   const int64_t groups = (p.n_work + 7) / 8;
   const int blocks = std::max(1, static_cast<int>(std::min<int64_t>((groups + 7) / 8, h->num_sms * 16)));
   CSD_CUDA(cudaFuncSetAttribute(csd::k_epilogue, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem)));
   csd::k_epilogue<<<blocks, 256, smem, h->stream>>>(p);
+  CSD_LAUNCH();
+}
+
+template <int KP>
+void launch_resid_dmma_t(csd_handle* h, const csd::ResidParams& r) {
+  const size_t smem = sizeof(double) * (static_cast<size_t>(h->Np) * KP + 8 * static_cast<size_t>(KP) * 8);
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_resid_dmma<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  const int64_t groups = (r.n_work + 7) / 8;
+  const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(h->num_sms, (groups + 7) / 8)));
+  csd::k_resid_dmma<KP><<<blocks, 256, smem, h->stream>>>(r);
+  CSD_LAUNCH();
+}
+
+// Residual / R^2 / BIC / scatter pass.  With the M tiles in shared memory the
+// residuals run on the FP64 tensor cores (k_resid_dmma) and a light per-voxel
+// pass scatters the results (k_finalize); otherwise k_epilogue does both.
+void launch_epilogue(csd_handle* h, const csd::EpilogueParams& p) {
+  if (!h->dmma_resid || p.n_work == 0) {
+    if (p.n_work > 0) launch_epilogue_ffma(h, p);
+    return;
+  }
+  const int64_t V = p.V;
+  h->resid_v.ensure(sizeof(double) * V);
+  h->sst_v.ensure(sizeof(double) * V);
+  csd::ResidParams r{};
+  r.data = p.data;
+  r.vox = p.vox;
+  r.sig = h->sig_compact;
+  r.list = p.list;
+  r.n_work = p.n_work;
+  r.N = h->N;
+  r.Np = h->Np;
+  r.mfrag = h->mfrag.as<double>();
+  r.X = p.X;
+  r.resid_out = p.resid_out ? p.resid_out : h->resid_v.as<double>();
+  r.sst_out = (p.scatter && p.r2) ? h->sst_v.as<double>() : nullptr;
+  switch (h->Kp) {
+    case 8: launch_resid_dmma_t<8>(h, r); break;
+    case 32: launch_resid_dmma_t<32>(h, r); break;
+    case 72: launch_resid_dmma_t<72>(h, r); break;
+    default: throw Error{CSD_ERR_INVALID, "unsupported coefficient count"};
+  }
+  if (!p.scatter && !p.nnz_out) return;
+  csd::FinalizeParams f{};
+  f.vox = p.vox;
+  f.list = p.list;
+  f.n_work = p.n_work;
+  f.N = p.N;
+  f.K = p.K;
+  f.Kp = p.Kp;
+  f.X = p.X;
+  f.resid = r.resid_out;
+  f.sst = r.sst_out;
+  f.iters = p.iters;
+  f.zero_v = p.zero_v;
+  f.alpha_v = p.alpha_v;
+  f.alpha = p.alpha;
+  f.kind = p.kind;
+  f.scatter = p.scatter;
+  f.coeffs = p.coeffs;
+  f.r2 = p.r2;
+  f.resid_map = p.resid;
+  f.alpha_map = p.alpha_map;
+  f.bic_map = p.bic_map;
+  f.iter_map = p.iter_map;
+  f.kind_map = p.kind_map;
+  f.nnz_out = p.nnz_out;
+  const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((p.n_work + 7) / 8, h->num_sms * 16)));
+  csd::k_finalize<<<blocks, 256, 0, h->stream>>>(f);
   CSD_LAUNCH();
 }
 
@@ -478,8 +664,10 @@ void record(csd_handle* h, int i) { CSD_CUDA(cudaEventRecord(h->ev[i], h->stream
 
 // The whole-volume fit on device buffers.
 FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64_t nvol,
-                const HostGtab& g, const csd_shore_spec* spec, double path_eps, const DevOut& out) {
+                const HostGtab& g, const csd_shore_spec* spec, double path_eps, const DevOut& out,
+                bool data_on_host = false) {
   FitInfo info;
+  h->sig_compact = nullptr;
   cudaStream_t st = h->stream;
   h->launches = 0;
   const bool is_l1 = spec->regularization == CSD_REG_L1;
@@ -525,7 +713,15 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   h->nnz_v.ensure(sizeof(int) * V);
   CSD_CUDA(cudaMemsetAsync(h->itotal.p, 0, sizeof(unsigned long long), st));
 
-  launch_rhs(h, d_data, V);
+  if (data_on_host) {
+    // `d_data` aliases pinned host memory: read each masked row once over the
+    // bus and keep a compact device copy for every later pass.
+    h->sig.ensure(sizeof(float) * static_cast<size_t>(V) * N);
+    launch_rhs(h, d_data, V, h->sig.as<float>());
+    h->sig_compact = h->sig.as<float>();
+  } else {
+    launch_rhs(h, d_data, V);
+  }
   record(h, 2);
 
   csd::EpilogueParams ep{};
@@ -554,6 +750,7 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   fp.queue = h->queue.as<unsigned long long>();
   fp.iter_total = h->itotal.as<unsigned long long>();
   fp.n_work = V;
+  if (is_l1) ensure_mom(h, spec->max_iter);
 
   const double* Xfinal = h->X.as<double>();
   const uint32_t* it_final = h->iters.as<uint32_t>();
@@ -848,6 +1045,7 @@ int csd_create(csd_handle** out, int32_t device, char* err, size_t err_len) {
       throw Error{CSD_ERR_CUDA, std::string("this library is built for sm_100a (B200); device is ") +
                                     prop.name};
     h->num_sms = prop.multiProcessorCount;
+    h->smem_optin = static_cast<int>(prop.sharedMemPerBlockOptin);
     CSD_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     for (auto& e : h->ev) CSD_CUDA(cudaEventCreate(&e));
   } catch (const Error& e) {
@@ -863,9 +1061,9 @@ void csd_destroy(csd_handle* h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  DevBuf* bufs[] = {&h->bvals, &h->bvecs, &h->M, &h->Mt, &h->G, &h->A, &h->gfrag, &h->scal, &h->ok,
+  DevBuf* bufs[] = {&h->bvals, &h->bvecs, &h->M, &h->Mt, &h->G, &h->A, &h->gfrag, &h->mfrag, &h->mtfrag, &h->sst_v, &h->mom, &h->scal, &h->ok,
                     &h->data, &h->mask, &h->coeffs, &h->r2, &h->resid, &h->iters_map, &h->kind_map,
-                    &h->alpha_map, &h->bic_map, &h->rss_map, &h->blk, &h->total, &h->vox, &h->B, &h->X,
+                    &h->alpha_map, &h->bic_map, &h->rss_map, &h->blk, &h->total, &h->vox, &h->B, &h->X, &h->sig,
                     &h->iters, &h->conv, &h->queue, &h->itotal, &h->resid_v, &h->nnz_v, &h->amax,
                     &h->zero, &h->alpha_v, &h->Xsel, &h->Xfb, &h->Xl2, &h->rss_l2, &h->list, &h->active,
                     &h->pbest, &h->psel, &h->pact, &h->palpha_sel, &h->pit_sel, &h->pconv_sel,
@@ -938,12 +1136,28 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
     const int N = gtab->n;
     const int K = n_coeffs(spec->radial_order);
     cudaStream_t st = h->stream;
-    h->data.ensure(sizeof(float) * static_cast<size_t>(nvol) * N);
     h->mask.ensure(static_cast<size_t>(nvol));
     h->coeffs.ensure(sizeof(float) * static_cast<size_t>(nvol) * K);
-    CSD_CUDA(cudaMemcpyAsync(h->data.p, data, sizeof(float) * static_cast<size_t>(nvol) * N,
-                             cudaMemcpyHostToDevice, st));
     CSD_CUDA(cudaMemcpyAsync(h->mask.p, mask, static_cast<size_t>(nvol), cudaMemcpyHostToDevice, st));
+    // Pinned (page-locked, mapped) input volumes are read in place by the
+    // right-hand-side kernel, masked rows only; pageable ones are copied whole.
+    const float* d_data = nullptr;
+    bool on_host = false;
+    {
+      cudaPointerAttributes attr{};
+      if (cudaPointerGetAttributes(&attr, data) == cudaSuccess && attr.type == cudaMemoryTypeHost &&
+          attr.devicePointer && h->dmma_rhs_possible(N, K)) {
+        d_data = static_cast<const float*>(attr.devicePointer);
+        on_host = true;
+      }
+      cudaGetLastError();  // a pageable pointer may leave an error code behind
+    }
+    if (!on_host) {
+      h->data.ensure(sizeof(float) * static_cast<size_t>(nvol) * N);
+      CSD_CUDA(cudaMemcpyAsync(h->data.p, data, sizeof(float) * static_cast<size_t>(nvol) * N,
+                               cudaMemcpyHostToDevice, st));
+      d_data = h->data.as<float>();
+    }
     const bool diag = spec->diagnostics != 0;
     auto map_f = [&](DevBuf& b, void* host) -> float* {
       if (!diag || !host) return nullptr;
@@ -965,7 +1179,7 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
       h->kind_map.ensure(nvol);
       d.kind = h->kind_map.as<uint8_t>();
     }
-    FitInfo info = run_fit(h, h->data.as<float>(), h->mask.as<uint8_t>(), nvol, g, spec, path_eps, d);
+    FitInfo info = run_fit(h, d_data, h->mask.as<uint8_t>(), nvol, g, spec, path_eps, d, on_host);
     CSD_CUDA(cudaMemcpyAsync(out->coefficients, d.coeffs, sizeof(float) * static_cast<size_t>(nvol) * K,
                              cudaMemcpyDeviceToHost, st));
     const bool is_l1 = spec->regularization == CSD_REG_L1;

@@ -177,10 +177,12 @@ __global__ void __launch_bounds__(256) k_rhs(const float* __restrict__ data,
 // ------------------------------------------------------------------ FISTA
 
 // D(8x8) += A(8x4, row) * B(4x8, col) in FP64 on the tensor cores.
+// Not volatile: the instruction has no side effects, so the compiler may
+// interleave independent DMMAs with the fragment loads.
 __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
 }
 
 struct FistaParams {
@@ -202,6 +204,7 @@ struct FistaParams {
   const int64_t* list;         // work list of voxel positions, or nullptr (= 0..V-1)
   int64_t n_work;              // length of the work list
   unsigned long long* iter_total;  // executed iterations, summed (nullable)
+  const double* mom;           // Nesterov momentum (t_k - 1) / t_{k+1}, k < max_iter
 };
 
 // One warp fits 8 voxels at a time (the 8 columns of an m8n8k4 tile).  Lane
@@ -366,6 +369,170 @@ __global__ void __launch_bounds__(256) k_fista_fp64(FistaParams p) {
         need[j] = true;
       }
     }
+  }
+  if (p.iter_total) {
+    for (int o = 16; o > 0; o >>= 1) executed += __shfl_xor_sync(kFull, executed, o);
+    if (lane == 0) atomicAdd(p.iter_total, executed);
+  }
+}
+
+// FISTA, one warp per 8 voxel slots (as k_fista_fp64) with a lighter
+// per-iteration path:
+//  * y lives only in the warp's shared B-operand buffer and b in a
+//    thread-private shared buffer, so registers hold just x and the
+//    accumulators and 12 warps fit per SM;
+//  * the k-step loop is outermost, so consecutive DMMAs update different
+//    accumulators (no dependent DMMA back to back);
+//  * the momentum (t_k - 1) / t_{k+1} comes from a table: t_k depends only on
+//    the iteration index, and the host evaluates the same IEEE expressions;
+//  * the stopping test sqrt(dx2) / max(sqrt(xn2), 1e-12) < tol is evaluated
+//    exactly only when dx2 <= 4 tol^2 max(xn2, 1e-24); above that bound the
+//    ratio exceeds 2 tol, far outside rounding, so the decision is unchanged.
+// The per-element update and the accumulation order of G y are those of
+// k_fista_fp64, so both kernels return identical iterates.
+template <int MT, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
+  constexpr int KP = 8 * MT, KT = 2 * MT;
+  extern __shared__ __align__(16) double smem3[];
+  double* sG = smem3;                                             // MT * KT * 32 (k_pack_gfrag)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* ybuf = smem3 + MT * KT * 32 + warp * (2 * KP * 8);      // KP x 8 [k][voxel]
+  double* bbuf = ybuf + KP * 8;                                    // thread-private [mt][lane][2]
+  for (int i = threadIdx.x; i < MT * KT * 32; i += blockDim.x) sG[i] = p.gfrag[i];
+  __syncthreads();
+
+  const int g = lane >> 2, q = lane & 3;
+  double x[MT][2];
+  int64_t vid[2] = {-1, -1};
+  int it[2] = {0, 0};
+  double thr[2] = {p.thr, p.thr};
+  bool need[2] = {true, true};
+  bool exhausted = false;
+  unsigned long long executed = 0;
+  const double tol2x4 = 4.0 * p.tol * p.tol;
+
+  while (true) {
+    // ---- refill (warp-aggregated queue)
+    {
+      const unsigned n0 = __ballot_sync(kFull, lane < 4 && need[0]);
+      const unsigned n1 = __ballot_sync(kFull, lane < 4 && need[1]);
+      unsigned colmask = 0;
+#pragma unroll
+      for (int l = 0; l < 4; ++l)
+        colmask |= (((n0 >> l) & 1u) << (2 * l)) | (((n1 >> l) & 1u) << (2 * l + 1));
+      const int nneed = __popc(colmask);
+      if (nneed > 0) {
+        const unsigned long long V_END = static_cast<unsigned long long>(p.n_work);
+        unsigned long long base = V_END;
+        if (!exhausted) {
+          if (lane == 0) base = atomicAdd(p.queue, static_cast<unsigned long long>(nneed));
+          base = __shfl_sync(kFull, base, 0);
+          if (base + nneed >= V_END) exhausted = true;
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          if (!need[j]) continue;
+          const int col = 2 * q + j;
+          const unsigned long long cand = base + __popc(colmask & ((1u << col) - 1u));
+          const int64_t nv = (cand < V_END) ? (p.list ? p.list[cand] : static_cast<int64_t>(cand)) : -1;
+          vid[j] = nv;
+          it[j] = 0;
+          thr[j] = (p.alpha_v && nv >= 0) ? __dmul_rn(p.step, p.alpha_v[nv]) : p.thr;
+          need[j] = false;
+#pragma unroll
+          for (int mt = 0; mt < MT; ++mt) {
+            const int row = 8 * mt + g;
+            double bv = 0.0, xv = 0.0;
+            if (nv >= 0) {
+              bv = p.B[nv * KP + row];
+              xv = p.warm ? p.warm[nv * KP + row] : 0.0;
+            }
+            x[mt][j] = xv;
+            bbuf[(mt * 32 + lane) * 2 + j] = bv;
+            ybuf[row * 8 + col] = xv;
+          }
+        }
+      }
+    }
+    if (!__any_sync(kFull, vid[0] >= 0 || vid[1] >= 0)) break;
+    executed += (g == 0) ? ((vid[0] >= 0) + (vid[1] >= 0)) : 0;
+    __syncwarp();
+
+    // ---- acc = G y on the FP64 tensor cores
+    double acc[MT][2];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) acc[mt][0] = acc[mt][1] = 0.0;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+      const double bf = ybuf[(4 * kt + q) * 8 + g];
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) dmma_m8n8k4(acc[mt][0], acc[mt][1], sG[(mt * KT + kt) * 32 + lane], bf);
+    }
+    __syncwarp();
+
+    // ---- proximal gradient step and momentum (fista.rs:141-173)
+    double mom[2], dx2[2] = {0.0, 0.0}, xn2[2] = {0.0, 0.0};
+#pragma unroll
+    for (int j = 0; j < 2; ++j) mom[j] = (vid[j] >= 0) ? p.mom[it[j]] : 0.0;
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+      const int row = 8 * mt + g;
+      const double2 yv = *reinterpret_cast<const double2*>(&ybuf[row * 8 + 2 * q]);
+      const double2 bv = *reinterpret_cast<const double2*>(&bbuf[(mt * 32 + lane) * 2]);
+      const double yy[2] = {yv.x, yv.y}, bb[2] = {bv.x, bv.y};
+      double yo[2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const double grad = __dmul_rn(__dsub_rn(acc[mt][j], bb[j]), p.n_inv);
+        const double cand = __dsub_rn(yy[j], __dmul_rn(p.step, grad));
+        double sv;
+        if (cand > thr[j])
+          sv = __dsub_rn(cand, thr[j]);
+        else if (cand < -thr[j])
+          sv = __dadd_rn(cand, thr[j]);
+        else
+          sv = 0.0;
+        const double xn = p.non_negative ? fmax(sv, 0.0) : sv;
+        const double d = __dsub_rn(xn, x[mt][j]);
+        yo[j] = __dadd_rn(xn, __dmul_rn(mom[j], d));
+        dx2[j] = fma(d, d, dx2[j]);
+        xn2[j] = fma(xn, xn, xn2[j]);
+        x[mt][j] = xn;
+      }
+      *reinterpret_cast<double2*>(&ybuf[row * 8 + 2 * q]) = make_double2(yo[0], yo[1]);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+#pragma unroll
+      for (int o = 4; o < 32; o <<= 1) {
+        dx2[j] += __shfl_xor_sync(kFull, dx2[j], o);
+        xn2[j] += __shfl_xor_sync(kFull, xn2[j], o);
+      }
+    }
+
+    // ---- per-voxel stopping rule (fista.rs:166-179) and write-out
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      if (vid[j] < 0) continue;
+      it[j] += 1;
+      bool converged = false;
+      if (!(dx2[j] > tol2x4 * fmax(xn2[j], 1e-24))) {
+        const double rel = sqrt(dx2[j]) / fmax(sqrt(xn2[j]), 1e-12);
+        converged = rel < p.tol;
+      }
+      if (converged || it[j] >= p.max_iter) {
+        const int64_t v = vid[j];
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) p.X[v * KP + 8 * mt + g] = x[mt][j];
+        if (g == 0) {
+          p.iters[v] = static_cast<uint32_t>(it[j]);
+          p.conv[v] = converged ? 1 : 0;
+        }
+        need[j] = true;
+        vid[j] = -1;
+      }
+    }
+    __syncwarp();
   }
   if (p.iter_total) {
     for (int o = 16; o > 0; o >>= 1) executed += __shfl_xor_sync(kFull, executed, o);
@@ -593,6 +760,273 @@ __global__ void __launch_bounds__(256) k_epilogue(EpilogueParams p) {
       }
     }
     __syncwarp();
+  }
+}
+
+// ------------------------------------------------- DMMA residual / rhs
+
+// Pack a row-major rows x cols matrix (leading dimension ld) into m8n8k4
+// A-operand tiles of an Rp x Cp zero-padded copy:
+// frag[(mt * (Cp / 4) + kt) * 32 + lane] = A[8 mt + lane / 4][4 kt + lane % 4],
+// where A = src (transpose = 0) or src^T (transpose = 1).
+__global__ void k_pack_afrag(const double* __restrict__ src, int rows, int cols, int ld, int transpose,
+                             int Rp, int Cp, double* __restrict__ frag) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= Rp * Cp) return;
+  const int lane = idx & 31, tile = idx >> 5;
+  const int CT = Cp / 4;
+  const int mt = tile / CT, kt = tile % CT;
+  const int r = 8 * mt + lane / 4, c = 4 * kt + (lane & 3);
+  double v = 0.0;
+  if (!transpose) {
+    if (r < rows && c < cols) v = src[static_cast<size_t>(r) * ld + c];
+  } else {
+    if (r < cols && c < rows) v = src[static_cast<size_t>(c) * ld + r];
+  }
+  frag[idx] = v;
+}
+
+// b_v = M^T s_v on the FP64 tensor cores, eight voxels per warp: the packed
+// M^T tiles (K_pad x N_pad) are staged once per persistent CTA; each warp
+// stages its voxels' signals (float32, padded rows) and accumulates
+// D(K_pad x 8) over the N_pad / 4 k-steps in row order.
+//
+// `data` may be device memory or pinned host memory mapped into the device
+// address space; each masked voxel's row is read exactly once, and when
+// `sig_out` is set the rows are also written there, compacted (V x N), for the
+// residual pass.
+template <int KP>
+__global__ void __launch_bounds__(256) k_rhs_dmma(const float* __restrict__ data,
+                                                  const int64_t* __restrict__ vox, int64_t V, int N,
+                                                  int Np, const double* __restrict__ mtfrag,
+                                                  double* __restrict__ B, float* __restrict__ sig_out) {
+  constexpr int MT = KP / 8;
+  extern __shared__ __align__(16) double rd_sm[];
+  const int KTN = Np / 4;
+  const int SLD = Np + 4;  // padded row stride (floats) of a staged signal
+  double* sA = rd_sm;      // KP * Np
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* sbuf = reinterpret_cast<float*>(rd_sm + static_cast<size_t>(KP) * Np) + warp * 8 * SLD;
+  for (int i = threadIdx.x; i < KP * Np; i += blockDim.x) sA[i] = mtfrag[i];
+  __syncthreads();
+  const int g = lane >> 2, q = lane & 3;
+  const int64_t groups = (V + 7) / 8;
+  for (int64_t gi = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp; gi < groups;
+       gi += static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5)) {
+    const int64_t v0 = gi * 8;
+    const int nv = static_cast<int>((V - v0) < 8 ? (V - v0) : 8);
+    for (int j = 0; j < 8; ++j) {
+      const float* src = (j < nv) ? data + vox[v0 + j] * N : nullptr;
+      float* dst = (sig_out && j < nv) ? sig_out + (v0 + j) * N : nullptr;
+      for (int i = lane; i < Np; i += 32) {
+        const float v = (src && i < N) ? src[i] : 0.0f;
+        sbuf[j * SLD + i] = v;
+        if (dst && i < N) dst[i] = v;
+      }
+    }
+    __syncwarp();
+    double acc[MT][2];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) acc[mt][0] = acc[mt][1] = 0.0;
+    for (int kt = 0; kt < KTN; ++kt) {
+      const double bf = static_cast<double>(sbuf[g * SLD + 4 * kt + q]);
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) dmma_m8n8k4(acc[mt][0], acc[mt][1], sA[(mt * KTN + kt) * 32 + lane], bf);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int col = 2 * q + j;
+      if (col < nv) {
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) B[(v0 + col) * KP + 8 * mt + g] = acc[mt][j];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+struct ResidParams {
+  const float* data;
+  const int64_t* vox;
+  const float* sig;      // compact signals (V x N) indexed by position, or nullptr (= data via vox)
+  const int64_t* list;   // positions to process, or nullptr (= 0..n_work-1)
+  int64_t n_work;
+  int N, Np;
+  const double* mfrag;   // packed M tiles (N_pad x K_pad)
+  const double* X;       // V x K_pad
+  double* resid_out;     // V: ||s - M c||
+  double* sst_out;       // V: sum (s - mean)^2, or nullptr
+};
+
+// ||s_v - M c_v|| and sum (s_v - mean_v)^2 on the FP64 tensor cores, eight
+// voxels per warp; packed M tiles staged once per persistent CTA.  Three row
+// tiles are accumulated at a time (three independent DMMA chains), the signal
+// is read at the accumulator's (row, voxel) positions, and the per-voxel sums
+// are reduced over the eight lanes of each voxel column.  The mean is taken
+// before the sum of squared deviations (src/fit.rs:120-128).
+template <int KP>
+__global__ void __launch_bounds__(256) k_resid_dmma(ResidParams p) {
+  constexpr int KT = KP / 4;
+  extern __shared__ __align__(16) double re_sm[];
+  double* sA = re_sm;  // Np * KP
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* xbuf = re_sm + static_cast<size_t>(p.Np) * KP + warp * (KP * 8);
+  for (int i = threadIdx.x; i < p.Np * KP; i += blockDim.x) sA[i] = p.mfrag[i];
+  __syncthreads();
+  const int g = lane >> 2, q = lane & 3;
+  const int MTN = p.Np / 8;
+  const int64_t groups = (p.n_work + 7) / 8;
+  for (int64_t gi = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp; gi < groups;
+       gi += static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5)) {
+    const int64_t w0 = gi * 8;
+    const int nv = static_cast<int>((p.n_work - w0) < 8 ? (p.n_work - w0) : 8);
+    // lanes 0..7 resolve voxel position / volume index of column `lane`
+    int64_t my_v = 0, my_li = 0;
+    if (lane < nv) {
+      my_v = p.list ? p.list[w0 + lane] : w0 + lane;
+      my_li = p.sig ? my_v : p.vox[my_v];
+    }
+    for (int e = lane; e < KP * 8; e += 32) {
+      const int k = e >> 3, j = e & 7;
+      const int64_t vj = __shfl_sync(kFull, my_v, j);
+      xbuf[e] = (j < nv) ? p.X[vj * KP + k] : 0.0;
+    }
+    // the loop above has every lane take part in every shuffle (KP * 8 is a
+    // multiple of 32)
+    __syncwarp();
+    const int64_t li0 = __shfl_sync(kFull, my_li, 2 * q);
+    const int64_t li1 = __shfl_sync(kFull, my_li, 2 * q + 1);
+    const bool ok0 = 2 * q < nv, ok1 = 2 * q + 1 < nv;
+    const float* sbase = p.sig ? p.sig : p.data;
+    const float* s0 = sbase + li0 * p.N;
+    const float* s1 = sbase + li1 * p.N;
+    double rss[2] = {0.0, 0.0}, ssum[2] = {0.0, 0.0};
+    for (int mt0 = 0; mt0 < MTN; mt0 += 3) {
+      double acc[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+      for (int kt = 0; kt < KT; ++kt) {
+        const double bf = xbuf[(4 * kt + q) * 8 + g];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (mt0 + c < MTN) dmma_m8n8k4(acc[c][0], acc[c][1], sA[((mt0 + c) * KT + kt) * 32 + lane], bf);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int row = 8 * (mt0 + c) + g;
+        if (mt0 + c < MTN && row < p.N) {
+          if (ok0) {
+            const double sv = static_cast<double>(s0[row]);
+            const double r = sv - acc[c][0];
+            rss[0] = fma(r, r, rss[0]);
+            ssum[0] += sv;
+          }
+          if (ok1) {
+            const double sv = static_cast<double>(s1[row]);
+            const double r = sv - acc[c][1];
+            rss[1] = fma(r, r, rss[1]);
+            ssum[1] += sv;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int o = 4; o < 32; o <<= 1) {
+        rss[j] += __shfl_xor_sync(kFull, rss[j], o);
+        ssum[j] += __shfl_xor_sync(kFull, ssum[j], o);
+      }
+    double sst[2] = {0.0, 0.0};
+    if (p.sst_out) {
+      const double mean0 = ssum[0] / static_cast<double>(p.N), mean1 = ssum[1] / static_cast<double>(p.N);
+      for (int row = g; row < p.N; row += 8) {
+        if (ok0) {
+          const double d = static_cast<double>(s0[row]) - mean0;
+          sst[0] = fma(d, d, sst[0]);
+        }
+        if (ok1) {
+          const double d = static_cast<double>(s1[row]) - mean1;
+          sst[1] = fma(d, d, sst[1]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int o = 4; o < 32; o <<= 1) sst[j] += __shfl_xor_sync(kFull, sst[j], o);
+    }
+    const int64_t v0 = __shfl_sync(kFull, my_v, 2 * q);
+    const int64_t v1 = __shfl_sync(kFull, my_v, 2 * q + 1);
+    if (g == 0) {
+      if (ok0) {
+        p.resid_out[v0] = sqrt(rss[0]);
+        if (p.sst_out) p.sst_out[v0] = sst[0];
+      }
+      if (ok1) {
+        p.resid_out[v1] = sqrt(rss[1]);
+        if (p.sst_out) p.sst_out[v1] = sst[1];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+struct FinalizeParams {
+  const int64_t* vox;
+  const int64_t* list;
+  int64_t n_work;
+  int N, K, Kp;
+  const double* X;          // V x Kp
+  const double* resid;      // V (from k_resid_dmma)
+  const double* sst;        // V, or nullptr (only needed with maps)
+  const uint32_t* iters;    // V or nullptr (iteration count 1)
+  const uint8_t* zero_v;    // V or nullptr
+  const double* alpha_v;    // V or nullptr
+  double alpha;
+  uint8_t kind;
+  bool scatter;
+  float* coeffs;
+  float *r2, *resid_map, *alpha_map, *bic_map;
+  uint32_t* iter_map;
+  uint8_t* kind_map;
+  int* nnz_out;
+};
+
+// Scatter of one voxel per warp: coefficients to the (X, Y, Z, K) volume,
+// exactly-non-zero count, R^2 = 1 - RSS / SST, BIC and the map entries.
+__global__ void __launch_bounds__(256) k_finalize(FinalizeParams p) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t warps_total = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t w = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp; w < p.n_work; w += warps_total) {
+    const int64_t v = p.list ? p.list[w] : w;
+    const int64_t li = p.vox[v];
+    int nnz = 0;
+    for (int k = lane; k < p.K; k += 32) {
+      const double c = p.X[v * p.Kp + k];
+      nnz += (c != 0.0) ? 1 : 0;
+      if (p.scatter) p.coeffs[li * p.K + k] = static_cast<float>(c);
+    }
+    for (int o = 16; o > 0; o >>= 1) nnz += __shfl_xor_sync(kFull, nnz, o);
+    if (lane == 0) {
+      if (p.nnz_out) p.nnz_out[v] = nnz;
+      if (p.scatter) {
+        const bool zero = p.zero_v && p.zero_v[v];
+        const double resid = zero ? 0.0 : p.resid[v];
+        const double ss_res = resid * resid;
+        const double sst = p.sst ? p.sst[v] : 0.0;
+        if (p.r2) p.r2[li] = static_cast<float>(sst > 0.0 ? 1.0 - ss_res / sst : 0.0);
+        if (p.resid_map) p.resid_map[li] = static_cast<float>(resid);
+        if (p.iter_map) p.iter_map[li] = p.iters ? p.iters[v] : 1u;
+        if (p.kind_map) p.kind_map[li] = p.kind;
+        if (p.alpha_map) p.alpha_map[li] = static_cast<float>(p.alpha_v ? p.alpha_v[v] : p.alpha);
+        if (p.bic_map) {
+          const double n = static_cast<double>(p.N);
+          const double rc = fmax(ss_res, 2.2250738585072014e-308);
+          p.bic_map[li] = zero ? 0.0f
+                               : static_cast<float>(n * log(rc / n) + log(n) * static_cast<double>(nnz));
+        }
+      }
+    }
   }
 }
 

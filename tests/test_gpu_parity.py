@@ -213,3 +213,44 @@ def test_shore_model_interface(ph, oracle):
     assert fit.sidecar["solver"]["kind"] == "tikhonov" and not fit.single_shell
     sp = fit.sparsity[ph.mask]
     assert sp[0] == 0.0 and sp[1:].min() > 0.9 and "256 voxels" in repr(fit)
+
+
+@pytest.mark.parametrize("variant", ["0", "3", "4"])
+def test_fista_kernel_variants_match_oracle(ph, oracle, variant, monkeypatch):
+    """Every FISTA kernel variant (k_fista_fp64; k_fista_v3 with 12 or 16
+    warps per CTA) runs the same per-voxel iteration."""
+    monkeypatch.setenv("CSD_FISTA_VARIANT", variant)
+    for mode in ("fixed", "l2-anchored"):
+        gpu, ref = both(ph, oracle, alpha_mode=mode, alpha=0.01)
+        same = np.isclose(gpu["alpha"][ph.mask], ref["alpha"][ph.mask], rtol=1e-9, atol=0)
+        assert same.mean() >= 0.98
+        r = rel_rows(gpu["coef64"], ref["coef64"])
+        nz = np.linalg.norm(ref["coef64"], axis=1) > 0
+        assert r[same & nz].max() <= 1e-5, (variant, mode, r[same & nz].max())
+        it_g = gpu["iterations"][ph.mask].astype(int)
+        it_o = ref["iterations"][ph.mask].astype(int)
+        assert np.abs(it_g - it_o)[same].max() <= 1
+
+
+def test_pinned_input_and_output_buffers_match(ph):
+    """A page-locked input volume is read in place (masked rows only) and a
+    caller-supplied output is filled completely; both give the same result
+    as pageable buffers."""
+    import torch
+    from cs_dmri_b200 import shore_fit
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, diagnostics=True, return_coef64=True)
+    for mode in ("fixed", "l2-anchored"):
+        ref = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, alpha_mode=mode, alpha=0.01, **kw)
+        pin = torch.empty(ph.data.shape, dtype=torch.float32, pin_memory=True)
+        pin.numpy()[...] = ph.data
+        out = torch.full(ph.data.shape[:3] + (72,), float("nan"), dtype=torch.float32, pin_memory=True)
+        got = shore_fit(pin.numpy(), ph.bvals, ph.bvecs, ph.mask, alpha_mode=mode, alpha=0.01,
+                        coefficients_out=out.numpy(), **kw)
+        assert got["coefficients"] is out.numpy() or np.shares_memory(got["coefficients"], out.numpy())
+        np.testing.assert_array_equal(out.numpy(), ref["coefficients"])
+        np.testing.assert_array_equal(got["coef64"], ref["coef64"])
+        for k in ("r2", "residual_l2", "iterations", "alpha", "bic"):
+            np.testing.assert_array_equal(got[k], ref[k])
+    with pytest.raises(ValueError, match="coefficients_out"):
+        shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, coefficients_out=np.zeros((2, 2, 2, 72), np.float32),
+                  big_delta=ph.big_delta, small_delta=ph.small_delta)
