@@ -12,9 +12,12 @@ zeta 700), L1 FISTA with a fixed alpha = 0.01 at the reference defaults
           of the host volume over the bus, fits, and copies the coefficient
           volume back (host clock around the blocking call).
 * roofline  the dominant kernel (FP64 FISTA on DMMA tensor cores): algorithmic
-          FLOPs = executed voxel-iterations x (2K^2 + 8K) per launch over the
-          kernel's event-timed duration, against the FP64 DMMA peak measured
-          live by libcsdpeak (no FP64 figure exists in MEASURED_PEAKS.json).
+          FLOPs = executed voxel-iterations x (2K^2 + 8K) per launch (the dense
+          Gram form) over the kernel's event-timed duration, against the FP64
+          DMMA peak measured live by libcsdpeak (no FP64 figure exists in
+          MEASURED_PEAKS.json).  The kernel skips k-steps whose iterate entries
+          are all exactly zero, so the tensor FLOPs it executes (counted on the
+          device, also reported) are fewer than the algorithmic count.
 * cpu_baseline  the CPU FP64 oracle (a restatement of the reference's rayon
           path: the Rust reference cannot be built without cargo) on all host
           threads, on a bounded sample of the same voxels.
@@ -271,7 +274,7 @@ def run_ours(args):
     barrier(world)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    kernel_ms, solve_flops, launches, iters = [], [], 0, []
+    kernel_ms, tensor_flops, launches, iters = [], [], 0, []
     with ClockSampler(device) as clocks:
         torch.cuda.synchronize(device)
         ev0.record(stream)
@@ -279,6 +282,7 @@ def run_ours(args):
             res = device_step()
             tm = _abi.last_timing(device)
             kernel_ms.append(tm.ms_solve_kernel)
+            tensor_flops.append(tm.tensor_flops)
             iters.append(res.total_iterations)
             launches += tm.launches
         ev1.record(stream)
@@ -315,6 +319,7 @@ def run_ours(args):
     k_ms = statistics.median(kernel_ms)
     it_launch = statistics.median(iters)
     achieved = it_launch * flops_per_iter / (k_ms * 1e-3) / 1e12
+    executed = statistics.median(tensor_flops) / (k_ms * 1e-3) / 1e12
     dmma_peak, dfma_peak = fp64_peak_tflops(device)
     traffic = traffic_from_profile()
 
@@ -339,6 +344,10 @@ def run_ours(args):
                          "frac": (achieved / dmma_peak) if dmma_peak else None, "traffic": traffic,
                          "kernel": "k_fista_v3<9,16>", "kernel_ms": k_ms,
                          "flops_per_launch": it_launch * flops_per_iter,
+                         "flops_basis": "dense Gram form, executed voxel-iterations x (2K^2 + 8K)",
+                         "executed_tensor_flops_per_launch": statistics.median(tensor_flops),
+                         "executed_tensor_tflops": executed,
+                         "executed_tensor_frac": (executed / dmma_peak) if dmma_peak else None,
                          "peak_source": "FP64 DMMA microbenchmark measured in this run (libcsdpeak); "
                                         f"scalar DFMA measured {dfma_peak:.1f} TFLOP/s" if dmma_peak else None},
             "gpu_launches": launches,

@@ -94,6 +94,7 @@ class Timing(C.Structure):
         ("ms_total", C.c_float),
         ("launches", C.c_int32),
         ("ms_solve_kernel", C.c_float),
+        ("tensor_flops", C.c_double),
     ]
 
 

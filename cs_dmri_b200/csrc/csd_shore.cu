@@ -708,10 +708,10 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   h->iters.ensure(sizeof(uint32_t) * V);
   h->conv.ensure(V);
   h->queue.ensure(sizeof(unsigned long long));
-  h->itotal.ensure(sizeof(unsigned long long));
+  h->itotal.ensure(2 * sizeof(unsigned long long));
   h->resid_v.ensure(sizeof(double) * V);
   h->nnz_v.ensure(sizeof(int) * V);
-  CSD_CUDA(cudaMemsetAsync(h->itotal.p, 0, sizeof(unsigned long long), st));
+  CSD_CUDA(cudaMemsetAsync(h->itotal.p, 0, 2 * sizeof(unsigned long long), st));
 
   if (data_on_host) {
     // `d_data` aliases pinned host memory: read each masked row once over the
@@ -749,6 +749,7 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   fp.non_negative = spec->non_negative;
   fp.queue = h->queue.as<unsigned long long>();
   fp.iter_total = h->itotal.as<unsigned long long>();
+  fp.kstep_total = h->itotal.as<unsigned long long>() + 1;
   fp.n_work = V;
   if (is_l1) ensure_mom(h, spec->max_iter);
 
@@ -937,12 +938,15 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   record(h, 3);
 
   // executed iteration total and the alpha distribution
-  unsigned long long itot = 0;
+  unsigned long long itot[2] = {0, 0};
   if (spec->regularization != CSD_REG_L2) {
-    CSD_CUDA(cudaMemcpyAsync(&itot, h->itotal.p, sizeof itot, cudaMemcpyDeviceToHost, st));
+    CSD_CUDA(cudaMemcpyAsync(itot, h->itotal.p, sizeof itot, cudaMemcpyDeviceToHost, st));
   }
   CSD_CUDA(cudaStreamSynchronize(st));
-  if (spec->regularization != CSD_REG_L2) info.total_iterations = itot;
+  if (spec->regularization != CSD_REG_L2) info.total_iterations = itot[0];
+  // executed FP64 tensor work of the FISTA launches: k-steps x row tiles x
+  // one m8n8k4 DMMA (8 x 8 x 4 FMA)
+  h->timing.tensor_flops = static_cast<double>(itot[1]) * (Kp / 8) * 512.0;
   if (is_l1 && mode != CSD_ALPHA_FIXED) {
     // median / p10 / p90 by nearest rank (src/fit.rs:334-352)
     std::vector<double> a(V);

@@ -205,6 +205,7 @@ struct FistaParams {
   int64_t n_work;              // length of the work list
   unsigned long long* iter_total;  // executed iterations, summed (nullable)
   const double* mom;           // Nesterov momentum (t_k - 1) / t_{k+1}, k < max_iter
+  unsigned long long* kstep_total;  // executed DMMA k-steps (each MT DMMAs), summed (nullable)
 };
 
 // One warp fits 8 voxels at a time (the 8 columns of an m8n8k4 tile).  Lane
@@ -382,7 +383,9 @@ __global__ void __launch_bounds__(256) k_fista_fp64(FistaParams p) {
 //    thread-private shared buffer, so registers hold just x and the
 //    accumulators and 12 warps fit per SM;
 //  * the k-step loop is outermost, so consecutive DMMAs update different
-//    accumulators (no dependent DMMA back to back);
+//    accumulators (no dependent DMMA back to back), and a k-step whose y
+//    entries are exactly zero for all eight voxels is skipped (it would add
+//    only zeros): the iterates are sparse, so about half the DMMAs go;
 //  * the momentum (t_k - 1) / t_{k+1} comes from a table: t_k depends only on
 //    the iteration index, and the host evaluates the same IEEE expressions;
 //  * the stopping test sqrt(dx2) / max(sqrt(xn2), 1e-12) < tol is evaluated
@@ -408,7 +411,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
   double thr[2] = {p.thr, p.thr};
   bool need[2] = {true, true};
   bool exhausted = false;
-  unsigned long long executed = 0;
+  unsigned long long executed = 0, ksteps = 0;
   const double tol2x4 = 4.0 * p.tol * p.tol;
 
   while (true) {
@@ -465,8 +468,13 @@ __global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
 #pragma unroll
     for (int kt = 0; kt < KT; ++kt) {
       const double bf = ybuf[(4 * kt + q) * 8 + g];
+      // A k-step whose four y entries are exactly zero for all eight voxels
+      // adds only zeros: skip it (soft thresholding keeps most of y at 0).
+      if (__any_sync(kFull, bf != 0.0)) {
+        ++ksteps;
 #pragma unroll
-      for (int mt = 0; mt < MT; ++mt) dmma_m8n8k4(acc[mt][0], acc[mt][1], sG[(mt * KT + kt) * 32 + lane], bf);
+        for (int mt = 0; mt < MT; ++mt) dmma_m8n8k4(acc[mt][0], acc[mt][1], sG[(mt * KT + kt) * 32 + lane], bf);
+      }
     }
     __syncwarp();
 
@@ -538,6 +546,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
     for (int o = 16; o > 0; o >>= 1) executed += __shfl_xor_sync(kFull, executed, o);
     if (lane == 0) atomicAdd(p.iter_total, executed);
   }
+  if (p.kstep_total && lane == 0) atomicAdd(p.kstep_total, ksteps);
 }
 
 // max_iter == 0: every voxel of the work list keeps its starting point.

@@ -210,6 +210,7 @@ typedef struct csd_fit_timing {
   float ms_total;       /* device time from first to last kernel */
   int32_t launches;     /* kernels launched by the fit */
   float ms_solve_kernel;/* duration of the dominant solve kernel alone */
+  double tensor_flops;  /* FP64 tensor-core FLOPs the FISTA launches executed */
 } csd_fit_timing;
 
 int csd_last_timing(const csd_handle* h, csd_fit_timing* out);
