@@ -375,14 +375,15 @@ void launch_fista_t(csd_handle* h, const csd::FistaParams& p) {
   CSD_LAUNCH();
 }
 
-template <int MT, int WARPS>
+template <int MT, int WARPS, bool G_IN_SMEM = true>
 void launch_fista_v3_t(csd_handle* h, const csd::FistaParams& p) {
   constexpr int KP = 8 * MT;
-  const size_t smem = sizeof(double) * (2 * static_cast<size_t>(MT) * MT * 32 + WARPS * 2 * KP * 8);  // Gram tiles + y, b
-  CSD_CUDA(cudaFuncSetAttribute(csd::k_fista_v3<MT, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  // Gram tiles (when staged) + per-warp y and b buffers
+  const size_t smem = sizeof(double) * ((G_IN_SMEM ? 2 * static_cast<size_t>(MT) * MT * 32 : 0) + WARPS * 2 * KP * 8);
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_fista_v3<MT, WARPS, G_IN_SMEM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem)));
   int per_sm = 0;
-  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_fista_v3<MT, WARPS>, 32 * WARPS, smem));
+  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_fista_v3<MT, WARPS, G_IN_SMEM>, 32 * WARPS, smem));
   per_sm = std::max(per_sm, 1);
   const int64_t warps_needed = (p.n_work + 7) / 8;
   int64_t blocks = std::min<int64_t>(static_cast<int64_t>(h->num_sms) * per_sm, (warps_needed + WARPS - 1) / WARPS);
@@ -390,7 +391,7 @@ void launch_fista_v3_t(csd_handle* h, const csd::FistaParams& p) {
   csd::FistaParams q = p;
   q.gfrag = h->gfrag.as<double>();
   q.mom = h->mom.as<double>();
-  csd::k_fista_v3<MT, WARPS><<<static_cast<unsigned>(blocks), 32 * WARPS, smem, h->stream>>>(q);
+  csd::k_fista_v3<MT, WARPS, G_IN_SMEM><<<static_cast<unsigned>(blocks), 32 * WARPS, smem, h->stream>>>(q);
   CSD_LAUNCH();
 }
 
@@ -423,12 +424,16 @@ void launch_fista(csd_handle* h, int MT, const csd::FistaParams& p) {
       default: break;
     }
   }
+  if (MT == 19) {  // radial order 8 (K = 145): Gram tiles through the caches
+    launch_fista_v3_t<19, 8, false>(h, p);
+    return;
+  }
   switch (MT) {
     case 1: launch_fista_t<1>(h, p); break;
     case 4: launch_fista_t<4>(h, p); break;
     case 9: launch_fista_t<9>(h, p); break;
     default:
-      throw Error{CSD_ERR_INVALID, "FISTA kernel is built for radial orders 2, 4 and 6 (K <= 72); got K = " +
+      throw Error{CSD_ERR_INVALID, "FISTA kernels are built for radial orders 2, 4, 6 and 8 (K <= 145); got K = " +
                                        std::to_string(h->K)};
   }
 }

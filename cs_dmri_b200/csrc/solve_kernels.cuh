@@ -393,16 +393,22 @@ __global__ void __launch_bounds__(256) k_fista_fp64(FistaParams p) {
 //    ratio exceeds 2 tol, far outside rounding, so the decision is unchanged.
 // The per-element update and the accumulation order of G y are those of
 // k_fista_fp64, so both kernels return identical iterates.
-template <int MT, int WARPS>
+//
+// G_IN_SMEM = false (large K, where the tiles would crowd out the warp
+// buffers): the tiles are read through the L1/L2 caches instead.
+template <int MT, int WARPS, bool G_IN_SMEM>
 __global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
   constexpr int KP = 8 * MT, KT = 2 * MT;
+  constexpr int G_WORDS = G_IN_SMEM ? MT * KT * 32 : 0;
   extern __shared__ __align__(16) double smem3[];
-  double* sG = smem3;                                             // MT * KT * 32 (k_pack_gfrag)
+  const double* sG = G_IN_SMEM ? smem3 : p.gfrag;                 // MT * KT * 32 (k_pack_gfrag)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* ybuf = smem3 + MT * KT * 32 + warp * (2 * KP * 8);      // KP x 8 [k][voxel]
+  double* ybuf = smem3 + G_WORDS + warp * (2 * KP * 8);           // KP x 8 [k][voxel]
   double* bbuf = ybuf + KP * 8;                                    // thread-private [mt][lane][2]
-  for (int i = threadIdx.x; i < MT * KT * 32; i += blockDim.x) sG[i] = p.gfrag[i];
-  __syncthreads();
+  if (G_IN_SMEM) {
+    for (int i = threadIdx.x; i < MT * KT * 32; i += blockDim.x) smem3[i] = p.gfrag[i];
+    __syncthreads();
+  }
 
   const int g = lane >> 2, q = lane & 3;
   double x[MT][2];
@@ -473,7 +479,10 @@ __global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
       if (__any_sync(kFull, bf != 0.0)) {
         ++ksteps;
 #pragma unroll
-        for (int mt = 0; mt < MT; ++mt) dmma_m8n8k4(acc[mt][0], acc[mt][1], sG[(mt * KT + kt) * 32 + lane], bf);
+        for (int mt = 0; mt < MT; ++mt) {
+          const double af = G_IN_SMEM ? sG[(mt * KT + kt) * 32 + lane] : __ldg(sG + (mt * KT + kt) * 32 + lane);
+          dmma_m8n8k4(acc[mt][0], acc[mt][1], af, bf);
+        }
       }
     }
     __syncwarp();

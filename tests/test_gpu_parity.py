@@ -254,3 +254,25 @@ def test_pinned_input_and_output_buffers_match(ph):
     with pytest.raises(ValueError, match="coefficients_out"):
         shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, coefficients_out=np.zeros((2, 2, 2, 72), np.float32),
                   big_delta=ph.big_delta, small_delta=ph.small_delta)
+
+
+@pytest.mark.parametrize("order", [2, 4, 8])
+def test_other_radial_orders(order, oracle):
+    """Radial orders 2, 4 and 8 (K = 8, 29, 145) run the same kernels with other
+    tile counts; order 8 reads its Gram tiles through the caches and uses the
+    FFMA right-hand-side and residual passes."""
+    from cs_dmri_b200.phantom import make_phantom
+    ph = make_phantom((5, 4, 3), seed=31 + order)
+    for kw in (dict(alpha_mode="fixed", alpha=0.01), dict(alpha_mode="l2-anchored"),
+               dict(regularization="l2", lambda_n=0.05, lambda_l=0.05)):
+        gpu, ref = both(ph, oracle, radial_order=order, **kw)
+        assert gpu["coefficients"].shape[-1] == oracle.n_coeffs(order)
+        if kw.get("regularization") == "l2":
+            r = rel_rows(gpu["coef64"], ref["coef64"])
+            assert r.max() <= 1e-8, (order, r.max())
+            continue
+        same = np.isclose(gpu["alpha"][ph.mask], ref["alpha"][ph.mask], rtol=1e-9, atol=0)
+        assert same.mean() >= 0.95, (order, kw, same.mean())
+        r = rel_rows(gpu["coef64"], ref["coef64"])
+        nz = np.linalg.norm(ref["coef64"], axis=1) > 0
+        assert r[same & nz].max() <= 1e-5, (order, kw, r[same & nz].max())
