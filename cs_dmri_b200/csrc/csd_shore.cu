@@ -20,7 +20,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <map>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -34,6 +36,7 @@
 #include "path_kernels.cuh"
 #include "setup_kernels.cuh"
 #include "solve_kernels.cuh"
+#include "icls_kernels.cuh"
 
 namespace {
 
@@ -166,6 +169,58 @@ int n_coeffs(int radial_order) {
 // Solve-kernel tile count for K coefficients (rows padded to 8).
 int mt_for(int K) { return (K + 7) / 8; }
 
+// Amplitude-constraint directions: a 642-vertex geodesic icosphere (regular
+// icosahedron, three midpoint subdivisions projected to the unit sphere) and
+// one direction of each antipodal pair, 321 unit vectors.  The reference uses
+// DSI Studio's ODF8 hemisphere, a sphere of the same construction and size
+// (src/solver/shore_icls.rs:52).
+std::vector<double> hemisphere_directions() {
+  const double ph = (1.0 + std::sqrt(5.0)) / 2.0;
+  std::vector<std::array<double, 3>> v = {{-1, ph, 0}, {1, ph, 0},   {-1, -ph, 0}, {1, -ph, 0},
+                                          {0, -1, ph}, {0, 1, ph},   {0, -1, -ph}, {0, 1, -ph},
+                                          {ph, 0, -1}, {ph, 0, 1},   {-ph, 0, -1}, {-ph, 0, 1}};
+  for (auto& a : v) {
+    const double n = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    for (auto& c : a) c /= n;
+  }
+  std::vector<std::array<int, 3>> f = {{0, 11, 5}, {0, 5, 1},  {0, 1, 7},   {0, 7, 10}, {0, 10, 11},
+                                       {1, 5, 9},  {5, 11, 4}, {11, 10, 2}, {10, 7, 6}, {7, 1, 8},
+                                       {3, 9, 4},  {3, 4, 2},  {3, 2, 6},   {3, 6, 8},  {3, 8, 9},
+                                       {4, 9, 5},  {2, 4, 11}, {6, 2, 10},  {8, 6, 7},  {9, 8, 1}};
+  for (int level = 0; level < 3; ++level) {
+    std::map<std::pair<int, int>, int> mid;
+    auto midpoint = [&](int a, int b) {
+      const auto key = std::make_pair(std::min(a, b), std::max(a, b));
+      const auto it = mid.find(key);
+      if (it != mid.end()) return it->second;
+      std::array<double, 3> c = {v[a][0] + v[b][0], v[a][1] + v[b][1], v[a][2] + v[b][2]};
+      const double n = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+      for (auto& e : c) e /= n;
+      v.push_back(c);
+      mid[key] = static_cast<int>(v.size()) - 1;
+      return static_cast<int>(v.size()) - 1;
+    };
+    std::vector<std::array<int, 3>> nf;
+    nf.reserve(f.size() * 4);
+    for (const auto& t : f) {
+      const int a = midpoint(t[0], t[1]), b = midpoint(t[1], t[2]), c = midpoint(t[2], t[0]);
+      nf.push_back({t[0], a, c});
+      nf.push_back({t[1], b, a});
+      nf.push_back({t[2], c, b});
+      nf.push_back({a, b, c});
+    }
+    f.swap(nf);
+  }
+  std::vector<double> out;
+  const double e = 1e-12;
+  for (const auto& a : v) {
+    const bool keep = (a[2] > e) || (std::fabs(a[2]) <= e && a[1] > e) ||
+                      (std::fabs(a[2]) <= e && std::fabs(a[1]) <= e && a[0] > 0.0);
+    if (keep) out.insert(out.end(), a.begin(), a.end());
+  }
+  return out;
+}
+
 }  // namespace
 
 struct csd_handle {
@@ -196,6 +251,11 @@ struct csd_handle {
   }
   DevBuf mom;      // Nesterov momentum table (t_k - 1) / t_{k+1}
   int mom_len = 0;
+  // amplitude-ICLS setup: constraint C (m x K), factor of M^T M + eps I, W = L^{-1} C^T
+  bool icls_valid = false;
+  uint64_t icls_key = 0;
+  int icls_m = 0, icls_m_pad = 0, icls_lmax = 0, icls_qmax = 0;
+  DevBuf dirs, Cmat, Le, Wi, Q1, ovf;
 
   // per-fit buffers
   DevBuf data, mask, coeffs, r2, resid, iters_map, kind_map, alpha_map, bic_map, rss_map;
@@ -226,6 +286,7 @@ void ensure_setup(csd_handle* h, const HostGtab& g, int radial_order, double zet
   if (!(h->setup_valid && h->setup_key == key)) {
     h->setup_valid = false;
     h->chol_valid = false;
+    h->icls_valid = false;
     h->N = N;
     h->K = K;
     h->Kp = Kp;
@@ -312,6 +373,49 @@ void ensure_setup(csd_handle* h, const HostGtab& g, int radial_order, double zet
       h->chol_valid = true;
     }
   }
+}
+
+// Setup of the amplitude-positivity fit (src/solver/shore_icls.rs:41-71,
+// src/solver/icls.rs:183-222): constraint matrix on the hemisphere, Cholesky
+// factor of M^T M + eps I and W = L^{-1} C^T.  Cached per table and epsilon.
+void ensure_icls_setup(csd_handle* h, int radial_order, double zeta, double eps) {
+  cudaStream_t st = h->stream;
+  uint64_t key = fnv1a(h->setup_key, &eps, sizeof eps);
+  if (h->icls_valid && h->icls_key == key) return;
+  const int K = h->K, Kp = h->Kp;
+  const std::vector<double> dirs = hemisphere_directions();
+  const int m = static_cast<int>(dirs.size() / 3);
+  const int m_pad = 32 * ((m + 31) / 32);
+  const int lmax = radial_order - (radial_order % 2);
+  h->icls_m = m;
+  h->icls_m_pad = m_pad;
+  h->icls_lmax = lmax;
+  h->icls_qmax = (lmax + 1) * (lmax + 2) / 2;  // rank of C <= number of SH coefficients
+  h->dirs.ensure(sizeof(double) * dirs.size());
+  CSD_CUDA(cudaMemcpyAsync(h->dirs.p, dirs.data(), sizeof(double) * dirs.size(), cudaMemcpyHostToDevice, st));
+  h->Cmat.ensure(sizeof(double) * static_cast<size_t>(m) * K);
+  csd::k_constraint<<<(m * K + 255) / 256, 256, 0, st>>>(h->dirs.as<double>(), m, K, radial_order, zeta,
+                                                        h->Cmat.as<double>());
+  CSD_LAUNCH();
+  h->Le.ensure(sizeof(double) * Kp * Kp);
+  CSD_CUDA(cudaMemcpyAsync(h->Le.p, h->G.p, sizeof(double) * Kp * Kp, cudaMemcpyDeviceToDevice, st));
+  csd::k_add_diag<<<(K + 255) / 256, 256, 0, st>>>(h->Le.as<double>(), K, Kp, eps);
+  CSD_LAUNCH();
+  const size_t csm = sizeof(double) * static_cast<size_t>(K) * K;
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_cholesky, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(csm)));
+  csd::k_cholesky<<<1, 256, csm, st>>>(h->Le.as<double>(), K, Kp, h->ok.as<int>());
+  CSD_LAUNCH();
+  int okv = 0;
+  CSD_CUDA(cudaMemcpyAsync(&okv, h->ok.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CSD_CUDA(cudaStreamSynchronize(st));
+  if (!okv) throw Error{CSD_ERR_NUMERICAL, "H^T H + eps I must be positive definite"};
+  h->Wi.ensure(sizeof(double) * static_cast<size_t>(K) * m_pad);
+  csd::k_icls_w<<<(m_pad + 127) / 128, 128, 0, st>>>(h->Le.as<double>(), K, Kp, h->Cmat.as<double>(), m, m_pad,
+                                                      h->Wi.as<double>());
+  CSD_LAUNCH();
+  h->icls_key = key;
+  h->icls_valid = true;
 }
 
 // Masked voxel list; returns V.
@@ -578,6 +682,36 @@ void launch_epilogue(csd_handle* h, const csd::EpilogueParams& p) {
   CSD_LAUNCH();
 }
 
+template <int RPL>
+void launch_icls_t(csd_handle* h, csd::IclsParams p) {
+  const size_t smem = sizeof(double) * csd::kIclsWarps *
+                      static_cast<size_t>(csd::icls_warp_words(h->K, h->icls_qmax, h->icls_m_pad));
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_icls<RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  int per_sm = 0;
+  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_icls<RPL>, 32 * csd::kIclsWarps, smem));
+  per_sm = std::max(per_sm, 1);
+  const int64_t warps_needed = p.V;
+  int64_t blocks = std::min<int64_t>(static_cast<int64_t>(h->num_sms) * per_sm,
+                                     (warps_needed + csd::kIclsWarps - 1) / csd::kIclsWarps);
+  blocks = std::max<int64_t>(blocks, 1);
+  h->Q1.ensure(sizeof(double) * static_cast<size_t>(blocks) * csd::kIclsWarps * h->K * h->icls_qmax);
+  p.Q1 = h->Q1.as<double>();
+  csd::k_icls<RPL><<<static_cast<unsigned>(blocks), 32 * csd::kIclsWarps, smem, h->stream>>>(p);
+  CSD_LAUNCH();
+}
+
+void launch_icls(csd_handle* h, const csd::IclsParams& p) {
+  switch ((h->K + 31) / 32) {
+    case 1: launch_icls_t<1>(h, p); break;
+    case 2: launch_icls_t<2>(h, p); break;
+    case 3: launch_icls_t<3>(h, p); break;
+    case 4: launch_icls_t<4>(h, p); break;
+    case 5: launch_icls_t<5>(h, p); break;
+    default: throw Error{CSD_ERR_INVALID, "amplitude-ICLS kernel supports K <= 160"};
+  }
+}
+
 // Device outputs of one fit (all device pointers; maps nullable).
 struct DevOut {
   float* coeffs;
@@ -595,6 +729,7 @@ struct FitInfo {
   const double* Xfinal = nullptr;  // device V x Kp
   const uint8_t* conv_final = nullptr;
   std::string warnings;
+  int lmax = 0, n_constraint_dirs = 0;
 };
 
 // Validation shared by both entry points (src/fit.rs:555-591, 691-730;
@@ -677,8 +812,6 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   h->launches = 0;
   const bool is_l1 = spec->regularization == CSD_REG_L1;
   const int mode = spec->alpha_mode;
-  if (spec->regularization == CSD_REG_NONNEG)
-    throw Error{CSD_ERR_INVALID, "regularization 'nonneg' (amplitude ICLS) is not available in this build"};
   const bool need_chol = spec->regularization == CSD_REG_L2 || (is_l1 && mode == CSD_ALPHA_L2_ANCHORED);
 
   record(h, 0);
@@ -766,7 +899,44 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   uint8_t kind = 1;
   double alpha_const = 0.0;
 
-  if (spec->regularization == CSD_REG_L2) {
+  if (spec->regularization == CSD_REG_NONNEG) {
+    // Goldfarb-Idnani ICLS on the ODF amplitudes (src/fit.rs:783-795)
+    kind = 3;
+    ensure_icls_setup(h, spec->radial_order, spec->zeta, spec->nonneg_epsilon);
+    h->ovf.ensure(sizeof(int));
+    CSD_CUDA(cudaMemsetAsync(h->ovf.p, 0, sizeof(int), st));
+    CSD_CUDA(cudaMemsetAsync(h->queue.p, 0, sizeof(unsigned long long), st));
+    csd::IclsParams ip{};
+    ip.B = h->B.as<double>();
+    ip.L = h->Le.as<double>();
+    ip.W = h->Wi.as<double>();
+    ip.X = h->X.as<double>();
+    ip.iters = h->iters.as<uint32_t>();
+    ip.conv = h->conv.as<uint8_t>();
+    ip.V = V;
+    ip.K = K;
+    ip.Kp = Kp;
+    ip.m = h->icls_m;
+    ip.m_pad = h->icls_m_pad;
+    ip.qmax = h->icls_qmax;
+    ip.max_iter = spec->nonneg_max_iter;
+    ip.tol = spec->nonneg_tol;
+    ip.queue = h->queue.as<unsigned long long>();
+    ip.overflow = h->ovf.as<int>();
+    ip.iter_total = h->itotal.as<unsigned long long>();
+    record(h, 6);
+    launch_icls(h, ip);
+    record(h, 7);
+    int ovf = 0;
+    CSD_CUDA(cudaMemcpyAsync(&ovf, h->ovf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CSD_CUDA(cudaStreamSynchronize(st));
+    if (ovf > 0)
+      info.warnings += std::to_string(ovf) +
+                       " voxel(s) reached an active set larger than the constraint rank; their fits are "
+                       "marked not converged\n";
+    info.lmax = h->icls_lmax;
+    info.n_constraint_dirs = h->icls_m;
+  } else if (spec->regularization == CSD_REG_L2) {
     kind = 2;
     record(h, 6);
     launch_tikhonov(h, h->B.as<double>(), h->X.as<double>(), V);
@@ -992,8 +1162,8 @@ void fill_scalars(const HostGtab& g, const FitInfo& info, const csd_shore_spec* 
   out->delta_source = g.delta_source;
   out->n_shells = static_cast<int32_t>(std::min<size_t>(g.shells.size(), 32));
   for (int i = 0; i < out->n_shells; ++i) out->dwi_shells[i] = g.shells[i];
-  out->lmax = 0;
-  out->n_constraint_dirs = 0;
+  out->lmax = info.lmax;
+  out->n_constraint_dirs = info.n_constraint_dirs;
   out->total_iterations = info.total_iterations;
 }
 
@@ -1070,7 +1240,7 @@ void csd_destroy(csd_handle* h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  DevBuf* bufs[] = {&h->bvals, &h->bvecs, &h->M, &h->Mt, &h->G, &h->A, &h->gfrag, &h->mfrag, &h->mtfrag, &h->sst_v, &h->mom, &h->scal, &h->ok,
+  DevBuf* bufs[] = {&h->bvals, &h->bvecs, &h->M, &h->Mt, &h->G, &h->A, &h->gfrag, &h->mfrag, &h->mtfrag, &h->sst_v, &h->mom, &h->scal, &h->ok, &h->dirs, &h->Cmat, &h->Le, &h->Wi, &h->Q1, &h->ovf,
                     &h->data, &h->mask, &h->coeffs, &h->r2, &h->resid, &h->iters_map, &h->kind_map,
                     &h->alpha_map, &h->bic_map, &h->rss_map, &h->blk, &h->total, &h->vox, &h->B, &h->X, &h->sig,
                     &h->iters, &h->conv, &h->queue, &h->itotal, &h->resid_v, &h->nnz_v, &h->amax,
@@ -1121,6 +1291,7 @@ int csd_shore_fit_volume_device(csd_handle* h, const float* d_data, const uint8_
       CSD_CUDA(cudaMemcpyAsync(out->converged, info.conv_final, info.V, cudaMemcpyDeviceToDevice, h->stream));
     CSD_CUDA(cudaStreamSynchronize(h->stream));
     fill_scalars(g, info, spec, out);
+    warnings += info.warnings;
     std::snprintf(out->warnings, sizeof out->warnings, "%s", warnings.c_str());
   } catch (const Error& e) {
     set_err(err, err_len, e.msg);
@@ -1214,6 +1385,7 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
       CSD_CUDA(cudaMemcpyAsync(out->converged, info.conv_final, info.V, cudaMemcpyDeviceToHost, st));
     CSD_CUDA(cudaStreamSynchronize(st));
     fill_scalars(g, info, spec, out);
+    warnings += info.warnings;
     std::snprintf(out->warnings, sizeof out->warnings, "%s", warnings.c_str());
   } catch (const Error& e) {
     set_err(err, err_len, e.msg);

@@ -276,3 +276,35 @@ def test_other_radial_orders(order, oracle):
         r = rel_rows(gpu["coef64"], ref["coef64"])
         nz = np.linalg.norm(ref["coef64"], axis=1) > 0
         assert r[same & nz].max() <= 1e-5, (order, kw, r[same & nz].max())
+
+
+@pytest.mark.parametrize("order", [4, 6])
+def test_amplitude_icls_parity(order, oracle):
+    """Goldfarb-Idnani positivity QP (src/solver/icls.rs via shore_icls.rs).
+    The minimiser is unique, so coefficients agree with the oracle's to the
+    QP's conditioning; every constraint holds to the solver tolerance and the
+    objective matches."""
+    from cs_dmri_b200.phantom import make_phantom
+    ph = make_phantom((6, 5, 4), seed=41 + order)
+    kw = dict(regularization="nonneg", radial_order=order)
+    gpu, ref = both(ph, oracle, **kw)
+    assert gpu["sidecar"]["solver"] == ref["sidecar"]["solver"]
+    assert gpu["sidecar"]["solver"]["n_constraint_dirs"] == 321
+    assert np.all(gpu["regularization_kind"][ph.mask] == 3)
+    assert gpu["converged"].all() and ref["converged"].all()
+    r = rel_rows(gpu["coef64"], ref["coef64"])
+    assert np.median(r) <= 1e-8 and r.max() <= 1e-5, (np.median(r), r.max())
+    # feasibility on the constraint sphere and equal objective values
+    M = oracle.design_matrix(ph.bvals, ph.bvecs, order, 700.0, big_delta=ph.big_delta, small_delta=ph.small_delta)
+    lmax = order
+    Cm = oracle.sh2amp_cart(oracle.odf8_hemisphere(), lmax) @ oracle.shore_to_tournier(order, 700.0, lmax)
+    S = ph.data.reshape(-1, ph.data.shape[-1])[ph.mask.ravel()].astype(np.float64)
+    scale = np.abs(Cm @ gpu["coef64"].T).max()
+    assert (Cm @ gpu["coef64"].T).min() >= -1e-7 * max(scale, 1.0)
+    obj_g = 0.5 * ((gpu["coef64"] @ M.T - S) ** 2).sum(1)
+    obj_o = 0.5 * ((ref["coef64"] @ M.T - S) ** 2).sum(1)
+    np.testing.assert_allclose(obj_g, obj_o, rtol=1e-9)
+    it_g = gpu["iterations"][ph.mask].astype(int)
+    it_o = ref["iterations"][ph.mask].astype(int)
+    assert np.mean(np.abs(it_g - it_o) <= 1) >= 0.9
+    np.testing.assert_allclose(gpu["residual_l2"], ref["residual_l2"], rtol=1e-6)
