@@ -16,7 +16,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libcsdshore.so"
 OK, ERR_INVALID, ERR_FIT_REFUSED, ERR_NUMERICAL, ERR_CUDA, ERR_TIMEOUT = range(6)
 REG_L1, REG_L2, REG_NONNEG = 1, 2, 3
 ALPHA_FIXED, ALPHA_RATIO, ALPHA_PATH_BIC, ALPHA_L2_ANCHORED = range(4)
-PRECISION_FP64 = 0
+PRECISION_FP64, PRECISION_MIXED = 0, 1
 
 
 class Gtab(C.Structure):
@@ -95,6 +95,9 @@ class Timing(C.Structure):
         ("launches", C.c_int32),
         ("ms_solve_kernel", C.c_float),
         ("tensor_flops", C.c_double),
+        ("ms_mixed_kernel", C.c_float),
+        ("int8_tensor_ops", C.c_double),
+        ("fp64_rerun_voxels", C.c_uint64),
     ]
 
 

@@ -22,6 +22,7 @@ from . import _abi
 TORTOISE_DEFAULT_GMAX = 80e-3  # src/qspace.rs:262
 
 _REGS = {"l1": _abi.REG_L1, "l2": _abi.REG_L2, "nonneg": _abi.REG_NONNEG}
+_PRECISIONS = {"fp64": _abi.PRECISION_FP64, "mixed": _abi.PRECISION_MIXED}
 _MODES = {"fixed": _abi.ALPHA_FIXED, "alpha-ratio": _abi.ALPHA_RATIO,
           "path-bic": _abi.ALPHA_PATH_BIC, "l2-anchored": _abi.ALPHA_L2_ANCHORED}
 
@@ -40,7 +41,8 @@ def affine_rotation(affine) -> np.ndarray:
 def build_spec(*, radial_order=6, zeta=700.0, regularization="l1", alpha_mode="l2-anchored", alpha=1.0,
                alpha_ratio=1e-3, path_n_alphas=20, path_eps=None, slack=0.05, max_iter=1000, tol=1e-6,
                non_negative=False, lambda_n=1e-8, lambda_l=1e-8, nonneg_max_iter=200, nonneg_tol=1e-9,
-               nonneg_epsilon=1e-10, diagnostics=False, allow_single_shell=False) -> _abi.Spec:
+               nonneg_epsilon=1e-10, diagnostics=False, allow_single_shell=False,
+               precision="fp64") -> _abi.Spec:
     """Flat ShoreFitSpec from the binding's keyword arguments, with the
     binding's string checks (python/src/models.rs:112-144)."""
     if regularization not in _REGS:
@@ -69,7 +71,9 @@ def build_spec(*, radial_order=6, zeta=700.0, regularization="l1", alpha_mode="l
     s.nonneg_epsilon = float(nonneg_epsilon)
     s.diagnostics = int(bool(diagnostics))
     s.allow_single_shell = int(bool(allow_single_shell))
-    s.precision = _abi.PRECISION_FP64
+    if precision not in _PRECISIONS:
+        raise ValueError(f"precision must be fp64 or mixed, got {precision!r}")
+    s.precision = _PRECISIONS[precision]
     return s
 
 
@@ -143,7 +147,7 @@ def sidecar(res: _abi.FitResult, kw: dict, bvec_frame: str) -> dict:
 
 _SPEC_KEYS = ("radial_order", "zeta", "regularization", "alpha_mode", "alpha", "alpha_ratio", "path_n_alphas",
               "path_eps", "slack", "max_iter", "tol", "non_negative", "lambda_n", "lambda_l", "nonneg_max_iter",
-              "nonneg_tol", "nonneg_epsilon", "diagnostics", "allow_single_shell")
+              "nonneg_tol", "nonneg_epsilon", "diagnostics", "allow_single_shell", "precision")
 
 
 def shore_fit(data, bvals, bvecs, mask, *, big_delta=None, small_delta=None, b0_threshold=50.0,
@@ -152,7 +156,7 @@ def shore_fit(data, bvals, bvecs, mask, *, big_delta=None, small_delta=None, b0_
               slack=0.05, max_iter=1000, tol=1e-6, non_negative=False, lambda_n=1e-8, lambda_l=1e-8,
               nonneg_max_iter=200, nonneg_tol=1e-9, nonneg_epsilon=1e-10, diagnostics=False,
               allow_single_shell=False, n_threads=None, device: int = 0, return_coef64: bool = False,
-              coefficients_out=None) -> dict:
+              coefficients_out=None, precision: str = "fp64") -> dict:
     """SHORE fit of every masked voxel on the GPU (``_cs_dmri.shore_fit``).
 
     ``n_threads`` is accepted for signature compatibility and ignored: the fit
@@ -161,7 +165,9 @@ def shore_fit(data, bvals, bvecs, mask, *, big_delta=None, small_delta=None, b0_
     ``coefficients_out`` may supply the (X, Y, Z, K) float32 C-contiguous output
     array (for example in page-locked memory, which makes the copy back
     faster); every element is overwritten.  A page-locked ``data`` volume is
-    read in place, masked voxels only.
+    read in place, masked voxels only.  ``precision="mixed"`` (radial order 6)
+    runs the L1 iterations with int8 digit-slice tensor-core Gram products and
+    FP64 state; the default ``"fp64"`` is the reference arithmetic.
     """
     if bvec_frame not in ("image-axis", "world-ras"):
         raise ValueError(f"bvec_frame must be 'image-axis' or 'world-ras', got {bvec_frame!r}")
@@ -169,7 +175,7 @@ def shore_fit(data, bvals, bvecs, mask, *, big_delta=None, small_delta=None, b0_
               alpha=alpha, alpha_ratio=alpha_ratio, path_n_alphas=path_n_alphas, path_eps=path_eps, slack=slack,
               max_iter=max_iter, tol=tol, non_negative=non_negative, lambda_n=lambda_n, lambda_l=lambda_l,
               nonneg_max_iter=nonneg_max_iter, nonneg_tol=nonneg_tol, nonneg_epsilon=nonneg_epsilon,
-              diagnostics=diagnostics, allow_single_shell=allow_single_shell)
+              diagnostics=diagnostics, allow_single_shell=allow_single_shell, precision=precision)
     spec = build_spec(**kw)
     data = np.asarray(data)
     if data.ndim != 4:

@@ -37,6 +37,7 @@
 #include "setup_kernels.cuh"
 #include "solve_kernels.cuh"
 #include "icls_kernels.cuh"
+#include "mixed_kernels.cuh"
 
 namespace {
 
@@ -228,7 +229,7 @@ struct csd_handle {
   cudaStream_t stream = nullptr;
   int num_sms = 0;
   int launches = 0;
-  cudaEvent_t ev[8] = {};
+  cudaEvent_t ev[10] = {};  // 8, 9: the mixed-precision FISTA kernel
   csd_fit_timing timing{};
 
   // setup cache
@@ -256,6 +257,9 @@ struct csd_handle {
   uint64_t icls_key = 0;
   int icls_m = 0, icls_m_pad = 0, icls_lmax = 0, icls_qmax = 0;
   DevBuf dirs, Cmat, Le, Wi, Q1, ovf;
+  // int8 digit planes of G for the mixed-precision FISTA (radial order 6)
+  DevBuf gdig, gfexp;
+  int precision = CSD_PRECISION_FP64;  // precision of the current fit
 
   // per-fit buffers
   DevBuf data, mask, coeffs, r2, resid, iters_map, kind_map, alpha_map, bic_map, rss_map;
@@ -263,6 +267,9 @@ struct csd_handle {
   const float* sig_compact = nullptr;  // compact masked signals of the current fit, if any
   DevBuf amax, zero, alpha_v, Xsel, Xfb, Xl2, rss_l2, list, active, pbest, psel, pact, palpha_sel,
       pit_sel, pconv_sel, palpha_fb, pit_fb, pconv_fb, pcode;
+  DevBuf flagged, mixstat;  // guard re-run list; [n_flagged, batches, error]
+  double mixed_ms = 0.0, mixed_ops = 0.0;
+  unsigned long long mixed_rerun = 0;
 };
 
 namespace {
@@ -325,6 +332,13 @@ void ensure_setup(csd_handle* h, const HostGtab& g, int radial_order, double zet
     csd::k_transpose_design<<<(Kp * N + 255) / 256, 256, 0, st>>>(h->M.as<double>(), N, K, Kp,
                                                                   h->Mt.as<double>());
     CSD_LAUNCH();
+    if (K == csd::i8::KC) {
+      h->gdig.ensure(csd::i8::B_BYTES);
+      h->gfexp.ensure(sizeof(int) * csd::i8::NB);
+      CSD_CUDA(cudaMemsetAsync(h->gdig.p, 0, csd::i8::B_BYTES, st));
+      csd::k_gdigits<<<csd::i8::NB, 128, 0, st>>>(h->G.as<double>(), Kp, h->gdig.as<uint8_t>(), h->gfexp.as<int>());
+      CSD_LAUNCH();
+    }
     // DMMA operand tiles of M (residual pass) and M^T (right-hand sides),
     // used when they fit in one CTA's shared memory next to the warp buffers.
     const int Np = 8 * ((N + 7) / 8);
@@ -508,7 +522,79 @@ int fista_variant() {
   return 4;
 }
 
+void launch_fista(csd_handle* h, int MT, const csd::FistaParams& p);
+
+// Mixed-precision FISTA: int8 digit-slice Gram products on the tensor cores,
+// FP64 state; the voxels the stop-decision guard flags are then re-fitted by
+// the FP64 kernel from the same starting point.
+void launch_fista_mixed(csd_handle* h, const csd::FistaParams& p) {
+  using namespace csd::i8;
+  cudaStream_t st = h->stream;
+  h->flagged.ensure(sizeof(int64_t) * std::max<int64_t>(p.n_work, 1));
+  h->mixstat.ensure(4 * sizeof(unsigned long long));
+  CSD_CUDA(cudaMemsetAsync(h->mixstat.p, 0, 4 * sizeof(unsigned long long), st));
+  csd::MixedParams q{};
+  q.gdig = h->gdig.as<uint8_t>();
+  q.fexp = h->gfexp.as<int>();
+  q.B = p.B;
+  q.X = p.X;
+  q.warm = p.warm;
+  q.iters = p.iters;
+  q.conv = p.conv;
+  q.c_step = p.step * p.n_inv;
+  q.thr = p.thr;
+  q.step = p.step;
+  q.alpha_v = p.alpha_v;
+  q.tol = p.tol;
+  q.band = 0.01;
+  q.max_iter = p.max_iter;
+  q.non_negative = p.non_negative;
+  q.queue = p.queue;
+  q.list = p.list;
+  q.n_work = p.n_work;
+  q.mom = h->mom.as<double>();
+  q.iter_total = p.iter_total;
+  q.flagged = h->flagged.as<int64_t>();
+  unsigned long long* stat = h->mixstat.as<unsigned long long>();
+  q.n_flagged = stat;
+  q.batches = stat + 1;
+  q.error = reinterpret_cast<int*>(stat + 2);
+  const size_t smem = csd::kMixedSmem;
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_fista_i8, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  const int64_t tiles = (p.n_work + TILE - 1) / TILE;
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(h->num_sms, tiles)));
+  CSD_CUDA(cudaEventRecord(h->ev[8], st));
+  csd::k_fista_i8<<<grid, THREADS, smem, st>>>(q);
+  CSD_LAUNCH();
+  CSD_CUDA(cudaEventRecord(h->ev[9], st));
+  unsigned long long hs[3] = {0, 0, 0};
+  CSD_CUDA(cudaMemcpyAsync(hs, stat, sizeof hs, cudaMemcpyDeviceToHost, st));
+  CSD_CUDA(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, h->ev[8], h->ev[9]) == cudaSuccess) h->mixed_ms += ms;
+  h->mixed_ops += static_cast<double>(hs[1]) * MMAS_PER_ITER * 2.0 * TILE * NB * 32;
+  if (static_cast<int>(hs[2]) != 0)
+    throw Error{CSD_ERR_TIMEOUT, "mixed-precision FISTA: a tensor-core completion wait gave up"};
+  if (hs[0] > 0) {
+    h->mixed_rerun += hs[0];
+    csd::FistaParams r = p;
+    r.list = h->flagged.as<int64_t>();
+    r.n_work = static_cast<int64_t>(hs[0]);
+    r.iter_total = nullptr;  // executed iterations count the mixed pass once
+    CSD_CUDA(cudaMemsetAsync(p.queue, 0, sizeof(unsigned long long), st));
+    const int saved = h->precision;
+    h->precision = CSD_PRECISION_FP64;
+    launch_fista(h, KC / 8, r);
+    h->precision = saved;
+  }
+}
+
 void launch_fista(csd_handle* h, int MT, const csd::FistaParams& p) {
+  if (h->precision == CSD_PRECISION_MIXED && MT * 8 == csd::i8::KC && p.max_iter > 0) {
+    launch_fista_mixed(h, p);
+    return;
+  }
   if (p.max_iter <= 0) {
     // An empty iteration loop: the warm start (or zero) is the result, with
     // 0 iterations and not converged (fista.rs:126-140 with max_iter = 0).
@@ -738,7 +824,11 @@ double validate(const csd_shore_spec* s, const HostGtab& g, std::string& warning
   if (s->radial_order <= 0 || s->radial_order % 2 != 0)
     throw Error{CSD_ERR_INVALID,
                 "radial_order must be a positive even number, got " + std::to_string(s->radial_order)};
-  if (s->precision != CSD_PRECISION_FP64) throw Error{CSD_ERR_INVALID, "unknown precision"};
+  if (s->precision != CSD_PRECISION_FP64 && s->precision != CSD_PRECISION_MIXED)
+    throw Error{CSD_ERR_INVALID, "unknown precision"};
+  if (s->precision == CSD_PRECISION_MIXED && s->regularization == CSD_REG_L1 && s->radial_order != 6)
+    throw Error{CSD_ERR_INVALID, "precision 'mixed' is built for radial order 6, got " +
+                                     std::to_string(s->radial_order)};
   if (s->max_iter < 0) throw Error{CSD_ERR_INVALID, "max_iter must be >= 0"};
   double path_eps = s->path_eps;
   if (s->regularization == CSD_REG_L1) {
@@ -810,6 +900,10 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   h->sig_compact = nullptr;
   cudaStream_t st = h->stream;
   h->launches = 0;
+  h->precision = spec->precision;
+  h->mixed_ms = 0.0;
+  h->mixed_ops = 0.0;
+  h->mixed_rerun = 0;
   const bool is_l1 = spec->regularization == CSD_REG_L1;
   const int mode = spec->alpha_mode;
   const bool need_chol = spec->regularization == CSD_REG_L2 || (is_l1 && mode == CSD_ALPHA_L2_ANCHORED);
@@ -1122,6 +1216,9 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   // executed FP64 tensor work of the FISTA launches: k-steps x row tiles x
   // one m8n8k4 DMMA (8 x 8 x 4 FMA)
   h->timing.tensor_flops = static_cast<double>(itot[1]) * (Kp / 8) * 512.0;
+  h->timing.ms_mixed_kernel = static_cast<float>(h->mixed_ms);
+  h->timing.int8_tensor_ops = h->mixed_ops;
+  h->timing.fp64_rerun_voxels = h->mixed_rerun;
   if (is_l1 && mode != CSD_ALPHA_FIXED) {
     // median / p10 / p90 by nearest rank (src/fit.rs:334-352)
     std::vector<double> a(V);

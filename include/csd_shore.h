@@ -72,9 +72,15 @@ enum csd_alpha_mode {
 
 /* Arithmetic of the FISTA iterations.  FP64 is the reference-faithful path:
  * the same iteration, step 1/L and stopping rule as src/solver/fista.rs:70-143
- * evaluated in IEEE double. */
+ * evaluated in IEEE double.  MIXED (radial order 6 only; L2 and nonneg fits
+ * ignore it) keeps the iterates, the stopping rule and the gradient
+ * accumulator in FP64 and forms the per-iteration Gram product G (x_k -
+ * x_{k-1}) exactly from int8 digit slices on the tensor cores, accurate to
+ * about 2^-32 relative; voxels whose stopping decision falls within 1 % of
+ * tol are re-fitted in FP64. */
 enum csd_precision {
-  CSD_PRECISION_FP64 = 0
+  CSD_PRECISION_FP64 = 0,
+  CSD_PRECISION_MIXED = 1
 };
 
 /* Gradient table (src/qspace.rs:90-130).  big_delta / small_delta in seconds;
@@ -211,6 +217,9 @@ typedef struct csd_fit_timing {
   int32_t launches;     /* kernels launched by the fit */
   float ms_solve_kernel;/* duration of the dominant solve kernel alone */
   double tensor_flops;  /* FP64 tensor-core FLOPs the FISTA launches executed */
+  float ms_mixed_kernel;/* the mixed-precision FISTA kernel alone (0 in FP64) */
+  double int8_tensor_ops;      /* int8 tensor-core ops it issued (2 per MAC) */
+  uint64_t fp64_rerun_voxels;  /* voxels the stop-decision guard re-ran in FP64 */
 } csd_fit_timing;
 
 int csd_last_timing(const csd_handle* h, csd_fit_timing* out);

@@ -51,7 +51,8 @@ def test_struct_layout_matches_header(lib_built):
               "csd_fit_result": (_abi.FitResult, ["n_coeffs", "n_voxels", "alpha_distribution",
                                                   "dwi_shells", "total_iterations", "warnings"]),
               "csd_gtab": (_abi.Gtab, ["n", "big_delta", "b0_threshold"]),
-              "csd_fit_timing": (_abi.Timing, ["launches", "ms_solve_kernel", "tensor_flops"])}
+              "csd_fit_timing": (_abi.Timing, ["launches", "ms_solve_kernel", "tensor_flops", "ms_mixed_kernel",
+                                                  "int8_tensor_ops", "fp64_rerun_voxels"])}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{ROOT}/include/csd_shore.h"',
              'int main(void){']
     for st, (_, fs) in fields.items():
