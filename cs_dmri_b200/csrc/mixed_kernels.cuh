@@ -49,10 +49,16 @@ constexpr int THREADS = 256;                   // two threads per voxel
 constexpr int TMEM_COLS = 512;                 // NLEV * NB = 400 used
 constexpr int D_BITS = 30, G_BITS = 38;
 constexpr int MMAS_PER_ITER = 3 + 5 + 8 + 10 + 10;
-// dynamic shared memory: A, B, u [KC][TILE], column exponents, per-voxel state
-constexpr size_t kSmem = A_BYTES + B_BYTES + sizeof(double) * KC * TILE + sizeof(int) * NB +
-                         sizeof(double) * 5 * TILE + sizeof(int64_t) * 2 * TILE + sizeof(unsigned) * 2 * TILE +
-                         sizeof(int) * 3 * TILE;
+constexpr uint64_t kWaitNs = 2000000000ull;    // give up on one MMA batch after 2 s
+constexpr int RING = 16;                       // prefetched voxels per CTA
+constexpr int MOM_SMEM = 1024;                 // momentum factors held in shared memory
+constexpr int PRODUCER_WARP = 7;               // tops the prefetch ring up while the MMAs run
+// dynamic shared memory: A, B, u [KC][TILE], prefetch ring (b and warm rows),
+// momentum table, column exponents, per-voxel state
+constexpr size_t kSmem = A_BYTES + B_BYTES + sizeof(double) * KC * TILE + sizeof(double) * 2 * RING * KC +
+                         sizeof(double) * MOM_SMEM + sizeof(double) * RING + sizeof(int64_t) * RING +
+                         sizeof(int) * NB + sizeof(double) * 5 * TILE + sizeof(int64_t) * 2 * TILE +
+                         sizeof(unsigned) * 2 * TILE + sizeof(int) * 4 * TILE;
 
 // Byte offset of digit plane s, coefficient j of voxel row r in the A operand
 // (canonical K-major, no swizzle: 8 rows x 16 bytes per core matrix).
@@ -152,9 +158,19 @@ __device__ __forceinline__ void ld4(uint32_t taddr, uint32_t (&v)[4]) {
                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
                : "r"(taddr));
 }
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 __device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
 __device__ __forceinline__ uint32_t try_wait(const uint64_t* bar, uint32_t parity) {
   uint32_t done;
   asm volatile(
@@ -165,10 +181,11 @@ __device__ __forceinline__ uint32_t try_wait(const uint64_t* bar, uint32_t parit
   return done;
 }
 
-// Exact int32 -> double (|v| < 2^31) without a conversion instruction.
+// Exact int32 -> double without a conversion instruction: the bit pattern
+// (0x43380000, v + 2^31) is the double 1.5 * 2^52 + 2^31 + v.
 __device__ __forceinline__ double i2d(int v) {
   return __hiloint2double(0x43380000, static_cast<int>(static_cast<unsigned>(v) ^ 0x80000000u)) -
-         6755401746153472.0 - 2147483648.0;
+         (0x1.8p52 + 0x1p31);
 }
 // Recombined level sums 256 * (L0 + 2^-8 L1 + 2^-16 L2 + 2^-24 L3 + 2^-32 L4)
 // = A + 2^-16 B + 2^-24 C with A = 256 L0 + L1, B = 256 L2 + L3, C = L4, all
@@ -185,7 +202,7 @@ __device__ __forceinline__ double pow2(int e) { return __hiloint2double((e + 102
 // q = rint(d * scale) for |d * scale| <= 2^30, then the four balanced digits
 // as the bytes of a word: byte b = digit (3 - b).
 __device__ __forceinline__ uint32_t digits(double d, double scale) {
-  const double t = fma(d, scale, 6755399441055744.0);  // + 1.5 * 2^52: rounds to an integer
+  const double t = fma(d, scale, 0x1.8p52);  // + 1.5 * 2^52: rounds to an integer in the low word
   const uint32_t q = static_cast<uint32_t>(__double2loint(t));
   return (q + 0x00808080u) ^ 0x00808080u;
 }
@@ -214,7 +231,12 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
   unsigned char* sA = smem_i8;                                   // A_BYTES
   unsigned char* sB = sA + A_BYTES;                              // B_BYTES
   double* sU = reinterpret_cast<double*>(sB + B_BYTES);          // [KC][TILE]
-  int* sF = reinterpret_cast<int*>(sU + KC * TILE);              // [NB]
+  double* rB = sU + KC * TILE;                                   // [RING][KC] prefetched b rows
+  double* rW = rB + RING * KC;                                   // [RING][KC] prefetched warm rows
+  double* sMom = rW + RING * KC;                                 // [MOM_SMEM]
+  double* rThr = sMom + MOM_SMEM;                                // [RING]
+  int64_t* rVid = reinterpret_cast<int64_t*>(rThr + RING);       // [RING]
+  int* sF = reinterpret_cast<int*>(rVid + RING);                 // [NB]
   double* sDx = reinterpret_cast<double*>(sF + NB);              // [2][TILE]
   double* sXn = sDx + 2 * TILE;                                  // [2][TILE]
   double* sThr = sXn + 2 * TILE;                                 // [TILE]
@@ -223,27 +245,31 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
   unsigned* sMax = reinterpret_cast<unsigned*>(sOld + TILE);     // [2][TILE] max |d| high words
   int* sIt = reinterpret_cast<int*>(sMax + 2 * TILE);            // [TILE]
   int* sNear = sIt + TILE;                                       // [TILE]
-  int* sFin = sNear + TILE;                                      // [TILE] 1: write out sOld
+  int* sFin = sNear + TILE;                                      // [TILE] 1: slot emptied this pass
+  int* sSrc = sFin + TILE;                                       // [TILE] ring entry of a new voxel, -1: direct
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_slot;
-  __shared__ int s_exit, s_abort;
+  __shared__ int s_abort, s_head, s_tail, s_exhausted;
 
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int part = tid >> 7, r = tid & (TILE - 1);
   // warp w reads TMEM lanes 32 (w % 4) .. + 31: the rows of its voxels
   const uint32_t lane_base = static_cast<uint32_t>((warp & 3) * 32) << 16;
+  const int n_mom = min(p.max_iter, MOM_SMEM);
 
   // ---- one-time setup: zero the A operand (pads stay zero), stage G's digits
   for (int i = tid; i < A_BYTES / 16; i += THREADS) reinterpret_cast<uint4*>(sA)[i] = make_uint4(0, 0, 0, 0);
   for (int i = tid; i < B_BYTES / 16; i += THREADS)
     reinterpret_cast<uint4*>(sB)[i] = reinterpret_cast<const uint4*>(p.gdig)[i];
   for (int i = tid; i < NB; i += THREADS) sF[i] = p.fexp[i];
+  for (int i = tid; i < n_mom; i += THREADS) sMom[i] = p.mom[i];
   if (tid < TILE) {
     sVid[tid] = -1;
     sOld[tid] = -1;
     sIt[tid] = 0;
     sNear[tid] = 0;
     sFin[tid] = 0;
+    sSrc[tid] = -1;
     sThr[tid] = p.thr;
   }
   if (warp == 0) {
@@ -254,8 +280,10 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    s_exit = 0;
     s_abort = 0;
+    s_head = 0;
+    s_tail = 0;
+    s_exhausted = 0;
   }
   fence_before();
   __syncthreads();
@@ -268,7 +296,6 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
   int e_vox = 0;          // exponent of this voxel's current digits
   uint32_t phase = 0;
   bool have_p = false;    // TMEM holds P for the current voxels
-  bool exhausted = false;
   unsigned long long executed = 0, n_batches = 0;
   const double tol = p.tol;
   const double lo_band = tol * (1.0 - p.band), hi_band = tol * (1.0 + p.band);
@@ -276,10 +303,13 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
 
   while (true) {
     const int64_t vid = sVid[r];
-    // ---- phase 1: FP64 update from P = G d (skipped before the first MMA)
-    if (have_p && vid >= 0) {
+    // ---- phase 1: FP64 update from P = G d (skipped before the first MMA).
+    // tcgen05.ld / wait::ld are .sync.aligned: every lane of the warp runs
+    // them, empty slots included; an empty slot's results are discarded (its
+    // x and d are cleared below and the stopping rule skips it).
+    if (have_p) {
       const int it = sIt[r];
-      const double mom_prev = it > 0 ? p.mom[it - 1] : 0.0;
+      const double mom_prev = it == 0 ? 0.0 : (it <= n_mom ? sMom[it - 1] : p.mom[it - 1]);
       const double thr = sThr[r];
       const double c = p.c_step;
       double dx2 = 0.0, xn2 = 0.0;
@@ -312,13 +342,14 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
       sDx[part * TILE + r] = dx2;
       sXn[part * TILE + r] = xn2;
     }
+    if (warp == PRODUCER_WARP) cp_async_wait_all();  // prefetched rows have landed
     fence_before();
-    __syncthreads();  // B1: partial norms visible; TMEM reads of this iteration done
+    __syncthreads();  // B1: partial norms and prefetched rows visible; TMEM reads done
 
     // ---- stopping rule, guard and refill decision (one thread per voxel)
     if (part == 0) {
       const int64_t v = sVid[r];
-      bool finish = false;
+      bool finish = false, write_out = true;
       if (have_p && v >= 0) {
         ++executed;
         const int it = sIt[r] + 1;
@@ -341,40 +372,57 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
         }
         if (flag) {
           // a stopping decision within the guard band: the FP64 kernel re-runs
-          // this voxel and overwrites its outputs, so it leaves the tile now
+          // this voxel and overwrites its outputs, so it leaves the tile now.
+          // Its X row is left untouched: a path fit warm-starts from X in
+          // place, and the re-run must start from the same point.
           const unsigned long long k = atomicAdd(p.n_flagged, 1ull);
           p.flagged[k] = v;
           finish = true;
+          write_out = false;
         }
       }
       sFin[r] = finish ? 1 : 0;
-      sOld[r] = finish ? v : -1;
-      if (finish || v < 0) {
-        // refill from the work queue
-        int64_t nv = -1;
-        if (!exhausted) {
-          const unsigned long long k = atomicAdd(p.queue, 1ull);
-          if (k < static_cast<unsigned long long>(p.n_work))
-            nv = p.list ? p.list[k] : static_cast<int64_t>(k);
-          else
-            exhausted = true;
+      sOld[r] = (finish && write_out) ? v : -1;
+      // refill: the next prefetched voxel, else straight from the work queue
+      const bool need = finish || v < 0;
+      const unsigned m = __ballot_sync(0xffffffffu, need);
+      if (m) {
+        const int leader = __ffs(m) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&s_head, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (need) {
+          const int pos = base + __popc(m & ((1u << lane) - 1u));
+          int64_t nv = -1;
+          int src = -1;
+          double thr = p.thr;
+          if (pos < s_tail) {
+            src = pos % RING;
+            nv = rVid[src];
+            thr = rThr[src];
+          } else if (!*reinterpret_cast<volatile int*>(&s_exhausted)) {
+            const unsigned long long k = atomicAdd(p.queue, 1ull);
+            if (k < static_cast<unsigned long long>(p.n_work)) {
+              nv = p.list ? p.list[k] : static_cast<int64_t>(k);
+              if (p.alpha_v) thr = p.step * p.alpha_v[nv];
+            } else {
+              atomicExch(&s_exhausted, 1);
+            }
+          }
+          sVid[r] = nv;
+          sSrc[r] = src;
+          sIt[r] = 0;
+          sNear[r] = 0;
+          sThr[r] = thr;
         }
-        sVid[r] = nv;
-        sIt[r] = 0;
-        sNear[r] = 0;
-        sThr[r] = (p.alpha_v && nv >= 0) ? p.step * p.alpha_v[nv] : p.thr;
       }
     }
     __syncthreads();  // B2
-    if (tid == 0) {
-      int any = 0;
-      for (int i = 0; i < TILE; ++i) any |= (sVid[i] >= 0);
-      s_exit = any ? 0 : 1;
-    }
+    if (tid == 0 && s_head > s_tail) s_head = s_tail;  // positions past the tail went to the queue
 
     // ---- write out finished voxels, load new ones, partial max |d|
     {
-      if (sFin[r]) {
+      if (sFin[r] && sOld[r] >= 0) {
         const int64_t ov = sOld[r];
 #pragma unroll
         for (int i = 0; i < CPT; ++i) p.X[ov * KC + coef_of(part, i)] = x[i];
@@ -392,17 +440,24 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
         }
       }
       if (fresh) {
-        // u = -b for the new voxel (a rolled loop: nothing held in registers).
-        // A warm start x_0 enters as d = x_0, so the first product gives
-        // u_0 = G x_0 - b and the first update sees y_0 = x_0.
-#pragma unroll 1
-        for (int i = 0; i < CPT; ++i) {
-          const int j = coef_of(part, i);
-          sU[j * TILE + r] = -p.B[nv * KC + j];
-        }
-        if (p.warm) {
+        // u = -b for the new voxel.  A warm start x_0 enters as d = x_0, so the
+        // first product gives u_0 = G x_0 - b and the first update sees y_0 = x_0.
+        const int src = sSrc[r];
+        if (src >= 0) {
 #pragma unroll
-          for (int i = 0; i < CPT; ++i) x[i] = d[i] = p.warm[nv * KC + coef_of(part, i)];
+          for (int i = 0; i < CPT; ++i) {
+            const int j = coef_of(part, i);
+            sU[j * TILE + r] = -rB[src * KC + j];
+            if (p.warm) x[i] = d[i] = rW[src * KC + j];
+          }
+        } else {
+          // direct loads (the first fill, or an empty ring): all in flight at once
+#pragma unroll
+          for (int i = 0; i < CPT; ++i) d[i] = p.B[nv * KC + coef_of(part, i)];
+#pragma unroll
+          for (int i = 0; i < CPT; ++i) sU[coef_of(part, i) * TILE + r] = -d[i];
+#pragma unroll
+          for (int i = 0; i < CPT; ++i) x[i] = d[i] = p.warm ? p.warm[nv * KC + coef_of(part, i)] : 0.0;
         }
       }
       unsigned mx = 0;
@@ -410,8 +465,8 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
       for (int i = 0; i < CPT; ++i) mx = max(mx, static_cast<unsigned>(__double2hiint(d[i])) & 0x7FFFFFFFu);
       sMax[part * TILE + r] = mx;
     }
-    __syncthreads();  // B3
-    if (s_exit) break;
+    const int any = __syncthreads_or(part == 0 && sVid[r] >= 0);  // B3
+    if (!any) break;
 
     // ---- digits of d (per-voxel exponent) into the A operand
     {
@@ -429,19 +484,19 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
           uint32_t t[4];
           planes4(digits(d[i], sc), digits(d[i + 1], sc), digits(d[i + 2], sc), digits(d[i + 3], sc), t);
 #pragma unroll
-          for (int s = 0; s < 4; ++s) pl[s][w4] = t[s];
+          for (int q = 0; q < 4; ++q) pl[q][w4] = t[q];
         }
         const int j0 = coef_of(part, 16 * g16);
 #pragma unroll
-        for (int s = 0; s < 4; ++s)
-          *reinterpret_cast<uint4*>(sA + a_off(r, s, j0)) = make_uint4(pl[s][0], pl[s][1], pl[s][2], pl[s][3]);
+        for (int q = 0; q < 4; ++q)
+          *reinterpret_cast<uint4*>(sA + a_off(r, q, j0)) = make_uint4(pl[q][0], pl[q][1], pl[q][2], pl[q][3]);
       }
       {
         uint32_t t[4];
         planes4(digits(d[32], sc), digits(d[33], sc), digits(d[34], sc), digits(d[35], sc), t);
         const int j0 = coef_of(part, 32);
 #pragma unroll
-        for (int s = 0; s < 4; ++s) *reinterpret_cast<uint32_t*>(sA + a_off(r, s, j0)) = t[s];
+        for (int q = 0; q < 4; ++q) *reinterpret_cast<uint32_t*>(sA + a_off(r, q, j0)) = t[q];
       }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -466,9 +521,39 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
                    : "memory");
       ++n_batches;
     }
+    // ---- while the products run: top the prefetch ring up (ids, thresholds,
+    // b rows and warm rows by cp.async; they are waited for before B1)
+    if (warp == PRODUCER_WARP && !*reinterpret_cast<volatile int*>(&s_exhausted)) {
+      const int head = s_head, tail = s_tail;
+      const int space = RING - (tail - head);
+      if (space > 0) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(p.queue, static_cast<unsigned long long>(space));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        const unsigned long long nw = static_cast<unsigned long long>(p.n_work);
+        const int ok = base >= nw ? 0 : static_cast<int>(min(static_cast<unsigned long long>(space), nw - base));
+        if (lane < ok) {
+          const int e = (tail + lane) % RING;
+          const int64_t nv = p.list ? p.list[base + lane] : static_cast<int64_t>(base + lane);
+          rVid[e] = nv;
+          rThr[e] = p.alpha_v ? p.step * p.alpha_v[nv] : p.thr;
+          for (int c = 0; c < KC / 2; ++c) {
+            cp_async16(rB + e * KC + 2 * c, p.B + nv * KC + 2 * c);
+            if (p.warm) cp_async16(rW + e * KC + 2 * c, p.warm + nv * KC + 2 * c);
+          }
+        }
+        cp_async_commit();
+        __syncwarp();
+        if (lane == 0) {
+          s_tail = tail + ok;
+          if (ok < space) s_exhausted = 1;
+        }
+      }
+    }
     // ---- wait for the products (bounded)
     uint32_t done = 0;
-    for (int spin = 0; spin < (1 << 24) && !done; ++spin) done = try_wait(&mbar, phase);
+    const uint64_t t_start = globaltimer_ns();
+    while (!done && globaltimer_ns() - t_start < kWaitNs) done = try_wait(&mbar, phase);
     if (!done) {
       s_abort = 1;
       atomicExch(p.error, 1);
@@ -479,16 +564,18 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
     __syncthreads();
     if (s_abort) break;
   }
+  if (warp == PRODUCER_WARP) cp_async_wait_all();
   if (s_abort && tid == 0) {
     // let any products still in flight land before the columns are freed
     uint32_t done = 0;
-    for (int spin = 0; spin < (1 << 24) && !done; ++spin) done = try_wait(&mbar, phase ^ 1u);
+    const uint64_t t_start = globaltimer_ns();
+    while (!done && globaltimer_ns() - t_start < kWaitNs) done = try_wait(&mbar, phase ^ 1u);
   }
 
   if (tid == 0 && p.batches) atomicAdd(p.batches, n_batches);
   if (p.iter_total && part == 0) {
     for (int o = 16; o > 0; o >>= 1) executed += __shfl_xor_sync(0xffffffffu, executed, o);
-    if ((tid & 31) == 0) atomicAdd(p.iter_total, executed);
+    if (lane == 0) atomicAdd(p.iter_total, executed);
   }
   fence_before();
   __syncthreads();
