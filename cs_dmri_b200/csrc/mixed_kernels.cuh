@@ -299,7 +299,11 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
   unsigned long long executed = 0, n_batches = 0;
   const double tol = p.tol;
   const double lo_band = tol * (1.0 - p.band), hi_band = tol * (1.0 + p.band);
-  const double pre = 4.0 * hi_band * hi_band;
+  // The stopping rule ||dx|| < tol max(||x||, 1e-12) (fista.rs:166-179) and
+  // the guard band, compared in squares: a rounding-level difference from the
+  // square-root form can only matter inside the band, where the FP64 kernel
+  // decides anyway.
+  const double tol2 = tol * tol, lo2 = lo_band * lo_band, hi2 = hi_band * hi_band;
 
   while (true) {
     const int64_t vid = sVid[r];
@@ -313,6 +317,7 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
       const double thr = sThr[r];
       const double c = p.c_step;
       double dx2 = 0.0, xn2 = 0.0;
+      unsigned mx = 0;
 #pragma unroll
       for (int g4 = 0; g4 < CPT / 4; ++g4) {  // 4-coefficient batches
         const int j0 = coef_of(part, 4 * g4);
@@ -335,12 +340,14 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
           const double dn = xn - x[i];
           dx2 = fma(dn, dn, dx2);
           xn2 = fma(xn, xn, xn2);
+          mx = max(mx, static_cast<unsigned>(__double2hiint(dn)) & 0x7FFFFFFFu);
           x[i] = xn;
           d[i] = dn;
         }
       }
       sDx[part * TILE + r] = dx2;
       sXn[part * TILE + r] = xn2;
+      sMax[part * TILE + r] = mx;
     }
     if (warp == PRODUCER_WARP) cp_async_wait_all();  // prefetched rows have landed
     fence_before();
@@ -354,16 +361,15 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
         ++executed;
         const int it = sIt[r] + 1;
         sIt[r] = it;
-        const double dx2 = sDx[r] + sDx[TILE + r], xn2 = sXn[r] + sXn[TILE + r];
-        double rel = 2.0 * hi_band;
-        if (!(dx2 > pre * fmax(xn2, 1e-24))) rel = sqrt(dx2) / fmax(sqrt(xn2), 1e-12);
-        const bool converged = rel < tol;  // fista.rs:166-179
+        const double dx2 = sDx[r] + sDx[TILE + r];
+        const double ref2 = fmax(sXn[r] + sXn[TILE + r], 1e-24);
+        const bool converged = dx2 < tol2 * ref2;
         bool flag;
         if (converged) {
-          flag = rel >= lo_band;
+          flag = dx2 >= lo2 * ref2;
         } else {
           flag = sNear[r] != 0;
-          sNear[r] = rel < hi_band ? 1 : 0;
+          sNear[r] = dx2 < hi2 * ref2 ? 1 : 0;
         }
         if (converged || it >= p.max_iter) {
           finish = true;
@@ -429,14 +435,14 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
       }
       const int64_t nv = sVid[r];
       const bool fresh = nv >= 0 && (sFin[r] || vid < 0);
-      {
-        // slots that keep their voxel keep x and d; new and empty slots start
-        // from zero (bitwise, so a non-finite finished voxel cannot leak)
-        const unsigned long long keep = (nv >= 0 && !fresh) ? ~0ull : 0ull;
+      const bool reset = fresh || nv < 0;  // slots that keep their voxel keep x and d
+      if (reset) {
+        // new and emptied slots start from zero (bitwise, so a non-finite
+        // finished voxel cannot leak into the next one)
 #pragma unroll
         for (int i = 0; i < CPT; ++i) {
-          x[i] = __longlong_as_double(__double_as_longlong(x[i]) & keep);
-          d[i] = __longlong_as_double(__double_as_longlong(d[i]) & keep);
+          x[i] = __longlong_as_double(0ll);
+          d[i] = __longlong_as_double(0ll);
         }
       }
       if (fresh) {
@@ -460,10 +466,12 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
           for (int i = 0; i < CPT; ++i) x[i] = d[i] = p.warm ? p.warm[nv * KC + coef_of(part, i)] : 0.0;
         }
       }
-      unsigned mx = 0;
+      if (reset) {  // continuing voxels wrote max |d| in phase 1
+        unsigned mx = 0;
 #pragma unroll
-      for (int i = 0; i < CPT; ++i) mx = max(mx, static_cast<unsigned>(__double2hiint(d[i])) & 0x7FFFFFFFu);
-      sMax[part * TILE + r] = mx;
+        for (int i = 0; i < CPT; ++i) mx = max(mx, static_cast<unsigned>(__double2hiint(d[i])) & 0x7FFFFFFFu);
+        sMax[part * TILE + r] = mx;
+      }
     }
     const int any = __syncthreads_or(part == 0 && sVid[r] >= 0);  // B3
     if (!any) break;
