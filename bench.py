@@ -3,7 +3,12 @@
 Workload: the brain-sized synthetic volume (96 x 114 x 96 grid, ellipsoidal
 mask of 299,432 voxels, CS-DSI table with N = 259, radial order 6 -> K = 72,
 zeta 700), L1 FISTA with a fixed alpha = 0.01 at the reference defaults
-(max_iter 1000, tol 1e-6), FP64.  One step = one whole-volume fit.
+(max_iter 1000, tol 1e-6).  One step = one whole-volume fit.  Both GPU paths
+run on the same volume: FP64 (the reference arithmetic, FISTA on FP64 DMMA
+tensor cores) and mixed (int8 digit-slice Gram products on tcgen05 tensor
+cores, FP64 state); `value` is the faster of the two, both being within the
+1e-5 coefficient tolerance of FP64 (the line states which, and the measured
+error of the mixed path against the FP64 path).
 
 * value   voxels/s with the volume already resident in HBM (device entry
           point), CUDA events on the fit stream, max over ranks.
@@ -43,14 +48,14 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "SHORE L1-fit voxels/s (FP64, radial order 6, fixed alpha 0.01)"
+METRIC = "SHORE L1-fit voxels/s, mixed vs FP64 GPU at <=1e-5 rel err"
 WORKLOAD = "brain300k"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU sample")
@@ -118,9 +123,14 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # the timed region starts only once the sampler is producing samples
+            t0 = time.perf_counter()
+            while not self.lines and time.perf_counter() - t0 < 10.0 and self.proc.poll() is None:
+                time.sleep(0.02)
+            self.start = len(self.lines)
         except OSError:
             self.proc = None
         return self
@@ -140,7 +150,8 @@ class ClockSampler:
     def summary(self):
         mhz, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = self.lines[max(0, getattr(self, "start", 0) - 1):]  # from the last sample before the region
+        for ln in lines:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
                 continue
@@ -192,7 +203,7 @@ def barrier(world: int):
 
 def traffic_from_profile():
     """Per-launch DRAM bytes of the FISTA kernel from the committed ncu summary."""
-    p = ROOT / "profiles" / "k_fista_fp64_brain300k.md"
+    p = ROOT / "profiles" / "k_fista_v3_brain300k.md"
     if not p.exists():
         return None
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
@@ -262,9 +273,10 @@ def run_ours(args):
     coeffs = torch.empty((X, Y, Z, K), dtype=torch.float32, device=f"cuda:{device}")
     stream = torch.cuda.Stream(device=device)
 
-    def device_step():
+    def device_step(precision="fp64"):
         c, res = shore_fit_device(d_data, d_mask, ph.bvals, ph.bvecs, coefficients=coeffs, stream=stream,
-                                  device=device, big_delta=ph.big_delta, small_delta=ph.small_delta, **kw)
+                                  device=device, big_delta=ph.big_delta, small_delta=ph.small_delta,
+                                  precision=precision, **kw)
         return res
 
     # ---- value: inputs resident in HBM (1.09 GB volume > 126 MB L2 per step)
@@ -292,6 +304,41 @@ def run_ours(args):
     V = int(ph.mask.sum())
     value = world * V * args.steps / (ms / 1e3)
 
+    # ---- the mixed-precision path on the same volume
+    for _ in range(args.warmup):
+        device_step("mixed")
+    torch.cuda.synchronize(device)
+    barrier(world)
+    mix_kernel_ms, mix_ops, mix_rerun, mix_launches = [], [], [], 0
+    with ClockSampler(device) as mix_clocks:
+        torch.cuda.synchronize(device)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            device_step("mixed")
+            tm = _abi.last_timing(device)
+            mix_kernel_ms.append(tm.ms_mixed_kernel)
+            mix_ops.append(tm.int8_tensor_ops)
+            mix_rerun.append(int(tm.fp64_rerun_voxels))
+            mix_launches += tm.launches
+        ev1.record(stream)
+        torch.cuda.synchronize(device)
+    ms_mix = max_over_ranks(ev0.elapsed_time(ev1), world, torch.device("cuda", device))
+    value_mix = world * V * args.steps / (ms_mix / 1e3)
+    # coefficient error of the mixed path against the FP64 path (FP64 outputs)
+    import numpy as np
+    common = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, device=device, return_coef64=True,
+                  diagnostics=True, **kw)
+    f64 = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, precision="fp64", **common)
+    mix = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, precision="mixed", **common)
+    a, b = mix["coef64"], f64["coef64"]
+    nz = np.linalg.norm(b, axis=1) > 0
+    per = np.linalg.norm(a - b, axis=1)[nz] / np.linalg.norm(b, axis=1)[nz]
+    err = {"global": float(np.linalg.norm(a - b) / np.linalg.norm(b)), "median": float(np.median(per)),
+           "p99": float(np.percentile(per, 99)), "max": float(per.max()),
+           "iterations_equal": float(np.mean(mix["iterations"][ph.mask] == f64["iterations"][ph.mask]))}
+    del f64, mix, a, b
+    path = "mixed" if value_mix > value and err["max"] <= 1e-5 else "fp64"
+
     # ---- e2e: host buffers through the C ABI (pinned host volume)
     pinned = torch.empty(ph.data.shape, dtype=torch.float32, pin_memory=True)
     pinned.numpy()[...] = ph.data
@@ -304,7 +351,8 @@ def run_ours(args):
         barrier(world)
         t = time.perf_counter()
         out = shore_fit(host_data, ph.bvals, ph.bvecs, ph.mask, big_delta=ph.big_delta,
-                        small_delta=ph.small_delta, device=device, coefficients_out=host_out, **kw)
+                        small_delta=ph.small_delta, device=device, coefficients_out=host_out, precision=path,
+                        **kw)
         dt = time.perf_counter() - t
         if i >= args.warmup:
             e2e_t.append(dt)
@@ -330,13 +378,29 @@ def run_ours(args):
                "sample": f"{count} of the {V} masked voxels ({t:.1f} s, CPU FP64 oracle on all host threads)"}
 
     if rank == 0:
+        mk_ms = statistics.median(mix_kernel_ms)
+        paths = {
+            "fp64": {"value": value, "unit": "voxels/s", "ms_per_step": ms / args.steps,
+                     "kernel": "k_fista_v3<9,16> (FP64 DMMA mma.sync.m8n8k4)", "kernel_ms": statistics.median(kernel_ms),
+                     "gpu_launches": launches},
+            "mixed": {"value": value_mix, "unit": "voxels/s", "ms_per_step": ms_mix / args.steps,
+                      "speedup_vs_fp64": value_mix / value,
+                      "kernel": "k_fista_i8 (tcgen05.mma kind::i8, 36 MMAs 128x80x32 per iteration)",
+                      "kernel_ms": mk_ms, "int8_tensor_ops_per_launch": statistics.median(mix_ops),
+                      "executed_int8_tops": statistics.median(mix_ops) / (mk_ms * 1e-3) / 1e12 if mk_ms else None,
+                      "fp64_rerun_voxels": statistics.median(mix_rerun),
+                      "coef_rel_err_vs_fp64": err, "gpu_launches": mix_launches,
+                      "clocks": mix_clocks.summary()},
+        }
         line = {
-            "metric": METRIC, "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64",
+            "metric": METRIC, "value": value if path == "fp64" else value_mix, "unit": "voxels/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": (ms if path == "fp64" else ms_mix) / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if path == "fp64" else "s8 digit-slice products, f64 state",
             "data": "synthetic (seeded CS-DSI multi-tensor phantom, S0 1000, SNR 25)",
             "config": {"workload": WORKLOAD, "voxels": V, "grid": [X, Y, Z], "N": N, "K": K, "alpha": 0.01,
-                       "solver": "FISTA fixed alpha, FP64 (reference stopping rule)",
+                       "solver": "FISTA fixed alpha (reference stopping rule)", "path": path,
                        "l2": "inputs larger than L2 (1.09 GB volume per step)",
                        "parallelism": f"{world} independent volume(s), one per GPU"},
             "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -350,7 +414,8 @@ def run_ours(args):
                          "executed_tensor_frac": (executed / dmma_peak) if dmma_peak else None,
                          "peak_source": "FP64 DMMA microbenchmark measured in this run (libcsdpeak); "
                                         f"scalar DFMA measured {dfma_peak:.1f} TFLOP/s" if dmma_peak else None},
-            "gpu_launches": launches,
+            "gpu_launches": launches if path == "fp64" else mix_launches,
+            "paths": paths,
             "clocks": clocks.summary(),
             "iterations_per_voxel": it_launch / V,
         }
