@@ -66,6 +66,13 @@ def lib() -> C.CDLL:
             "oracle_bic": (d, [i32, d, i32]),
             "oracle_shore_fit_volume": (C.c_int, [p, p, C.c_int64, C.c_int64, C.c_int64, p, p, p, i32, p,
                                                   C.c_size_t]),
+            "oracle_shore_predict": (C.c_int, [p, C.c_int64, C.c_int64, C.c_int64, i32, d, p, p, p, C.c_size_t]),
+            "oracle_shore_odf_sh": (C.c_int, [p, C.c_int64, C.c_int64, C.c_int64, i32, d, i32, p, p, p,
+                                              C.c_size_t]),
+            "oracle_shore_microstructure": (C.c_int, [p, C.c_int64, C.c_int64, C.c_int64, i32, d, p, p, i32, i32,
+                                                      C.c_float, p, p, p, p, p, p, p, C.c_size_t]),
+            "oracle_microstructure_voxel": (None, [p, i32, d, p, p]),
+            "oracle_micro_alpha_factor": (d, [C.c_uint32, C.c_uint32, d]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -292,3 +299,70 @@ def shore_fit(data, bvals, bvecs, mask, *, n_threads: int = 0, big_delta=None, s
 
 def cpu_count() -> int:
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+# ------------------------------------------------ synth / odf / scalars
+
+def _coeff_volume(coefficients, radial_order):
+    c = np.ascontiguousarray(np.asarray(coefficients, dtype=np.float32))
+    if c.ndim != 4 or c.shape[3] != n_coeffs(radial_order):
+        raise ValueError(f"coefficients have {c.shape[-1]} channels but a radial-order-{radial_order} SHORE "
+                         f"basis has {n_coeffs(radial_order)}")
+    return c
+
+
+def shore_predict(coefficients, radial_order, zeta, bvals, bvecs, *, big_delta=None, small_delta=None):
+    """synthesize_volume (synth.rs:15-84) through the binding's gradient table."""
+    c = _coeff_volume(coefficients, radial_order)
+    g, keep = _gtab(bvals, bvecs, big_delta, small_delta, 50.0)
+    X, Y, Z, _ = c.shape
+    out = np.zeros((X, Y, Z, g.n), np.float32)
+    err = C.create_string_buffer(1024)
+    if lib().oracle_shore_predict(_p(c), X, Y, Z, radial_order, zeta, C.addressof(g), _p(out), err, len(err)):
+        raise ValueError(err.value.decode())
+    return out
+
+
+def shore_odf_sh(coefficients, radial_order, zeta, lmax, mask=None):
+    """shore_odf_sh (python/src/models.rs:201-250)."""
+    c = _coeff_volume(coefficients, radial_order)
+    X, Y, Z, _ = c.shape
+    nsh = (lmax + 1) * (lmax + 2) // 2
+    out = np.zeros((X, Y, Z, nsh), np.float32)
+    m = None if mask is None else np.ascontiguousarray(np.asarray(mask, bool)).view(np.uint8)
+    err = C.create_string_buffer(1024)
+    if lib().oracle_shore_odf_sh(_p(c), X, Y, Z, radial_order, zeta, lmax, None if m is None else _p(m), _p(out),
+                                 err, len(err)):
+        raise ValueError(err.value.decode())
+    return out
+
+
+def shore_microstructure(coefficients, radial_order, zeta, mask, directions=None, *, units="um",
+                         outlier_factor=10.0):
+    """shore_microstructure (python/src/models.rs:283-341)."""
+    c = _coeff_volume(coefficients, radial_order)
+    X, Y, Z, _ = c.shape
+    m = np.ascontiguousarray(np.asarray(mask, bool)).view(np.uint8)
+    d = None if directions is None else np.ascontiguousarray(np.asarray(directions, np.float32))
+    maps = {k: np.zeros((X, Y, Z), np.float32) for k in ("rtop", "rtap", "rtpp", "msd", "qiv", "ng")}
+    err = C.create_string_buffer(1024)
+    reject = outlier_factor is not None
+    code = lib().oracle_shore_microstructure(
+        _p(c), X, Y, Z, radial_order, zeta, _p(m), None if d is None else _p(d), 1 if units == "mm" else 0,
+        int(reject), float(outlier_factor if reject else 0.0), *(_p(maps[k]) for k in maps), err, len(err))
+    if code:
+        raise ValueError(err.value.decode())
+    return maps
+
+
+def microstructure_voxel(coefs, radial_order, zeta, direction=None):
+    """{rtop, msd, qiv, ng, rtap, rtpp} of one FP64 coefficient vector."""
+    c = _f64(coefs)
+    out = np.zeros(6)
+    dp = None if direction is None else _f64(direction)
+    lib().oracle_microstructure_voxel(_p(c), radial_order, zeta, None if dp is None else _p(dp), _p(out))
+    return dict(zip(("rtop", "msd", "qiv", "ng", "rtap", "rtpp"), out))
+
+
+def micro_alpha_factor(n, l, zeta):
+    return lib().oracle_micro_alpha_factor(n, l, zeta)

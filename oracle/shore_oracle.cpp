@@ -1517,3 +1517,333 @@ int oracle_shore_fit_volume(const float* data, const uint8_t* mask, int64_t X, i
 }
 
 }  // extern "C"
+
+
+// ------------------------------------------------- synth.rs / odf projection
+
+namespace {
+
+// y = A c with A (R x K) and the products summed in column order, as the
+// reference's gemv / per-row loop (synth.rs:60, models.rs:238-243).
+void apply_rows(const Mat& A, const double* c, double* y) {
+  for (int i = 0; i < A.rows; ++i) {
+    double acc = 0.0;
+    for (int k = 0; k < A.cols; ++k) acc += A(i, k) * c[k];
+    y[i] = acc;
+  }
+}
+
+}  // namespace
+
+int oracle_shore_predict(const float* coeffs, int64_t X, int64_t Y, int64_t Z, int32_t radial_order,
+                         double zeta, const csd_gtab* target, float* out, char* err, size_t err_len) {
+  try {
+    const Gtab g = make_gtab(target);
+    const Mat M = design_matrix(g, radial_order, zeta);
+    const int K = M.cols, N = M.rows;
+    std::vector<double> c(K), y(N);
+    for (int64_t v = 0; v < X * Y * Z; ++v) {
+      const float* cv = coeffs + v * K;
+      float* ov = out + v * N;
+      bool any = false;
+      for (int k = 0; k < K; ++k) any |= (cv[k] != 0.0f);  // synth.rs:55-58
+      if (!any) {
+        for (int t = 0; t < N; ++t) ov[t] = 0.0f;
+        continue;
+      }
+      for (int k = 0; k < K; ++k) c[k] = static_cast<double>(cv[k]);
+      apply_rows(M, c.data(), y.data());
+      for (int t = 0; t < N; ++t) ov[t] = static_cast<float>(y[t]);
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    set_err(err, err_len, e.what());
+    return 1;
+  }
+}
+
+int oracle_shore_odf_sh(const float* coeffs, int64_t X, int64_t Y, int64_t Z, int32_t radial_order,
+                        double zeta, int32_t lmax, const uint8_t* mask, float* out, char* err,
+                        size_t err_len) {
+  try {
+    const Mat P = shore_to_tournier(radial_order, zeta, lmax);
+    const int K = P.cols, R = P.rows;
+    std::vector<double> c(K), y(R);
+    for (int64_t v = 0; v < X * Y * Z; ++v) {
+      float* ov = out + v * R;
+      if (mask && !mask[v]) {
+        for (int i = 0; i < R; ++i) ov[i] = 0.0f;
+        continue;
+      }
+      for (int k = 0; k < K; ++k) c[k] = static_cast<double>(coeffs[v * K + k]);
+      apply_rows(P, c.data(), y.data());
+      for (int i = 0; i < R; ++i) ov[i] = static_cast<float>(y[i]);
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    set_err(err, err_len, e.what());
+    return 1;
+  }
+}
+
+// ------------------------------------------------ scalars/microstructure.rs
+
+namespace {
+
+double binomial_float(double n, uint32_t k) {  // math.rs:150-152
+  return gamma_fn(n + 1.0) / (factorial(k) * gamma_fn(n - static_cast<double>(k) + 1.0));
+}
+
+struct NlBlock {
+  int n, l, start, len;
+};
+
+std::vector<NlBlock> nl_blocks(int radial_order) {  // microstructure.rs:42-58
+  std::vector<NlBlock> b;
+  int start = 0;
+  for (int n = 0; n <= radial_order; ++n)
+    for (int l = 0; l <= n; l += 2) {
+      b.push_back({n, l, start, 2 * l + 1});
+      start += 2 * l + 1;
+    }
+  return b;
+}
+
+int n00_index(const std::vector<NlBlock>& b, int n) {  // microstructure.rs:62-71
+  for (const auto& x : b)
+    if (x.n == n && x.l == 0) return x.start;
+  return -1;
+}
+
+// Ê(0) = sum_n c_(n,0,0) kappa(n, 0) L_n^(1/2)(0) / sqrt(4 pi) (:76-88).
+double predict_e0(const double* c, int radial_order, double zeta, const std::vector<NlBlock>& b) {
+  double e0 = 0.0;
+  const double inv = 1.0 / std::sqrt(4.0 * kPi);
+  for (int n = 0; n <= radial_order; ++n) {
+    const double r0 = kappa(zeta, n, 0) * gen_laguerre(n, 0.5, 0.0);
+    e0 += c[n00_index(b, n)] * r0 * inv;
+  }
+  return e0;
+}
+
+double alpha_factor(uint32_t n, uint32_t l, double zeta) {  // :272-278
+  const double sign = ((l / 2) % 2 == 0) ? 1.0 : -1.0;
+  const double num = 2.0 * kPi * std::pow(zeta, 1.5) * gamma_fn(static_cast<double>(n) + 1.5);
+  const double den = std::pow(2.0, static_cast<int>(l)) * factorial(n - l);
+  return sign * std::sqrt(num / den);
+}
+
+double rtap_kappa(uint32_t j, uint32_t l) {  // :284-298
+  const double jf = j, lf = l;
+  const double kap = std::pow(-1.0, static_cast<int>(j) - 1) * std::pow(2.0, -(lf + 3.0) / 2.0) / kPi;
+  double sum = 0.0;
+  for (uint32_t k = 0; k < j; ++k) {
+    const double kf = k;
+    const double sign = (k % 2 == 0) ? 1.0 : -1.0;
+    const double bin = binomial_float(jf + lf - 0.5, j - k - 1);
+    const double g = gamma_fn((lf + 1.0) / 2.0 + kf);
+    const double hp = std::pow(0.5, (lf + 1.0) / 2.0 + kf);
+    sum += sign * bin * g / (factorial(k) * hp);
+  }
+  return 2.0 * kap * sum;
+}
+
+double rtpp_kappa(uint32_t j, uint32_t l) {  // :301-315
+  const double jf = j, lf = l;
+  const double pre = std::pow(-0.5, lf / 2.0) / std::sqrt(kPi);
+  double sum = 0.0;
+  for (uint32_t k = 0; k < j; ++k) {
+    const double kf = k;
+    const double sign = (k % 2 == 0) ? 1.0 : -1.0;
+    const double bin = binomial_float(jf + lf - 0.5, j - k - 1);
+    const double g = gamma_fn(lf / 2.0 + kf + 0.5);
+    const double hp = std::pow(0.5, lf / 2.0 + 0.5 + kf);
+    sum += sign * bin * g / (factorial(k) * hp);
+  }
+  return pre * sum;
+}
+
+// RTAP (rtap = true) / RTPP along `dir` (:209-270).
+double direction_scalar(const double* c, int radial_order, double zeta, const std::vector<NlBlock>& b,
+                        const double* dir, bool rtap) {
+  if (!dir) return std::nan("");
+  const double norm = std::sqrt(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+  if (!std::isfinite(norm) || norm == 0.0) return std::nan("");
+  const double e0 = predict_e0(c, radial_order, zeta, b);
+  if (!std::isfinite(e0) || e0 == 0.0) return std::nan("");
+  const double inv = 1.0 / norm;
+  double r, theta, phi;
+  cart2sphere(dir[0] * inv, dir[1] * inv, dir[2] * inv, &r, &theta, &phi);
+  double acc = 0.0;
+  double sh[32];
+  for (const auto& blk : b) {
+    const uint32_t j = static_cast<uint32_t>(blk.n - blk.l + 1);
+    const double kern = rtap ? rtap_kappa(j, blk.l) : rtpp_kappa(j, blk.l);
+    if (kern == 0.0) continue;
+    const double scale = kern / alpha_factor(blk.n, blk.l, zeta);
+    brainsuite_sh_block(blk.l, theta, phi, sh);
+    double inner = 0.0;
+    for (int k = 0; k < blk.len; ++k) inner += (c[blk.start + k] / e0) * sh[k];
+    acc += scale * inner;
+  }
+  const double mu = 1.0 / (2.0 * kPi * std::sqrt(zeta));
+  const double pre = rtap ? 1.0 / (mu * mu) : 1.0 / mu;
+  return std::max(pre * acc, 0.0);
+}
+
+void micro_voxel(const double* c, int K, int radial_order, double zeta, const std::vector<NlBlock>& b,
+                 const double* dir, double* out) {
+  const double nan = std::nan("");
+  const double e0 = predict_e0(c, radial_order, zeta, b);
+  const bool bad = !std::isfinite(e0) || e0 == 0.0;
+  // RTOP (:98-118)
+  double rtop = nan;
+  if (!bad) {
+    double acc = 0.0;
+    for (int n = 0; n <= radial_order; ++n) {
+      const double cn = c[n00_index(b, n)] / e0;
+      const double sign = (n % 2 == 0) ? 1.0 : -1.0;
+      const double w = std::sqrt(16.0 * kPi * std::pow(zeta, 1.5) * gamma_fn(n + 1.5) / factorial(n));
+      acc += cn * sign * w;
+    }
+    rtop = std::max(acc, 0.0);
+  }
+  // MSD (:122-140)
+  double msd = nan;
+  if (!bad) {
+    double acc = 0.0;
+    for (int n = 0; n <= radial_order; ++n) {
+      const double cn = c[n00_index(b, n)] / e0;
+      const double sign = (n % 2 == 0) ? 1.0 : -1.0;
+      const double w = std::sqrt(9.0 * gamma_fn(n + 1.5) /
+                                 (8.0 * std::pow(kPi, 6) * std::pow(zeta, 3.5) * factorial(n)));
+      const double hyp = hyp2f1(-static_cast<double>(n), 2.5, 1.5, 2.0);
+      acc += cn * sign * w * hyp;
+    }
+    msd = std::max(acc, 0.0);
+  }
+  // QIV (:155-182)
+  double qiv = nan;
+  if (!bad) {
+    const double pre = 6.0 * std::sqrt(2.0 * kPi) * std::pow(zeta, 2.5);
+    double q2i = 0.0;
+    for (int n = 0; n <= radial_order; ++n) {
+      const double cn = c[n00_index(b, n)] / e0;
+      q2i += cn * kappa(zeta, n, 0) * gamma_fn(n + 1.5) / factorial(n) *
+             hyp2f1(-static_cast<double>(n), 2.5, 1.5, 2.0);
+    }
+    const double q2 = pre * q2i;
+    if (std::isfinite(q2) && q2 > 0.0) qiv = 1.0 / q2;
+  }
+  // NG (:186-198)
+  double ng = nan;
+  if (!bad) {
+    double total = 0.0;
+    for (int k = 0; k < K; ++k) {
+      const double cn = c[k] / e0;
+      total += cn * cn;
+    }
+    if (total == 0.0) {
+      ng = 0.0;
+    } else {
+      const double c0 = c[0] / e0;
+      ng = std::sqrt(std::max(1.0 - (c0 * c0) / total, 0.0));
+    }
+  }
+  out[0] = rtop;
+  out[1] = msd;
+  out[2] = qiv;
+  out[3] = ng;
+  out[4] = direction_scalar(c, radial_order, zeta, b, dir, true);
+  out[5] = direction_scalar(c, radial_order, zeta, b, dir, false);
+}
+
+// Nearest-rank percentile of the finite values (io/microstructure.rs:303-313).
+bool percentile_value(const std::vector<float>& xs, double percentile, float* out) {
+  std::vector<float> f;
+  for (float v : xs)
+    if (std::isfinite(v)) f.push_back(v);
+  if (f.empty()) return false;
+  std::sort(f.begin(), f.end());
+  const size_t n = f.size();
+  const double p = std::min(std::max(percentile, 0.0), 100.0) / 100.0;
+  const size_t idx = std::min(static_cast<size_t>(std::round(p * static_cast<double>(n - 1))), n - 1);
+  *out = f[idx];
+  return true;
+}
+
+}  // namespace
+
+void oracle_microstructure_voxel(const double* coefs, int32_t radial_order, double zeta, const double* dir,
+                                 double* out) {
+  const auto b = nl_blocks(radial_order);
+  const int K = static_cast<int>(shore_indices(radial_order).size());
+  micro_voxel(coefs, K, radial_order, zeta, b, dir, out);
+}
+
+double oracle_micro_alpha_factor(uint32_t n, uint32_t l, double zeta) { return alpha_factor(n, l, zeta); }
+
+int oracle_shore_microstructure(const float* coeffs, int64_t X, int64_t Y, int64_t Z, int32_t radial_order,
+                                double zeta, const uint8_t* mask, const float* directions, int32_t units,
+                                int32_t reject, float outlier_factor, float* rtop, float* rtap, float* rtpp,
+                                float* msd, float* qiv, float* ng, char* err, size_t err_len) {
+  try {
+    const int K = static_cast<int>(shore_indices(radial_order).size());
+    const auto b = nl_blocks(radial_order);
+    // unit scales (io/microstructure.rs:162-173): rtop, rtap, rtpp, msd, qiv, ng
+    const float sc_um[6] = {1e-9f, 1e-6f, 1e-3f, 1e6f, 1e15f, 1.0f};
+    const float sc_mm[6] = {1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f};
+    const float* sc = units == 1 ? sc_mm : sc_um;
+    const int64_t nvox = X * Y * Z;
+    std::vector<int64_t> idx;
+    for (int64_t v = 0; v < nvox; ++v)
+      if (mask[v]) idx.push_back(v);
+    std::vector<float> s[6];  // rtop, rtap, rtpp, msd, qiv, ng (masked order)
+    for (auto& a : s) a.resize(idx.size());
+    std::vector<double> c(K);
+    double out[6];
+    for (size_t i = 0; i < idx.size(); ++i) {
+      const int64_t v = idx[i];
+      for (int k = 0; k < K; ++k) c[k] = static_cast<double>(coeffs[v * K + k]);
+      double dir[3];
+      const double* dp = nullptr;
+      if (directions) {
+        const float* d = directions + v * 3;
+        const bool any = d[0] != 0.0f || d[1] != 0.0f || d[2] != 0.0f;
+        const bool fin = std::isfinite(d[0]) && std::isfinite(d[1]) && std::isfinite(d[2]);
+        if (any && fin) {
+          dir[0] = d[0];
+          dir[1] = d[1];
+          dir[2] = d[2];
+          dp = dir;
+        }
+      }
+      micro_voxel(c.data(), K, radial_order, zeta, b, dp, out);
+      // out = {rtop, msd, qiv, ng, rtap, rtpp}; f64 -> f32, then the f32 unit scale
+      s[0][i] = static_cast<float>(out[0]) * sc[0];
+      s[1][i] = static_cast<float>(out[4]) * sc[1];
+      s[2][i] = static_cast<float>(out[5]) * sc[2];
+      s[3][i] = static_cast<float>(out[1]) * sc[3];
+      s[4][i] = static_cast<float>(out[2]) * sc[4];
+      s[5][i] = static_cast<float>(out[3]) * sc[5];
+    }
+    if (reject) {  // io/microstructure.rs:222-270 and nan_above (:317-326)
+      for (auto& a : s) {
+        float p99;
+        if (!percentile_value(a, 99.0, &p99)) continue;
+        const float thr = outlier_factor * p99;
+        for (float& v : a)
+          if (std::isfinite(v) && v > thr) v = std::nanf("");
+      }
+    }
+    float* maps[6] = {rtop, rtap, rtpp, msd, qiv, ng};
+    for (int m = 0; m < 6; ++m) {
+      for (int64_t v = 0; v < nvox; ++v) maps[m][v] = 0.0f;
+      for (size_t i = 0; i < idx.size(); ++i) maps[m][idx[i]] = s[m][i];
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    set_err(err, err_len, e.what());
+    return 1;
+  }
+}

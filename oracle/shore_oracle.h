@@ -85,6 +85,33 @@ int oracle_shore_fit_volume(const float* data, const uint8_t* mask, int64_t X, i
 
 void oracle_default_spec(csd_shore_spec* spec);
 
+/* synth.rs:15-84 / python/src/models.rs:252-278: signal of a coefficient
+ * volume (X, Y, Z, K) f32 on a new gradient table -> (X, Y, Z, N) f32. */
+int oracle_shore_predict(const float* coeffs, int64_t X, int64_t Y, int64_t Z, int32_t radial_order,
+                         double zeta, const csd_gtab* target, float* out, char* err, size_t err_len);
+
+/* python/src/models.rs:201-250 with odf.rs:79-102: Tournier-ordered ODF SH
+ * coefficients (X, Y, Z, (lmax+1)(lmax+2)/2) f32; mask may be NULL. */
+int oracle_shore_odf_sh(const float* coeffs, int64_t X, int64_t Y, int64_t Z, int32_t radial_order,
+                        double zeta, int32_t lmax, const uint8_t* mask, float* out, char* err,
+                        size_t err_len);
+
+/* scalars/microstructure.rs + io/microstructure.rs:155-298 as exposed by
+ * python/src/models.rs:283-341: six (X, Y, Z) f32 maps, zero outside the
+ * mask.  units 0 = um, 1 = mm; reject != 0 applies the p99 outlier rule with
+ * factor `outlier_factor`.  directions (X, Y, Z, 3) f32 may be NULL. */
+int oracle_shore_microstructure(const float* coeffs, int64_t X, int64_t Y, int64_t Z,
+                                int32_t radial_order, double zeta, const uint8_t* mask,
+                                const float* directions, int32_t units, int32_t reject,
+                                float outlier_factor, float* rtop, float* rtap, float* rtpp,
+                                float* msd, float* qiv, float* ng, char* err, size_t err_len);
+
+/* Per-voxel scalars of one FP64 coefficient vector (scalars/microstructure.rs):
+ * out = {rtop, msd, qiv, ng, rtap, rtpp}; dir may be NULL (RTAP/RTPP NaN). */
+void oracle_microstructure_voxel(const double* coefs, int32_t radial_order, double zeta,
+                                 const double* dir, double* out);
+double oracle_micro_alpha_factor(uint32_t n, uint32_t l, double zeta);
+
 #ifdef __cplusplus
 }
 #endif
