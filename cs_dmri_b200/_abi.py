@@ -114,6 +114,9 @@ EXPORTS = (
     "csd_shore_design_matrix",
     "csd_last_timing",
     "csd_shore_fista_batch_noalloc",
+    "csd_shore_predict",
+    "csd_shore_odf_sh",
+    "csd_shore_microstructure",
 )
 
 _lib = None
@@ -147,6 +150,14 @@ def _declare(lib: C.CDLL) -> C.CDLL:
     lib.csd_shore_fista_batch_noalloc.restype = C.c_int
     lib.csd_shore_fista_batch_noalloc.argtypes = [C.POINTER(Gtab), C.POINTER(Spec), C.c_void_p, C.c_int64,
                                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]
+    vol = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_double]
+    lib.csd_shore_predict.restype = C.c_int
+    lib.csd_shore_predict.argtypes = vol + [C.POINTER(Gtab), C.c_void_p, C.c_char_p, C.c_size_t]
+    lib.csd_shore_odf_sh.restype = C.c_int
+    lib.csd_shore_odf_sh.argtypes = vol + [C.c_int32, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]
+    lib.csd_shore_microstructure.restype = C.c_int
+    lib.csd_shore_microstructure.argtypes = vol + [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_float] + \
+        [C.c_void_p] * 6 + [C.c_char_p, C.c_size_t]
     return lib
 
 

@@ -291,3 +291,92 @@ def design_matrix(bvals, bvecs, radial_order=6, zeta=700.0, *, big_delta=None, s
     del keep
     _abi.check(code, err)
     return out
+
+
+# ------------------------------------------------------------ post-fit maps
+
+def _coefficient_volume(coefficients, radial_order):
+    c = np.asarray(coefficients)
+    if c.ndim != 4:
+        raise ValueError(f"coefficients must be 4-D (X, Y, Z, K), got shape {c.shape}")
+    K = _abi.load().csd_shore_n_coeffs(int(radial_order))
+    if c.shape[3] != K:  # python/src/models.rs:216-222
+        raise ValueError(f"coefficients have {c.shape[3]} channels but a radial-order-{radial_order} SHORE basis "
+                         f"has {K}")
+    return np.ascontiguousarray(c, dtype=np.float32)
+
+
+def shore_predict(coefficients, radial_order, zeta, bvals, bvecs, *, big_delta=None, small_delta=None,
+                  n_threads=None, device: int = 0):
+    """Signal of a coefficient volume on a new gradient table, (X, Y, Z, N)
+    float32 (``_cs_dmri.shore_predict``, python/src/models.rs:252-278, over
+    synthesize_volume, src/synth.rs:15-84).  ``n_threads`` is accepted and
+    ignored (the work runs on CUDA device ``device``)."""
+    c = _coefficient_volume(coefficients, radial_order)
+    g, keep = build_gtab(bvals, bvecs, 50.0, big_delta, small_delta)
+    X, Y, Z, _ = c.shape
+    out = np.empty((X, Y, Z, g.n), np.float32)
+    err = C.create_string_buffer(4096)
+    code = _abi.load().csd_shore_predict(_abi.handle(device), c.ctypes.data, X, Y, Z, int(radial_order),
+                                         float(zeta), C.byref(g), out.ctypes.data, err, len(err))
+    del keep
+    _abi.check(code, err)
+    return out
+
+
+def shore_odf_sh(coefficients, radial_order, zeta, lmax, mask=None, *, n_threads=None, device: int = 0):
+    """Tournier-ordered ODF SH coefficients, (X, Y, Z, (lmax+1)(lmax+2)/2)
+    float32, zeros outside ``mask`` (``_cs_dmri.shore_odf_sh``,
+    python/src/models.rs:201-250; projection of src/odf.rs:79-102)."""
+    if lmax % 2 != 0 or lmax > radial_order:
+        raise ValueError(f"lmax must be even and \u2264 radial_order ({radial_order}), got {lmax}")
+    c = _coefficient_volume(coefficients, radial_order)
+    X, Y, Z, _ = c.shape
+    m8 = None
+    if mask is not None:
+        m = np.asarray(mask)
+        if m.shape != (X, Y, Z):
+            raise ValueError("mask does not match the coefficient grid")
+        m8 = np.ascontiguousarray(m.astype(bool)).view(np.uint8)
+    out = np.empty((X, Y, Z, (lmax + 1) * (lmax + 2) // 2), np.float32)
+    err = C.create_string_buffer(4096)
+    code = _abi.load().csd_shore_odf_sh(_abi.handle(device), c.ctypes.data, X, Y, Z, int(radial_order), float(zeta),
+                                        int(lmax), None if m8 is None else m8.ctypes.data, out.ctypes.data, err,
+                                        len(err))
+    _abi.check(code, err)
+    return out
+
+
+_MICRO = ("rtop", "rtap", "rtpp", "msd", "qiv", "ng")
+
+
+def shore_microstructure(coefficients, radial_order, zeta, mask, directions=None, *, units="um",
+                         outlier_factor=10.0, n_threads=None, device: int = 0):
+    """RTOP, RTAP, RTPP, MSD, QIV and NG maps (zero outside ``mask``; NaN
+    where a value is rejected as a fit failure, ``outlier_factor`` x its p99;
+    ``outlier_factor=None`` keeps every value).  RTAP / RTPP need
+    ``directions`` (X, Y, Z, 3) in the coefficients' frame and are NaN where
+    a direction is zero or missing (``_cs_dmri.shore_microstructure``,
+    python/src/models.rs:283-341; src/io/microstructure.rs:155-298)."""
+    if units not in ("um", "mm"):
+        raise ValueError(f"units must be 'um' or 'mm', got {units!r}")
+    c = _coefficient_volume(coefficients, radial_order)
+    X, Y, Z, _ = c.shape
+    m = np.asarray(mask)
+    if m.shape != (X, Y, Z):
+        raise ValueError("mask does not match the coefficient grid")
+    m8 = np.ascontiguousarray(m.astype(bool)).view(np.uint8)
+    d = None
+    if directions is not None:
+        d = np.ascontiguousarray(np.asarray(directions, dtype=np.float32))
+        if d.shape != (X, Y, Z, 3):
+            raise ValueError(f"directions must have shape {(X, Y, Z, 3)}, got {d.shape}")
+    maps = {k: np.empty((X, Y, Z), np.float32) for k in _MICRO}
+    err = C.create_string_buffer(4096)
+    reject = outlier_factor is not None
+    code = _abi.load().csd_shore_microstructure(
+        _abi.handle(device), c.ctypes.data, X, Y, Z, int(radial_order), float(zeta), m8.ctypes.data,
+        None if d is None else d.ctypes.data, 0 if units == "um" else 1, int(reject),
+        float(outlier_factor) if reject else 0.0, *(maps[k].ctypes.data for k in _MICRO), err, len(err))
+    _abi.check(code, err)
+    return maps

@@ -38,6 +38,7 @@
 #include "solve_kernels.cuh"
 #include "icls_kernels.cuh"
 #include "mixed_kernels.cuh"
+#include "epilogue_kernels.cuh"
 
 namespace {
 
@@ -268,6 +269,7 @@ struct csd_handle {
   DevBuf amax, zero, alpha_v, Xsel, Xfb, Xl2, rss_l2, list, active, pbest, psel, pact, palpha_sel,
       pit_sel, pconv_sel, palpha_fb, pit_fb, pconv_fb, pcode;
   DevBuf flagged, mixstat;  // guard re-run list; [n_flagged, batches, error]
+  DevBuf pcoef, pmat, pout, pgt, pgv, pdir, pconst;  // post-fit maps
   double mixed_ms = 0.0, mixed_ops = 0.0;
   unsigned long long mixed_rerun = 0;
 };
@@ -1503,6 +1505,191 @@ int csd_shore_design_matrix(csd_handle* h, const csd_gtab* gtab, int32_t radial_
     ensure_setup(h, g, radial_order, zeta, false, 0.0, 0.0);
     CSD_CUDA(cudaMemcpyAsync(out, h->M.p, sizeof(double) * h->N * h->K, cudaMemcpyDeviceToHost, h->stream));
     CSD_CUDA(cudaStreamSynchronize(h->stream));
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+void check_coeff_args(int64_t X, int64_t Y, int64_t Z, int32_t radial_order) {
+  if (X < 0 || Y < 0 || Z < 0) throw Error{CSD_ERR_INVALID, "volume dimensions must be non-negative"};
+  if (radial_order < 0 || radial_order % 2 != 0 || radial_order > 14)
+    throw Error{CSD_ERR_INVALID, "radial_order must be an even number <= 14, got " + std::to_string(radial_order)};
+}
+
+// Copy the coefficient volume to the device and launch k_apply_rows with AT
+// (K x R, device) over it; the result comes back into `out`.
+void apply_rows_volume(csd_handle* h, const float* coefficients, int64_t nvox, int K, const double* AT, int R,
+                       const uint8_t* d_mask, bool skip_zero, float* out) {
+  cudaStream_t st = h->stream;
+  h->pcoef.ensure(sizeof(float) * std::max<int64_t>(nvox * K, 1));
+  h->pout.ensure(sizeof(float) * std::max<int64_t>(nvox * R, 1));
+  if (nvox == 0) return;
+  CSD_CUDA(cudaMemcpyAsync(h->pcoef.p, coefficients, sizeof(float) * nvox * K, cudaMemcpyHostToDevice, st));
+  const size_t smem = sizeof(double) * csd::kApplyTile * K;
+  const int64_t tiles = (nvox + csd::kApplyTile - 1) / csd::kApplyTile;
+  const int grid = static_cast<int>(std::min<int64_t>(tiles, static_cast<int64_t>(h->num_sms) * 8));
+  csd::k_apply_rows<<<grid, 256, smem, st>>>(h->pcoef.as<float>(), nvox, K, AT, R, d_mask, skip_zero ? 1 : 0,
+                                             h->pout.as<float>());
+  CSD_LAUNCH();
+  CSD_CUDA(cudaMemcpyAsync(out, h->pout.p, sizeof(float) * nvox * R, cudaMemcpyDeviceToHost, st));
+  CSD_CUDA(cudaStreamSynchronize(st));
+}
+
+// Nearest-rank percentile of the finite values (io/microstructure.rs:303-313).
+bool finite_percentile(const float* xs, int64_t n, double percentile, float* out) {
+  std::vector<float> f;
+  f.reserve(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i)
+    if (std::isfinite(xs[i])) f.push_back(xs[i]);
+  if (f.empty()) return false;
+  const size_t m = f.size();
+  const double p = std::min(std::max(percentile, 0.0), 100.0) / 100.0;
+  const size_t idx = std::min(static_cast<size_t>(std::round(p * static_cast<double>(m - 1))), m - 1);
+  std::nth_element(f.begin(), f.begin() + static_cast<std::ptrdiff_t>(idx), f.end());
+  *out = f[idx];
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int csd_shore_predict(csd_handle* h, const float* coefficients, int64_t X, int64_t Y, int64_t Z,
+                      int32_t radial_order, double zeta, const csd_gtab* target, float* signal_out, char* err,
+                      size_t err_len) {
+  if (!h || !target || target->n <= 0 || (!coefficients && X * Y * Z > 0) || (!signal_out && X * Y * Z > 0)) {
+    set_err(err, err_len, "invalid argument");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    check_coeff_args(X, Y, Z, radial_order);
+    CSD_CUDA(cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    HostGtab g = make_gtab(target);
+    const int N = static_cast<int>(g.bvals.size());
+    const int K = n_coeffs(radial_order);
+    h->pgv.ensure(sizeof(double) * 4 * N);
+    CSD_CUDA(cudaMemcpyAsync(h->pgv.p, g.bvals.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st));
+    CSD_CUDA(cudaMemcpyAsync(h->pgv.as<double>() + N, g.bvecs.data(), sizeof(double) * 3 * N,
+                             cudaMemcpyHostToDevice, st));
+    h->pmat.ensure(sizeof(double) * static_cast<size_t>(N) * K);
+    h->pgt.ensure(sizeof(double) * static_cast<size_t>(K) * N);
+    const double qdenom = 4.0 * kPi * kPi * g.tau;  // src/qspace.rs:384-385
+    const long long nk = static_cast<long long>(N) * K;
+    csd::k_design<<<static_cast<unsigned>((nk + 255) / 256), 256, 0, st>>>(
+        h->pgv.as<double>(), h->pgv.as<double>() + N, N, K, radial_order, zeta, qdenom, g.b0, h->pmat.as<double>());
+    CSD_LAUNCH();
+    csd::k_transpose_design<<<(K * N + 255) / 256, 256, 0, st>>>(h->pmat.as<double>(), N, K, K, h->pgt.as<double>());
+    CSD_LAUNCH();
+    apply_rows_volume(h, coefficients, X * Y * Z, K, h->pgt.as<double>(), N, nullptr, true, signal_out);
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}
+
+int csd_shore_odf_sh(csd_handle* h, const float* coefficients, int64_t X, int64_t Y, int64_t Z,
+                     int32_t radial_order, double zeta, int32_t lmax, const uint8_t* mask, float* sh_out, char* err,
+                     size_t err_len) {
+  if (!h || (!coefficients && X * Y * Z > 0) || (!sh_out && X * Y * Z > 0)) {
+    set_err(err, err_len, "invalid argument");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    check_coeff_args(X, Y, Z, radial_order);
+    if (lmax < 0 || lmax % 2 != 0 || lmax > radial_order)  // python/src/models.rs:212-214
+      throw Error{CSD_ERR_INVALID, "lmax must be even and \xe2\x89\xa4 radial_order (" + std::to_string(radial_order) +
+                                       "), got " + std::to_string(lmax)};
+    CSD_CUDA(cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    const int K = n_coeffs(radial_order);
+    const int R = (lmax + 1) * (lmax + 2) / 2;
+    const int64_t nvox = X * Y * Z;
+    h->pgt.ensure(sizeof(double) * static_cast<size_t>(K) * R);
+    CSD_CUDA(cudaMemsetAsync(h->pgt.p, 0, sizeof(double) * static_cast<size_t>(K) * R, st));
+    csd::k_tournier_projT<<<grid1(K), 256, 0, st>>>(K, radial_order, zeta, lmax, R, h->pgt.as<double>());
+    CSD_LAUNCH();
+    const uint8_t* d_mask = nullptr;
+    if (mask && nvox > 0) {
+      h->mask.ensure(std::max<int64_t>(nvox, 1));
+      CSD_CUDA(cudaMemcpyAsync(h->mask.p, mask, nvox, cudaMemcpyHostToDevice, st));
+      d_mask = h->mask.as<uint8_t>();
+    }
+    apply_rows_volume(h, coefficients, nvox, K, h->pgt.as<double>(), R, d_mask, false, sh_out);
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}
+
+int csd_shore_microstructure(csd_handle* h, const float* coefficients, int64_t X, int64_t Y, int64_t Z,
+                             int32_t radial_order, double zeta, const uint8_t* mask, const float* directions,
+                             int32_t units, int32_t reject_outliers, float outlier_factor, float* rtop, float* rtap,
+                             float* rtpp, float* msd, float* qiv, float* ng, char* err, size_t err_len) {
+  float* maps[6] = {rtop, rtap, rtpp, msd, qiv, ng};
+  const int64_t nvox = X * Y * Z;
+  bool outs_ok = true;
+  for (float* m : maps) outs_ok = outs_ok && (m || nvox == 0);
+  if (!h || !outs_ok || ((!coefficients || !mask) && nvox > 0)) {
+    set_err(err, err_len, "invalid argument");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    check_coeff_args(X, Y, Z, radial_order);
+    if (units != 0 && units != 1) throw Error{CSD_ERR_INVALID, "units must be 0 (um) or 1 (mm)"};
+    CSD_CUDA(cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    const int K = n_coeffs(radial_order);
+    for (float* m : maps)
+      if (nvox > 0) std::fill(m, m + nvox, 0.0f);
+    if (nvox == 0) return CSD_OK;
+    h->mask.ensure(nvox);
+    CSD_CUDA(cudaMemcpyAsync(h->mask.p, mask, nvox, cudaMemcpyHostToDevice, st));
+    const int64_t V = compact(h, h->mask.as<uint8_t>(), nvox, h->vox);
+    if (V == 0) return CSD_OK;
+    h->pcoef.ensure(sizeof(float) * nvox * K);
+    CSD_CUDA(cudaMemcpyAsync(h->pcoef.p, coefficients, sizeof(float) * nvox * K, cudaMemcpyHostToDevice, st));
+    const float* d_dirs = nullptr;
+    if (directions) {
+      h->pdir.ensure(sizeof(float) * nvox * 3);
+      CSD_CUDA(cudaMemcpyAsync(h->pdir.p, directions, sizeof(float) * nvox * 3, cudaMemcpyHostToDevice, st));
+      d_dirs = h->pdir.as<float>();
+    }
+    h->pconst.ensure(sizeof(csd::MicroConsts));
+    csd::k_micro_consts<<<1, 1, 0, st>>>(radial_order, zeta, h->pconst.as<csd::MicroConsts>());
+    CSD_LAUNCH();
+    // unit scales (io/microstructure.rs:162-173)
+    const bool um = units == 0;
+    h->pout.ensure(sizeof(float) * 6 * V);
+    csd::k_microstructure<<<grid1(V, 128), 128, 0, st>>>(
+        h->pcoef.as<float>(), h->vox.as<int64_t>(), V, d_dirs, h->pconst.as<csd::MicroConsts>(), um ? 1e-9f : 1.0f,
+        um ? 1e-6f : 1.0f, um ? 1e-3f : 1.0f, um ? 1e6f : 1.0f, um ? 1e15f : 1.0f, 1.0f, h->pout.as<float>());
+    CSD_LAUNCH();
+    std::vector<float> s(static_cast<size_t>(6 * V));
+    std::vector<int64_t> vox(static_cast<size_t>(V));
+    CSD_CUDA(cudaMemcpyAsync(s.data(), h->pout.p, sizeof(float) * 6 * V, cudaMemcpyDeviceToHost, st));
+    CSD_CUDA(cudaMemcpyAsync(vox.data(), h->vox.p, sizeof(int64_t) * V, cudaMemcpyDeviceToHost, st));
+    CSD_CUDA(cudaStreamSynchronize(st));
+    for (int m = 0; m < 6; ++m) {
+      float* a = s.data() + static_cast<size_t>(m) * V;
+      if (reject_outliers) {  // io/microstructure.rs:222-270, nan_above (:317-326)
+        float p99;
+        if (finite_percentile(a, V, 99.0, &p99)) {
+          const float thr = outlier_factor * p99;
+          for (int64_t i = 0; i < V; ++i)
+            if (std::isfinite(a[i]) && a[i] > thr) a[i] = std::nanf("");
+        }
+      }
+      for (int64_t i = 0; i < V; ++i) maps[m][vox[static_cast<size_t>(i)]] = a[i];
+    }
   } catch (const Error& e) {
     set_err(err, err_len, e.msg);
     return e.code;

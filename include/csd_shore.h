@@ -224,6 +224,37 @@ typedef struct csd_fit_timing {
 
 int csd_last_timing(const csd_handle* h, csd_fit_timing* out);
 
+/* ---- post-fit maps over a coefficient volume (X, Y, Z, K) f32, C order;
+ * host buffers in and out; the radial order fixes K. */
+
+/* Signal predicted by the coefficients on a new gradient table,
+ * (X, Y, Z, target->n) f32; voxels whose coefficients are all zero are
+ * written as zeros.  Replaces synthesize_volume (src/synth.rs:15-84) and
+ * _cs_dmri.shore_predict (python/src/models.rs:252-278). */
+int csd_shore_predict(csd_handle* h, const float* coefficients, int64_t X, int64_t Y, int64_t Z,
+                      int32_t radial_order, double zeta, const csd_gtab* target, float* signal_out,
+                      char* err, size_t err_len);
+
+/* Tournier-ordered ODF SH coefficients, (X, Y, Z, (lmax+1)(lmax+2)/2) f32,
+ * zeros outside `mask` (NULL = every voxel); lmax even and <= radial_order.
+ * Replaces _cs_dmri.shore_odf_sh (python/src/models.rs:201-250) with the
+ * projection of src/odf.rs:79-102. */
+int csd_shore_odf_sh(csd_handle* h, const float* coefficients, int64_t X, int64_t Y, int64_t Z,
+                     int32_t radial_order, double zeta, int32_t lmax, const uint8_t* mask,
+                     float* sh_out, char* err, size_t err_len);
+
+/* RTOP, RTAP, RTPP, MSD, QIV and NG maps, each (X, Y, Z) f32, zero outside
+ * `mask`.  `directions` (X, Y, Z, 3) f32 may be NULL (RTAP / RTPP NaN);
+ * units 0 = micrometre (the reference default), 1 = millimetre; with
+ * `reject_outliers` a scalar above outlier_factor x its p99 is NaN.
+ * Replaces _cs_dmri.shore_microstructure (python/src/models.rs:283-341) and
+ * compute_microstructure (src/io/microstructure.rs:155-298). */
+int csd_shore_microstructure(csd_handle* h, const float* coefficients, int64_t X, int64_t Y, int64_t Z,
+                             int32_t radial_order, double zeta, const uint8_t* mask,
+                             const float* directions, int32_t units, int32_t reject_outliers,
+                             float outlier_factor, float* rtop, float* rtap, float* rtpp, float* msd,
+                             float* qiv, float* ng, char* err, size_t err_len);
+
 /* Allocation-free fixed-alpha FISTA fit of a batch of voxels.
  *
  * No counterpart in the reference: it exists for callers that cannot let a
