@@ -134,6 +134,49 @@ class ShoreFit:
         out[self.mask] = (self.coefficients[self.mask] != 0).mean(-1)
         return out
 
+    def odf_sh(self, lmax: int | None = None, *, n_threads=None) -> np.ndarray:
+        """Tournier (MRtrix) SH coefficients of the ODF, (X, Y, Z, n_sh);
+        ``lmax`` defaults to the largest even value <= the radial order
+        (python/cs_dmri/shore.py:152-157)."""
+        lmax = self.radial_order - self.radial_order % 2 if lmax is None else lmax
+        return _core.shore_odf_sh(self.coefficients, self.radial_order, self.zeta, lmax, self.mask, n_threads=n_threads)
+
+    def predict(self, gtab=None, *, clip: bool = True, n_threads=None) -> np.ndarray:
+        """Signal for ``gtab`` (default: the fit's own), (X, Y, Z, N); ``gtab``
+        is in the image's voxel-axis frame and is rotated into the fit frame
+        (python/cs_dmri/shore.py:159-181)."""
+        if gtab is None:
+            if self.model is None:
+                raise ValueError("pass a gradient table: this fit has no model")
+            gtab = self.model.gtab
+        gtab = as_gradient_table(gtab)
+        if self.single_shell:
+            fitted = self.dwi_shells[0]
+            dw = gtab.bvals[gtab.bvals > gtab.b0_threshold]
+            if np.any(np.abs(dw - fitted) > 50):
+                warnings.warn(
+                    f"this fit used a single shell (b = {fitted:.0f}); signals at other b-values are "
+                    "extrapolated by the regularization, not the measurements", stacklevel=2)
+        out = _core.shore_predict(self.coefficients, self.radial_order, self.zeta, gtab.bvals,
+                                  _rotate(gtab.bvecs, self._rotation), big_delta=self.sidecar["big_delta_seconds"],
+                                  small_delta=self.sidecar["small_delta_seconds"], n_threads=n_threads)
+        return np.maximum(out, 0) if clip else out
+
+    def microstructure(self, directions=None, *, units: str = "um", outlier_factor: float | None = 10.0,
+                       n_threads=None) -> dict:
+        """RTOP, RTAP, RTPP, MSD, QIV and NG maps (python/cs_dmri/shore.py:183-205).
+        RTAP / RTPP need ``directions`` (X, Y, Z, 3) in the image's voxel-axis
+        frame; without them they are NaN.  Raises ``ValueError`` for a
+        single-shell fit, whose radial decay the data do not determine."""
+        if self.single_shell:
+            raise ValueError(
+                "propagator-derived scalars are not determined by single-shell data "
+                f"(this fit used b = {self.dwi_shells[0]:.0f} only)")
+        if directions is not None:
+            directions = _rotate(directions, self._rotation).astype(np.float32)
+        return _core.shore_microstructure(self.coefficients, self.radial_order, self.zeta, self.mask, directions,
+                                          units=units, outlier_factor=outlier_factor, n_threads=n_threads)
+
     def __repr__(self) -> str:
         r2 = "" if self.r2 is None else f", mean R² {float(self.r2[self.mask].mean()):.3f}"
         return f"ShoreFit(radial_order={self.radial_order}, {int(self.mask.sum())} voxels{r2}, frame={self.frame})"

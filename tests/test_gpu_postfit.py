@@ -113,3 +113,20 @@ def test_postfit_argument_errors(vol):
         shore_microstructure(c, 6, 700.0, mask, units="nm")
     with pytest.raises(ValueError, match="mask does not match"):
         shore_microstructure(c, 6, 700.0, mask[:-1])
+
+
+def test_shore_fit_methods(vol, oracle):
+    """ShoreFit.odf_sh / predict / microstructure (python/cs_dmri/shore.py:152-205)."""
+    from cs_dmri_b200 import ShoreModel, shore_odf_sh
+    from cs_dmri_b200.gradients import GradientTable
+    ph, mask, _ = vol
+    gt = GradientTable(ph.bvals, ph.bvecs, big_delta=ph.big_delta, small_delta=ph.small_delta)
+    fit = ShoreModel(gt, regularization="l2", lambda_n=0.05, lambda_l=0.05).fit(ph.data, mask)
+    np.testing.assert_array_equal(fit.odf_sh(), shore_odf_sh(fit.coefficients, 6, 700.0, 6, mask))
+    s = fit.predict()
+    assert s.shape == ph.data.shape and s.min() >= 0
+    raw = fit.predict(clip=False)
+    np.testing.assert_array_equal(s, np.maximum(raw, 0))
+    maps = fit.microstructure()
+    want = oracle.shore_microstructure(fit.coefficients, 6, 700.0, mask)
+    np.testing.assert_allclose(maps["msd"][mask], want["msd"][mask], rtol=1e-6)
