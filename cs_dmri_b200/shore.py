@@ -53,7 +53,7 @@ class ShoreModel:
                  max_iter: int = 1000, tol: float = 1e-6, non_negative: bool = False,
                  lambda_n: float = 1e-8, lambda_l: float = 1e-8, nonneg_max_iter: int = 200,
                  nonneg_tol: float = 1e-9, nonneg_epsilon: float = 1e-10, bvec_frame: str = "auto",
-                 allow_single_shell: bool = False, device: int = 0):
+                 allow_single_shell: bool = False, device: int = 0, precision: str = "fp64"):
         if regularization not in _REGULARIZATIONS:
             raise ValueError(f"regularization must be one of {_REGULARIZATIONS}, got {regularization!r}")
         if alpha_mode not in _ALPHA_MODES:
@@ -68,7 +68,7 @@ class ShoreModel:
             alpha_mode=alpha_mode, alpha=alpha, alpha_ratio=alpha_ratio, path_n_alphas=path_n_alphas,
             path_eps=path_eps, slack=slack, max_iter=max_iter, tol=tol, non_negative=non_negative,
             lambda_n=lambda_n, lambda_l=lambda_l, nonneg_max_iter=nonneg_max_iter, nonneg_tol=nonneg_tol,
-            nonneg_epsilon=nonneg_epsilon, allow_single_shell=allow_single_shell)
+            nonneg_epsilon=nonneg_epsilon, allow_single_shell=allow_single_shell, precision=precision)
 
     def fit(self, data, mask=None, *, affine=None, diagnostics: bool = True,
             n_threads: int | None = None) -> "ShoreFit":
