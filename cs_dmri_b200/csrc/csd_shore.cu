@@ -249,7 +249,8 @@ struct csd_handle {
     const int kp = 8 * ((k + 7) / 8);
     const int np = 8 * ((n + 7) / 8);
     const size_t bytes = sizeof(double) * static_cast<size_t>(np) * kp + sizeof(float) * 8 * 8 * (np + 4);
-    return (kp == 8 || kp == 32 || kp == 72) && bytes <= static_cast<size_t>(smem_optin);
+    // k_rhs_dmma holds up to 9 samples per lane (N_pad <= 288)
+    return (kp == 8 || kp == 32 || kp == 72) && np <= 288 && bytes <= static_cast<size_t>(smem_optin);
   }
   DevBuf mom;      // Nesterov momentum table (t_k - 1) / t_{k+1}
   int mom_len = 0;
@@ -349,7 +350,7 @@ void ensure_setup(csd_handle* h, const HostGtab& g, int radial_order, double zet
     const size_t rhs_smem = sizeof(double) * static_cast<size_t>(Np) * Kp + sizeof(float) * 8 * 8 * (Np + 4);
     const bool small_k = (Kp == 8 || Kp == 32 || Kp == 72);
     h->dmma_resid = small_k && resid_smem <= static_cast<size_t>(h->smem_optin);
-    h->dmma_rhs = small_k && rhs_smem <= static_cast<size_t>(h->smem_optin);
+    h->dmma_rhs = small_k && Np <= 288 && rhs_smem <= static_cast<size_t>(h->smem_optin);
     if (h->dmma_resid || h->dmma_rhs) {
       h->mfrag.ensure(sizeof(double) * static_cast<size_t>(Np) * Kp);
       h->mtfrag.ensure(sizeof(double) * static_cast<size_t>(Np) * Kp);

@@ -819,6 +819,7 @@ __global__ void __launch_bounds__(256) k_rhs_dmma(const float* __restrict__ data
                                                   int Np, const double* __restrict__ mtfrag,
                                                   double* __restrict__ B, float* __restrict__ sig_out) {
   constexpr int MT = KP / 8;
+  constexpr int LPV = 9;   // signal values per lane per voxel: the host selects this kernel for N_pad <= 288
   extern __shared__ __align__(16) double rd_sm[];
   const int KTN = Np / 4;
   const int SLD = Np + 4;  // padded row stride (floats) of a staged signal
@@ -829,20 +830,41 @@ __global__ void __launch_bounds__(256) k_rhs_dmma(const float* __restrict__ data
   __syncthreads();
   const int g = lane >> 2, q = lane & 3;
   const int64_t groups = (V + 7) / 8;
-  for (int64_t gi = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp; gi < groups;
-       gi += static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5)) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  // The next group's signals are loaded into registers while the current
+  // group's DMMAs run (72 loads in flight per lane), so the signal fetch
+  // latency hides behind the tensor work.
+  float pre[8][LPV];
+  auto fetch = [&](int64_t gi) {
+    const int64_t v0 = gi * 8;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const bool ok = gi < groups && v0 + j < V;
+      const float* src = ok ? data + vox[v0 + j] * N : nullptr;
+#pragma unroll
+      for (int t = 0; t < LPV; ++t) {
+        const int i = lane + 32 * t;
+        pre[j][t] = (src && i < N) ? __ldg(src + i) : 0.0f;
+      }
+    }
+  };
+  int64_t gi = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
+  fetch(gi);
+  for (; gi < groups; gi += stride) {
     const int64_t v0 = gi * 8;
     const int nv = static_cast<int>((V - v0) < 8 ? (V - v0) : 8);
+#pragma unroll
     for (int j = 0; j < 8; ++j) {
-      const float* src = (j < nv) ? data + vox[v0 + j] * N : nullptr;
       float* dst = (sig_out && j < nv) ? sig_out + (v0 + j) * N : nullptr;
-      for (int i = lane; i < Np; i += 32) {
-        const float v = (src && i < N) ? src[i] : 0.0f;
-        sbuf[j * SLD + i] = v;
-        if (dst && i < N) dst[i] = v;
+#pragma unroll
+      for (int t = 0; t < LPV; ++t) {
+        const int i = lane + 32 * t;
+        if (i < Np) sbuf[j * SLD + i] = pre[j][t];
+        if (dst && i < N) dst[i] = pre[j][t];
       }
     }
     __syncwarp();
+    fetch(gi + stride);
     double acc[MT][2];
 #pragma unroll
     for (int mt = 0; mt < MT; ++mt) acc[mt][0] = acc[mt][1] = 0.0;
