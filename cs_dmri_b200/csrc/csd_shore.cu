@@ -271,6 +271,11 @@ struct csd_handle {
       pit_sel, pconv_sel, palpha_fb, pit_fb, pconv_fb, pcode;
   DevBuf flagged, mixstat;  // guard re-run list; [n_flagged, batches, error]
   DevBuf pcoef, pmat, pout, pgt, pgv, pdir, pconst;  // post-fit maps
+  // pipelined host-buffer fit: rhs stream + two compute streams, chunk events
+  cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t pev[20] = {};
+  DevBuf iota;
+  int sm_cap = 0;  // > 0: FISTA grids use at most this many SMs
   double mixed_ms = 0.0, mixed_ops = 0.0;
   unsigned long long mixed_rerun = 0;
 };
@@ -507,7 +512,8 @@ void launch_fista_v3_t(csd_handle* h, const csd::FistaParams& p) {
   CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_fista_v3<MT, WARPS, G_IN_SMEM>, 32 * WARPS, smem));
   per_sm = std::max(per_sm, 1);
   const int64_t warps_needed = (p.n_work + 7) / 8;
-  int64_t blocks = std::min<int64_t>(static_cast<int64_t>(h->num_sms) * per_sm, (warps_needed + WARPS - 1) / WARPS);
+  const int sms = h->sm_cap > 0 ? std::min(h->sm_cap, h->num_sms) : h->num_sms;
+  int64_t blocks = std::min<int64_t>(static_cast<int64_t>(sms) * per_sm, (warps_needed + WARPS - 1) / WARPS);
   blocks = std::max<int64_t>(blocks, 1);
   csd::FistaParams q = p;
   q.gfrag = h->gfrag.as<double>();
@@ -1250,6 +1256,177 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   return info;
 }
 
+// Fixed-alpha L1 fit of a page-locked host volume with the transfers
+// overlapped.  The masked voxels are cut into two chunks.  Three streams,
+// ordered by events only (no kernel waits on another):
+//   rhs:     right-hand side of chunk 0 on every SM (it reads its rows over
+//            the bus, in place), then of chunk 1 on kPipeRhsCtas SMs while
+//            chunk 0 iterates on the others;
+//   compute: FISTA + residual / scatter of chunk 0, then of chunk 1 (on every
+//            SM: no right-hand side is left to run beside it);
+//   copy:    the slab of the coefficient volume that chunk k covers, back to
+//            the host as soon as chunk k's scatter is done.
+// Results are those of run_fit (same kernels, same per-voxel arithmetic).
+constexpr int kPipeRhsCtas = 8;
+
+FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64_t nvol,
+                          const HostGtab& g, const csd_shore_spec* spec, float* d_coeffs, float* host_coeffs) {
+  FitInfo info;
+  h->sig_compact = nullptr;
+  cudaStream_t st = h->stream;
+  h->launches = 0;
+  h->precision = spec->precision;
+  h->mixed_ms = 0.0;
+  h->mixed_ops = 0.0;
+  h->mixed_rerun = 0;
+  record(h, 0);
+  ensure_setup(h, g, spec->radial_order, spec->zeta, false, 0.0, 0.0);
+  const int N = h->N, K = h->K, Kp = h->Kp;
+  record(h, 1);
+  CSD_CUDA(cudaMemsetAsync(d_coeffs, 0, sizeof(float) * static_cast<size_t>(nvol) * K, st));
+  const int64_t V = compact(h, d_mask, nvol, h->vox);
+  info.V = V;
+  if (V == 0) {
+    for (int i : {2, 6, 7, 3}) record(h, i);
+    CSD_CUDA(cudaMemcpyAsync(host_coeffs, d_coeffs, sizeof(float) * static_cast<size_t>(nvol) * K,
+                             cudaMemcpyDeviceToHost, st));
+    CSD_CUDA(cudaStreamSynchronize(st));
+    return info;
+  }
+  const int C = V >= 65536 ? 2 : 1;
+  h->B.ensure(sizeof(double) * V * Kp);
+  h->X.ensure(sizeof(double) * V * Kp);
+  h->iters.ensure(sizeof(uint32_t) * V);
+  h->conv.ensure(V);
+  h->queue.ensure(sizeof(unsigned long long) * C);
+  h->itotal.ensure(2 * sizeof(unsigned long long));
+  h->resid_v.ensure(sizeof(double) * V);
+  h->sst_v.ensure(sizeof(double) * V);
+  h->nnz_v.ensure(sizeof(int) * V);
+  h->sig.ensure(sizeof(float) * static_cast<size_t>(V) * N);
+  h->iota.ensure(sizeof(int64_t) * V);
+  h->sig_compact = h->sig.as<float>();
+  CSD_CUDA(cudaMemsetAsync(h->itotal.p, 0, 2 * sizeof(unsigned long long), st));
+  CSD_CUDA(cudaMemsetAsync(h->queue.p, 0, sizeof(unsigned long long) * C, st));
+  csd::k_iota<<<grid1(V), 256, 0, st>>>(h->iota.as<int64_t>(), V);
+  CSD_LAUNCH();
+  ensure_mom(h, spec->max_iter);
+  // chunk boundaries in voxel positions and their volume indices (for the
+  // slab copies back)
+  std::vector<int64_t> c0(C + 1), vb(C + 1, nvol);
+  for (int k = 0; k <= C; ++k) c0[k] = V * k / C;
+  for (int k = 1; k < C; ++k)
+    CSD_CUDA(cudaMemcpyAsync(&vb[k], h->vox.as<int64_t>() + c0[k], sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  vb[0] = 0;
+  for (auto& p : h->pipe)
+    if (!p) CSD_CUDA(cudaStreamCreateWithFlags(&p, cudaStreamNonBlocking));
+  for (auto& e : h->pev)
+    if (!e) CSD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  CSD_CUDA(cudaStreamSynchronize(st));  // boundaries on the host; set-up done
+  record(h, 2);
+  record(h, 6);
+
+  const size_t rhs_smem = sizeof(double) * static_cast<size_t>(h->Np) * Kp + sizeof(float) * 8 * 8 * (h->Np + 4);
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_rhs_dmma<72>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(rhs_smem)));
+  csd::FistaParams fp{};
+  fp.B = h->B.as<double>();
+  fp.X = h->X.as<double>();
+  fp.iters = h->iters.as<uint32_t>();
+  fp.conv = h->conv.as<uint8_t>();
+  fp.V = V;
+  fp.n_inv = 1.0 / static_cast<double>(N);
+  fp.step = 1.0 / h->lipschitz;
+  fp.thr = fp.step * spec->alpha;
+  fp.tol = spec->tol;
+  fp.max_iter = spec->max_iter;
+  fp.non_negative = spec->non_negative;
+  fp.iter_total = h->itotal.as<unsigned long long>();
+  fp.kstep_total = h->itotal.as<unsigned long long>() + 1;
+  csd::EpilogueParams ep{};
+  ep.data = d_data;
+  ep.vox = h->vox.as<int64_t>();
+  ep.V = V;
+  ep.N = N;
+  ep.K = K;
+  ep.Kp = Kp;
+  ep.Mt = h->Mt.as<double>();
+  ep.X = h->X.as<double>();
+  ep.iters = h->iters.as<uint32_t>();
+  ep.coeffs = d_coeffs;
+  ep.scatter = true;
+  ep.kind = 1;
+  ep.alpha = spec->alpha;
+
+  struct Restore {
+    csd_handle* h;
+    cudaStream_t st;
+    ~Restore() {
+      h->stream = st;
+      h->sm_cap = 0;
+    }
+  } restore{h, st};
+  cudaStream_t rs = h->pipe[0], cs = h->pipe[1], ds = h->pipe[2];
+  for (int k = 0; k < C; ++k) {
+    const int64_t a = c0[k], n = c0[k + 1] - c0[k];
+    const int64_t groups = (n + 7) / 8;
+    const int rhs_grid = static_cast<int>(std::min<int64_t>(k == 0 ? h->num_sms : kPipeRhsCtas, (groups + 7) / 8));
+    csd::k_rhs_dmma<72><<<std::max(rhs_grid, 1), 256, rhs_smem, rs>>>(
+        d_data, h->vox.as<int64_t>() + a, n, N, h->Np, h->mtfrag.as<double>(), h->B.as<double>() + a * Kp,
+        h->sig.as<float>() + a * N);
+    CSD_LAUNCH();
+    CSD_CUDA(cudaEventRecord(h->pev[k], rs));
+  }
+  for (int k = 0; k < C; ++k) {
+    const int64_t a = c0[k], n = c0[k + 1] - c0[k];
+    CSD_CUDA(cudaStreamWaitEvent(cs, h->pev[k], 0));
+    h->stream = cs;
+    h->sm_cap = (k + 1 < C) ? h->num_sms - kPipeRhsCtas : 0;
+    csd::FistaParams f = fp;
+    f.list = h->iota.as<int64_t>() + a;
+    f.n_work = n;
+    f.queue = h->queue.as<unsigned long long>() + k;
+    launch_fista(h, Kp / 8, f);
+    h->sm_cap = 0;
+    csd::EpilogueParams e = ep;
+    e.list = h->iota.as<int64_t>() + a;
+    e.n_work = n;
+    launch_epilogue(h, e);
+    h->stream = st;
+    CSD_CUDA(cudaEventRecord(h->pev[8 + k], cs));
+    CSD_CUDA(cudaStreamWaitEvent(ds, h->pev[8 + k], 0));
+    const int64_t lo = vb[k], hi = vb[k + 1];
+    CSD_CUDA(cudaMemcpyAsync(host_coeffs + lo * K, d_coeffs + lo * K, sizeof(float) * static_cast<size_t>(hi - lo) * K,
+                             cudaMemcpyDeviceToHost, ds));
+  }
+  CSD_CUDA(cudaEventRecord(h->pev[16], ds));
+  CSD_CUDA(cudaStreamWaitEvent(st, h->pev[16], 0));
+  CSD_CUDA(cudaEventRecord(h->pev[17], cs));
+  CSD_CUDA(cudaStreamWaitEvent(st, h->pev[17], 0));
+  record(h, 7);
+  record(h, 3);
+  unsigned long long itot[2] = {0, 0};
+  CSD_CUDA(cudaMemcpyAsync(itot, h->itotal.p, sizeof itot, cudaMemcpyDeviceToHost, st));
+  CSD_CUDA(cudaStreamSynchronize(st));
+  info.total_iterations = itot[0];
+  info.representative_alpha = spec->alpha;
+  info.Xfinal = h->X.as<double>();
+  info.conv_final = h->conv.as<uint8_t>();
+  h->timing.tensor_flops = static_cast<double>(itot[1]) * (Kp / 8) * 512.0;
+  h->timing.ms_mixed_kernel = 0.f;
+  h->timing.int8_tensor_ops = 0.0;
+  h->timing.fp64_rerun_voxels = 0;
+  float ms = 0;
+  h->timing.ms_setup = (cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]) == cudaSuccess) ? ms : 0.f;
+  h->timing.ms_rhs = 0.f;  // overlapped with the iterations
+  h->timing.ms_solve = (cudaEventElapsedTime(&ms, h->ev[2], h->ev[7]) == cudaSuccess) ? ms : 0.f;
+  h->timing.ms_solve_kernel = h->timing.ms_solve;
+  h->timing.ms_epilogue = 0.f;
+  h->timing.ms_total = (cudaEventElapsedTime(&ms, h->ev[0], h->ev[3]) == cudaSuccess) ? ms : 0.f;
+  h->timing.launches = h->launches;
+  return info;
+}
+
 void fill_scalars(const HostGtab& g, const FitInfo& info, const csd_shore_spec* spec, csd_fit_result* out) {
   out->n_coeffs = n_coeffs(spec->radial_order);
   out->n_voxels = info.V;
@@ -1346,10 +1523,18 @@ void csd_destroy(csd_handle* h) {
                     &h->iters, &h->conv, &h->queue, &h->itotal, &h->resid_v, &h->nnz_v, &h->amax,
                     &h->zero, &h->alpha_v, &h->Xsel, &h->Xfb, &h->Xl2, &h->rss_l2, &h->list, &h->active,
                     &h->pbest, &h->psel, &h->pact, &h->palpha_sel, &h->pit_sel, &h->pconv_sel,
-                    &h->palpha_fb, &h->pit_fb, &h->pconv_fb, &h->pcode};
+                    &h->palpha_fb, &h->pit_fb, &h->pconv_fb, &h->pcode, &h->gdig, &h->gfexp, &h->flagged,
+                    &h->mixstat, &h->pcoef, &h->pmat, &h->pout, &h->pgt, &h->pgv, &h->pdir, &h->pconst,
+                    &h->iota};
+  for (auto s : h->pipe)
+    if (s) cudaStreamSynchronize(s);
   for (DevBuf* b : bufs) b->release();
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : h->pev)
+    if (e) cudaEventDestroy(e);
+  for (auto s : h->pipe)
+    if (s) cudaStreamDestroy(s);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -1459,9 +1644,17 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
       h->kind_map.ensure(nvol);
       d.kind = h->kind_map.as<uint8_t>();
     }
-    FitInfo info = run_fit(h, d_data, h->mask.as<uint8_t>(), nvol, g, spec, path_eps, d, on_host);
-    CSD_CUDA(cudaMemcpyAsync(out->coefficients, d.coeffs, sizeof(float) * static_cast<size_t>(nvol) * K,
-                             cudaMemcpyDeviceToHost, st));
+    // Fixed-alpha FP64 L1 of a page-locked volume with nothing but the
+    // coefficients requested: the pipelined path (transfers overlap the fit).
+    const bool pipelined = on_host && K == 72 && spec->regularization == CSD_REG_L1 &&
+                           spec->alpha_mode == CSD_ALPHA_FIXED && spec->precision == CSD_PRECISION_FP64 &&
+                           !diag && !out->coef64 && !out->converged && spec->max_iter > 0 && fista_variant() == 4;
+    FitInfo info = pipelined
+                       ? run_fit_pipelined(h, d_data, h->mask.as<uint8_t>(), nvol, g, spec, d.coeffs, out->coefficients)
+                       : run_fit(h, d_data, h->mask.as<uint8_t>(), nvol, g, spec, path_eps, d, on_host);
+    if (!pipelined)
+      CSD_CUDA(cudaMemcpyAsync(out->coefficients, d.coeffs, sizeof(float) * static_cast<size_t>(nvol) * K,
+                               cudaMemcpyDeviceToHost, st));
     const bool is_l1 = spec->regularization == CSD_REG_L1;
     if (diag) {
       if (d.r2) CSD_CUDA(cudaMemcpyAsync(out->r2, d.r2, sizeof(float) * nvol, cudaMemcpyDeviceToHost, st));

@@ -1081,6 +1081,11 @@ __global__ void k_transpose_design(const double* __restrict__ M, int N, int K, i
   Mt[idx] = (k < K) ? M[static_cast<size_t>(i) * K + k] : 0.0;
 }
 
+__global__ void k_iota(int64_t* __restrict__ a, int64_t n) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = i;
+}
+
 __global__ void k_fill_f64(double* __restrict__ a, int64_t n, double v) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < n) a[i] = v;
