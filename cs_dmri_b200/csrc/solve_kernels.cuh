@@ -942,6 +942,16 @@ __global__ void __launch_bounds__(256) k_resid_dmma(ResidParams p) {
     const float* s1 = sbase + li1 * p.N;
     double rss[2] = {0.0, 0.0}, ssum[2] = {0.0, 0.0};
     for (int mt0 = 0; mt0 < MTN; mt0 += 3) {
+      // this chunk's samples are requested before its DMMAs, so their
+      // latency overlaps the tensor work
+      float sa[3][2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int row = 8 * (mt0 + c) + g;
+        const bool in = mt0 + c < MTN && row < p.N;
+        sa[c][0] = (in && ok0) ? __ldg(s0 + row) : 0.0f;
+        sa[c][1] = (in && ok1) ? __ldg(s1 + row) : 0.0f;
+      }
       double acc[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
       for (int kt = 0; kt < KT; ++kt) {
@@ -956,13 +966,13 @@ __global__ void __launch_bounds__(256) k_resid_dmma(ResidParams p) {
         const int row = 8 * (mt0 + c) + g;
         if (mt0 + c < MTN && row < p.N) {
           if (ok0) {
-            const double sv = static_cast<double>(s0[row]);
+            const double sv = static_cast<double>(sa[c][0]);
             const double r = sv - acc[c][0];
             rss[0] = fma(r, r, rss[0]);
             ssum[0] += sv;
           }
           if (ok1) {
-            const double sv = static_cast<double>(s1[row]);
+            const double sv = static_cast<double>(sa[c][1]);
             const double r = sv - acc[c][1];
             rss[1] = fma(r, r, rss[1]);
             ssum[1] += sv;
