@@ -4,7 +4,9 @@ fitted by the CUDA library."""
 
 from __future__ import annotations
 
+import json
 import warnings
+from pathlib import Path
 
 import numpy as np
 
@@ -30,6 +32,11 @@ def _fit_frame(bvec_frame: str, affine):
             raise ValueError("bvec_frame='world' needs an affine (fit a DWI, or pass affine=)")
         return "world", _core.affine_rotation(np.asarray(affine, dtype=np.float64))
     return "image", np.eye(3)
+
+
+def _stem(path: Path) -> str:
+    """foo.nii.gz -> foo, foo.nii -> foo (src/io/coeffs.rs:152-160)."""
+    return str(path)[: -len(".nii.gz")] if str(path).endswith(".nii.gz") else str(path.with_suffix(""))
 
 
 def _rotate(vectors, R):
@@ -176,6 +183,52 @@ class ShoreFit:
             directions = _rotate(directions, self._rotation).astype(np.float32)
         return _core.shore_microstructure(self.coefficients, self.radial_order, self.zeta, self.mask, directions,
                                           units=units, outlier_factor=outlier_factor, n_threads=n_threads)
+
+    def save(self, path, *, overwrite: bool = False) -> None:
+        """Write the coefficient NIfTI, its JSON sidecar and the diagnostic
+        siblings (``<stem>_r2.nii.gz``, ``_rmse``, ``_alpha``, ``_bic``,
+        ``_rss_l2``, ``_sparsity``) in the layout ``cs-fit`` uses
+        (python/cs_dmri/shore.py:249-271, src/io/coeffs.rs:92-130)."""
+        from . import nifti
+
+        if self.affine is None:
+            raise ValueError("saving needs an affine")
+        path = Path(path)
+        stem = _stem(path)
+        outputs = {path: self.coefficients, Path(stem + ".json"): None}
+        for name in ("r2", "rmse", "alpha", "bic", "rss_l2"):
+            if getattr(self, name) is not None:
+                outputs[Path(f"{stem}_{name}.nii.gz")] = np.asarray(getattr(self, name), dtype=np.float32)
+        if self.r2 is not None:
+            outputs[Path(f"{stem}_sparsity.nii.gz")] = self.sparsity
+        if not overwrite:
+            existing = [str(p) for p in outputs if p.exists()]
+            if existing:
+                raise FileExistsError(f"refusing to overwrite {existing}; pass overwrite=True")
+        for p, arr in outputs.items():
+            if arr is None:
+                p.write_text(json.dumps(self.sidecar, indent=2))
+            else:
+                nifti.write(p, arr, self.affine)
+
+    @classmethod
+    def load(cls, path, mask=None) -> "ShoreFit":
+        """Read a coefficient NIfTI written by :meth:`save` or ``cs-fit``
+        (python/cs_dmri/shore.py:273-292)."""
+        from . import nifti
+
+        path = Path(path)
+        stem = _stem(path)
+        img = nifti.read(path)
+        sidecar = json.loads(Path(stem + ".json").read_text())
+        arrays = {"coefficients": np.asarray(img.data, dtype=np.float32), "sidecar": sidecar}
+        for name in ("r2", "rmse", "alpha", "bic", "rss_l2"):
+            p = Path(f"{stem}_{name}.nii.gz")
+            if p.exists():
+                arrays[name] = np.asarray(nifti.read(p).data, dtype=np.float32)
+        frame = "world" if sidecar.get("bvec_frame") == "world-ras" else "image"
+        rotation = _core.affine_rotation(img.affine) if frame == "world" else None
+        return cls(arrays, mask=mask, affine=img.affine, frame=frame, rotation=rotation)
 
     def __repr__(self) -> str:
         r2 = "" if self.r2 is None else f", mean R² {float(self.r2[self.mask].mean()):.3f}"
