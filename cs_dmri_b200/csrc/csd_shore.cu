@@ -1262,10 +1262,11 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
 //   rhs:     right-hand side of chunk 0 on every SM (it reads its rows over
 //            the bus, in place), then of chunk 1 on kPipeRhsCtas SMs while
 //            chunk 0 iterates on the others;
-//   compute: FISTA + residual / scatter of chunk 0, then of chunk 1 (on every
-//            SM: no right-hand side is left to run beside it);
-//   copy:    the slab of the coefficient volume that chunk k covers, back to
-//            the host as soon as chunk k's scatter is done.
+//   chunk k: a stream per chunk runs its FISTA, residual / scatter and the
+//            copy of the slab of the coefficient volume it covers back to the
+//            host.  Chunk 1 starts once its right-hand side (the last one) is
+//            done, so its CTAs take the SMs that chunk 0's tail frees, and it
+//            runs on every SM: no right-hand side is left to run beside it.
 // Results are those of run_fit (same kernels, same per-voxel arithmetic).
 constexpr int kPipeRhsCtas = 8;
 
@@ -1366,7 +1367,7 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
       h->sm_cap = 0;
     }
   } restore{h, st};
-  cudaStream_t rs = h->pipe[0], cs = h->pipe[1], ds = h->pipe[2];
+  cudaStream_t rs = h->pipe[0];
   for (int k = 0; k < C; ++k) {
     const int64_t a = c0[k], n = c0[k + 1] - c0[k];
     const int64_t groups = (n + 7) / 8;
@@ -1379,8 +1380,9 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   }
   for (int k = 0; k < C; ++k) {
     const int64_t a = c0[k], n = c0[k + 1] - c0[k];
-    CSD_CUDA(cudaStreamWaitEvent(cs, h->pev[k], 0));
-    h->stream = cs;
+    cudaStream_t ks = h->pipe[1 + (k & 1)];
+    CSD_CUDA(cudaStreamWaitEvent(ks, h->pev[k], 0));
+    h->stream = ks;
     h->sm_cap = (k + 1 < C) ? h->num_sms - kPipeRhsCtas : 0;
     csd::FistaParams f = fp;
     f.list = h->iota.as<int64_t>() + a;
@@ -1393,16 +1395,14 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
     e.n_work = n;
     launch_epilogue(h, e);
     h->stream = st;
-    CSD_CUDA(cudaEventRecord(h->pev[8 + k], cs));
-    CSD_CUDA(cudaStreamWaitEvent(ds, h->pev[8 + k], 0));
     const int64_t lo = vb[k], hi = vb[k + 1];
     CSD_CUDA(cudaMemcpyAsync(host_coeffs + lo * K, d_coeffs + lo * K, sizeof(float) * static_cast<size_t>(hi - lo) * K,
-                             cudaMemcpyDeviceToHost, ds));
+                             cudaMemcpyDeviceToHost, ks));
   }
-  CSD_CUDA(cudaEventRecord(h->pev[16], ds));
-  CSD_CUDA(cudaStreamWaitEvent(st, h->pev[16], 0));
-  CSD_CUDA(cudaEventRecord(h->pev[17], cs));
-  CSD_CUDA(cudaStreamWaitEvent(st, h->pev[17], 0));
+  for (int j = 1; j <= 2; ++j) {
+    CSD_CUDA(cudaEventRecord(h->pev[15 + j], h->pipe[j]));
+    CSD_CUDA(cudaStreamWaitEvent(st, h->pev[15 + j], 0));
+  }
   record(h, 7);
   record(h, 3);
   unsigned long long itot[2] = {0, 0};
