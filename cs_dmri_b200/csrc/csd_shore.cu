@@ -1257,18 +1257,25 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
 }
 
 // Fixed-alpha L1 fit of a page-locked host volume with the transfers
-// overlapped.  The masked voxels are cut into two chunks.  Three streams,
-// ordered by events only (no kernel waits on another):
+// overlapped.  The masked voxels are cut into chunks (kPipePlan: fractions of
+// the voxels).  Three streams, ordered by events only (no kernel waits on
+// another):
 //   rhs:     right-hand side of chunk 0 on every SM (it reads its rows over
-//            the bus, in place), then of chunk 1 on kPipeRhsCtas SMs while
-//            chunk 0 iterates on the others;
-//   chunk k: a stream per chunk runs its FISTA, residual / scatter and the
-//            copy of the slab of the coefficient volume it covers back to the
-//            host.  Chunk 1 starts once its right-hand side (the last one) is
-//            done, so its CTAs take the SMs that chunk 0's tail frees, and it
-//            runs on every SM: no right-hand side is left to run beside it.
+//            the bus, in place), then of the later chunks, one after another,
+//            on kPipeRhsCtas SMs while the earlier chunks iterate on the rest;
+//   solve:   chunks alternate between two streams, each running its FISTA,
+//            residual / scatter and the copy of the slab of the coefficient
+//            volume it covers back to the host.  Chunk k starts once its
+//            right-hand side is done, so its CTAs take the SMs that chunk
+//            k-1's tail frees; it leaves kPipeRhsCtas SMs free while a later
+//            right-hand side may still be running.
+// A small first chunk shortens the fill (the first right-hand side runs
+// alone); a small last chunk shortens the drain (its copy back runs alone).
 // Results are those of run_fit (same kernels, same per-voxel arithmetic).
-constexpr int kPipeRhsCtas = 8;
+constexpr int kPipeRhsCtas = 16;
+constexpr double kPipePlan[] = {0.2, 0.4, 0.4};
+constexpr int kPipeChunks = sizeof(kPipePlan) / sizeof(kPipePlan[0]);
+static_assert(kPipeChunks <= 15, "pipeline events");
 
 FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64_t nvol,
                           const HostGtab& g, const csd_shore_spec* spec, float* d_coeffs, float* host_coeffs) {
@@ -1294,7 +1301,7 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
     CSD_CUDA(cudaStreamSynchronize(st));
     return info;
   }
-  const int C = V >= 65536 ? 2 : 1;
+  const int C = V >= 65536 ? kPipeChunks : 1;
   h->B.ensure(sizeof(double) * V * Kp);
   h->X.ensure(sizeof(double) * V * Kp);
   h->iters.ensure(sizeof(uint32_t) * V);
@@ -1315,7 +1322,13 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   // chunk boundaries in voxel positions and their volume indices (for the
   // slab copies back)
   std::vector<int64_t> c0(C + 1), vb(C + 1, nvol);
-  for (int k = 0; k <= C; ++k) c0[k] = V * k / C;
+  c0[0] = 0;
+  c0[C] = V;
+  double acc = 0.0;
+  for (int k = 1; k < C; ++k) {
+    acc += kPipePlan[k - 1];
+    c0[k] = std::min<int64_t>(V, static_cast<int64_t>(acc * static_cast<double>(V)) & ~int64_t(7));
+  }
   for (int k = 1; k < C; ++k)
     CSD_CUDA(cudaMemcpyAsync(&vb[k], h->vox.as<int64_t>() + c0[k], sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   vb[0] = 0;

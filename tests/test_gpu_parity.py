@@ -339,7 +339,7 @@ def test_pipelined_host_fit_matches_the_device_fit():
     from cs_dmri_b200.phantom import make_phantom
     rng = np.random.default_rng(2)
     mask = rng.random((48, 48, 48)) < 0.9
-    ph = make_phantom((48, 48, 48), mask=mask, seed=5)   # ~99.5 k voxels -> 3 chunks
+    ph = make_phantom((48, 48, 48), mask=mask, seed=5)   # ~99.5 k voxels -> 3 chunks (0.2 / 0.4 / 0.4)
     kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, alpha_mode="fixed", alpha=0.01)
     pin = torch.empty(ph.data.shape, dtype=torch.float32, pin_memory=True)
     pin.numpy()[...] = ph.data
