@@ -117,6 +117,13 @@ EXPORTS = (
     "csd_shore_predict",
     "csd_shore_odf_sh",
     "csd_shore_microstructure",
+    "csd_shore_fit_batch_device",
+    "csd_shore_fit_adjoint_device",
+    "csd_apply_rows_device",
+    "csd_shore_odf_matrix",
+    "csd_shore_rtop_device",
+    "csd_shore_rtop_adjoint_device",
+    "csd_geodesic_sphere",
 )
 
 _lib = None
@@ -158,6 +165,27 @@ def _declare(lib: C.CDLL) -> C.CDLL:
     lib.csd_shore_microstructure.restype = C.c_int
     lib.csd_shore_microstructure.argtypes = vol + [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_float] + \
         [C.c_void_p] * 6 + [C.c_char_p, C.c_size_t]
+    tail = [C.c_void_p, C.c_char_p, C.c_size_t]  # stream, err, err_len
+    lib.csd_shore_fit_batch_device.restype = C.c_int
+    lib.csd_shore_fit_batch_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(Gtab), C.POINTER(Spec),
+                                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + tail
+    lib.csd_shore_fit_adjoint_device.restype = C.c_int
+    lib.csd_shore_fit_adjoint_device.argtypes = [C.c_void_p, C.POINTER(Gtab), C.POINTER(Spec), C.c_void_p,
+                                                 C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p] + tail
+    lib.csd_apply_rows_device.restype = C.c_int
+    lib.csd_apply_rows_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int64,
+                                          C.c_void_p] + tail
+    lib.csd_shore_odf_matrix.restype = C.c_int
+    lib.csd_shore_odf_matrix.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_void_p, C.c_int32, C.c_void_p,
+                                         C.c_char_p, C.c_size_t]
+    lib.csd_shore_rtop_device.restype = C.c_int
+    lib.csd_shore_rtop_device.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_void_p, C.c_int64,
+                                          C.c_void_p] + tail
+    lib.csd_shore_rtop_adjoint_device.restype = C.c_int
+    lib.csd_shore_rtop_adjoint_device.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_void_p, C.c_int64,
+                                                  C.c_void_p, C.c_void_p] + tail
+    lib.csd_geodesic_sphere.restype = C.c_int
+    lib.csd_geodesic_sphere.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_int32]
     return lib
 
 

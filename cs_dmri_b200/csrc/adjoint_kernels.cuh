@@ -1,0 +1,373 @@
+// Derivatives of the SHORE fit and of the maps taken on its coefficients.
+//
+// The reference has no derivatives; these kernels differentiate the solution
+// maps its solvers compute:
+//
+//   L1 (src/solver/fista.rs:70-143) minimises (1/(2n)) ||M c - s||^2 + alpha ||c||_1
+//   (with c >= 0 when non_negative).  On the support S = {k : c_k != 0} the
+//   optimality condition is  G_SS c_S = M_S^T s - n alpha sign(c_S),  G = M^T M,
+//   so dc_S/ds = G_SS^{-1} M_S^T, dc_S/dalpha = -n G_SS^{-1} sign(c_S) and the
+//   off-support derivatives vanish (implicit differentiation on the converged
+//   support).  For an upstream gradient gc the adjoint is
+//       w_S = G_SS^{-1} gc_S  (w = 0 off S),   grad_s = M w,
+//       grad_alpha = -n sign(c_S) . w_S.
+//
+//   L2 (src/solver/tikhonov.rs:26-76) solves H c = M^T s with
+//   H = M^T M + lambda_N N + lambda_L L, one factor H = L L^T for all voxels:
+//       w = H^{-1} gc,  grad_s = M w,
+//       grad_lambda_N = -w . (N c),  grad_lambda_L = -w . (L c).
+//
+// Every sum runs in index order with separate multiply and add (no fused
+// multiply-add), as a sequential FP64 evaluation does.
+#pragma once
+
+namespace csd {
+
+struct AdjointParams {
+  const double* G;     // L1: Kp x Kp Gram M^T M; L2: the lower Cholesky factor of H (row-major, Kp stride)
+  const double* Mt;    // Kp x N transposed design
+  const double* X;     // fitted coefficients, V rows of stride ldx
+  int64_t ldx;
+  const double* GC;    // upstream gradient on the coefficients, V rows of stride ldg
+  int64_t ldg;
+  int64_t V;
+  int N, K, Kp, radial_order;
+  double n_samples;    // n of the 1/(2n) data term
+  float* gs32;         // V x N gradient on the signal, f32 (nullable)
+  double* gs64;        // V x N, f64 (nullable)
+  double* ghyper;      // V x 2 (nullable): L1 (d/dalpha, 0); L2 (d/dlambda_N, d/dlambda_L)
+  double* W;           // V x Kp adjoint solution w (nullable)
+  unsigned long long* n_singular;  // voxels whose G_SS was not positive definite (nullable)
+};
+
+// Start of column j of a packed lower triangle of order s stored by columns.
+__device__ __forceinline__ int packed_col(int j, int s) { return j * s - (j * (j - 1)) / 2; }
+
+// Per-warp shared memory of k_l1_adjoint, in doubles: the packed factor
+// (K (K + 1) / 2), the dense w (Kp), the support list (K ints).
+__host__ __device__ __forceinline__ int l1_adjoint_warp_doubles(int K, int Kp) {
+  return ((K * (K + 1) / 2 + Kp + (K + 1) / 2) + 1) & ~1;
+}
+
+// grad_s[n] = sum over k in index order of M[n][k] w[k], written for the
+// voxel's row; w dense in shared memory, zero off the support.
+__device__ __forceinline__ void adjoint_signal_row(const AdjointParams& p, int64_t v, const double* sw,
+                                                   const int* sidx, int s, int lane) {
+  for (int n = lane; n < p.N; n += 32) {
+    double acc = 0.0;
+    if (sidx) {
+      for (int q = 0; q < s; ++q) {
+        const int k = sidx[q];
+        acc = __dadd_rn(acc, __dmul_rn(p.Mt[static_cast<size_t>(k) * p.N + n], sw[k]));
+      }
+    } else {
+      for (int k = 0; k < p.K; ++k) acc = __dadd_rn(acc, __dmul_rn(p.Mt[static_cast<size_t>(k) * p.N + n], sw[k]));
+    }
+    if (p.gs64) p.gs64[v * p.N + n] = acc;
+    if (p.gs32) p.gs32[v * p.N + n] = static_cast<float>(acc);
+  }
+}
+
+// L1 adjoint, one warp per voxel.  The support is compacted with ballots
+// (index order), G_SS gathered into the warp's packed lower triangle and
+// factored right-looking (every entry receives its updates in index order,
+// as a sequential L L^T does), then L y = gc_S by columns and L^T w = y by
+// columns from the last row up.  A support matrix that is not positive
+// definite leaves the voxel's gradients NaN and is counted.
+template <int RPL>  // ceil(K / 32)
+__global__ void __launch_bounds__(256) k_l1_adjoint(AdjointParams p) {
+  extern __shared__ __align__(16) double adj_smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nw = blockDim.x >> 5;
+  const int K = p.K, Kp = p.Kp;
+  double* T = adj_smem + static_cast<size_t>(warp) * l1_adjoint_warp_doubles(K, Kp);
+  double* sw = T + K * (K + 1) / 2;
+  int* sidx = reinterpret_cast<int*>(sw + Kp);
+  const double nan = __longlong_as_double(0x7ff8000000000000ll);
+  for (int64_t v = static_cast<int64_t>(blockIdx.x) * nw + warp; v < p.V;
+       v += static_cast<int64_t>(gridDim.x) * nw) {
+    const double* x = p.X + v * p.ldx;
+    int s = 0;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int k = lane + 32 * r;
+      const bool nz = k < K && x[k] != 0.0;
+      const unsigned b = __ballot_sync(kFull, nz);
+      if (nz) sidx[s + __popc(b & ((1u << lane) - 1u))] = k;
+      s += __popc(b);
+    }
+    __syncwarp();
+    double rv[RPL], sg[RPL];
+#pragma unroll
+    for (int c = 0; c < RPL; ++c) {
+      const int q = lane + 32 * c;
+      rv[c] = 0.0;
+      sg[c] = 0.0;
+      if (q < s) {
+        const int k = sidx[q];
+        rv[c] = p.GC[v * p.ldg + k];
+        sg[c] = x[k] > 0.0 ? 1.0 : -1.0;
+      }
+    }
+    for (int j = 0; j < s; ++j) {
+      const int cj = packed_col(j, s);
+      const double* gj = p.G + static_cast<size_t>(sidx[j]) * Kp;
+      for (int i = j + lane; i < s; i += 32) T[cj + i - j] = gj[sidx[i]];
+    }
+    __syncwarp();
+    bool ok = true;
+    for (int j = 0; j < s; ++j) {
+      const int cj = packed_col(j, s);
+      const double d = T[cj];
+      if (!(d > 0.0)) {  // every lane read the same pivot
+        ok = false;
+        break;
+      }
+      const double ljj = sqrt(d);
+      __syncwarp();
+      if (lane == 0) T[cj] = ljj;
+      for (int i = j + 1 + lane; i < s; i += 32) T[cj + i - j] = __ddiv_rn(T[cj + i - j], ljj);
+      __syncwarp();
+      for (int k = j + 1; k < s; ++k) {
+        const int ck = packed_col(k, s);
+        const double lkj = T[cj + k - j];
+        for (int i = k + lane; i < s; i += 32) T[ck + i - k] = __dsub_rn(T[ck + i - k], __dmul_rn(T[cj + i - j], lkj));
+      }
+      __syncwarp();
+    }
+    if (!ok) {
+      for (int n = lane; n < p.N; n += 32) {
+        if (p.gs64) p.gs64[v * p.N + n] = nan;
+        if (p.gs32) p.gs32[v * p.N + n] = static_cast<float>(nan);
+      }
+      if (p.W)
+        for (int k = lane; k < Kp; k += 32) p.W[v * Kp + k] = nan;
+      if (lane == 0) {
+        if (p.ghyper) {
+          p.ghyper[2 * v] = nan;
+          p.ghyper[2 * v + 1] = nan;
+        }
+        if (p.n_singular) atomicAdd(p.n_singular, 1ull);
+      }
+      __syncwarp();
+      continue;
+    }
+    // L y = gc_S
+    for (int i = 0; i < s; ++i) {
+      const int ci = packed_col(i, s);
+      const int owner = i & 31, oc = i >> 5;
+      double yi = 0.0;
+#pragma unroll
+      for (int c = 0; c < RPL; ++c)
+        if (c == oc && lane == owner) yi = __ddiv_rn(rv[c], T[ci]);
+      yi = __shfl_sync(kFull, yi, owner);
+#pragma unroll
+      for (int c = 0; c < RPL; ++c) {
+        const int q = lane + 32 * c;
+        if (q > i && q < s) rv[c] = __dsub_rn(rv[c], __dmul_rn(T[ci + q - i], yi));
+        if (q == i) rv[c] = yi;
+      }
+    }
+    // L^T w = y
+    for (int i = s - 1; i >= 0; --i) {
+      const int owner = i & 31, oc = i >> 5;
+      double wi = 0.0;
+#pragma unroll
+      for (int c = 0; c < RPL; ++c)
+        if (c == oc && lane == owner) wi = __ddiv_rn(rv[c], T[packed_col(i, s)]);
+      wi = __shfl_sync(kFull, wi, owner);
+#pragma unroll
+      for (int c = 0; c < RPL; ++c) {
+        const int q = lane + 32 * c;
+        if (q < i) rv[c] = __dsub_rn(rv[c], __dmul_rn(T[packed_col(q, s) + i - q], wi));
+        if (q == i) rv[c] = wi;
+      }
+    }
+    double dot = 0.0;
+#pragma unroll
+    for (int c = 0; c < RPL; ++c) dot = __dadd_rn(dot, __dmul_rn(sg[c], rv[c]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(kFull, dot, o);
+    for (int k = lane; k < Kp; k += 32) sw[k] = 0.0;
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < RPL; ++c) {
+      const int q = lane + 32 * c;
+      if (q < s) sw[sidx[q]] = rv[c];
+    }
+    __syncwarp();
+    if (p.W)
+      for (int k = lane; k < Kp; k += 32) p.W[v * Kp + k] = sw[k];
+    adjoint_signal_row(p, v, sw, sidx, s, lane);
+    if (lane == 0 && p.ghyper) {
+      p.ghyper[2 * v] = -p.n_samples * dot;
+      p.ghyper[2 * v + 1] = 0.0;
+    }
+    __syncwarp();
+  }
+}
+
+// L2 adjoint, one warp per voxel, the factor of H staged once per CTA with
+// a padded row stride; then the hyper-parameter gradients and grad_s.
+template <int RPL>
+__global__ void __launch_bounds__(256) k_l2_adjoint(AdjointParams p) {
+  extern __shared__ __align__(16) double adj_smem[];
+  const int K = p.K, Kp = p.Kp, ld = K + 1;
+  double* sL = adj_smem;
+  for (int i = threadIdx.x; i < K * K; i += blockDim.x) sL[(i / K) * ld + (i % K)] = p.G[(i / K) * Kp + (i % K)];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nw = blockDim.x >> 5;
+  double* sw = adj_smem + ((K * ld + 1) & ~1) + static_cast<size_t>(warp) * Kp;
+  for (int64_t v = static_cast<int64_t>(blockIdx.x) * nw + warp; v < p.V;
+       v += static_cast<int64_t>(gridDim.x) * nw) {
+    double r[RPL];
+#pragma unroll
+    for (int c = 0; c < RPL; ++c) {
+      const int row = lane + 32 * c;
+      r[c] = (row < K) ? p.GC[v * p.ldg + row] : 0.0;
+    }
+    for (int i = 0; i < K; ++i) {
+      const int owner = i & 31, oc = i >> 5;
+      double yi = 0.0;
+#pragma unroll
+      for (int c = 0; c < RPL; ++c)
+        if (c == oc && lane == owner) yi = __ddiv_rn(r[c], sL[i * ld + i]);
+      yi = __shfl_sync(kFull, yi, owner);
+#pragma unroll
+      for (int c = 0; c < RPL; ++c) {
+        const int row = lane + 32 * c;
+        if (row > i && row < K) r[c] = __dsub_rn(r[c], __dmul_rn(sL[row * ld + i], yi));
+        if (row == i) r[c] = yi;
+      }
+    }
+    for (int i = K - 1; i >= 0; --i) {
+      const int owner = i & 31, oc = i >> 5;
+      double xi = 0.0;
+#pragma unroll
+      for (int c = 0; c < RPL; ++c)
+        if (c == oc && lane == owner) xi = __ddiv_rn(r[c], sL[i * ld + i]);
+      xi = __shfl_sync(kFull, xi, owner);
+#pragma unroll
+      for (int c = 0; c < RPL; ++c) {
+        const int row = lane + 32 * c;
+        if (row < i) r[c] = __dsub_rn(r[c], __dmul_rn(sL[i * ld + row], xi));
+        if (row == i) r[c] = xi;
+      }
+    }
+    double dn = 0.0, dl = 0.0;
+    const double* x = p.X + v * p.ldx;
+#pragma unroll
+    for (int c = 0; c < RPL; ++c) {
+      const int row = lane + 32 * c;
+      if (row < K) {
+        int n = 0, l = 0, kk = 0;
+        col_to_nlk(p.radial_order, row, &n, &l, &kk);
+        const double nn = static_cast<double>(n * (n + 1)), ll = static_cast<double>(l * (l + 1));
+        const double wc = __dmul_rn(r[c], x[row]);
+        dn = __dadd_rn(dn, __dmul_rn(wc, nn * nn));
+        dl = __dadd_rn(dl, __dmul_rn(wc, ll * ll));
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      dn += __shfl_xor_sync(kFull, dn, o);
+      dl += __shfl_xor_sync(kFull, dl, o);
+    }
+#pragma unroll
+    for (int c = 0; c < RPL; ++c) {
+      const int row = lane + 32 * c;
+      if (row < Kp) sw[row] = (row < K) ? r[c] : 0.0;
+    }
+    __syncwarp();
+    if (p.W)
+      for (int k = lane; k < Kp; k += 32) p.W[v * Kp + k] = sw[k];
+    adjoint_signal_row(p, v, sw, nullptr, K, lane);
+    if (lane == 0 && p.ghyper) {
+      p.ghyper[2 * v] = -dn;
+      p.ghyper[2 * v + 1] = -dl;
+    }
+    __syncwarp();
+  }
+}
+
+// out[v][r] = sum over k < cols, in index order, of At[k * rows + r] in[v][k]:
+// a fixed matrix A (rows x cols, stored transposed so that a warp's lanes
+// read consecutive rows) applied to every voxel's vector.  Eight voxels per
+// warp, so each coalesced load of a column of A feeds eight products.
+__global__ void __launch_bounds__(256) k_apply64(const double* __restrict__ At, int rows, int cols,
+                                                 const double* __restrict__ in, int64_t ldin, int64_t V,
+                                                 double* __restrict__ out, int64_t ldout) {
+  const int lane = threadIdx.x & 31;
+  const int64_t groups = (V + 7) / 8;
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); g < groups;
+       g += nwarps) {
+    const int64_t v0 = 8 * g;
+    const int nv = V - v0 < 8 ? static_cast<int>(V - v0) : 8;
+    for (int r = lane; r < rows; r += 32) {
+      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int k = 0; k < cols; ++k) {
+        const double a = At[static_cast<size_t>(k) * rows + r];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (j < nv) acc[j] = __dadd_rn(acc[j], __dmul_rn(a, in[(v0 + j) * ldin + k]));
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (j < nv) out[(v0 + j) * ldout + r] = acc[j];
+    }
+  }
+}
+
+// RTOP of FP64 coefficients (src/scalars/microstructure.rs:98-118):
+// max(sum_n (c_n00 / E0) (-1)^n w_n, 0), NaN when E0 is zero or not finite.
+__device__ __forceinline__ double rtop64(const MicroConsts& mc, const double* c, double* e0_out) {
+  double e0 = 0.0;
+  const double inv = 1.0 / sqrt(4.0 * CUDART_PI);
+  for (int n = 0; n <= mc.radial_order; ++n) e0 += c[mc.n00[n]] * mc.r0[n] * inv;
+  *e0_out = e0;
+  if (!isfinite(e0) || e0 == 0.0) return __longlong_as_double(0x7ff8000000000000ll);
+  double a = 0.0;
+  for (int n = 0; n <= mc.radial_order; ++n) {
+    const double sign = (n % 2 == 0) ? 1.0 : -1.0;
+    a += (c[mc.n00[n]] / e0) * sign * mc.rtop_w[n];
+  }
+  return fmax(a, 0.0);
+}
+
+__global__ void k_rtop64(const MicroConsts* __restrict__ mcp, const double* __restrict__ C, int64_t ldc, int64_t V,
+                         double* __restrict__ out) {
+  const int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  double e0;
+  out[v] = rtop64(*mcp, C + v * ldc, &e0);
+}
+
+// d RTOP / d c_(n,0,0) = ((-1)^n w_n - RTOP r0_n / sqrt(4 pi)) / E0 where
+// RTOP > 0; zero where the clamp at 0 is active; NaN where RTOP is NaN and
+// the upstream gradient is not zero.  Other coefficients get zero.
+__global__ void k_rtop64_adjoint(const MicroConsts* __restrict__ mcp, const double* __restrict__ C, int64_t ldc,
+                                 int64_t V, const double* __restrict__ g, double* __restrict__ GC, int64_t ldgc) {
+  const int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  const MicroConsts& mc = *mcp;
+  double e0;
+  const double rt = rtop64(mc, C + v * ldc, &e0);
+  double* o = GC + v * ldgc;
+  for (int k = 0; k < mc.K; ++k) o[k] = 0.0;
+  const double gv = g[v];
+  if (isnan(rt)) {
+    if (gv != 0.0)
+      for (int k = 0; k < mc.K; ++k) o[k] = rt;
+    return;
+  }
+  if (!(rt > 0.0)) return;
+  const double inv = 1.0 / sqrt(4.0 * CUDART_PI);
+  for (int n = 0; n <= mc.radial_order; ++n) {
+    const double sign = (n % 2 == 0) ? 1.0 : -1.0;
+    o[mc.n00[n]] = gv * ((sign * mc.rtop_w[n] - rt * mc.r0[n] * inv) / e0);
+  }
+}
+
+}  // namespace csd

@@ -39,6 +39,7 @@
 #include "icls_kernels.cuh"
 #include "mixed_kernels.cuh"
 #include "epilogue_kernels.cuh"
+#include "adjoint_kernels.cuh"
 
 namespace {
 
@@ -275,6 +276,7 @@ struct csd_handle {
   cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t pev[20] = {};
   DevBuf iota;
+  DevBuf adjstat;  // adjoint: count of voxels with a singular support matrix
   int sm_cap = 0;  // > 0: FISTA grids use at most this many SMs
   double mixed_ms = 0.0, mixed_ops = 0.0;
   unsigned long long mixed_rerun = 0;
@@ -1538,7 +1540,7 @@ void csd_destroy(csd_handle* h) {
                     &h->pbest, &h->psel, &h->pact, &h->palpha_sel, &h->pit_sel, &h->pconv_sel,
                     &h->palpha_fb, &h->pit_fb, &h->pconv_fb, &h->pcode, &h->gdig, &h->gfexp, &h->flagged,
                     &h->mixstat, &h->pcoef, &h->pmat, &h->pout, &h->pgt, &h->pgv, &h->pdir, &h->pconst,
-                    &h->iota};
+                    &h->iota, &h->adjstat};
   for (auto s : h->pipe)
     if (s) cudaStreamSynchronize(s);
   for (DevBuf* b : bufs) b->release();
@@ -2143,3 +2145,5 @@ extern "C" int csd_shore_fista_batch_noalloc(const csd_gtab* gtab, const csd_sho
   }
   return CSD_OK;
 }
+
+#include "differentiable_host.cuh"

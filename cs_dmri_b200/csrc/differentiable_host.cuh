@@ -1,0 +1,378 @@
+// Host side of the differentiable fit: a batch fit of device-resident voxel
+// signals with FP64 coefficients out (fixed or per-voxel alpha, optional warm
+// start), its adjoint, and the linear / ratio maps on coefficients (ODF
+// amplitudes on a sphere, predicted signals, RTOP) with theirs.  Included once
+// at the end of csd_shore.cu: it uses that file's handle and helpers.
+#pragma once
+
+namespace {
+
+// Class I geodesic sphere: every face of the icosahedron split into f^2
+// triangles on a flat barycentric grid, the grid points projected on the unit
+// sphere, shared edge points kept once (in first-seen order).  Frequency 6
+// gives 362 vertices.  With `hemisphere` one vertex of each antipodal pair is
+// kept (z > 0, or z = 0 and y > 0, or z = y = 0 and x > 0).
+std::vector<double> geodesic_sphere(int f, bool hemisphere) {
+  const double ph = (1.0 + std::sqrt(5.0)) / 2.0;
+  std::vector<std::array<double, 3>> ico = {{-1, ph, 0}, {1, ph, 0},   {-1, -ph, 0}, {1, -ph, 0},
+                                            {0, -1, ph}, {0, 1, ph},   {0, -1, -ph}, {0, 1, -ph},
+                                            {ph, 0, -1}, {ph, 0, 1},   {-ph, 0, -1}, {-ph, 0, 1}};
+  for (auto& a : ico) {
+    const double n = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    for (auto& c : a) c /= n;
+  }
+  const int faces[20][3] = {{0, 11, 5}, {0, 5, 1},  {0, 1, 7},   {0, 7, 10}, {0, 10, 11},
+                            {1, 5, 9},  {5, 11, 4}, {11, 10, 2}, {10, 7, 6}, {7, 1, 8},
+                            {3, 9, 4},  {3, 4, 2},  {3, 2, 6},   {3, 6, 8},  {3, 8, 9},
+                            {4, 9, 5},  {2, 4, 11}, {6, 2, 10},  {8, 6, 7},  {9, 8, 1}};
+  std::vector<double> out;
+  std::map<std::array<long long, 3>, int> seen;
+  for (const auto& t : faces)
+    for (int i = 0; i <= f; ++i)
+      for (int j = 0; i + j <= f; ++j) {
+        const double wa = static_cast<double>(f - i - j) / f, wb = static_cast<double>(i) / f,
+                     wc = static_cast<double>(j) / f;
+        std::array<double, 3> p;
+        for (int d = 0; d < 3; ++d) p[d] = wa * ico[t[0]][d] + wb * ico[t[1]][d] + wc * ico[t[2]][d];
+        const double n = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+        for (auto& c : p) c /= n;
+        const std::array<long long, 3> key = {std::llround(p[0] * 1e9), std::llround(p[1] * 1e9),
+                                              std::llround(p[2] * 1e9)};
+        if (seen.count(key)) continue;
+        seen[key] = 1;
+        const double e = 1e-12;
+        const bool keep = !hemisphere || (p[2] > e) || (std::fabs(p[2]) <= e && p[1] > e) ||
+                          (std::fabs(p[2]) <= e && std::fabs(p[1]) <= e && p[0] > 0.0);
+        if (keep) out.insert(out.end(), p.begin(), p.end());
+      }
+  return out;
+}
+
+struct StreamScope {
+  csd_handle* h;
+  cudaStream_t saved;
+  StreamScope(csd_handle* hh, void* stream) : h(hh), saved(hh->stream) {
+    if (stream) h->stream = static_cast<cudaStream_t>(stream);
+  }
+  ~StreamScope() { h->stream = saved; }
+};
+
+// b = M^T s for every row, then FISTA (fixed or per-voxel alpha, optional
+// warm start) or the Tikhonov solve; FP64 coefficients (V x K) out.
+void run_fit_batch(csd_handle* h, const float* d_sig, int64_t V, const HostGtab& g, const csd_shore_spec* spec,
+                   const double* d_alpha, const double* d_warm, double* d_coef, uint32_t* d_iters) {
+  cudaStream_t st = h->stream;
+  h->launches = 0;
+  h->precision = spec->precision;
+  const bool is_l1 = spec->regularization == CSD_REG_L1;
+  ensure_setup(h, g, spec->radial_order, spec->zeta, !is_l1, spec->lambda_n, spec->lambda_l);
+  const int N = h->N, K = h->K, Kp = h->Kp;
+  if (V == 0) return;
+  h->vox.ensure(sizeof(int64_t) * V);
+  h->B.ensure(sizeof(double) * V * Kp);
+  h->X.ensure(sizeof(double) * V * Kp);
+  h->iters.ensure(sizeof(uint32_t) * V);
+  h->conv.ensure(V);
+  h->queue.ensure(sizeof(unsigned long long));
+  csd::k_iota<<<grid1(V), 256, 0, st>>>(h->vox.as<int64_t>(), V);
+  CSD_LAUNCH();
+  launch_rhs(h, d_sig, V);
+  if (is_l1) {
+    ensure_mom(h, spec->max_iter);
+    if (d_warm) {
+      CSD_CUDA(cudaMemsetAsync(h->X.p, 0, sizeof(double) * V * Kp, st));
+      CSD_CUDA(cudaMemcpy2DAsync(h->X.p, sizeof(double) * Kp, d_warm, sizeof(double) * K, sizeof(double) * K, V,
+                                 cudaMemcpyDeviceToDevice, st));
+    }
+    csd::FistaParams fp{};
+    fp.gfrag = h->gfrag.as<double>();
+    fp.B = h->B.as<double>();
+    fp.X = h->X.as<double>();
+    fp.warm = d_warm ? h->X.as<double>() : nullptr;  // read at slot fill, before the slot's voxel is written
+    fp.iters = h->iters.as<uint32_t>();
+    fp.conv = h->conv.as<uint8_t>();
+    fp.V = V;
+    fp.n_inv = 1.0 / static_cast<double>(N);
+    fp.step = 1.0 / h->lipschitz;
+    fp.thr = fp.step * spec->alpha;
+    fp.alpha_v = d_alpha;
+    fp.tol = spec->tol;
+    fp.max_iter = spec->max_iter;
+    fp.non_negative = spec->non_negative;
+    fp.queue = h->queue.as<unsigned long long>();
+    fp.n_work = V;
+    CSD_CUDA(cudaMemsetAsync(h->queue.p, 0, sizeof(unsigned long long), st));
+    launch_fista(h, Kp / 8, fp);
+    if (d_iters)
+      CSD_CUDA(cudaMemcpyAsync(d_iters, h->iters.p, sizeof(uint32_t) * V, cudaMemcpyDeviceToDevice, st));
+  } else {
+    launch_tikhonov(h, h->B.as<double>(), h->X.as<double>(), V);
+    if (d_iters) {
+      std::vector<uint32_t> ones(static_cast<size_t>(V), 1u);
+      CSD_CUDA(cudaMemcpyAsync(d_iters, ones.data(), sizeof(uint32_t) * V, cudaMemcpyHostToDevice, st));
+      CSD_CUDA(cudaStreamSynchronize(st));
+    }
+  }
+  CSD_CUDA(cudaMemcpy2DAsync(d_coef, sizeof(double) * K, h->X.p, sizeof(double) * Kp, sizeof(double) * K, V,
+                             cudaMemcpyDeviceToDevice, st));
+}
+
+template <int RPL>
+void launch_l1_adjoint_t(csd_handle* h, const csd::AdjointParams& p) {
+  const size_t per_warp = sizeof(double) * static_cast<size_t>(csd::l1_adjoint_warp_doubles(p.K, p.Kp));
+  const int warps = static_cast<int>(std::min<size_t>(8, static_cast<size_t>(h->smem_optin) / per_warp));
+  if (warps < 1) throw Error{CSD_ERR_INVALID, "coefficient count too large for the L1 adjoint"};
+  const size_t smem = per_warp * warps;
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_l1_adjoint<RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  int per_sm = 0;
+  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_l1_adjoint<RPL>, 32 * warps, smem));
+  const int64_t blocks = std::max<int64_t>(
+      1, std::min<int64_t>((p.V + warps - 1) / warps, static_cast<int64_t>(h->num_sms) * std::max(per_sm, 1)));
+  csd::k_l1_adjoint<RPL><<<static_cast<unsigned>(blocks), 32 * warps, smem, h->stream>>>(p);
+  CSD_LAUNCH();
+}
+
+template <int RPL>
+void launch_l2_adjoint_t(csd_handle* h, const csd::AdjointParams& p) {
+  const int warps = 8;
+  const size_t smem =
+      sizeof(double) * ((static_cast<size_t>(p.K) * (p.K + 1) + 1) / 2 * 2 + static_cast<size_t>(warps) * p.Kp);
+  if (smem > static_cast<size_t>(h->smem_optin))
+    throw Error{CSD_ERR_INVALID, "coefficient count too large for the L2 adjoint"};
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_l2_adjoint<RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  const int64_t blocks =
+      std::max<int64_t>(1, std::min<int64_t>((p.V + warps - 1) / warps, static_cast<int64_t>(h->num_sms) * 2));
+  csd::k_l2_adjoint<RPL><<<static_cast<unsigned>(blocks), 32 * warps, smem, h->stream>>>(p);
+  CSD_LAUNCH();
+}
+
+template <template <int> class F>
+void dispatch_rpl(int K, csd_handle* h, const csd::AdjointParams& p) {
+  switch ((K + 31) / 32) {
+    case 1: F<1>::run(h, p); break;
+    case 2: F<2>::run(h, p); break;
+    case 3: F<3>::run(h, p); break;
+    case 4: F<4>::run(h, p); break;
+    case 5: F<5>::run(h, p); break;
+    default: throw Error{CSD_ERR_INVALID, "adjoint kernels support K <= 160"};
+  }
+}
+template <int R>
+struct L1Adj {
+  static void run(csd_handle* h, const csd::AdjointParams& p) { launch_l1_adjoint_t<R>(h, p); }
+};
+template <int R>
+struct L2Adj {
+  static void run(csd_handle* h, const csd::AdjointParams& p) { launch_l2_adjoint_t<R>(h, p); }
+};
+
+void launch_apply64(csd_handle* h, const double* At, int rows, int cols, const double* in, int64_t ldin, int64_t V,
+                    double* out, int64_t ldout) {
+  const int64_t groups = (V + 7) / 8;
+  const int64_t blocks =
+      std::max<int64_t>(1, std::min<int64_t>((groups + 7) / 8, static_cast<int64_t>(h->num_sms) * 8));
+  csd::k_apply64<<<static_cast<unsigned>(blocks), 256, 0, h->stream>>>(At, rows, cols, in, ldin, V, out, ldout);
+  CSD_LAUNCH();
+}
+
+const csd::MicroConsts* micro_consts(csd_handle* h, int radial_order, double zeta) {
+  if (radial_order < 0 || radial_order > csd::kMicroMaxN - 1)
+    throw Error{CSD_ERR_INVALID, "radial order out of range for the RTOP constants"};
+  h->pconst.ensure(sizeof(csd::MicroConsts));
+  csd::k_micro_consts<<<1, 1, 0, h->stream>>>(radial_order, zeta, h->pconst.as<csd::MicroConsts>());
+  CSD_LAUNCH();
+  return h->pconst.as<csd::MicroConsts>();
+}
+
+}  // namespace
+
+extern "C" {
+
+int csd_geodesic_sphere(int32_t frequency, int32_t hemisphere, double* out, int32_t capacity) {
+  if (frequency < 1 || frequency > 64) return -1;
+  const std::vector<double> v = geodesic_sphere(frequency, hemisphere != 0);
+  const int n = static_cast<int>(v.size() / 3);
+  if (out && capacity >= n) std::memcpy(out, v.data(), sizeof(double) * v.size());
+  return n;
+}
+
+int csd_shore_fit_batch_device(csd_handle* h, const float* d_signals, int64_t n_voxels, const csd_gtab* gtab,
+                               const csd_shore_spec* spec, const double* d_alpha, const double* d_warm,
+                               double* d_coef, uint32_t* d_iterations, void* stream, char* err, size_t err_len) {
+  if (!h || !gtab || !spec || n_voxels < 0 || (n_voxels > 0 && (!d_signals || !d_coef))) {
+    set_err(err, err_len, "invalid argument: null pointer or negative voxel count");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    CSD_CUDA(cudaSetDevice(h->device));
+    HostGtab g = make_gtab(gtab);
+    std::string warnings;
+    validate(spec, g, warnings);
+    if (spec->regularization == CSD_REG_NONNEG)
+      throw Error{CSD_ERR_INVALID, "the batch fit takes regularization l1 or l2"};
+    if (spec->regularization == CSD_REG_L1 && spec->alpha_mode != CSD_ALPHA_FIXED)
+      throw Error{CSD_ERR_INVALID, "the batch fit takes alpha_mode fixed (one alpha, or one per voxel)"};
+    StreamScope scope(h, stream);
+    run_fit_batch(h, d_signals, n_voxels, g, spec, d_alpha, d_warm, d_coef, d_iterations);
+    CSD_CUDA(cudaStreamSynchronize(h->stream));
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}
+
+int csd_shore_fit_adjoint_device(csd_handle* h, const csd_gtab* gtab, const csd_shore_spec* spec,
+                                 const double* d_coef, const double* d_grad_coef, int64_t n_voxels,
+                                 float* d_grad_signal, double* d_grad_signal64, double* d_grad_hyper, void* stream,
+                                 char* err, size_t err_len) {
+  if (!h || !gtab || !spec || n_voxels < 0 || (n_voxels > 0 && (!d_coef || !d_grad_coef))) {
+    set_err(err, err_len, "invalid argument: null pointer or negative voxel count");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    CSD_CUDA(cudaSetDevice(h->device));
+    HostGtab g = make_gtab(gtab);
+    if (spec->regularization == CSD_REG_NONNEG)
+      throw Error{CSD_ERR_INVALID, "the adjoint covers regularization l1 and l2"};
+    StreamScope scope(h, stream);
+    const bool is_l1 = spec->regularization == CSD_REG_L1;
+    h->launches = 0;
+    ensure_setup(h, g, spec->radial_order, spec->zeta, !is_l1, spec->lambda_n, spec->lambda_l);
+    if (n_voxels == 0) return CSD_OK;
+    csd::AdjointParams p{};
+    p.G = is_l1 ? h->G.as<double>() : h->A.as<double>();
+    p.Mt = h->Mt.as<double>();
+    p.X = d_coef;
+    p.ldx = h->K;
+    p.GC = d_grad_coef;
+    p.ldg = h->K;
+    p.V = n_voxels;
+    p.N = h->N;
+    p.K = h->K;
+    p.Kp = h->Kp;
+    p.radial_order = spec->radial_order;
+    p.n_samples = static_cast<double>(h->N);
+    p.gs32 = d_grad_signal;
+    p.gs64 = d_grad_signal64;
+    p.ghyper = d_grad_hyper;
+    h->adjstat.ensure(sizeof(unsigned long long));
+    CSD_CUDA(cudaMemsetAsync(h->adjstat.p, 0, sizeof(unsigned long long), h->stream));
+    p.n_singular = h->adjstat.as<unsigned long long>();
+    if (is_l1)
+      dispatch_rpl<L1Adj>(h->K, h, p);
+    else
+      dispatch_rpl<L2Adj>(h->K, h, p);
+    unsigned long long bad = 0;
+    CSD_CUDA(cudaMemcpyAsync(&bad, h->adjstat.p, sizeof bad, cudaMemcpyDeviceToHost, h->stream));
+    CSD_CUDA(cudaStreamSynchronize(h->stream));
+    if (bad > 0)
+      set_err(err, err_len,
+              (std::to_string(bad) + " voxel(s) have a support Gram matrix that is not positive definite; "
+                                     "their gradients are NaN")
+                  .c_str());
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}
+
+int csd_apply_rows_device(csd_handle* h, const double* d_At, int32_t rows, int32_t cols, const double* d_in,
+                          int64_t n_voxels, double* d_out, void* stream, char* err, size_t err_len) {
+  if (!h || rows <= 0 || cols <= 0 || n_voxels < 0 || (n_voxels > 0 && (!d_At || !d_in || !d_out))) {
+    set_err(err, err_len, "invalid argument: null pointer or bad shape");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    CSD_CUDA(cudaSetDevice(h->device));
+    StreamScope scope(h, stream);
+    h->launches = 0;
+    if (n_voxels > 0) launch_apply64(h, d_At, rows, cols, d_in, cols, n_voxels, d_out, rows);
+    CSD_CUDA(cudaStreamSynchronize(h->stream));
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}
+
+int csd_shore_odf_matrix(csd_handle* h, int32_t radial_order, double zeta, const double* dirs, int32_t n_dirs,
+                         double* out, char* err, size_t err_len) {
+  if (!h || !dirs || !out || n_dirs <= 0 || radial_order < 0 || radial_order % 2 != 0) {
+    set_err(err, err_len, "invalid argument: null pointer, no directions or odd radial order");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    CSD_CUDA(cudaSetDevice(h->device));
+    const int K = n_coeffs(radial_order);
+    cudaStream_t st = h->stream;
+    h->pdir.ensure(sizeof(double) * 3 * n_dirs);
+    h->pmat.ensure(sizeof(double) * static_cast<size_t>(n_dirs) * K);
+    CSD_CUDA(cudaMemcpyAsync(h->pdir.p, dirs, sizeof(double) * 3 * n_dirs, cudaMemcpyHostToDevice, st));
+    h->launches = 0;
+    csd::k_constraint<<<(n_dirs * K + 255) / 256, 256, 0, st>>>(h->pdir.as<double>(), n_dirs, K, radial_order, zeta,
+                                                               h->pmat.as<double>());
+    CSD_LAUNCH();
+    CSD_CUDA(cudaMemcpyAsync(out, h->pmat.p, sizeof(double) * static_cast<size_t>(n_dirs) * K,
+                             cudaMemcpyDeviceToHost, st));
+    CSD_CUDA(cudaStreamSynchronize(st));
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}
+
+int csd_shore_rtop_device(csd_handle* h, int32_t radial_order, double zeta, const double* d_coef, int64_t n_voxels,
+                          double* d_rtop, void* stream, char* err, size_t err_len) {
+  if (!h || n_voxels < 0 || (n_voxels > 0 && (!d_coef || !d_rtop))) {
+    set_err(err, err_len, "invalid argument: null pointer or negative voxel count");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    CSD_CUDA(cudaSetDevice(h->device));
+    StreamScope scope(h, stream);
+    h->launches = 0;
+    const csd::MicroConsts* mc = micro_consts(h, radial_order, zeta);
+    if (n_voxels > 0) {
+      csd::k_rtop64<<<grid1(n_voxels), 256, 0, h->stream>>>(mc, d_coef, n_coeffs(radial_order), n_voxels, d_rtop);
+      CSD_LAUNCH();
+    }
+    CSD_CUDA(cudaStreamSynchronize(h->stream));
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}
+
+int csd_shore_rtop_adjoint_device(csd_handle* h, int32_t radial_order, double zeta, const double* d_coef,
+                                  int64_t n_voxels, const double* d_grad_rtop, double* d_grad_coef, void* stream,
+                                  char* err, size_t err_len) {
+  if (!h || n_voxels < 0 || (n_voxels > 0 && (!d_coef || !d_grad_rtop || !d_grad_coef))) {
+    set_err(err, err_len, "invalid argument: null pointer or negative voxel count");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    CSD_CUDA(cudaSetDevice(h->device));
+    StreamScope scope(h, stream);
+    h->launches = 0;
+    const csd::MicroConsts* mc = micro_consts(h, radial_order, zeta);
+    const int K = n_coeffs(radial_order);
+    if (n_voxels > 0) {
+      csd::k_rtop64_adjoint<<<grid1(n_voxels), 256, 0, h->stream>>>(mc, d_coef, K, n_voxels, d_grad_rtop,
+                                                                    d_grad_coef, K);
+      CSD_LAUNCH();
+    }
+    CSD_CUDA(cudaStreamSynchronize(h->stream));
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}
+
+}  // extern "C"

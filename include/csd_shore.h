@@ -255,6 +255,69 @@ int csd_shore_microstructure(csd_handle* h, const float* coefficients, int64_t X
                              float outlier_factor, float* rtop, float* rtap, float* rtpp, float* msd,
                              float* qiv, float* ng, char* err, size_t err_len);
 
+/* ---- differentiable fit.  No counterpart in the reference, which computes
+ * no derivatives: these entry points differentiate the solution maps of its
+ * solvers (LASSO, src/solver/fista.rs:70-143; Tikhonov,
+ * src/solver/tikhonov.rs:26-76) and of the maps taken on coefficients.  All
+ * arrays are DEVICE memory of the handle's device, row-major; work is queued
+ * on `stream` (NULL = the handle's stream) and the calls return after it has
+ * finished. */
+
+/* Fit of a batch of voxel signals, float32 (n_voxels, N): regularization L1
+ * with alpha_mode FIXED (spec->alpha, or one alpha per voxel in `d_alpha`,
+ * nullable) and an optional warm start `d_warm` (n_voxels, K), or L2.
+ * FP64 coefficients (n_voxels, K) out; `d_iterations` (n_voxels) nullable.
+ * The per-voxel arithmetic is that of csd_shore_fit_volume. */
+int csd_shore_fit_batch_device(csd_handle* h, const float* d_signals, int64_t n_voxels,
+                               const csd_gtab* gtab, const csd_shore_spec* spec,
+                               const double* d_alpha, const double* d_warm, double* d_coef,
+                               uint32_t* d_iterations, void* stream, char* err, size_t err_len);
+
+/* Adjoint of that fit at the coefficients `d_coef` (n_voxels, K) for the
+ * upstream gradient `d_grad_coef` (n_voxels, K).  L1: implicit derivative on
+ * the support of each voxel's coefficients, w_S = G_SS^-1 g_S with
+ * G = M^T M; L2: w = H^-1 g with H the normal matrix.  Outputs (each
+ * nullable): the gradient on the signals M w as float32 and / or float64
+ * (n_voxels, N), and per voxel (n_voxels, 2) the gradient on the
+ * hyper-parameters: L1 (d/dalpha, 0) with d/dalpha = -N sign(c_S) . w_S, L2
+ * (d/dlambda_n, d/dlambda_l).  A voxel whose support matrix is not positive
+ * definite gets NaN gradients and a note in `err` (status stays 0). */
+int csd_shore_fit_adjoint_device(csd_handle* h, const csd_gtab* gtab, const csd_shore_spec* spec,
+                                 const double* d_coef, const double* d_grad_coef, int64_t n_voxels,
+                                 float* d_grad_signal, double* d_grad_signal64, double* d_grad_hyper,
+                                 void* stream, char* err, size_t err_len);
+
+/* out[v][r] = sum_k A[r][k] in[v][k] for a fixed matrix A given TRANSPOSED,
+ * `d_At` (cols, rows): in (n_voxels, cols), out (n_voxels, rows), FP64.
+ * With A an ODF matrix (below) this samples ODFs; with the design matrix of
+ * a target table it predicts signals (src/synth.rs:15-84); with A^T (pass A
+ * itself as d_At) it is the adjoint of either. */
+int csd_apply_rows_device(csd_handle* h, const double* d_At, int32_t rows, int32_t cols,
+                          const double* d_in, int64_t n_voxels, double* d_out, void* stream,
+                          char* err, size_t err_len);
+
+/* ODF amplitudes on `n_dirs` directions (n_dirs x 3, host) per SHORE
+ * coefficient: (n_dirs, K) host FP64 = sh2amp(dirs, radial_order) x the
+ * SHORE-to-Tournier projection (src/odf.rs:79-102), the SH values rounded to
+ * float32 as the reference's sh2amp table is. */
+int csd_shore_odf_matrix(csd_handle* h, int32_t radial_order, double zeta, const double* dirs,
+                         int32_t n_dirs, double* out, char* err, size_t err_len);
+
+/* RTOP (src/scalars/microstructure.rs:98-118) of FP64 coefficients
+ * (n_voxels, K) -> (n_voxels), and its adjoint: the gradient on the
+ * coefficients (n_voxels, K) for an upstream gradient (n_voxels). */
+int csd_shore_rtop_device(csd_handle* h, int32_t radial_order, double zeta, const double* d_coef,
+                          int64_t n_voxels, double* d_rtop, void* stream, char* err, size_t err_len);
+int csd_shore_rtop_adjoint_device(csd_handle* h, int32_t radial_order, double zeta,
+                                  const double* d_coef, int64_t n_voxels, const double* d_grad_rtop,
+                                  double* d_grad_coef, void* stream, char* err, size_t err_len);
+
+/* Class I geodesic sphere of `frequency` (10 f^2 + 2 vertices; 362 at f = 6),
+ * or one vertex per antipodal pair with `hemisphere`.  Writes the unit
+ * vectors (count x 3) to `out` when `capacity` >= count; returns the count,
+ * -1 for a frequency outside 1..64. */
+int csd_geodesic_sphere(int32_t frequency, int32_t hemisphere, double* out, int32_t capacity);
+
 /* Allocation-free fixed-alpha FISTA fit of a batch of voxels.
  *
  * No counterpart in the reference: it exists for callers that cannot let a

@@ -366,3 +366,98 @@ def microstructure_voxel(coefs, radial_order, zeta, direction=None):
 
 def micro_alpha_factor(n, l, zeta):
     return lib().oracle_micro_alpha_factor(n, l, zeta)
+
+
+# ------------------------------------------------------ derivatives of the fit
+# The reference computes no derivatives.  These restate, in plain FP64 numpy,
+# the implicit-function derivatives of the solution maps its solvers define:
+# the LASSO fit of src/solver/fista.rs:70-143, which minimises
+# (1/(2n)) ||M c - s||^2 + alpha ||c||_1 (c >= 0 when non_negative), and the
+# Tikhonov fit of src/solver/tikhonov.rs:26-76, H c = M^T s with
+# H = M^T M + lambda_N N + lambda_L L (src/basis/shore.rs:180-195).
+
+def l1_adjoint(M, c, gc):
+    """Adjoint of the LASSO solution map at ``c`` for the upstream gradient
+    ``gc``: on the support S the optimality condition
+    G_SS c_S = M_S^T s - n alpha sign(c_S) gives w_S = G_SS^-1 gc_S,
+    grad_s = M w and grad_alpha = -n sign(c_S) . w_S.  Returns
+    (grad_s, grad_alpha, w)."""
+    M, c, gc = _f64(M), _f64(c), _f64(gc)
+    n = M.shape[0]
+    S = np.flatnonzero(c != 0.0)
+    w = np.zeros_like(c)
+    if S.size:
+        MS = M[:, S]
+        w[S] = np.linalg.solve(MS.T @ MS, gc[S])
+    return M @ w, float(-n * (np.sign(c[S]) @ w[S])), w
+
+
+def l2_adjoint(M, c, gc, n_diag, l_diag, lambda_n, lambda_l):
+    """Adjoint of the Tikhonov solution map: w = H^-1 gc, grad_s = M w,
+    grad_lambda_N = -w . (N c), grad_lambda_L = -w . (L c).  Returns
+    (grad_s, (grad_lambda_N, grad_lambda_L), w)."""
+    M, c, gc, nd, ld = _f64(M), _f64(c), _f64(gc), _f64(n_diag), _f64(l_diag)
+    H = M.T @ M + np.diag(lambda_n * nd + lambda_l * ld)
+    w = np.linalg.solve(H, gc)
+    return M @ w, (float(-(w @ (nd * c))), float(-(w @ (ld * c)))), w
+
+
+def lasso_polish(M, s, alpha, c0, non_negative=False, margin=1e-6):
+    """The exact LASSO minimiser from an approximate one: solve the optimality
+    condition on the support and signs of ``c0``, then certify it - the signs
+    hold on the support and |M_j^T r| / n < alpha (1 - margin) off it
+    (M_j^T r / n > -alpha (1 - margin) with non_negative), r = s - M c.
+    Returns (c, certified)."""
+    M, s, c0 = _f64(M), _f64(s), _f64(c0)
+    n = M.shape[0]
+    S = np.flatnonzero(c0 != 0.0)
+    sg = np.sign(c0[S])
+    c = np.zeros_like(c0)
+    if S.size:
+        MS = M[:, S]
+        c[S] = np.linalg.solve(MS.T @ MS, MS.T @ s - n * alpha * sg)
+    corr = M.T @ (s - M @ c) / n
+    off = np.setdiff1d(np.arange(c0.size), S)
+    ok = bool(np.all(np.sign(c[S]) == sg))
+    if non_negative:
+        ok = ok and bool(np.all(sg > 0)) and bool(np.all(corr[off] < alpha * (1.0 - margin)))
+    else:
+        ok = ok and bool(np.all(np.abs(corr[off]) < alpha * (1.0 - margin)))
+    return c, ok
+
+
+def geodesic_sphere(frequency, hemisphere=False):
+    """Class I geodesic sphere: each icosahedron face cut into f^2 triangles on
+    a flat barycentric grid, the points projected on the unit sphere and the
+    shared ones kept once; 10 f^2 + 2 vertices.  Returned sorted
+    lexicographically (the product keeps generation order)."""
+    ph = (1.0 + math.sqrt(5.0)) / 2.0
+    ico = np.array([[-1, ph, 0], [1, ph, 0], [-1, -ph, 0], [1, -ph, 0], [0, -1, ph], [0, 1, ph], [0, -1, -ph],
+                    [0, 1, -ph], [ph, 0, -1], [ph, 0, 1], [-ph, 0, -1], [-ph, 0, 1]], dtype=np.float64)
+    ico /= np.linalg.norm(ico, axis=1, keepdims=True)
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+             (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    pts = {}
+    f = int(frequency)
+    for a, b, c in faces:
+        for i in range(f + 1):
+            for j in range(f + 1 - i):
+                p = ((f - i - j) * ico[a] + i * ico[b] + j * ico[c]) / f
+                p = p / np.linalg.norm(p)
+                pts.setdefault(tuple(np.round(p * 1e9).astype(np.int64)), p)
+    v = np.array(sorted(pts.values(), key=tuple))
+    if hemisphere:
+        e = 1e-12
+        keep = (v[:, 2] > e) | ((np.abs(v[:, 2]) <= e) & (v[:, 1] > e)) | \
+            ((np.abs(v[:, 2]) <= e) & (np.abs(v[:, 1]) <= e) & (v[:, 0] > 0))
+        v = v[keep]
+    return v
+
+
+def odf_matrix(dirs, radial_order, zeta):
+    """ODF amplitudes per SHORE coefficient on ``dirs``: sh2amp (Tournier, the
+    values rounded to float32) times the SHORE-to-Tournier projection at
+    lmax = radial_order (src/odf.rs:79-102)."""
+    lmax = radial_order - radial_order % 2
+    return sh2amp_cart(dirs, lmax) @ shore_to_tournier(radial_order, zeta, lmax)
