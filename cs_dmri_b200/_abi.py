@@ -171,7 +171,8 @@ def _declare(lib: C.CDLL) -> C.CDLL:
                                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + tail
     lib.csd_shore_fit_adjoint_device.restype = C.c_int
     lib.csd_shore_fit_adjoint_device.argtypes = [C.c_void_p, C.POINTER(Gtab), C.POINTER(Spec), C.c_void_p,
-                                                 C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p] + tail
+                                                 C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p] + tail
     lib.csd_apply_rows_device.restype = C.c_int
     lib.csd_apply_rows_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int64,
                                           C.c_void_p] + tail

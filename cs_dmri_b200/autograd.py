@@ -33,7 +33,6 @@ to the fit's own tolerance.
 from __future__ import annotations
 
 import ctypes as C
-import warnings
 
 import numpy as np
 import torch
@@ -149,6 +148,7 @@ class DifferentiableShore:
         self.device_index = int(device)
         self.device = torch.device("cuda", self.device_index)
         self._mats: dict = {}
+        self._singular = torch.zeros(1, dtype=torch.int64, device=self.device)
 
     # ---------------------------------------------------------------- public
     def fit(self, signals: torch.Tensor, alpha=None, *, lambda_n=None, lambda_l=None, warm=None) -> torch.Tensor:
@@ -267,12 +267,16 @@ class DifferentiableShore:
         gs32 = torch.empty((V, self.N), dtype=torch.float32, device=self.device) if signal32 else None
         gs64 = torch.empty((V, self.N), dtype=torch.float64, device=self.device) if signal64 else None
         gh = torch.empty((V, 2), dtype=torch.float64, device=self.device)
-        note = _call(_abi.load().csd_shore_fit_adjoint_device, _abi.handle(self.device_index), C.byref(self._g),
-                     C.byref(spec), coef.contiguous().data_ptr(), g.data_ptr(), V, _ptr(gs32), _ptr(gs64),
-                     gh.data_ptr(), _stream(g))
-        if note:
-            warnings.warn(note, RuntimeWarning, stacklevel=3)
+        _call(_abi.load().csd_shore_fit_adjoint_device, _abi.handle(self.device_index), C.byref(self._g),
+              C.byref(spec), coef.contiguous().data_ptr(), g.data_ptr(), V, _ptr(gs32), _ptr(gs64),
+              gh.data_ptr(), _ptr(self._singular), _stream(g))
         return (gs64 if signal64 else gs32), gh
+
+    @property
+    def singular_voxels(self) -> int:
+        """Voxels, over every backward pass so far, whose support Gram matrix
+        was not positive definite (their gradients are NaN)."""
+        return int(self._singular.item())
 
     def _apply_raw(self, At, rows, cols, x) -> torch.Tensor:
         x = x.detach().to(self.device, torch.float64).contiguous()

@@ -17,75 +17,64 @@
 //       w = H^{-1} gc,  grad_s = M w,
 //       grad_lambda_N = -w . (N c),  grad_lambda_L = -w . (L c).
 //
-// Every sum runs in index order with separate multiply and add (no fused
-// multiply-add), as a sequential FP64 evaluation does.
+// The factorisations and solves run every sum in index order with separate
+// multiply and add (no fused multiply-add), as a sequential FP64 evaluation
+// does; grad_s = M w is a fixed-matrix apply (k_apply64).
 #pragma once
 
 namespace csd {
 
 struct AdjointParams {
   const double* G;     // L1: Kp x Kp Gram M^T M; L2: the lower Cholesky factor of H (row-major, Kp stride)
-  const double* Mt;    // Kp x N transposed design
   const double* X;     // fitted coefficients, V rows of stride ldx
   int64_t ldx;
   const double* GC;    // upstream gradient on the coefficients, V rows of stride ldg
   int64_t ldg;
   int64_t V;
-  int N, K, Kp, radial_order;
+  int K, Kp, radial_order;
   double n_samples;    // n of the 1/(2n) data term
-  float* gs32;         // V x N gradient on the signal, f32 (nullable)
-  double* gs64;        // V x N, f64 (nullable)
+  double* W;           // V x Kp adjoint solution w (zero off the support)
   double* ghyper;      // V x 2 (nullable): L1 (d/dalpha, 0); L2 (d/dlambda_N, d/dlambda_L)
-  double* W;           // V x Kp adjoint solution w (nullable)
   unsigned long long* n_singular;  // voxels whose G_SS was not positive definite (nullable)
+  // L1 two-pass schedule: voxels whose support exceeds `cap` are appended to
+  // `overflow` in the first pass and solved by a second pass with cap = K
+  // over that list (`list`, length *list_len).
+  int cap;
+  const int64_t* list;
+  const unsigned long long* list_len;
+  int64_t* overflow;
+  unsigned long long* n_overflow;
 };
 
 // Start of column j of a packed lower triangle of order s stored by columns.
 __device__ __forceinline__ int packed_col(int j, int s) { return j * s - (j * (j - 1)) / 2; }
 
-// Per-warp shared memory of k_l1_adjoint, in doubles: the packed factor
-// (K (K + 1) / 2), the dense w (Kp), the support list (K ints).
-__host__ __device__ __forceinline__ int l1_adjoint_warp_doubles(int K, int Kp) {
-  return ((K * (K + 1) / 2 + Kp + (K + 1) / 2) + 1) & ~1;
-}
-
-// grad_s[n] = sum over k in index order of M[n][k] w[k], written for the
-// voxel's row; w dense in shared memory, zero off the support.
-__device__ __forceinline__ void adjoint_signal_row(const AdjointParams& p, int64_t v, const double* sw,
-                                                   const int* sidx, int s, int lane) {
-  for (int n = lane; n < p.N; n += 32) {
-    double acc = 0.0;
-    if (sidx) {
-      for (int q = 0; q < s; ++q) {
-        const int k = sidx[q];
-        acc = __dadd_rn(acc, __dmul_rn(p.Mt[static_cast<size_t>(k) * p.N + n], sw[k]));
-      }
-    } else {
-      for (int k = 0; k < p.K; ++k) acc = __dadd_rn(acc, __dmul_rn(p.Mt[static_cast<size_t>(k) * p.N + n], sw[k]));
-    }
-    if (p.gs64) p.gs64[v * p.N + n] = acc;
-    if (p.gs32) p.gs32[v * p.N + n] = static_cast<float>(acc);
-  }
+// Per-warp shared memory of k_l1_adjoint, in doubles: the packed factor of a
+// support of up to `cap` (cap (cap + 1) / 2) and the support list (K ints).
+__host__ __device__ __forceinline__ int l1_adjoint_warp_doubles(int cap, int K) {
+  return ((cap * (cap + 1) / 2 + (K + 1) / 2) + 1) & ~1;
 }
 
 // L1 adjoint, one warp per voxel.  The support is compacted with ballots
 // (index order), G_SS gathered into the warp's packed lower triangle and
 // factored right-looking (every entry receives its updates in index order,
 // as a sequential L L^T does), then L y = gc_S by columns and L^T w = y by
-// columns from the last row up.  A support matrix that is not positive
-// definite leaves the voxel's gradients NaN and is counted.
+// columns from the last row up; w is scattered into the voxel's row of W.
+// A support matrix that is not positive definite leaves the voxel's w and
+// alpha gradient NaN and is counted.
 template <int RPL>  // ceil(K / 32)
 __global__ void __launch_bounds__(256) k_l1_adjoint(AdjointParams p) {
   extern __shared__ __align__(16) double adj_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nw = blockDim.x >> 5;
-  const int K = p.K, Kp = p.Kp;
-  double* T = adj_smem + static_cast<size_t>(warp) * l1_adjoint_warp_doubles(K, Kp);
-  double* sw = T + K * (K + 1) / 2;
-  int* sidx = reinterpret_cast<int*>(sw + Kp);
+  const int K = p.K, Kp = p.Kp, cap = p.cap;
+  double* T = adj_smem + static_cast<size_t>(warp) * l1_adjoint_warp_doubles(cap, K);
+  int* sidx = reinterpret_cast<int*>(T + cap * (cap + 1) / 2);
   const double nan = __longlong_as_double(0x7ff8000000000000ll);
-  for (int64_t v = static_cast<int64_t>(blockIdx.x) * nw + warp; v < p.V;
-       v += static_cast<int64_t>(gridDim.x) * nw) {
+  const int64_t n_items = p.list ? static_cast<int64_t>(*p.list_len) : p.V;
+  for (int64_t it = static_cast<int64_t>(blockIdx.x) * nw + warp; it < n_items;
+       it += static_cast<int64_t>(gridDim.x) * nw) {
+    const int64_t v = p.list ? p.list[it] : it;
     const double* x = p.X + v * p.ldx;
     int s = 0;
 #pragma unroll
@@ -97,6 +86,11 @@ __global__ void __launch_bounds__(256) k_l1_adjoint(AdjointParams p) {
       s += __popc(b);
     }
     __syncwarp();
+    if (s > cap) {  // solved by the second pass
+      if (lane == 0) p.overflow[atomicAdd(p.n_overflow, 1ull)] = v;
+      __syncwarp();
+      continue;
+    }
     double rv[RPL], sg[RPL];
 #pragma unroll
     for (int c = 0; c < RPL; ++c) {
@@ -135,13 +129,9 @@ __global__ void __launch_bounds__(256) k_l1_adjoint(AdjointParams p) {
       }
       __syncwarp();
     }
+    double* wrow = p.W + v * Kp;
     if (!ok) {
-      for (int n = lane; n < p.N; n += 32) {
-        if (p.gs64) p.gs64[v * p.N + n] = nan;
-        if (p.gs32) p.gs32[v * p.N + n] = static_cast<float>(nan);
-      }
-      if (p.W)
-        for (int k = lane; k < Kp; k += 32) p.W[v * Kp + k] = nan;
+      for (int k = lane; k < Kp; k += 32) wrow[k] = nan;
       if (lane == 0) {
         if (p.ghyper) {
           p.ghyper[2 * v] = nan;
@@ -188,17 +178,13 @@ __global__ void __launch_bounds__(256) k_l1_adjoint(AdjointParams p) {
     for (int c = 0; c < RPL; ++c) dot = __dadd_rn(dot, __dmul_rn(sg[c], rv[c]));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(kFull, dot, o);
-    for (int k = lane; k < Kp; k += 32) sw[k] = 0.0;
+    for (int k = lane; k < Kp; k += 32) wrow[k] = 0.0;
     __syncwarp();
 #pragma unroll
     for (int c = 0; c < RPL; ++c) {
       const int q = lane + 32 * c;
-      if (q < s) sw[sidx[q]] = rv[c];
+      if (q < s) wrow[sidx[q]] = rv[c];
     }
-    __syncwarp();
-    if (p.W)
-      for (int k = lane; k < Kp; k += 32) p.W[v * Kp + k] = sw[k];
-    adjoint_signal_row(p, v, sw, sidx, s, lane);
     if (lane == 0 && p.ghyper) {
       p.ghyper[2 * v] = -p.n_samples * dot;
       p.ghyper[2 * v + 1] = 0.0;
@@ -208,7 +194,8 @@ __global__ void __launch_bounds__(256) k_l1_adjoint(AdjointParams p) {
 }
 
 // L2 adjoint, one warp per voxel, the factor of H staged once per CTA with
-// a padded row stride; then the hyper-parameter gradients and grad_s.
+// a padded row stride: w = H^{-1} gc into W and the hyper-parameter
+// gradients.
 template <int RPL>
 __global__ void __launch_bounds__(256) k_l2_adjoint(AdjointParams p) {
   extern __shared__ __align__(16) double adj_smem[];
@@ -218,7 +205,6 @@ __global__ void __launch_bounds__(256) k_l2_adjoint(AdjointParams p) {
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nw = blockDim.x >> 5;
-  double* sw = adj_smem + ((K * ld + 1) & ~1) + static_cast<size_t>(warp) * Kp;
   for (int64_t v = static_cast<int64_t>(blockIdx.x) * nw + warp; v < p.V;
        v += static_cast<int64_t>(gridDim.x) * nw) {
     double r[RPL];
@@ -277,47 +263,63 @@ __global__ void __launch_bounds__(256) k_l2_adjoint(AdjointParams p) {
 #pragma unroll
     for (int c = 0; c < RPL; ++c) {
       const int row = lane + 32 * c;
-      if (row < Kp) sw[row] = (row < K) ? r[c] : 0.0;
+      if (row < Kp) p.W[v * Kp + row] = (row < K) ? r[c] : 0.0;
     }
-    __syncwarp();
-    if (p.W)
-      for (int k = lane; k < Kp; k += 32) p.W[v * Kp + k] = sw[k];
-    adjoint_signal_row(p, v, sw, nullptr, K, lane);
     if (lane == 0 && p.ghyper) {
       p.ghyper[2 * v] = -dn;
       p.ghyper[2 * v + 1] = -dl;
     }
-    __syncwarp();
   }
 }
 
-// out[v][r] = sum over k < cols, in index order, of At[k * rows + r] in[v][k]:
-// a fixed matrix A (rows x cols, stored transposed so that a warp's lanes
-// read consecutive rows) applied to every voxel's vector.  Eight voxels per
-// warp, so each coalesced load of a column of A feeds eight products.
+// out[v][r] = sum over k < cols of At[k * rows + r] in[v][k]: a fixed matrix
+// A (rows x cols, stored transposed so that a warp's lanes read consecutive
+// rows) applied to every voxel's vector, FP64 with fused multiply-adds in
+// index order.  Eight voxels per warp: their inputs are staged in the warp's
+// shared slice as [k][voxel], so each coalesced load of a column of A feeds
+// eight FMAs with operands from four 16-byte broadcast reads.  Outputs in
+// FP64 and / or rounded to FP32 (each nullable).
 __global__ void __launch_bounds__(256) k_apply64(const double* __restrict__ At, int rows, int cols,
                                                  const double* __restrict__ in, int64_t ldin, int64_t V,
-                                                 double* __restrict__ out, int64_t ldout) {
-  const int lane = threadIdx.x & 31;
+                                                 double* __restrict__ out, float* __restrict__ out32,
+                                                 int64_t ldout) {
+  extern __shared__ __align__(16) double apply_smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* sI = apply_smem + static_cast<size_t>(warp) * 8 * cols;
   const int64_t groups = (V + 7) / 8;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
-  for (int64_t g = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); g < groups;
-       g += nwarps) {
+  for (int64_t g = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp; g < groups; g += nwarps) {
     const int64_t v0 = 8 * g;
     const int nv = V - v0 < 8 ? static_cast<int>(V - v0) : 8;
+    __syncwarp();
+    for (int j = 0; j < 8; ++j)
+      for (int k = lane; k < cols; k += 32) sI[k * 8 + j] = j < nv ? in[(v0 + j) * ldin + k] : 0.0;
+    __syncwarp();
+    const double2* sI2 = reinterpret_cast<const double2*>(sI);
     for (int r = lane; r < rows; r += 32) {
       double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       for (int k = 0; k < cols; ++k) {
         const double a = At[static_cast<size_t>(k) * rows + r];
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (j < nv) acc[j] = __dadd_rn(acc[j], __dmul_rn(a, in[(v0 + j) * ldin + k]));
+        for (int j = 0; j < 4; ++j) {
+          const double2 xv = sI2[k * 4 + j];
+          acc[2 * j] = fma(a, xv.x, acc[2 * j]);
+          acc[2 * j + 1] = fma(a, xv.y, acc[2 * j + 1]);
+        }
       }
 #pragma unroll
       for (int j = 0; j < 8; ++j)
-        if (j < nv) out[(v0 + j) * ldout + r] = acc[j];
+        if (j < nv) {
+          if (out) out[(v0 + j) * ldout + r] = acc[j];
+          if (out32) out32[(v0 + j) * ldout + r] = static_cast<float>(acc[j]);
+        }
     }
   }
+}
+
+__global__ void k_fill_u32(uint32_t* __restrict__ a, int64_t n, uint32_t v) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
 }
 
 // RTOP of FP64 coefficients (src/scalars/microstructure.rs:98-118):

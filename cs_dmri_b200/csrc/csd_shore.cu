@@ -276,7 +276,10 @@ struct csd_handle {
   cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t pev[20] = {};
   DevBuf iota;
-  DevBuf adjstat;  // adjoint: count of voxels with a singular support matrix
+  // differentiable fit: adjoint solution w, overflow list and its count, RTOP constants
+  DevBuf adjW, adjovf, adjstat, adjconst;
+  int adjconst_order = -1;
+  double adjconst_zeta = 0.0;
   int sm_cap = 0;  // > 0: FISTA grids use at most this many SMs
   double mixed_ms = 0.0, mixed_ops = 0.0;
   unsigned long long mixed_rerun = 0;
@@ -1540,7 +1543,7 @@ void csd_destroy(csd_handle* h) {
                     &h->pbest, &h->psel, &h->pact, &h->palpha_sel, &h->pit_sel, &h->pconv_sel,
                     &h->palpha_fb, &h->pit_fb, &h->pconv_fb, &h->pcode, &h->gdig, &h->gfexp, &h->flagged,
                     &h->mixstat, &h->pcoef, &h->pmat, &h->pout, &h->pgt, &h->pgv, &h->pdir, &h->pconst,
-                    &h->iota, &h->adjstat};
+                    &h->iota, &h->adjW, &h->adjovf, &h->adjstat, &h->adjconst};
   for (auto s : h->pipe)
     if (s) cudaStreamSynchronize(s);
   for (DevBuf* b : bufs) b->release();

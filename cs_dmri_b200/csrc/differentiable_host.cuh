@@ -48,11 +48,14 @@ std::vector<double> geodesic_sphere(int f, bool hemisphere) {
   return out;
 }
 
+// Queue a call's work on the caller's stream; NULL is the legacy default
+// stream (the calls return without waiting, so the work must be ordered with
+// what the caller does next on that stream).
 struct StreamScope {
   csd_handle* h;
   cudaStream_t saved;
   StreamScope(csd_handle* hh, void* stream) : h(hh), saved(hh->stream) {
-    if (stream) h->stream = static_cast<cudaStream_t>(stream);
+    h->stream = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
   }
   ~StreamScope() { h->stream = saved; }
 };
@@ -108,42 +111,68 @@ void run_fit_batch(csd_handle* h, const float* d_sig, int64_t V, const HostGtab&
   } else {
     launch_tikhonov(h, h->B.as<double>(), h->X.as<double>(), V);
     if (d_iters) {
-      std::vector<uint32_t> ones(static_cast<size_t>(V), 1u);
-      CSD_CUDA(cudaMemcpyAsync(d_iters, ones.data(), sizeof(uint32_t) * V, cudaMemcpyHostToDevice, st));
-      CSD_CUDA(cudaStreamSynchronize(st));
+      csd::k_fill_u32<<<grid1(V), 256, 0, st>>>(d_iters, V, 1u);
+      CSD_LAUNCH();
     }
   }
   CSD_CUDA(cudaMemcpy2DAsync(d_coef, sizeof(double) * K, h->X.p, sizeof(double) * Kp, sizeof(double) * K, V,
                              cudaMemcpyDeviceToDevice, st));
 }
 
+// Shared memory per warp of the first L1 pass: supports of up to this many
+// coefficients (larger ones go to the second pass).
+constexpr int kAdjSmallCap = 40;
+
 template <int RPL>
-void launch_l1_adjoint_t(csd_handle* h, const csd::AdjointParams& p) {
-  const size_t per_warp = sizeof(double) * static_cast<size_t>(csd::l1_adjoint_warp_doubles(p.K, p.Kp));
+void launch_l1_adjoint_t(csd_handle* h, const csd::AdjointParams& p0) {
+  cudaStream_t st = h->stream;
+  csd::AdjointParams p = p0;
+  // pass 1: every voxel, supports up to kAdjSmallCap in a small per-warp slice
+  p.cap = std::min(p.K, kAdjSmallCap);
+  p.list = nullptr;
+  p.list_len = nullptr;
+  {
+    const size_t per_warp = sizeof(double) * static_cast<size_t>(csd::l1_adjoint_warp_doubles(p.cap, p.K));
+    const int warps = 8;
+    const size_t smem = per_warp * warps;
+    CSD_CUDA(cudaFuncSetAttribute(csd::k_l1_adjoint<RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(std::max(smem, per_warp * 8))));
+    int per_sm = 0;
+    CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_l1_adjoint<RPL>, 32 * warps, smem));
+    const int64_t blocks = std::max<int64_t>(
+        1, std::min<int64_t>((p.V + warps - 1) / warps, static_cast<int64_t>(h->num_sms) * std::max(per_sm, 1)));
+    csd::k_l1_adjoint<RPL><<<static_cast<unsigned>(blocks), 32 * warps, smem, st>>>(p);
+    CSD_LAUNCH();
+  }
+  if (p.cap >= p.K) return;
+  // pass 2: the listed voxels with the full-size slice (count read on device)
+  p.cap = p.K;
+  p.list = p.overflow;
+  p.list_len = p.n_overflow;
+  p.overflow = nullptr;
+  p.n_overflow = nullptr;
+  const size_t per_warp = sizeof(double) * static_cast<size_t>(csd::l1_adjoint_warp_doubles(p.K, p.K));
   const int warps = static_cast<int>(std::min<size_t>(8, static_cast<size_t>(h->smem_optin) / per_warp));
   if (warps < 1) throw Error{CSD_ERR_INVALID, "coefficient count too large for the L1 adjoint"};
   const size_t smem = per_warp * warps;
   CSD_CUDA(cudaFuncSetAttribute(csd::k_l1_adjoint<RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem)));
-  int per_sm = 0;
-  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_l1_adjoint<RPL>, 32 * warps, smem));
-  const int64_t blocks = std::max<int64_t>(
-      1, std::min<int64_t>((p.V + warps - 1) / warps, static_cast<int64_t>(h->num_sms) * std::max(per_sm, 1)));
-  csd::k_l1_adjoint<RPL><<<static_cast<unsigned>(blocks), 32 * warps, smem, h->stream>>>(p);
+  csd::k_l1_adjoint<RPL><<<static_cast<unsigned>(h->num_sms), 32 * warps, smem, st>>>(p);
   CSD_LAUNCH();
 }
 
 template <int RPL>
 void launch_l2_adjoint_t(csd_handle* h, const csd::AdjointParams& p) {
   const int warps = 8;
-  const size_t smem =
-      sizeof(double) * ((static_cast<size_t>(p.K) * (p.K + 1) + 1) / 2 * 2 + static_cast<size_t>(warps) * p.Kp);
+  const size_t smem = sizeof(double) * ((static_cast<size_t>(p.K) * (p.K + 1) + 1) / 2 * 2);
   if (smem > static_cast<size_t>(h->smem_optin))
     throw Error{CSD_ERR_INVALID, "coefficient count too large for the L2 adjoint"};
   CSD_CUDA(cudaFuncSetAttribute(csd::k_l2_adjoint<RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem)));
-  const int64_t blocks =
-      std::max<int64_t>(1, std::min<int64_t>((p.V + warps - 1) / warps, static_cast<int64_t>(h->num_sms) * 2));
+  int per_sm = 0;
+  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_l2_adjoint<RPL>, 32 * warps, smem));
+  const int64_t blocks = std::max<int64_t>(
+      1, std::min<int64_t>((p.V + warps - 1) / warps, static_cast<int64_t>(h->num_sms) * std::max(per_sm, 1)));
   csd::k_l2_adjoint<RPL><<<static_cast<unsigned>(blocks), 32 * warps, smem, h->stream>>>(p);
   CSD_LAUNCH();
 }
@@ -169,21 +198,34 @@ struct L2Adj {
 };
 
 void launch_apply64(csd_handle* h, const double* At, int rows, int cols, const double* in, int64_t ldin, int64_t V,
-                    double* out, int64_t ldout) {
+                    double* out, float* out32, int64_t ldout) {
+  const size_t per_warp = sizeof(double) * 8 * static_cast<size_t>(cols);
+  const int warps = static_cast<int>(std::max<size_t>(1, std::min<size_t>(8, (100u << 10) / per_warp)));
+  const size_t smem = per_warp * warps;
+  if (smem > static_cast<size_t>(h->smem_optin)) throw Error{CSD_ERR_INVALID, "matrix too wide to apply"};
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_apply64, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  int per_sm = 0;
+  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_apply64, 32 * warps, smem));
   const int64_t groups = (V + 7) / 8;
-  const int64_t blocks =
-      std::max<int64_t>(1, std::min<int64_t>((groups + 7) / 8, static_cast<int64_t>(h->num_sms) * 8));
-  csd::k_apply64<<<static_cast<unsigned>(blocks), 256, 0, h->stream>>>(At, rows, cols, in, ldin, V, out, ldout);
+  const int64_t blocks = std::max<int64_t>(
+      1, std::min<int64_t>((groups + warps - 1) / warps, static_cast<int64_t>(h->num_sms) * std::max(per_sm, 1)));
+  csd::k_apply64<<<static_cast<unsigned>(blocks), 32 * warps, smem, h->stream>>>(At, rows, cols, in, ldin, V, out,
+                                                                                 out32, ldout);
   CSD_LAUNCH();
 }
 
+// RTOP constants for (radial_order, zeta), built once and kept on the handle.
 const csd::MicroConsts* micro_consts(csd_handle* h, int radial_order, double zeta) {
-  if (radial_order < 0 || radial_order > csd::kMicroMaxN - 1)
-    throw Error{CSD_ERR_INVALID, "radial order out of range for the RTOP constants"};
-  h->pconst.ensure(sizeof(csd::MicroConsts));
-  csd::k_micro_consts<<<1, 1, 0, h->stream>>>(radial_order, zeta, h->pconst.as<csd::MicroConsts>());
-  CSD_LAUNCH();
-  return h->pconst.as<csd::MicroConsts>();
+  if (radial_order < 0 || radial_order > csd::kMicroMaxN - 1 || radial_order % 2 != 0)
+    throw Error{CSD_ERR_INVALID, "radial order must be even and at most 14 for the RTOP constants"};
+  if (!(h->adjconst.p && h->adjconst_order == radial_order && h->adjconst_zeta == zeta)) {
+    h->adjconst.ensure(sizeof(csd::MicroConsts));
+    csd::k_micro_consts<<<1, 1, 0, h->stream>>>(radial_order, zeta, h->adjconst.as<csd::MicroConsts>());
+    CSD_LAUNCH();
+    h->adjconst_order = radial_order;
+    h->adjconst_zeta = zeta;
+  }
+  return h->adjconst.as<csd::MicroConsts>();
 }
 
 }  // namespace
@@ -216,7 +258,6 @@ int csd_shore_fit_batch_device(csd_handle* h, const float* d_signals, int64_t n_
       throw Error{CSD_ERR_INVALID, "the batch fit takes alpha_mode fixed (one alpha, or one per voxel)"};
     StreamScope scope(h, stream);
     run_fit_batch(h, d_signals, n_voxels, g, spec, d_alpha, d_warm, d_coef, d_iterations);
-    CSD_CUDA(cudaStreamSynchronize(h->stream));
   } catch (const Error& e) {
     set_err(err, err_len, e.msg);
     return e.code;
@@ -226,8 +267,8 @@ int csd_shore_fit_batch_device(csd_handle* h, const float* d_signals, int64_t n_
 
 int csd_shore_fit_adjoint_device(csd_handle* h, const csd_gtab* gtab, const csd_shore_spec* spec,
                                  const double* d_coef, const double* d_grad_coef, int64_t n_voxels,
-                                 float* d_grad_signal, double* d_grad_signal64, double* d_grad_hyper, void* stream,
-                                 char* err, size_t err_len) {
+                                 float* d_grad_signal, double* d_grad_signal64, double* d_grad_hyper,
+                                 uint64_t* d_n_singular, void* stream, char* err, size_t err_len) {
   if (!h || !gtab || !spec || n_voxels < 0 || (n_voxels > 0 && (!d_coef || !d_grad_coef))) {
     set_err(err, err_len, "invalid argument: null pointer or negative voxel count");
     return CSD_ERR_INVALID;
@@ -242,37 +283,35 @@ int csd_shore_fit_adjoint_device(csd_handle* h, const csd_gtab* gtab, const csd_
     h->launches = 0;
     ensure_setup(h, g, spec->radial_order, spec->zeta, !is_l1, spec->lambda_n, spec->lambda_l);
     if (n_voxels == 0) return CSD_OK;
+    const int N = h->N, K = h->K, Kp = h->Kp;
+    h->adjW.ensure(sizeof(double) * static_cast<size_t>(n_voxels) * Kp);
     csd::AdjointParams p{};
     p.G = is_l1 ? h->G.as<double>() : h->A.as<double>();
-    p.Mt = h->Mt.as<double>();
     p.X = d_coef;
-    p.ldx = h->K;
+    p.ldx = K;
     p.GC = d_grad_coef;
-    p.ldg = h->K;
+    p.ldg = K;
     p.V = n_voxels;
-    p.N = h->N;
-    p.K = h->K;
-    p.Kp = h->Kp;
+    p.K = K;
+    p.Kp = Kp;
     p.radial_order = spec->radial_order;
-    p.n_samples = static_cast<double>(h->N);
-    p.gs32 = d_grad_signal;
-    p.gs64 = d_grad_signal64;
+    p.n_samples = static_cast<double>(N);
+    p.W = h->adjW.as<double>();
     p.ghyper = d_grad_hyper;
-    h->adjstat.ensure(sizeof(unsigned long long));
-    CSD_CUDA(cudaMemsetAsync(h->adjstat.p, 0, sizeof(unsigned long long), h->stream));
-    p.n_singular = h->adjstat.as<unsigned long long>();
-    if (is_l1)
-      dispatch_rpl<L1Adj>(h->K, h, p);
-    else
-      dispatch_rpl<L2Adj>(h->K, h, p);
-    unsigned long long bad = 0;
-    CSD_CUDA(cudaMemcpyAsync(&bad, h->adjstat.p, sizeof bad, cudaMemcpyDeviceToHost, h->stream));
-    CSD_CUDA(cudaStreamSynchronize(h->stream));
-    if (bad > 0)
-      set_err(err, err_len,
-              (std::to_string(bad) + " voxel(s) have a support Gram matrix that is not positive definite; "
-                                     "their gradients are NaN")
-                  .c_str());
+    p.n_singular = reinterpret_cast<unsigned long long*>(d_n_singular);
+    if (is_l1) {
+      h->adjovf.ensure(sizeof(int64_t) * static_cast<size_t>(n_voxels));
+      h->adjstat.ensure(sizeof(unsigned long long));
+      CSD_CUDA(cudaMemsetAsync(h->adjstat.p, 0, sizeof(unsigned long long), h->stream));
+      p.overflow = h->adjovf.as<int64_t>();
+      p.n_overflow = h->adjstat.as<unsigned long long>();
+      dispatch_rpl<L1Adj>(K, h, p);
+    } else {
+      dispatch_rpl<L2Adj>(K, h, p);
+    }
+    if (d_grad_signal || d_grad_signal64)  // grad_s = M w
+      launch_apply64(h, h->Mt.as<double>(), N, K, h->adjW.as<double>(), Kp, n_voxels, d_grad_signal64, d_grad_signal,
+                     N);
   } catch (const Error& e) {
     set_err(err, err_len, e.msg);
     return e.code;
@@ -290,8 +329,7 @@ int csd_apply_rows_device(csd_handle* h, const double* d_At, int32_t rows, int32
     CSD_CUDA(cudaSetDevice(h->device));
     StreamScope scope(h, stream);
     h->launches = 0;
-    if (n_voxels > 0) launch_apply64(h, d_At, rows, cols, d_in, cols, n_voxels, d_out, rows);
-    CSD_CUDA(cudaStreamSynchronize(h->stream));
+    if (n_voxels > 0) launch_apply64(h, d_At, rows, cols, d_in, cols, n_voxels, d_out, nullptr, rows);
   } catch (const Error& e) {
     set_err(err, err_len, e.msg);
     return e.code;
@@ -341,7 +379,6 @@ int csd_shore_rtop_device(csd_handle* h, int32_t radial_order, double zeta, cons
       csd::k_rtop64<<<grid1(n_voxels), 256, 0, h->stream>>>(mc, d_coef, n_coeffs(radial_order), n_voxels, d_rtop);
       CSD_LAUNCH();
     }
-    CSD_CUDA(cudaStreamSynchronize(h->stream));
   } catch (const Error& e) {
     set_err(err, err_len, e.msg);
     return e.code;
@@ -367,7 +404,6 @@ int csd_shore_rtop_adjoint_device(csd_handle* h, int32_t radial_order, double ze
                                                                     d_grad_coef, K);
       CSD_LAUNCH();
     }
-    CSD_CUDA(cudaStreamSynchronize(h->stream));
   } catch (const Error& e) {
     set_err(err, err_len, e.msg);
     return e.code;

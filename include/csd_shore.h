@@ -259,9 +259,12 @@ int csd_shore_microstructure(csd_handle* h, const float* coefficients, int64_t X
  * no derivatives: these entry points differentiate the solution maps of its
  * solvers (LASSO, src/solver/fista.rs:70-143; Tikhonov,
  * src/solver/tikhonov.rs:26-76) and of the maps taken on coefficients.  All
- * arrays are DEVICE memory of the handle's device, row-major; work is queued
- * on `stream` (NULL = the handle's stream) and the calls return after it has
- * finished. */
+ * arrays are DEVICE memory of the handle's device, row-major.  Work is
+ * queued on `stream` (NULL = the legacy default stream) and the calls return
+ * once it is queued, without waiting for it (a call that builds a new
+ * gradient table's setup waits for that setup): results are ready when the
+ * stream reaches them.  Calls on one handle share its scratch buffers, so they must
+ * be ordered on one stream. */
 
 /* Fit of a batch of voxel signals, float32 (n_voxels, N): regularization L1
  * with alpha_mode FIXED (spec->alpha, or one alpha per voxel in `d_alpha`,
@@ -281,11 +284,12 @@ int csd_shore_fit_batch_device(csd_handle* h, const float* d_signals, int64_t n_
  * (n_voxels, N), and per voxel (n_voxels, 2) the gradient on the
  * hyper-parameters: L1 (d/dalpha, 0) with d/dalpha = -N sign(c_S) . w_S, L2
  * (d/dlambda_n, d/dlambda_l).  A voxel whose support matrix is not positive
- * definite gets NaN gradients and a note in `err` (status stays 0). */
+ * definite gets NaN gradients and is added to the device counter
+ * `d_n_singular` (nullable). */
 int csd_shore_fit_adjoint_device(csd_handle* h, const csd_gtab* gtab, const csd_shore_spec* spec,
                                  const double* d_coef, const double* d_grad_coef, int64_t n_voxels,
                                  float* d_grad_signal, double* d_grad_signal64, double* d_grad_hyper,
-                                 void* stream, char* err, size_t err_len);
+                                 uint64_t* d_n_singular, void* stream, char* err, size_t err_len);
 
 /* out[v][r] = sum_k A[r][k] in[v][k] for a fixed matrix A given TRANSPOSED,
  * `d_At` (cols, rows): in (n_voxels, cols), out (n_voxels, rows), FP64.
