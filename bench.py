@@ -23,6 +23,10 @@ error of the mixed path against the FP64 path).
           MEASURED_PEAKS.json).  The kernel skips k-steps whose iterate entries
           are all exactly zero, so the tensor FLOPs it executes (counted on the
           device, also reported) are fewer than the algorithmic count.
+* fwd_bwd the metric's second half: the differentiable fit of 50,000 voxels
+          (fit + RTOP + 362-direction ODF, then backward to the signals and the
+          hyper-parameter), voxels/s for L1 and Tikhonov, and the ratio of the
+          forward+backward step to the forward step.
 * cpu_baseline  the CPU FP64 oracle (a restatement of the reference's rayon
           path: the Rust reference cannot be built without cargo) on all host
           threads, on a bounded sample of the same voxels.
@@ -48,7 +52,8 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "SHORE L1-fit voxels/s, mixed vs FP64 GPU at <=1e-5 rel err"
+METRIC = "SHORE L1-fit voxels/s, mixed vs FP64 GPU at \u22641e-5 rel err; fwd+bwd voxels/s"
+FWD_BWD_GRID = (50, 50, 20)  # the differentiable-fit workload: 50,000 voxels, radial order 6
 WORKLOAD = "brain300k"
 
 
@@ -362,6 +367,9 @@ def run_ours(args):
     h2d = V * N * 4 + ph.mask.nbytes
     d2h = out["coefficients"].nbytes
 
+    # ---- fwd+bwd: differentiable fit of 50k voxels
+    fwd_bwd = fwd_bwd_block(args, device, world)
+
     # ---- roofline of the FISTA kernel
     flops_per_iter = 2 * K * K + 8 * K
     k_ms = statistics.median(kernel_ms)
@@ -415,6 +423,7 @@ def run_ours(args):
                          "peak_source": "FP64 DMMA microbenchmark measured in this run (libcsdpeak); "
                                         f"scalar DFMA measured {dfma_peak:.1f} TFLOP/s" if dmma_peak else None},
             "gpu_launches": launches if path == "fp64" else mix_launches,
+            "fwd_bwd": fwd_bwd,
             "paths": paths,
             "clocks": clocks.summary(),
             "iterations_per_voxel": it_launch / V,
@@ -426,6 +435,67 @@ def run_ours(args):
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def fwd_bwd_block(args, device: int, world: int) -> dict:
+    """Differentiable fit (forward + adjoint) on 50,000 voxels of the same
+    generator, radial order 6.  One step: the fit (L1 at alpha 0.01, or
+    Tikhonov at lambda 0.05), RTOP and the ODF on the 362-vertex geodesic
+    sphere, then backward to the float32 signals and the float64
+    hyper-parameters, every kernel in libcsdshore.so.  CUDA events on the
+    stream the calls run on; max over ranks.  Inputs stay resident (52 MB of
+    signals; the step's own buffers exceed L2 several times over)."""
+    import torch
+
+    from cs_dmri_b200.autograd import DifferentiableShore
+    from cs_dmri_b200.phantom import make_phantom
+
+    ph = make_phantom(FWD_BWD_GRID, seed=4)
+    S = torch.from_numpy(ph.data.reshape(-1, ph.data.shape[-1])).to(f"cuda:{device}")
+    V = S.shape[0]
+    out = {"metric": "fwd+bwd voxels/s", "workload": f"diff50k: {V} voxels, radial order 6, N = {S.shape[1]}",
+           "unit": "voxels/s", "dtype": "f64 (signals f32)",
+           "step": "fit + RTOP + ODF (362 directions) forward, backward to signals and the hyper-parameter"}
+    for reg in ("l1", "l2"):
+        m = DifferentiableShore(ph.bvals, ph.bvecs, regularization=reg, big_delta=ph.big_delta,
+                                small_delta=ph.small_delta, device=device)
+
+        def step(bwd: bool):
+            s = S.detach().requires_grad_(bwd)
+            if reg == "l1":
+                a = torch.tensor(0.01, dtype=torch.float64, device=S.device, requires_grad=bwd)
+                c = m.fit(s, a)
+            else:
+                a = torch.tensor(0.05, dtype=torch.float64, device=S.device, requires_grad=bwd)
+                c = m.fit(s, lambda_n=a, lambda_l=a)
+            loss = m.rtop(c).sum() + 1e-3 * m.odf(c).square().sum()
+            if bwd:
+                loss.backward()
+
+        res = {}
+        for bwd in (False, True):
+            for _ in range(args.warmup):
+                step(bwd)
+            torch.cuda.synchronize(device)
+            barrier(world)
+            st = torch.cuda.current_stream(device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(args.steps):
+                step(bwd)
+            e1.record(st)
+            torch.cuda.synchronize(device)
+            ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, torch.device("cuda", device))
+            res["fwd_bwd" if bwd else "fwd"] = ms
+        block = {"value": world * V / (res["fwd_bwd"] * 1e-3), "ms_per_step": res["fwd_bwd"],
+                 "fwd_value": world * V / (res["fwd"] * 1e-3), "fwd_ms_per_step": res["fwd"],
+                 "fwd_bwd_over_fwd": res["fwd_bwd"] / res["fwd"]}
+        if reg == "l1":
+            out.update(block)
+            out["solver"] = "L1 FISTA, alpha 0.01 (tol 1e-6), implicit differentiation on the support"
+        else:
+            out["l2"] = dict(block, solver="Tikhonov, lambda_n = lambda_l = 0.05, transpose solve")
+    return out
 
 
 def main():

@@ -245,7 +245,7 @@ class DifferentiableShore:
     def _spec_for(self, hyper: torch.Tensor) -> _abi.Spec:
         kw = dict(self._kw)
         if self.regularization == "l1":
-            kw["alpha"] = float(hyper) if hyper.dim() == 0 else 0.0
+            kw["alpha"] = 0.0  # the fit reads alpha per voxel from the device (no host round trip)
         else:
             h = hyper.detach().cpu().numpy()
             kw["lambda_n"], kw["lambda_l"] = float(h[0]), float(h[1])
@@ -254,7 +254,7 @@ class DifferentiableShore:
     def _fit_raw(self, signals, hyper, spec, warm) -> torch.Tensor:
         s = signals.detach().contiguous()
         V = s.shape[0]
-        alpha_v = hyper.detach().contiguous() if (self.regularization == "l1" and hyper.dim() == 1) else None
+        alpha_v = hyper.detach().expand(V).contiguous() if self.regularization == "l1" else None
         coef = torch.empty((V, self.K), dtype=torch.float64, device=self.device)
         lib = _abi.load()
         _call(lib.csd_shore_fit_batch_device, _abi.handle(self.device_index), s.data_ptr(), V, C.byref(self._g),
