@@ -124,6 +124,7 @@ EXPORTS = (
     "csd_shore_rtop_device",
     "csd_shore_rtop_adjoint_device",
     "csd_geodesic_sphere",
+    "csd_shore_odf_peaks",
 )
 
 _lib = None
@@ -185,6 +186,9 @@ def _declare(lib: C.CDLL) -> C.CDLL:
     lib.csd_shore_rtop_adjoint_device.restype = C.c_int
     lib.csd_shore_rtop_adjoint_device.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_void_p, C.c_int64,
                                                   C.c_void_p, C.c_void_p] + tail
+    lib.csd_shore_odf_peaks.restype = C.c_int
+    lib.csd_shore_odf_peaks.argtypes = vol + [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double] + \
+        [C.c_void_p] * 4 + [C.c_char_p, C.c_size_t]
     lib.csd_geodesic_sphere.restype = C.c_int
     lib.csd_geodesic_sphere.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_int32]
     return lib

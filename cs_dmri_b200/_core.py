@@ -347,6 +347,41 @@ def shore_odf_sh(coefficients, radial_order, zeta, lmax, mask=None, *, n_threads
     return out
 
 
+def shore_odf_peaks(coefficients, radial_order, zeta, mask=None, *, sphere_frequency=6, npeaks=5,
+                    relative_peak_threshold=0.5, min_separation_angle=25.0, device: int = 0) -> dict:
+    """GFA and ODF peaks of a coefficient volume (the quantities the
+    reference's SHORE ODX export computes, src/io/odx_out.rs:1008-1090, with
+    its defaults npeaks 5, relative threshold 0.5, separation 25 degrees).
+
+    The ODF is sampled on the hemisphere of a class I geodesic sphere of
+    ``sphere_frequency`` (181 directions at 6), amplitudes clipped at 0.
+    Returns ``gfa`` (X, Y, Z), ``peak_dirs`` (X, Y, Z, npeaks, 3) unit
+    vectors in the fit frame, ``peak_values`` (X, Y, Z, npeaks) ODF
+    amplitudes and ``peak_qa`` (X, Y, Z, npeaks) amplitudes above the voxel's
+    smallest sampled amplitude; slots past the peaks found are zero, as is
+    everything outside ``mask``."""
+    c = _coefficient_volume(coefficients, radial_order)
+    X, Y, Z, _ = c.shape
+    m8 = None
+    if mask is not None:
+        m = np.asarray(mask)
+        if m.shape != (X, Y, Z):
+            raise ValueError("mask does not match the coefficient grid")
+        m8 = np.ascontiguousarray(m.astype(bool)).view(np.uint8)
+    npeaks = int(npeaks)
+    out = {"gfa": np.empty((X, Y, Z), np.float32), "peak_dirs": np.empty((X, Y, Z, max(npeaks, 0), 3), np.float32),
+           "peak_values": np.empty((X, Y, Z, max(npeaks, 0)), np.float32),
+           "peak_qa": np.empty((X, Y, Z, max(npeaks, 0)), np.float32)}
+    err = C.create_string_buffer(4096)
+    code = _abi.load().csd_shore_odf_peaks(
+        _abi.handle(device), c.ctypes.data, X, Y, Z, int(radial_order), float(zeta),
+        None if m8 is None else m8.ctypes.data, int(sphere_frequency), npeaks, float(relative_peak_threshold),
+        float(min_separation_angle), out["gfa"].ctypes.data, out["peak_dirs"].ctypes.data,
+        out["peak_values"].ctypes.data, out["peak_qa"].ctypes.data, err, len(err))
+    _abi.check(code, err)
+    return out
+
+
 _MICRO = ("rtop", "rtap", "rtpp", "msd", "qiv", "ng")
 
 

@@ -23,6 +23,7 @@
 #include <array>
 #include <cmath>
 #include <map>
+#include <set>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -40,6 +41,7 @@
 #include "mixed_kernels.cuh"
 #include "epilogue_kernels.cuh"
 #include "adjoint_kernels.cuh"
+#include "odf_kernels.cuh"
 
 namespace {
 
@@ -2149,4 +2151,6 @@ extern "C" int csd_shore_fista_batch_noalloc(const csd_gtab* gtab, const csd_sho
   return CSD_OK;
 }
 
+#include "sphere_host.cuh"
 #include "differentiable_host.cuh"
+#include "peaks_host.cuh"

@@ -7,47 +7,6 @@
 
 namespace {
 
-// Class I geodesic sphere: every face of the icosahedron split into f^2
-// triangles on a flat barycentric grid, the grid points projected on the unit
-// sphere, shared edge points kept once (in first-seen order).  Frequency 6
-// gives 362 vertices.  With `hemisphere` one vertex of each antipodal pair is
-// kept (z > 0, or z = 0 and y > 0, or z = y = 0 and x > 0).
-std::vector<double> geodesic_sphere(int f, bool hemisphere) {
-  const double ph = (1.0 + std::sqrt(5.0)) / 2.0;
-  std::vector<std::array<double, 3>> ico = {{-1, ph, 0}, {1, ph, 0},   {-1, -ph, 0}, {1, -ph, 0},
-                                            {0, -1, ph}, {0, 1, ph},   {0, -1, -ph}, {0, 1, -ph},
-                                            {ph, 0, -1}, {ph, 0, 1},   {-ph, 0, -1}, {-ph, 0, 1}};
-  for (auto& a : ico) {
-    const double n = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
-    for (auto& c : a) c /= n;
-  }
-  const int faces[20][3] = {{0, 11, 5}, {0, 5, 1},  {0, 1, 7},   {0, 7, 10}, {0, 10, 11},
-                            {1, 5, 9},  {5, 11, 4}, {11, 10, 2}, {10, 7, 6}, {7, 1, 8},
-                            {3, 9, 4},  {3, 4, 2},  {3, 2, 6},   {3, 6, 8},  {3, 8, 9},
-                            {4, 9, 5},  {2, 4, 11}, {6, 2, 10},  {8, 6, 7},  {9, 8, 1}};
-  std::vector<double> out;
-  std::map<std::array<long long, 3>, int> seen;
-  for (const auto& t : faces)
-    for (int i = 0; i <= f; ++i)
-      for (int j = 0; i + j <= f; ++j) {
-        const double wa = static_cast<double>(f - i - j) / f, wb = static_cast<double>(i) / f,
-                     wc = static_cast<double>(j) / f;
-        std::array<double, 3> p;
-        for (int d = 0; d < 3; ++d) p[d] = wa * ico[t[0]][d] + wb * ico[t[1]][d] + wc * ico[t[2]][d];
-        const double n = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
-        for (auto& c : p) c /= n;
-        const std::array<long long, 3> key = {std::llround(p[0] * 1e9), std::llround(p[1] * 1e9),
-                                              std::llround(p[2] * 1e9)};
-        if (seen.count(key)) continue;
-        seen[key] = 1;
-        const double e = 1e-12;
-        const bool keep = !hemisphere || (p[2] > e) || (std::fabs(p[2]) <= e && p[1] > e) ||
-                          (std::fabs(p[2]) <= e && std::fabs(p[1]) <= e && p[0] > 0.0);
-        if (keep) out.insert(out.end(), p.begin(), p.end());
-      }
-  return out;
-}
-
 // Queue a call's work on the caller's stream; NULL is the legacy default
 // stream (the calls return without waiting, so the work must be ordered with
 // what the caller does next on that stream).
@@ -234,7 +193,8 @@ extern "C" {
 
 int csd_geodesic_sphere(int32_t frequency, int32_t hemisphere, double* out, int32_t capacity) {
   if (frequency < 1 || frequency > 64) return -1;
-  const std::vector<double> v = geodesic_sphere(frequency, hemisphere != 0);
+  const SphereMesh m = geodesic_mesh(frequency);
+  const std::vector<double> v = hemisphere ? m.hemisphere() : m.v;
   const int n = static_cast<int>(v.size() / 3);
   if (out && capacity >= n) std::memcpy(out, v.data(), sizeof(double) * v.size());
   return n;

@@ -169,6 +169,19 @@ class ShoreFit:
                                   small_delta=self.sidecar["small_delta_seconds"], n_threads=n_threads)
         return np.maximum(out, 0) if clip else out
 
+    def peaks(self, *, npeaks: int = 5, relative_peak_threshold: float = 0.5, min_separation_angle: float = 25.0,
+              sphere_frequency: int = 6) -> dict:
+        """GFA and ODF peaks inside the mask (``shore_odf_peaks``; the
+        quantities of the reference's ODX export, src/io/odx_out.rs:1008-1090).
+        Peak directions are returned in the image's voxel-axis frame."""
+        out = _core.shore_odf_peaks(self.coefficients, self.radial_order, self.zeta, self.mask,
+                                    sphere_frequency=sphere_frequency, npeaks=npeaks,
+                                    relative_peak_threshold=relative_peak_threshold,
+                                    min_separation_angle=min_separation_angle)
+        d = out["peak_dirs"]
+        out["peak_dirs"] = _rotate(d.reshape(-1, 3), self._rotation.T).reshape(d.shape).astype(np.float32)
+        return out
+
     def microstructure(self, directions=None, *, units: str = "um", outlier_factor: float | None = 10.0,
                        n_threads=None) -> dict:
         """RTOP, RTAP, RTPP, MSD, QIV and NG maps (python/cs_dmri/shore.py:183-205).

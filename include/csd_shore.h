@@ -255,6 +255,26 @@ int csd_shore_microstructure(csd_handle* h, const float* coefficients, int64_t X
                              float outlier_factor, float* rtop, float* rtap, float* rtpp, float* msd,
                              float* qiv, float* ng, char* err, size_t err_len);
 
+/* GFA and ODF peaks of every masked voxel (NULL mask = every voxel): the
+ * quantities the reference's SHORE ODX export computes
+ * (src/io/odx_out.rs:1008-1090; defaults there: npeaks 5, relative
+ * threshold 0.5, separation 25 degrees).  The ODF is sampled on the
+ * hemisphere of the class I geodesic sphere of `sphere_frequency` (1..10;
+ * 181 directions at 6) - the reference samples DSI Studio's ODF8
+ * hemisphere, not available here - with amplitudes clipped at 0.  GFA per
+ * odx_out.rs:1036-1050; peaks are mesh local maxima in decreasing amplitude,
+ * stopping below relative_peak_threshold x the largest, skipping any within
+ * min_separation_angle_deg of a kept one, up to npeaks (1..8).  Outputs
+ * (host, f32): gfa (X, Y, Z); peak_dirs (X, Y, Z, npeaks, 3) unit vectors in
+ * the fit frame; peak_values / peak_qa (X, Y, Z, npeaks), the amplitude and
+ * the amplitude above the voxel's smallest sampled one; zeros past the peaks
+ * found and outside the mask. */
+int csd_shore_odf_peaks(csd_handle* h, const float* coefficients, int64_t X, int64_t Y, int64_t Z,
+                        int32_t radial_order, double zeta, const uint8_t* mask, int32_t sphere_frequency,
+                        int32_t npeaks, double relative_peak_threshold, double min_separation_angle_deg,
+                        float* gfa, float* peak_dirs, float* peak_values, float* peak_qa, char* err,
+                        size_t err_len);
+
 /* ---- differentiable fit.  No counterpart in the reference, which computes
  * no derivatives: these entry points differentiate the solution maps of its
  * solvers (LASSO, src/solver/fista.rs:70-143; Tikhonov,

@@ -461,3 +461,103 @@ def odf_matrix(dirs, radial_order, zeta):
     lmax = radial_order (src/odf.rs:79-102)."""
     lmax = radial_order - radial_order % 2
     return sh2amp_cart(dirs, lmax) @ shore_to_tournier(radial_order, zeta, lmax)
+
+
+# ------------------------------------------------------------- ODF peaks, GFA
+# The quantities of the SHORE ODX export (src/io/odx_out.rs:1008-1090): the ODF
+# sampled on a hemisphere, GFA in the form written at odx_out.rs:1036-1050,
+# peaks with a relative threshold and a separation angle.  The reference
+# samples DSI Studio's ODF8 hemisphere and finds peaks with odx-rs (source
+# absent); this restates a mesh local-maximum finder on the hemisphere of the
+# class I geodesic sphere, so directions and GFA are not pinned to the
+# reference's sphere.
+
+def geodesic_mesh(frequency):
+    """(vertices (n, 3), edges (m, 2), hemisphere index of every vertex) of the
+    class I geodesic sphere, vertices in generation order: faces of the
+    icosahedron in a fixed order, grid points (i, j) with i + j <= f."""
+    ph = (1.0 + math.sqrt(5.0)) / 2.0
+    ico = np.array([[-1, ph, 0], [1, ph, 0], [-1, -ph, 0], [1, -ph, 0], [0, -1, ph], [0, 1, ph], [0, -1, -ph],
+                    [0, 1, -ph], [ph, 0, -1], [ph, 0, 1], [-ph, 0, -1], [-ph, 0, 1]], dtype=np.float64)
+    ico /= np.linalg.norm(ico, axis=1, keepdims=True)
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+             (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    f = int(frequency)
+    ids, verts, edges = {}, [], set()
+    for a, b, c in faces:
+        grid = {}
+        for i in range(f + 1):
+            for j in range(f + 1 - i):
+                p = ((f - i - j) * ico[a] + i * ico[b] + j * ico[c]) / f
+                p = p / np.linalg.norm(p)
+                key = tuple(np.round(p * 1e9).astype(np.int64))
+                if key not in ids:
+                    ids[key] = len(verts)
+                    verts.append(p)
+                grid[i, j] = ids[key]
+        for i in range(f):
+            for j in range(f - i):
+                for u, w in ((grid[i, j], grid[i + 1, j]), (grid[i, j], grid[i, j + 1]),
+                             (grid[i + 1, j], grid[i, j + 1])):
+                    edges.add((min(u, w), max(u, w)))
+    v = np.array(verts)
+    e = 1e-12
+    upper = (v[:, 2] > e) | ((np.abs(v[:, 2]) <= e) & (v[:, 1] > e)) | \
+        ((np.abs(v[:, 2]) <= e) & (np.abs(v[:, 1]) <= e) & (v[:, 0] > 0))
+    hemi = np.full(len(v), -1)
+    hemi[upper] = np.arange(upper.sum())
+    for i in np.flatnonzero(~upper):
+        j = ids.get(tuple(np.round(-v[i] * 1e9).astype(np.int64)))
+        if j is not None:
+            hemi[i] = hemi[j]
+    return v, np.array(sorted(edges)), hemi
+
+
+def _is_upper(p, e=1e-12):
+    return p[2] > e or (abs(p[2]) <= e and p[1] > e) or (abs(p[2]) <= e and abs(p[1]) <= e and p[0] > 0)
+
+
+def odf_peaks(coefs, radial_order, zeta, frequency=6, npeaks=5, relative_peak_threshold=0.5,
+              min_separation_angle=25.0):
+    """GFA, peak directions (npeaks, 3), amplitudes and QA of one voxel's
+    coefficients: amplitudes on the hemisphere clipped at 0; GFA =
+    sqrt(max(0, n/(n-1) (m2 - m1^2/n) / m2)); local maxima of the mesh (not
+    below any neighbour, antipodes folded), in decreasing amplitude, stop below
+    the relative threshold x the largest, skip any within the separation
+    angle of a kept peak."""
+    v, edges, hemi = geodesic_mesh(frequency)
+    R = int(hemi.max()) + 1
+    dirs = np.zeros((R, 3))
+    first = np.full(R, -1)
+    for i in range(len(v)):  # the upper vertex of each pair comes first in hemisphere numbering
+        if first[hemi[i]] < 0 and _is_upper(v[i]):
+            first[hemi[i]] = i
+            dirs[hemi[i]] = v[i]
+    nbrs = [set() for _ in range(R)]
+    for a, b in edges:
+        ha, hb = hemi[a], hemi[b]
+        if ha >= 0 and hb >= 0 and ha != hb:
+            nbrs[ha].add(hb)
+            nbrs[hb].add(ha)
+    A = odf_matrix(dirs, radial_order, zeta)
+    amp = np.maximum(A @ _f64(coefs), 0.0)
+    n = float(R)
+    m1, m2 = amp.sum(), (amp * amp).sum()
+    gfa = math.sqrt(max((n / (n - 1.0)) * (m2 - m1 * m1 / n) / m2, 0.0)) if m2 > 0 and R > 1 else 0.0
+    cand = [r for r in range(R) if amp[r] > 0 and all(amp[r] >= amp[q] for q in nbrs[r])]
+    cand.sort(key=lambda r: (-amp[r], r))
+    cos_sep = math.cos(math.radians(min_separation_angle))
+    out_d, out_v = [], []
+    for r in cand:
+        if len(out_d) == npeaks or amp[r] < relative_peak_threshold * amp[cand[0]]:
+            break
+        if all(abs(dirs[r] @ d) < cos_sep for d in out_d):
+            out_d.append(dirs[r])
+            out_v.append(amp[r])
+    D = np.zeros((npeaks, 3))
+    Vv = np.zeros(npeaks)
+    D[:len(out_d)] = out_d
+    Vv[:len(out_v)] = out_v
+    qa = np.where(Vv > 0, np.maximum(Vv - amp.min(), 0.0), 0.0)
+    return gfa, D, Vv, qa, amp
