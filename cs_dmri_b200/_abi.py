@@ -125,6 +125,7 @@ EXPORTS = (
     "csd_shore_rtop_adjoint_device",
     "csd_geodesic_sphere",
     "csd_shore_odf_peaks",
+    "csd_shore_fit_graddev_device",
 )
 
 _lib = None
@@ -189,6 +190,9 @@ def _declare(lib: C.CDLL) -> C.CDLL:
     lib.csd_shore_odf_peaks.restype = C.c_int
     lib.csd_shore_odf_peaks.argtypes = vol + [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_double] + \
         [C.c_void_p] * 4 + [C.c_char_p, C.c_size_t]
+    lib.csd_shore_fit_graddev_device.restype = C.c_int
+    lib.csd_shore_fit_graddev_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(Gtab),
+                                                 C.POINTER(Spec)] + [C.c_void_p] * 8 + tail
     lib.csd_geodesic_sphere.restype = C.c_int
     lib.csd_geodesic_sphere.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_int32]
     return lib

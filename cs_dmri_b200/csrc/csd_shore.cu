@@ -42,6 +42,7 @@
 #include "epilogue_kernels.cuh"
 #include "adjoint_kernels.cuh"
 #include "odf_kernels.cuh"
+#include "graddev_kernels.cuh"
 
 namespace {
 
@@ -280,6 +281,7 @@ struct csd_handle {
   DevBuf iota;
   // differentiable fit: adjoint solution w, overflow list and its count, RTOP constants
   DevBuf adjW, adjovf, adjstat, adjconst;
+  DevBuf gdtab, gdq;  // per-voxel-design fit: gradient table, queue and iteration count
   int adjconst_order = -1;
   double adjconst_zeta = 0.0;
   int sm_cap = 0;  // > 0: FISTA grids use at most this many SMs
@@ -1545,7 +1547,8 @@ void csd_destroy(csd_handle* h) {
                     &h->pbest, &h->psel, &h->pact, &h->palpha_sel, &h->pit_sel, &h->pconv_sel,
                     &h->palpha_fb, &h->pit_fb, &h->pconv_fb, &h->pcode, &h->gdig, &h->gfexp, &h->flagged,
                     &h->mixstat, &h->pcoef, &h->pmat, &h->pout, &h->pgt, &h->pgv, &h->pdir, &h->pconst,
-                    &h->iota, &h->adjW, &h->adjovf, &h->adjstat, &h->adjconst};
+                    &h->iota, &h->adjW, &h->adjovf, &h->adjstat, &h->adjconst,
+                    &h->gdtab, &h->gdq};
   for (auto s : h->pipe)
     if (s) cudaStreamSynchronize(s);
   for (DevBuf* b : bufs) b->release();
@@ -2154,3 +2157,4 @@ extern "C" int csd_shore_fista_batch_noalloc(const csd_gtab* gtab, const csd_sho
 #include "sphere_host.cuh"
 #include "differentiable_host.cuh"
 #include "peaks_host.cuh"
+#include "graddev_host.cuh"

@@ -1,0 +1,84 @@
+// Host side of the per-voxel-design fit (gradient deviation, dropped
+// samples).  Included once at the end of csd_shore.cu.
+#pragma once
+
+extern "C" int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signals, int64_t n_voxels,
+                                            const csd_gtab* gtab, const csd_shore_spec* spec,
+                                            const double* d_graddev, const uint8_t* d_keep,
+                                            const double* d_alpha, double* d_coef, uint32_t* d_iterations,
+                                            uint8_t* d_converged, double* d_lipschitz, int32_t* d_n_rows,
+                                            void* stream, char* err, size_t err_len) {
+  if (!h || !gtab || !spec || n_voxels < 0 ||
+      (n_voxels > 0 && (!d_signals || !d_coef || !d_iterations || !d_converged))) {
+    set_err(err, err_len, "invalid argument: null pointer or negative voxel count");
+    return CSD_ERR_INVALID;
+  }
+  try {
+    CSD_CUDA(cudaSetDevice(h->device));
+    HostGtab g = make_gtab(gtab);
+    std::string warnings;
+    validate(spec, g, warnings);
+    if (spec->regularization != CSD_REG_L1 || spec->alpha_mode != CSD_ALPHA_FIXED)
+      throw Error{CSD_ERR_INVALID, "the per-voxel-design fit takes regularization l1 with alpha_mode fixed"};
+    if (spec->radial_order != 6 && spec->radial_order != 8)
+      throw Error{CSD_ERR_INVALID, "the per-voxel-design fit is built for radial orders 6 and 8"};
+    StreamScope scope(h, stream);
+    cudaStream_t st = h->stream;
+    h->launches = 0;
+    const int N = static_cast<int>(g.bvals.size());
+    const int K = n_coeffs(spec->radial_order);
+    const csd::GdLayout lay(K, spec->radial_order, N);
+    if (lay.total_bytes + 64 > static_cast<size_t>(h->smem_optin))
+      throw Error{CSD_ERR_INVALID, "gradient table too long for the per-voxel-design fit (shared memory)"};
+    if (n_voxels == 0) return CSD_OK;
+    // the table itself (not the per-table setup cache: the designs are per voxel)
+    h->gdtab.ensure(sizeof(double) * 4 * static_cast<size_t>(N));
+    CSD_CUDA(cudaMemcpyAsync(h->gdtab.p, g.bvals.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st));
+    CSD_CUDA(cudaMemcpyAsync(h->gdtab.as<double>() + N, g.bvecs.data(), sizeof(double) * 3 * N,
+                             cudaMemcpyHostToDevice, st));
+    ensure_mom(h, spec->max_iter);
+    h->gdq.ensure(2 * sizeof(unsigned long long));
+    CSD_CUDA(cudaMemsetAsync(h->gdq.p, 0, 2 * sizeof(unsigned long long), st));
+    csd::GraddevParams p{};
+    p.S = d_signals;
+    p.T = d_graddev;
+    p.keep = d_keep;
+    p.bvals = h->gdtab.as<double>();
+    p.bvecs = h->gdtab.as<double>() + N;
+    p.N = N;
+    p.K = K;
+    p.radial_order = spec->radial_order;
+    p.zeta = spec->zeta;
+    p.qdenom = 4.0 * kPi * kPi * g.tau;  // src/qspace.rs:384-385
+    p.b0_thr = g.b0;
+    p.alpha = spec->alpha;
+    p.alpha_v = d_alpha;
+    p.tol = spec->tol;
+    p.max_iter = spec->max_iter;
+    p.non_negative = spec->non_negative;
+    p.mom = h->mom.as<double>();
+    p.V = n_voxels;
+    p.queue = h->gdq.as<unsigned long long>();
+    p.X = d_coef;
+    p.iters = d_iterations;
+    p.conv = d_converged;
+    p.lipschitz = d_lipschitz;
+    p.n_rows = d_n_rows;
+    p.iter_total = h->gdq.as<unsigned long long>() + 1;
+    auto go = [&](auto kern) {
+      CSD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(lay.total_bytes)));
+      const int grid = static_cast<int>(std::min<int64_t>(h->num_sms, n_voxels));
+      kern<<<grid, 256, lay.total_bytes, st>>>(p);
+      CSD_LAUNCH();
+    };
+    if (K == 72)
+      go(csd::k_graddev_fit<9>);
+    else
+      go(csd::k_graddev_fit<19>);
+  } catch (const Error& e) {
+    set_err(err, err_len, e.msg);
+    return e.code;
+  }
+  return CSD_OK;
+}

@@ -336,6 +336,24 @@ int csd_shore_rtop_adjoint_device(csd_handle* h, int32_t radial_order, double ze
                                   const double* d_coef, int64_t n_voxels, const double* d_grad_rtop,
                                   double* d_grad_coef, void* stream, char* err, size_t err_len);
 
+/* L1 fit (alpha_mode FIXED; one alpha per voxel in `d_alpha`, nullable) of
+ * a batch of voxel signals, float32 (n_voxels, N), each on its OWN design:
+ * the effective table of its gradient-deviation tensor (`d_graddev`,
+ * (n_voxels, 9) row-major T, nullable = identity; src/graddev.rs:160-185:
+ * q = T^T g, b_eff = b |q|^2, dir = q / |q|) restricted to the samples it
+ * keeps (`d_keep`, (n_voxels, N) non-zero = keep, nullable = all).  The
+ * reference computes that table but fits SHORE with one shared design.  Per
+ * voxel: G_v = M_v^T M_v, L_v = sigma_max(M_v)^2 / n_v and the FISTA of
+ * src/solver/fista.rs:70-143.  Radial orders 6 and 8.  Outputs (device):
+ * coefficients (n_voxels, K) FP64, iterations, converged, and (nullable) L_v
+ * and the kept sample count.  Asynchronous like the entry points above. */
+int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signals, int64_t n_voxels,
+                                 const csd_gtab* gtab, const csd_shore_spec* spec,
+                                 const double* d_graddev, const uint8_t* d_keep,
+                                 const double* d_alpha, double* d_coef, uint32_t* d_iterations,
+                                 uint8_t* d_converged, double* d_lipschitz, int32_t* d_n_rows,
+                                 void* stream, char* err, size_t err_len);
+
 /* Class I geodesic sphere of `frequency` (10 f^2 + 2 vertices; 362 at f = 6),
  * or one vertex per antipodal pair with `hemisphere`.  Writes the unit
  * vectors (count x 3) to `out` when `capacity` >= count; returns the count,

@@ -561,3 +561,34 @@ def odf_peaks(coefs, radial_order, zeta, frequency=6, npeaks=5, relative_peak_th
     Vv[:len(out_v)] = out_v
     qa = np.where(Vv > 0, np.maximum(Vv - amp.min(), 0.0), 0.0)
     return gfa, D, Vv, qa, amp
+
+
+# --------------------------------------------------- per-voxel designs (graddev)
+
+def effective_table(bvals, bvecs, T, b0_threshold=50.0):
+    """Effective table of one deviation tensor T (src/graddev.rs:160-185 with
+    the identity frame rotation): for a diffusion-weighted sample with a
+    non-zero direction g, q = T^T g/|g|, b_eff = b |q|^2, dir = q / |q|;
+    other samples keep their b and direction."""
+    b = _f64(bvals).copy()
+    d = _f64(bvecs).reshape(-1, 3).copy()
+    T = _f64(T).reshape(3, 3)
+    for i in range(b.size):
+        gn = np.linalg.norm(d[i])
+        if b[i] > b0_threshold and gn > 1e-12:
+            q = T.T @ (d[i] / gn)
+            b[i] = b[i] * (q @ q)
+            d[i] = q / np.linalg.norm(q)
+    return b, d
+
+
+def graddev_fit(signal, bvals, bvecs, T, keep, alpha, radial_order=8, zeta=700.0, big_delta=None, small_delta=None,
+                max_iter=1000, tol=1e-6, non_negative=False):
+    """One voxel on its own design: the effective table, the kept samples,
+    the design matrix of those rows and the reference FISTA on it.  Returns
+    (coefficients, iterations, converged, design)."""
+    b, d = effective_table(bvals, bvecs, T)
+    k = np.ones(b.size, bool) if keep is None else np.asarray(keep, bool)
+    M = design_matrix(b[k], d[k], radial_order, zeta, big_delta=big_delta, small_delta=small_delta)
+    c, it, conv, _ = fista_fit(M, _f64(signal)[k], alpha, max_iter=max_iter, tol=tol, non_negative=non_negative)
+    return c, it, conv, M

@@ -1,0 +1,79 @@
+"""Per-voxel-design fit on the GPU (csd_shore_fit_graddev_device) against the
+oracle: the effective table of each voxel's deviation tensor, its kept
+samples, the design of those rows and the reference FISTA (oracle.graddev_fit),
+at radial orders 8 (the workload's) and 6.
+
+Tolerances as for the shared-design fit: coefficients within 1e-5 of the
+largest coefficient (a stopping decision within rounding of tol can move the
+iterate by tol x |x|), iteration counts within 1; the Lipschitz constant
+sigma_max(M_v)^2 / n_v (Lanczos on G_v against the oracle's Jacobi
+eigensolve) at 1e-12.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def inputs():
+    from cs_dmri_b200.graddev import graddev_phantom
+    return graddev_phantom(96, seed=7)
+
+
+@pytest.mark.parametrize("order", [8, 6])
+def test_matches_oracle(oracle, inputs, order):
+    from cs_dmri_b200.graddev import shore_fit_graddev
+    S, bvals, bvecs, T, keep, big, small = inputs
+    out = shore_fit_graddev(S, bvals, bvecs, T, keep, alpha=0.01, radial_order=order, big_delta=big,
+                            small_delta=small)
+    c = out["coefficients"].cpu().numpy()
+    it = out["iterations"].cpu().numpy()
+    lip = out["lipschitz"].cpu().numpy()
+    assert np.array_equal(out["n_samples"].cpu().numpy(), keep.sum(1))
+    off = 0
+    for v in range(0, len(S), 3):
+        want, wit, wconv, M = oracle.graddev_fit(S[v], bvals, bvecs, T[v], keep[v], 0.01, radial_order=order,
+                                                 big_delta=big, small_delta=small)
+        np.testing.assert_allclose(lip[v], oracle.sigma_max(M) ** 2 / M.shape[0], rtol=1e-12)
+        np.testing.assert_allclose(c[v], want, rtol=0, atol=1e-5 * np.abs(want).max())
+        assert abs(int(it[v]) - wit) <= 1
+        off += int(it[v]) != wit
+    assert off <= 2
+
+
+def test_identity_matches_the_shared_design_fit(inputs):
+    import torch
+    from cs_dmri_b200.autograd import DifferentiableShore
+    from cs_dmri_b200.graddev import shore_fit_graddev
+    S, bvals, bvecs, T, keep, big, small = inputs
+    out = shore_fit_graddev(S, bvals, bvecs, None, None, alpha=0.01, radial_order=6, big_delta=big,
+                            small_delta=small)
+    m = DifferentiableShore(bvals, bvecs, big_delta=big, small_delta=small)
+    ref = m.fit(torch.from_numpy(S).cuda(), 0.01).cpu().numpy()
+    c = out["coefficients"].cpu().numpy()
+    scale = np.abs(ref).max(1, keepdims=True)
+    assert np.all(np.abs(c - ref) <= 1e-5 * scale)
+
+
+def test_per_voxel_alpha_and_edge_cases(inputs):
+    import torch
+    from cs_dmri_b200.graddev import shore_fit_graddev
+    S, bvals, bvecs, T, keep, big, small = inputs
+    kw = dict(radial_order=6, big_delta=big, small_delta=small)
+    a = np.where(np.arange(len(S)) % 2 == 0, 0.01, 0.05)
+    both = shore_fit_graddev(S, bvals, bvecs, T, keep, alpha=a, **kw)["coefficients"].cpu().numpy()
+    one = shore_fit_graddev(S, bvals, bvecs, T, keep, alpha=0.01, **kw)["coefficients"].cpu().numpy()
+    five = shore_fit_graddev(S, bvals, bvecs, T, keep, alpha=0.05, **kw)["coefficients"].cpu().numpy()
+    np.testing.assert_array_equal(both[0::2], one[0::2])
+    np.testing.assert_array_equal(both[1::2], five[1::2])
+    none = np.zeros_like(keep)
+    out = shore_fit_graddev(S[:4], bvals, bvecs, T[:4], none[:4], alpha=0.01, **kw)
+    assert float(out["coefficients"].abs().max()) == 0.0
+    assert int(out["iterations"].max()) == 0 and not bool(out["converged"].any())
+    with pytest.raises(ValueError, match="radial orders 6 and 8"):
+        shore_fit_graddev(S[:4], bvals, bvecs, radial_order=4, big_delta=big, small_delta=small)
+    with pytest.raises(ValueError, match="sample_mask"):
+        shore_fit_graddev(S[:4], bvals, bvecs, sample_mask=keep[:3], big_delta=big, small_delta=small)
+    assert torch.cuda.is_available()
