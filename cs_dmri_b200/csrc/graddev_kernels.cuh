@@ -17,15 +17,14 @@
 //      registers; b_v = M_v^T s_v alongside;
 //   3. lambda_max(G_v) by Lanczos (a fixed number of steps, the largest Ritz
 //      value by multisection of the tridiagonal's Sturm count across a warp);
-//   4. FISTA in the Gram form with G_v in shared memory (one warp per row of
-//      the product, lanes over the columns), the reference's update and
-//      stopping rule.
+//   4. FISTA in the Gram form with G_v in shared memory (one thread per row of
+//      the product, 16-byte loads), the reference's update and stopping rule.
 #pragma once
 
 namespace csd {
 
-constexpr int kGdChunk = 32;       // design rows per Gram chunk
-constexpr int kGdLanczos = 48;     // Lanczos steps (capped at K)
+constexpr int kGdChunk = 64;       // design rows per Gram chunk (one thread per row and value group)
+constexpr int kGdLanczos = 40;     // Lanczos steps (capped at K)
 
 struct GraddevParams {
   const float* S;           // V x N signals
@@ -52,26 +51,72 @@ struct GraddevParams {
 
 // Shared-memory plan (doubles unless noted), shared by host and device.
 struct GdLayout {
-  int K, Kp, LDM, NL, NSH;
-  size_t g, vec, red, tri, rows, colmap, total_bytes;
+  int K, Kp, LDG, LDM, NL, NSH, NLM, NTR;
+  size_t g, vec, red, tri, tab, rows, colmap, total_bytes;
   __host__ __device__ GdLayout(int K_, int radial_order, int N) {
     K = K_;
     Kp = 8 * ((K + 7) / 8);
-    LDM = Kp + 4;  // chunk row stride: conflict-free fragment loads
+    LDG = K + (K & 1);   // even row stride of G: 16-byte rows, conflict-free 16-byte loads
+    LDM = Kp + 4;        // chunk row stride: conflict-free fragment loads
     NL = 0;
     for (int n = 0; n <= radial_order; ++n) NL += n / 2 + 1;
     NSH = (radial_order / 2 + 1) * (radial_order + 1);
-    const size_t chunk = static_cast<size_t>(kGdChunk) * (LDM + NL + NSH + 4);
-    const size_t gsize = static_cast<size_t>(K) * K > chunk ? static_cast<size_t>(K) * K : chunk;
+    NLM = (radial_order / 2 + 1) * (radial_order / 2 + 1);  // P_l^m, l even, 0 <= m <= l
+    NTR = 2 * radial_order;                                  // cos(m theta), sin(m theta), m = 1..order
+    const size_t chunk = static_cast<size_t>(kGdChunk) * (LDM + NL + NLM + NTR + 8);
+    const size_t gk = static_cast<size_t>(K) * LDG;
+    const size_t gsize = gk > chunk ? gk : chunk;
     g = 0;
     vec = (gsize + 1) & ~static_cast<size_t>(1);           // b, x, y, gy, v_prev, v, w: 7 * Kp
-    red = vec + 7 * static_cast<size_t>(Kp);                 // 16 reduction slots
-    tri = red + 16;                                          // Lanczos alpha / beta: 2 * 64
-    rows = tri + 128;                                        // N ints, then the column map (2 K ints)
-    colmap = rows + (static_cast<size_t>(N) + 1) / 2;
-    total_bytes = 8 * (colmap + static_cast<size_t>(K) + 1);
+    red = vec + 7 * static_cast<size_t>(Kp);                 // 32 reduction slots
+    tri = red + 32;                                          // Lanczos alpha / beta: 2 * 64
+    tab = tri + 128;                                         // kappa per (n, l), SH norm per (l, k)
+    rows = tab + ((static_cast<size_t>(NL + NSH) + 1) & ~static_cast<size_t>(1));  // N ints
+    colmap = rows + (static_cast<size_t>(N) + 1) / 2;        // column and task maps (ints)
+    total_bytes = 8 * (colmap + static_cast<size_t>(K) + static_cast<size_t>(NL + NSH) + 2);
   }
 };
+
+// Block-wide sum of one value per thread; every thread gets the same result
+// (fixed order: warp trees, then the warp sums in order).  `red` has 32 slots.
+__device__ __forceinline__ double gd_block_sum(double a, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(kFull, a, o);
+  __syncthreads();
+  if (lane == 0) red[warp] = a;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += red[w];
+  return s;
+}
+
+// out[i] = sum_j G[i][j] v[j] for i < K, one thread per row: 16-byte loads of
+// G's row and of v (both in shared memory) into four independent partial
+// sums (j mod 4), added at the end.
+__device__ __forceinline__ void gd_gemv(const double* G, int LDG, int K, const double* v, double* out) {
+  for (int i = threadIdx.x; i < K; i += blockDim.x) {
+    const double2* gr = reinterpret_cast<const double2*>(G + static_cast<size_t>(i) * LDG);
+    const double2* v2 = reinterpret_cast<const double2*>(v);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    const int h = K >> 1;
+    int j = 0;
+    for (; j + 1 < h; j += 2) {
+      const double2 g0 = gr[j], w0 = v2[j], g1 = gr[j + 1], w1 = v2[j + 1];
+      a0 = fma(g0.x, w0.x, a0);
+      a1 = fma(g0.y, w0.y, a1);
+      a2 = fma(g1.x, w1.x, a2);
+      a3 = fma(g1.y, w1.y, a3);
+    }
+    if (j < h) {
+      const double2 g0 = gr[j], w0 = v2[j];
+      a0 = fma(g0.x, w0.x, a0);
+      a1 = fma(g0.y, w0.y, a1);
+    }
+    if (K & 1) a2 = fma(G[static_cast<size_t>(i) * LDG + K - 1], v[K - 1], a2);
+    out[i] = (a0 + a1) + (a2 + a3);
+  }
+}
 
 // Count of eigenvalues of the symmetric tridiagonal (a, b) below x (Sturm).
 __device__ __forceinline__ int sturm_below(const double* a, const double* b, int m, double x) {
@@ -87,18 +132,18 @@ __device__ __forceinline__ int sturm_below(const double* a, const double* b, int
 }
 
 template <int MT>
-__global__ void __launch_bounds__(256, 1) k_graddev_fit(GraddevParams p) {
+__global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevParams p) {
   constexpr int NT = MT * (MT + 1) / 2;  // upper-triangle tiles of G
   constexpr int TPW = (NT + 7) / 8;      // tiles per warp
-  constexpr int RPL = (8 * MT + 31) / 32;
   extern __shared__ __align__(16) double gd_smem[];
   const GdLayout L(p.K, p.radial_order, p.N);
   const int K = p.K, Kp = L.Kp, LDM = L.LDM, NL = L.NL, NSH = L.NSH, N = p.N;
   double* G = gd_smem + L.g;
   double* Mc = G;                                  // chunk: kGdChunk x LDM (aliases G while it is built)
-  double* rad = Mc + kGdChunk * LDM;               // kGdChunk x NL
-  double* shv = rad + kGdChunk * NL;               // kGdChunk x NSH
-  double* geo = shv + kGdChunk * NSH;              // kGdChunk x 4: r, theta, phi, signal
+  double* rad = Mc + kGdChunk * LDM;               // kGdChunk x NL radial factors
+  double* leg = rad + kGdChunk * NL;               // kGdChunk x NLM associated Legendre values
+  double* trg = leg + kGdChunk * L.NLM;            // kGdChunk x NTR cos / sin of m theta
+  double* geo = trg + kGdChunk * L.NTR;            // kGdChunk x 8: r, theta, phi, signal, cos phi, u, exp(-u/2)
   double* vb = gd_smem + L.vec;
   double* vx = vb + Kp;
   double* vy = vx + Kp;
@@ -109,25 +154,48 @@ __global__ void __launch_bounds__(256, 1) k_graddev_fit(GraddevParams p) {
   double* red = gd_smem + L.red;
   double* ta = gd_smem + L.tri;
   double* tb = ta + 64;
+  double* kap = gd_smem + L.tab;                   // NL: kappa(zeta, n, l)
+  double* shn = kap + NL;                          // NSH: SH normalisation of (l, k)
   int* rows = reinterpret_cast<int*>(gd_smem + L.rows);
-  int* col_nl = reinterpret_cast<int*>(gd_smem + L.colmap);
-  int* col_lk = col_nl + K;
+  int* col_map = reinterpret_cast<int*>(gd_smem + L.colmap);  // K: (radial block << 8) | SH entry
+  int* task_map = col_map + K;                                 // NL + NSH: (n or m) << 16 | l << 8 | k
   __shared__ int64_t s_v;
   __shared__ int s_n;
   __shared__ double s_lmax;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, q = lane & 3;
 
-  // column -> (radial block, SH entry) maps, once per CTA
+  // column -> (radial block, SH entry) and the per-(n, l) / per-(l, k)
+  // constants, once per CTA (the same expressions as dev_shore_radial and
+  // dev_brainsuite_sh evaluate per entry)
   for (int col = tid; col < K; col += blockDim.x) {
     int n, l, k;
     col_to_nlk(p.radial_order, col, &n, &l, &k);
     int nl = 0;
     for (int nn = 0; nn < n; ++nn) nl += nn / 2 + 1;
-    col_nl[col] = nl + l / 2;
     int lk = 0;
     for (int ll = 0; ll < l; ll += 2) lk += 2 * ll + 1;
-    col_lk[col] = lk + k;
+    col_map[col] = ((nl + l / 2) << 8) | (lk + k);
+  }
+  for (int j = tid; j < NL + NSH; j += blockDim.x) {
+    if (j < NL) {
+      int nn = 0, rem = j;
+      while (rem >= nn / 2 + 1) {
+        rem -= nn / 2 + 1;
+        ++nn;
+      }
+      kap[j] = dev_kappa(p.zeta, nn, 2 * rem);
+      task_map[j] = (nn << 16) | ((2 * rem) << 8);
+    } else {
+      int l = 0, rem = j - NL;
+      while (rem >= 2 * l + 1) {
+        rem -= 2 * l + 1;
+        l += 2;
+      }
+      const int m = (rem < l) ? l - rem : (rem == l ? 0 : rem - l);
+      shn[j - NL] = sqrt((2.0 * l + 1.0) / (4.0 * CUDART_PI) * dev_factorial(l - m) / dev_factorial(l + m));
+      task_map[j] = (m << 16) | (l << 8) | rem;
+    }
   }
   // this warp's tiles of the upper triangle, packed (mt << 8) | nt; nt >= MT
   // marks an unused slot
@@ -204,40 +272,94 @@ __global__ void __launch_bounds__(256, 1) k_graddev_fit(GraddevParams p) {
           if (isnan(th)) th = 0.0;
           sig = static_cast<double>(p.S[v * N + i]);
         }
-        geo[4 * tid] = rr;
-        geo[4 * tid + 1] = th;
-        geo[4 * tid + 2] = ph;
-        geo[4 * tid + 3] = (r < n) ? sig : 0.0;
+        const double u = rr * rr / p.zeta;
+        geo[8 * tid] = rr;
+        geo[8 * tid + 1] = th;
+        geo[8 * tid + 2] = ph;
+        geo[8 * tid + 3] = (r < n) ? sig : 0.0;
+        geo[8 * tid + 4] = cos(ph);
+        geo[8 * tid + 5] = u;
+        geo[8 * tid + 6] = exp(-u * 0.5);
       }
       __syncthreads();
-      for (int task = tid; task < kGdChunk * (NL + NSH); task += blockDim.x) {
-        const int t = task / (NL + NSH), j = task % (NL + NSH);
-        const bool ok = c0 + t < n;
-        if (j < NL) {
-          int nn = 0, rem = j;
-          while (rem >= nn / 2 + 1) {
-            rem -= nn / 2 + 1;
-            ++nn;
+      // per-row values, one thread per row in each of three groups: radial
+      // factors (group 0), cos / sin of m theta (group 1), associated
+      // Legendre values by the recurrence in l for each m (group 2); the
+      // operations are those of dev_shore_radial and dev_brainsuite_sh, so
+      // the entries equal the shared-design kernel's
+      {
+        const int t = tid % kGdChunk, grp = tid / kGdChunk;
+        const double* gt = geo + 8 * t;
+        const int R = p.radial_order;
+        if (grp == 0) {
+          double rp[8];
+          for (int l = 0; l <= R; l += 2) rp[l / 2] = pow(gt[5], static_cast<double>(l) / 2.0);
+          int j = 0;
+          for (int nn = 0; nn <= R; ++nn)
+            for (int l = 0; l <= nn; l += 2, ++j) {
+              const double lag = dev_gen_laguerre(nn - l, static_cast<double>(l) + 0.5, gt[5]);
+              rad[t * NL + j] = kap[j] * lag * gt[6] * rp[l / 2];
+            }
+        } else if (grp == 1) {
+          for (int mm = 1; mm <= R; ++mm) {
+            trg[t * L.NTR + mm - 1] = cos(static_cast<double>(mm) * gt[1]);
+            trg[t * L.NTR + R + mm - 1] = sin(static_cast<double>(mm) * gt[1]);
           }
-          rad[t * NL + j] = ok ? dev_shore_radial(nn, 2 * rem, geo[4 * t], p.zeta) : 0.0;
-        } else {
-          int l = 0, rem = j - NL;
-          while (rem >= 2 * l + 1) {
-            rem -= 2 * l + 1;
-            l += 2;
+        } else if (grp == 2) {
+          const double x = gt[4];
+          for (int mm = 0; mm <= R; ++mm) {  // P_l^m for l = m, m + 1, ..., R (dev_assoc_legendre's steps)
+            double pmm = 1.0;
+            if (mm > 0) {
+              const double somx2 = sqrt(fmax((1.0 - x) * (1.0 + x), 0.0));
+              double fact = 1.0;
+              for (int i = 0; i < mm; ++i) {
+                pmm *= -fact * somx2;
+                fact += 2.0;
+              }
+            }
+            if (mm % 2 == 0) leg[t * L.NLM + (mm / 2) * (mm / 2) + mm] = pmm;
+            if (mm + 1 > R) continue;
+            double pmmp1 = x * (2.0 * mm + 1.0) * pmm;
+            if ((mm + 1) % 2 == 0) leg[t * L.NLM + ((mm + 1) / 2) * ((mm + 1) / 2) + mm] = pmmp1;
+            for (int ll = mm + 2; ll <= R; ++ll) {
+              const double llf = ll, mf = mm;
+              const double pll = ((2.0 * llf - 1.0) * x * pmmp1 - (llf + mf - 1.0) * pmm) / (llf - mf);
+              pmm = pmmp1;
+              pmmp1 = pll;
+              if (ll % 2 == 0) leg[t * L.NLM + (ll / 2) * (ll / 2) + mm] = pll;
+            }
           }
-          shv[t * NSH + (j - NL)] = ok ? dev_brainsuite_sh(l, rem, geo[4 * t + 1], geo[4 * t + 2]) : 0.0;
         }
       }
       __syncthreads();
       for (int task = tid; task < kGdChunk * Kp; task += blockDim.x) {
         const int t = task / Kp, col = task % Kp;
-        Mc[t * LDM + col] = (col < K) ? rad[t * NL + col_nl[col]] * shv[t * NSH + col_lk[col]] : 0.0;
+        double val = 0.0;
+        if (col < K && c0 + t < n) {
+          const int cm = col_map[col];
+          const int lk = cm & 0xff, tm = task_map[NL + lk];
+          const int m = tm >> 16, l = (tm >> 8) & 0xff, k = tm & 0xff;
+          double sh;
+          if (l == 0) {
+            sh = 1.0 / sqrt(4.0 * CUDART_PI);
+          } else {
+            const double pl = shn[lk] * leg[t * L.NLM + (l / 2) * (l / 2) + m];
+            const double s2 = sqrt(2.0);
+            if (k < l)
+              sh = s2 * pl * trg[t * L.NTR + m - 1];
+            else if (k == l)
+              sh = pl;
+            else
+              sh = s2 * (((m + 1) % 2 == 0) ? 1.0 : -1.0) * pl * trg[t * L.NTR + p.radial_order + m - 1];
+          }
+          val = rad[t * NL + (cm >> 8)] * sh;
+        }
+        Mc[t * LDM + col] = val;
       }
       __syncthreads();
       for (int col = tid; col < K; col += blockDim.x) {
         double a = vb[col];
-        for (int t = 0; t < kGdChunk; ++t) a = __dadd_rn(a, __dmul_rn(Mc[t * LDM + col], geo[4 * t + 3]));
+        for (int t = 0; t < kGdChunk; ++t) a = __dadd_rn(a, __dmul_rn(Mc[t * LDM + col], geo[8 * t + 3]));
         vb[col] = a;
       }
 #pragma unroll 1
@@ -259,70 +381,51 @@ __global__ void __launch_bounds__(256, 1) k_graddev_fit(GraddevParams p) {
       for (int e = 0; e < 2; ++e) {
         const int j = 8 * nt + 2 * q + e;
         if (i < K && j < K) {
-          G[i * K + j] = acc[s][e];
-          if (mt != nt) G[j * K + i] = acc[s][e];  // a diagonal tile holds both halves itself
+          G[i * L.LDG + j] = acc[s][e];
+          if (mt != nt) G[j * L.LDG + i] = acc[s][e];  // a diagonal tile holds both halves itself
         }
       }
     }
     __syncthreads();
 
     // ---- 3. lambda_max(G) by Lanczos
+    const int LDG = L.LDG;
     const int m = min(K, kGdLanczos);
-    {
-      double nrm = 0.0;
-      for (int i = tid; i < Kp; i += blockDim.x) {
-        const double e = (i < K) ? 1.0 + 0.5 * sin(1.7 * i + 0.3) : 0.0;  // fixed start vector
-        lv[i] = e;
-        lv_prev[i] = 0.0;
-      }
-      __syncthreads();
-      for (int i = 0; i < K; ++i) nrm += lv[i] * lv[i];  // every thread, same order
-      const double inv = 1.0 / sqrt(nrm);
-      __syncthreads();
-      for (int i = tid; i < K; i += blockDim.x) lv[i] *= inv;
-      __syncthreads();
+    for (int i = tid; i < Kp; i += blockDim.x) {
+      lv[i] = (i < K) ? 1.0 + 0.5 * sin(1.7 * i + 0.3) : 0.0;  // fixed start vector
+      lv_prev[i] = 0.0;
     }
+    {
+      const double e = (tid < K) ? lv[tid] : 0.0;  // K <= blockDim.x
+      const double inv = 1.0 / sqrt(gd_block_sum(e * e, red));
+      if (tid < K) lv[tid] *= inv;
+    }
+    __syncthreads();
     int msteps = m;
     double beta_prev = 0.0;
     for (int j = 0; j < m; ++j) {
-      // w = G v
-      double vl[RPL];
-#pragma unroll
-      for (int c = 0; c < RPL; ++c) vl[c] = (lane + 32 * c < K) ? lv[lane + 32 * c] : 0.0;
-      for (int i = warp; i < K; i += 8) {
-        double a = 0.0;
-#pragma unroll
-        for (int c = 0; c < RPL; ++c)
-          if (lane + 32 * c < K) a = fma(G[i * K + lane + 32 * c], vl[c], a);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(kFull, a, o);
-        if (lane == 0) lw[i] = a;
-      }
+      gd_gemv(G, LDG, K, lv, lw);
       __syncthreads();
-      double al = 0.0;
-      for (int i = 0; i < K; ++i) al += lw[i] * lv[i];
-      __syncthreads();
-      for (int i = tid; i < K; i += blockDim.x) lw[i] = lw[i] - al * lv[i] - beta_prev * lv_prev[i];
-      __syncthreads();
-      double bt = 0.0;
-      for (int i = 0; i < K; ++i) bt += lw[i] * lw[i];
-      bt = sqrt(bt);
+      const double wi = (tid < K) ? lw[tid] : 0.0, vi = (tid < K) ? lv[tid] : 0.0;
+      const double al = gd_block_sum(wi * vi, red);
+      const double wn = (tid < K) ? wi - al * vi - beta_prev * lv_prev[tid] : 0.0;
+      const double bt = sqrt(gd_block_sum(wn * wn, red));
       if (tid == 0) {
         ta[j] = al;
         tb[j] = bt;
       }
-      if (!(bt > 1e-300 * fabs(al)) || j == m - 1) {
+      if (!(bt > 1e-300 * fabs(al)) || j == m - 1) {  // every thread holds the same bt
         msteps = j + 1;
-        __syncthreads();
         break;
       }
-      for (int i = tid; i < K; i += blockDim.x) {
-        lv_prev[i] = lv[i];
-        lv[i] = lw[i] / bt;
+      if (tid < K) {
+        lv_prev[tid] = vi;
+        lv[tid] = wn / bt;
       }
       beta_prev = bt;
       __syncthreads();
     }
+    __syncthreads();
     if (warp == 0) {  // largest eigenvalue of the tridiagonal: 32-point multisection
       double lo = 1e300, hi = -1e300;
       for (int i = 0; i < msteps; ++i) {
@@ -358,18 +461,7 @@ __global__ void __launch_bounds__(256, 1) k_graddev_fit(GraddevParams p) {
     int it = 0;
     bool converged = false;
     while (n > 0 && it < p.max_iter) {
-      double yl[RPL];
-#pragma unroll
-      for (int c = 0; c < RPL; ++c) yl[c] = (lane + 32 * c < K) ? vy[lane + 32 * c] : 0.0;
-      for (int i = warp; i < K; i += 8) {
-        double a = 0.0;
-#pragma unroll
-        for (int c = 0; c < RPL; ++c)
-          if (lane + 32 * c < K) a = fma(G[i * K + lane + 32 * c], yl[c], a);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(kFull, a, o);
-        if (lane == 0) vgy[i] = a;
-      }
+      gd_gemv(G, LDG, K, vy, vgy);
       __syncthreads();
       const double mom = p.mom[it];
       double dx2 = 0.0, xn2 = 0.0;

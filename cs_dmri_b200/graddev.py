@@ -36,12 +36,12 @@ def graddev_phantom(n_voxels, seed=3, sigma=0.02, drop_max=0.15):
     rng = np.random.default_rng(seed)
     T = np.eye(3)[None] + rng.normal(0.0, sigma, size=(n_voxels, 3, 3))
     dwi = np.flatnonzero(ph.bvals > 50.0)
-    keep = np.ones(S.shape, bool)
     frac = rng.uniform(0.0, drop_max, size=n_voxels)
-    for v in range(n_voxels):
-        k = int(frac[v] * dwi.size)  # at most drop_max of the samples
-        if k:
-            keep[v, rng.choice(dwi, size=k, replace=False)] = False
+    n_drop = (frac * dwi.size).astype(np.int64)  # at most drop_max of the samples
+    order = np.argsort(rng.random((n_voxels, dwi.size)), axis=1)  # a random permutation per voxel
+    keep = np.ones(S.shape, bool)
+    rows, cols = np.nonzero(np.arange(dwi.size)[None, :] < n_drop[:, None])
+    keep[rows, dwi[order[rows, cols]]] = False
     return S, ph.bvals, ph.bvecs, T, keep, ph.big_delta, ph.small_delta
 
 
