@@ -10,13 +10,15 @@
 //
 // One persistent CTA per SM takes voxels from a queue.  Per voxel:
 //   1. kept rows, effective b and direction per row;
-//   2. G_v = M_v^T M_v on the FP64 tensor cores (DMMA m8n8k4): the design is
-//      generated 32 rows at a time into shared memory (radial factors per
+//   2. G_v = M_v^T M_v on the FP64 tensor cores (DMMA m8n8k4): the geometry
+//      of every kept row first, then the design generated 64 rows at a time
+//      into shared memory (radial factors per
 //      (n, l) and SH values per (l, m), multiplied per column), each warp
 //      accumulating a fixed set of 8 x 8 tiles of the upper triangle in
 //      registers; b_v = M_v^T s_v alongside;
 //   3. lambda_max(G_v) by Lanczos (a fixed number of steps, the largest Ritz
-//      value by multisection of the tridiagonal's Sturm count across a warp);
+//      value by multisection of the tridiagonal's Sturm count, one point per
+//      thread);
 //   4. FISTA in the Gram form with G_v in shared memory (one thread per row of
 //      the product, 16-byte loads), the reference's update and stopping rule.
 #pragma once
@@ -63,7 +65,7 @@ struct GdLayout {
     NSH = (radial_order / 2 + 1) * (radial_order + 1);
     NLM = (radial_order / 2 + 1) * (radial_order / 2 + 1);  // P_l^m, l even, 0 <= m <= l
     NTR = 2 * radial_order;                                  // cos(m theta), sin(m theta), m = 1..order
-    const size_t chunk = static_cast<size_t>(kGdChunk) * (LDM + NL + NLM + NTR + 8);
+    const size_t chunk = static_cast<size_t>(kGdChunk) * (LDM + NL + NLM + NTR) + 8 * static_cast<size_t>(N);
     const size_t gk = static_cast<size_t>(K) * LDG;
     const size_t gsize = gk > chunk ? gk : chunk;
     g = 0;
@@ -92,8 +94,8 @@ __device__ __forceinline__ double gd_block_sum(double a, double* red) {
 }
 
 // out[i] = sum_j G[i][j] v[j] for i < K, one thread per row: 16-byte loads of
-// G's row and of v (both in shared memory) into four independent partial
-// sums (j mod 4), added at the end.
+// G's row and of v (both in shared memory), four per step, into four
+// independent partial sums added at the end.
 __device__ __forceinline__ void gd_gemv(const double* G, int LDG, int K, const double* v, double* out) {
   for (int i = threadIdx.x; i < K; i += blockDim.x) {
     const double2* gr = reinterpret_cast<const double2*>(G + static_cast<size_t>(i) * LDG);
@@ -101,14 +103,19 @@ __device__ __forceinline__ void gd_gemv(const double* G, int LDG, int K, const d
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
     const int h = K >> 1;
     int j = 0;
-    for (; j + 1 < h; j += 2) {
-      const double2 g0 = gr[j], w0 = v2[j], g1 = gr[j + 1], w1 = v2[j + 1];
+    for (; j + 3 < h; j += 4) {  // eight loads in flight per step
+      const double2 g0 = gr[j], g1 = gr[j + 1], g2 = gr[j + 2], g3 = gr[j + 3];
+      const double2 w0 = v2[j], w1 = v2[j + 1], w2 = v2[j + 2], w3 = v2[j + 3];
       a0 = fma(g0.x, w0.x, a0);
       a1 = fma(g0.y, w0.y, a1);
       a2 = fma(g1.x, w1.x, a2);
       a3 = fma(g1.y, w1.y, a3);
+      a0 = fma(g2.x, w2.x, a0);
+      a1 = fma(g2.y, w2.y, a1);
+      a2 = fma(g3.x, w3.x, a2);
+      a3 = fma(g3.y, w3.y, a3);
     }
-    if (j < h) {
+    for (; j < h; ++j) {
       const double2 g0 = gr[j], w0 = v2[j];
       a0 = fma(g0.x, w0.x, a0);
       a1 = fma(g0.y, w0.y, a1);
@@ -143,7 +150,7 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
   double* rad = Mc + kGdChunk * LDM;               // kGdChunk x NL radial factors
   double* leg = rad + kGdChunk * NL;               // kGdChunk x NLM associated Legendre values
   double* trg = leg + kGdChunk * L.NLM;            // kGdChunk x NTR cos / sin of m theta
-  double* geo = trg + kGdChunk * L.NTR;            // kGdChunk x 8: r, theta, phi, signal, cos phi, u, exp(-u/2)
+  double* gall = trg + kGdChunk * L.NTR;           // N x 8 per kept row: r, theta, phi, signal, cos phi, u, exp(-u/2)
   double* vb = gd_smem + L.vec;
   double* vx = vb + Kp;
   double* vy = vx + Kp;
@@ -162,6 +169,7 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
   __shared__ int64_t s_v;
   __shared__ int s_n;
   __shared__ double s_lmax;
+  __shared__ int s_first;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, q = lane & 3;
 
@@ -235,53 +243,51 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
     const int n = s_n;
 
     // ---- 2. Gram matrix and right-hand side
-    double acc[TPW][2];
+    // effective geometry of every kept row (one thread per row)
+    for (int r = tid; r < n; r += blockDim.x) {
+      const int i = rows[r];
+      const double b = p.bvals[i];
+      const double gx = p.bvecs[3 * i], gy = p.bvecs[3 * i + 1], gz = p.bvecs[3 * i + 2];
+      const double gn = sqrt(gx * gx + gy * gy + gz * gz);
+      double be = b, dx = gx, dy = gy, dz = gz;
+      if (b > p.b0_thr && gn > 1e-12) {  // graddev.rs:171-177 (identity frame rotation)
+        double Tm[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) Tm[e] = p.T ? p.T[v * 9 + e] : ((e % 4 == 0) ? 1.0 : 0.0);
+        const double ux = gx / gn, uy = gy / gn, uz = gz / gn;
+        const double qx = Tm[0] * ux + Tm[3] * uy + Tm[6] * uz;  // q = T^T g
+        const double qy = Tm[1] * ux + Tm[4] * uy + Tm[7] * uz;
+        const double qz = Tm[2] * ux + Tm[5] * uy + Tm[8] * uz;
+        const double q2 = qx * qx + qy * qy + qz * qz;
+        const double qn = sqrt(q2);
+        be = b * q2;
+        dx = qx / qn;
+        dy = qy / qn;
+        dz = qz / qn;
+      }
+      // q-value and spherical angles as in k_design (src/basis/shore.rs:122-178)
+      const double qv = (be <= p.b0_thr) ? 0.0 : sqrt(be / p.qdenom);
+      const double x = dx * qv, y = dy * qv, z = dz * qv;
+      const double rr = sqrt(x * x + y * y + z * z);
+      double th = atan2(y, x);
+      const double ph = (rr > 0.0) ? acos(fmin(fmax(z / rr, -1.0), 1.0)) : 0.0;
+      if (isnan(th)) th = 0.0;
+      const double u = rr * rr / p.zeta;
+      gall[8 * r] = rr;
+      gall[8 * r + 1] = th;
+      gall[8 * r + 2] = ph;
+      gall[8 * r + 3] = static_cast<double>(p.S[v * N + i]);
+      gall[8 * r + 4] = cos(ph);
+      gall[8 * r + 5] = u;
+      gall[8 * r + 6] = exp(-u * 0.5);
+    }
+    __syncthreads();
+    double acc[TPW][2];  // this warp's tiles of G (declared after the geometry: fewer live registers there)
 #pragma unroll
     for (int s = 0; s < TPW; ++s) acc[s][0] = acc[s][1] = 0.0;
     for (int c0 = 0; c0 < n; c0 += kGdChunk) {
-      if (tid < kGdChunk) {
-        const int r = c0 + tid;
-        double rr = 0.0, th = 0.0, ph = 0.0, sig = 0.0;
-        if (r < n) {
-          const int i = rows[r];
-          const double b = p.bvals[i];
-          const double gx = p.bvecs[3 * i], gy = p.bvecs[3 * i + 1], gz = p.bvecs[3 * i + 2];
-          const double gn = sqrt(gx * gx + gy * gy + gz * gz);
-          double be = b, dx = gx, dy = gy, dz = gz;
-          if (b > p.b0_thr && gn > 1e-12) {  // graddev.rs:171-177 (identity frame rotation)
-            double Tm[9];
-#pragma unroll
-            for (int e = 0; e < 9; ++e) Tm[e] = p.T ? p.T[v * 9 + e] : ((e % 4 == 0) ? 1.0 : 0.0);
-            const double ux = gx / gn, uy = gy / gn, uz = gz / gn;
-            const double qx = Tm[0] * ux + Tm[3] * uy + Tm[6] * uz;  // q = T^T g
-            const double qy = Tm[1] * ux + Tm[4] * uy + Tm[7] * uz;
-            const double qz = Tm[2] * ux + Tm[5] * uy + Tm[8] * uz;
-            const double q2 = qx * qx + qy * qy + qz * qz;
-            const double qn = sqrt(q2);
-            be = b * q2;
-            dx = qx / qn;
-            dy = qy / qn;
-            dz = qz / qn;
-          }
-          // q-value and spherical angles as in k_design (src/basis/shore.rs:122-178)
-          const double qv = (be <= p.b0_thr) ? 0.0 : sqrt(be / p.qdenom);
-          const double x = dx * qv, y = dy * qv, z = dz * qv;
-          rr = sqrt(x * x + y * y + z * z);
-          th = atan2(y, x);
-          ph = (rr > 0.0) ? acos(fmin(fmax(z / rr, -1.0), 1.0)) : 0.0;
-          if (isnan(th)) th = 0.0;
-          sig = static_cast<double>(p.S[v * N + i]);
-        }
-        const double u = rr * rr / p.zeta;
-        geo[8 * tid] = rr;
-        geo[8 * tid + 1] = th;
-        geo[8 * tid + 2] = ph;
-        geo[8 * tid + 3] = (r < n) ? sig : 0.0;
-        geo[8 * tid + 4] = cos(ph);
-        geo[8 * tid + 5] = u;
-        geo[8 * tid + 6] = exp(-u * 0.5);
-      }
-      __syncthreads();
+      const double* geo = gall + 8 * static_cast<size_t>(c0);
+
       // per-row values, one thread per row in each of three groups: radial
       // factors (group 0), cos / sin of m theta (group 1), associated
       // Legendre values by the recurrence in l for each m (group 2); the
@@ -291,7 +297,9 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
         const int t = tid % kGdChunk, grp = tid / kGdChunk;
         const double* gt = geo + 8 * t;
         const int R = p.radial_order;
-        if (grp == 0) {
+        if (c0 + t >= n) {
+          // past the last row: nothing to evaluate (the chunk entries are 0)
+        } else if (grp == 0) {
           double rp[8];
           for (int l = 0; l <= R; l += 2) rp[l / 2] = pow(gt[5], static_cast<double>(l) / 2.0);
           int j = 0;
@@ -332,38 +340,40 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
         }
       }
       __syncthreads();
-      for (int task = tid; task < kGdChunk * Kp; task += blockDim.x) {
-        const int t = task / Kp, col = task % Kp;
-        double val = 0.0;
-        if (col < K && c0 + t < n) {
-          const int cm = col_map[col];
-          const int lk = cm & 0xff, tm = task_map[NL + lk];
-          const int m = tm >> 16, l = (tm >> 8) & 0xff, k = tm & 0xff;
-          double sh;
-          if (l == 0) {
-            sh = 1.0 / sqrt(4.0 * CUDART_PI);
-          } else {
-            const double pl = shn[lk] * leg[t * L.NLM + (l / 2) * (l / 2) + m];
-            const double s2 = sqrt(2.0);
-            if (k < l)
-              sh = s2 * pl * trg[t * L.NTR + m - 1];
-            else if (k == l)
-              sh = pl;
-            else
-              sh = s2 * (((m + 1) % 2 == 0) ? 1.0 : -1.0) * pl * trg[t * L.NTR + p.radial_order + m - 1];
+      const int rows_here = min(kGdChunk, n - c0);
+      for (int t = warp; t < kGdChunk; t += 8) {
+        for (int col = lane; col < Kp; col += 32) {
+          double val = 0.0;
+          if (col < K && t < rows_here) {
+            const int cm = col_map[col];
+            const int lk = cm & 0xff, tm = task_map[NL + lk];
+            const int m = tm >> 16, l = (tm >> 8) & 0xff, k = tm & 0xff;
+            double sh;
+            if (l == 0) {
+              sh = 1.0 / sqrt(4.0 * CUDART_PI);
+            } else {
+              const double pl = shn[lk] * leg[t * L.NLM + (l / 2) * (l / 2) + m];
+              const double s2 = sqrt(2.0);
+              if (k < l)
+                sh = s2 * pl * trg[t * L.NTR + m - 1];
+              else if (k == l)
+                sh = pl;
+              else
+                sh = s2 * (((m + 1) % 2 == 0) ? 1.0 : -1.0) * pl * trg[t * L.NTR + p.radial_order + m - 1];
+            }
+            val = rad[t * NL + (cm >> 8)] * sh;
           }
-          val = rad[t * NL + (cm >> 8)] * sh;
+          Mc[t * LDM + col] = val;
         }
-        Mc[t * LDM + col] = val;
       }
       __syncthreads();
       for (int col = tid; col < K; col += blockDim.x) {
         double a = vb[col];
-        for (int t = 0; t < kGdChunk; ++t) a = __dadd_rn(a, __dmul_rn(Mc[t * LDM + col], geo[8 * t + 3]));
+        for (int t = 0; t < rows_here; ++t) a = __dadd_rn(a, __dmul_rn(Mc[t * LDM + col], geo[8 * t + 3]));
         vb[col] = a;
       }
 #pragma unroll 1
-      for (int kk = 0; kk < kGdChunk / 4; ++kk) {
+      for (int kk = 0; kk < (rows_here + 3) / 4; ++kk) {  // rows past n are zero
         const double* rowp = Mc + (4 * kk + q) * LDM + g;
 #pragma unroll
         for (int s = 0; s < TPW; ++s)
@@ -426,24 +436,27 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
       __syncthreads();
     }
     __syncthreads();
-    if (warp == 0) {  // largest eigenvalue of the tridiagonal: 32-point multisection
+    {  // largest eigenvalue of the tridiagonal: multisection at one point per thread
       double lo = 1e300, hi = -1e300;
       for (int i = 0; i < msteps; ++i) {
         const double r = (i > 0 ? fabs(tb[i - 1]) : 0.0) + (i < msteps - 1 ? fabs(tb[i]) : 0.0);
         lo = fmin(lo, ta[i] - r);
         hi = fmax(hi, ta[i] + r);
       }
-      for (int round = 0; round < 24 && hi - lo > 1e-16 * fmax(fabs(hi), fabs(lo)); ++round) {
-        const double x = lo + (hi - lo) * (lane + 1) / 33.0;
-        const bool all_below = sturm_below(ta, tb, msteps, x) == msteps;  // x above every eigenvalue
-        const unsigned bal = __ballot_sync(kFull, all_below);
-        const int first = bal ? __ffs(bal) - 1 : 32;  // lowest point above the top eigenvalue
-        const double nlo = lo + (hi - lo) * first / 33.0;
-        const double nhi = lo + (hi - lo) * (first + 1) / 33.0;
-        lo = __shfl_sync(kFull, nlo, 0);
-        hi = __shfl_sync(kFull, nhi, 0);
+      const int P = blockDim.x;  // points lo + (hi - lo) (t + 1) / (P + 1)
+      for (int round = 0; round < 12 && hi - lo > 1e-16 * fmax(fabs(hi), fabs(lo)); ++round) {
+        if (tid == 0) s_first = P;
+        __syncthreads();
+        const double x = lo + (hi - lo) * (tid + 1) / (P + 1.0);
+        if (sturm_below(ta, tb, msteps, x) == msteps) atomicMin(&s_first, tid);  // x above every eigenvalue
+        __syncthreads();
+        const int first = s_first;  // the top eigenvalue lies in (x_{first-1}, x_first]
+        const double nlo = lo + (hi - lo) * first / (P + 1.0);
+        hi = lo + (hi - lo) * (first + 1) / (P + 1.0);
+        lo = nlo;
+        __syncthreads();
       }
-      if (lane == 0) s_lmax = 0.5 * (lo + hi);
+      if (tid == 0) s_lmax = 0.5 * (lo + hi);
     }
     __syncthreads();
     const double nv = static_cast<double>(n);
