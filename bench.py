@@ -27,6 +27,8 @@ error of the mixed path against the FP64 path).
           (fit + RTOP + 362-direction ODF, then backward to the signals and the
           hyper-parameter), voxels/s for L1 and Tikhonov, and the ratio of the
           forward+backward step to the forward step.
+* graddev the per-voxel-design fit (BASELINE config 3 shapes: radial order 8,
+          a deviation tensor and dropped samples per voxel) on 100k voxels.
 * cpu_baseline  the CPU FP64 oracle (a restatement of the reference's rayon
           path: the Rust reference cannot be built without cargo) on all host
           threads, on a bounded sample of the same voxels.
@@ -54,6 +56,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "SHORE L1-fit voxels/s, mixed vs FP64 GPU at \u22641e-5 rel err; fwd+bwd voxels/s"
 FWD_BWD_GRID = (50, 50, 20)  # the differentiable-fit workload: 50,000 voxels, radial order 6
+GRADDEV_VOXELS = 100_000     # per-voxel-design workload (radial order 8), a third of the 300k volume
 WORKLOAD = "brain300k"
 
 
@@ -369,6 +372,8 @@ def run_ours(args):
 
     # ---- fwd+bwd: differentiable fit of 50k voxels
     fwd_bwd = fwd_bwd_block(args, device, world)
+    # ---- per-voxel designs (gradient deviation, dropped samples)
+    graddev = graddev_block(args, device, world)
 
     # ---- roofline of the FISTA kernel
     flops_per_iter = 2 * K * K + 8 * K
@@ -424,6 +429,7 @@ def run_ours(args):
                                         f"scalar DFMA measured {dfma_peak:.1f} TFLOP/s" if dmma_peak else None},
             "gpu_launches": launches if path == "fp64" else mix_launches,
             "fwd_bwd": fwd_bwd,
+            "graddev": graddev,
             "paths": paths,
             "clocks": clocks.summary(),
             "iterations_per_voxel": it_launch / V,
@@ -496,6 +502,40 @@ def fwd_bwd_block(args, device: int, world: int) -> dict:
         else:
             out["l2"] = dict(block, solver="Tikhonov, lambda_n = lambda_l = 0.05, transpose solve")
     return out
+
+
+def graddev_block(args, device: int, world: int) -> dict:
+    """L1 fit on a design per voxel: 100,000 voxels of the phantom, each with
+    its own gradient-deviation tensor (I + N(0, 0.02)) and 0-15 % of its
+    samples dropped, radial order 8 (K = 145), alpha 0.01, the reference's
+    FISTA.  CUDA events on the fit stream, max over ranks; min(steps, 3)
+    timed steps (each builds 100k Gram matrices of 145 x 145)."""
+    import torch
+
+    from cs_dmri_b200.graddev import graddev_phantom, shore_fit_graddev
+
+    S, bvals, bvecs, T, keep, big, small = graddev_phantom(GRADDEV_VOXELS, seed=3)
+    dev = f"cuda:{device}"
+    St, Tt, Kt = (torch.from_numpy(a).to(dev) for a in (S, T, keep))
+    kw = dict(alpha=0.01, radial_order=8, big_delta=big, small_delta=small, device=device)
+    for _ in range(args.warmup):
+        out = shore_fit_graddev(St, bvals, bvecs, Tt, Kt, **kw)
+    steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize(device)
+    barrier(world)
+    st = torch.cuda.current_stream(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        out = shore_fit_graddev(St, bvals, bvecs, Tt, Kt, **kw)
+    e1.record(st)
+    torch.cuda.synchronize(device)
+    ms = max_over_ranks(e0.elapsed_time(e1) / steps, world, torch.device("cuda", device))
+    return {"metric": "per-voxel-design L1-fit voxels/s", "value": world * GRADDEV_VOXELS / (ms * 1e-3),
+            "unit": "voxels/s", "ms_per_step": ms, "steps": steps,
+            "workload": f"graddev100k: {GRADDEV_VOXELS} voxels, radial order 8 (K = 145), N = {S.shape[1]}, "
+                        "deviation tensor and 0-15 % dropped samples per voxel",
+            "dtype": "f64", "iterations_per_voxel": float(out["iterations"].double().mean())}
 
 
 def main():
