@@ -317,6 +317,63 @@ __global__ void __launch_bounds__(256) k_apply64(const double* __restrict__ At, 
   }
 }
 
+// The same product on the FP64 tensor cores, for a matrix that fits in
+// shared memory: A is staged once per persistent CTA in m8n8k4 A-fragment
+// order, frag[(mt * KT + kt) * 32 + lane] = A[8 mt + lane / 4][4 kt + lane % 4]
+// (zero padded; read from At), so each fragment is one conflict-free 256-byte
+// read.  A warp takes 8 voxels at a time: out^T (rows x 8) = A in^T, the
+// voxels' inputs as B fragments (loaded once per k-step and reused across a
+// chunk of kApplyMtc row tiles held as accumulators).
+constexpr int kApplyMtc = 12;
+
+__global__ void __launch_bounds__(256, 1) k_apply_dmma(const double* __restrict__ At, int rows, int cols,
+                                                       const double* __restrict__ in, int64_t ldin, int64_t V,
+                                                       double* __restrict__ out, float* __restrict__ out32,
+                                                       int64_t ldout) {
+  extern __shared__ __align__(16) double sA[];
+  const int MT = (rows + 7) / 8, KT = (cols + 3) / 4;
+  for (int i = threadIdx.x; i < MT * KT * 32; i += blockDim.x) {
+    const int lane = i & 31, t = i >> 5, mt = t / KT, kt = t % KT;
+    const int r = 8 * mt + (lane >> 2), k = 4 * kt + (lane & 3);
+    sA[i] = (r < rows && k < cols) ? At[static_cast<size_t>(k) * rows + r] : 0.0;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, q = lane & 3;
+  const int64_t groups = (V + 7) / 8;
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t grp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp; grp < groups; grp += nwarps) {
+    const int64_t v0 = 8 * grp;
+    const int64_t vb = v0 + g;  // this lane's voxel in the B fragment
+    const bool vok = vb < V;
+    for (int mt0 = 0; mt0 < MT; mt0 += kApplyMtc) {
+      double d[kApplyMtc][2];
+#pragma unroll
+      for (int j = 0; j < kApplyMtc; ++j) d[j][0] = d[j][1] = 0.0;
+      for (int kt = 0; kt < KT; ++kt) {
+        const int k = 4 * kt + q;
+        const double b = (vok && k < cols) ? in[vb * ldin + k] : 0.0;
+#pragma unroll
+        for (int j = 0; j < kApplyMtc; ++j)
+          if (mt0 + j < MT) dmma_m8n8k4(d[j][0], d[j][1], sA[((mt0 + j) * KT + kt) * 32 + lane], b);
+      }
+#pragma unroll
+      for (int j = 0; j < kApplyMtc; ++j) {
+        const int r = 8 * (mt0 + j) + g;
+        if (mt0 + j >= MT || r >= rows) continue;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int64_t vv = v0 + 2 * q + e;
+          if (vv < V) {
+            if (out) out[vv * ldout + r] = d[j][e];
+            if (out32) out32[vv * ldout + r] = static_cast<float>(d[j][e]);
+          }
+        }
+      }
+    }
+  }
+}
+
 __global__ void k_fill_u32(uint32_t* __restrict__ a, int64_t n, uint32_t v) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < n) a[i] = v;

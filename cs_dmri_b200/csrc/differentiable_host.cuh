@@ -158,6 +158,18 @@ struct L2Adj {
 
 void launch_apply64(csd_handle* h, const double* At, int rows, int cols, const double* in, int64_t ldin, int64_t V,
                     double* out, float* out32, int64_t ldout) {
+  // tensor-core path when the matrix fits in one CTA's shared memory
+  const size_t dmma_smem = sizeof(double) * 32 * static_cast<size_t>((rows + 7) / 8) * ((cols + 3) / 4);
+  if (dmma_smem <= static_cast<size_t>(h->smem_optin)) {
+    CSD_CUDA(cudaFuncSetAttribute(csd::k_apply_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(dmma_smem)));
+    const int64_t groups = (V + 7) / 8;
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((groups + 7) / 8, h->num_sms));
+    csd::k_apply_dmma<<<static_cast<unsigned>(blocks), 256, dmma_smem, h->stream>>>(At, rows, cols, in, ldin, V,
+                                                                                    out, out32, ldout);
+    CSD_LAUNCH();
+    return;
+  }
   const size_t per_warp = sizeof(double) * 8 * static_cast<size_t>(cols);
   const int warps = static_cast<int>(std::max<size_t>(1, std::min<size_t>(8, (100u << 10) / per_warp)));
   const size_t smem = per_warp * warps;
