@@ -350,9 +350,17 @@ __global__ void __launch_bounds__(256, 1) k_apply_dmma(const double* __restrict_
       double d[kApplyMtc][2];
 #pragma unroll
       for (int j = 0; j < kApplyMtc; ++j) d[j][0] = d[j][1] = 0.0;
+      // B fragments two k-steps ahead, so a global load is in flight while
+      // the DMMAs of the current k-step issue
+      double bq[3];
+#pragma unroll
+      for (int u = 0; u < 3; ++u) bq[u] = (vok && 4 * u + q < cols && u < KT) ? in[vb * ldin + 4 * u + q] : 0.0;
       for (int kt = 0; kt < KT; ++kt) {
-        const int k = 4 * kt + q;
-        const double b = (vok && k < cols) ? in[vb * ldin + k] : 0.0;
+        const double b = bq[0];
+        bq[0] = bq[1];
+        bq[1] = bq[2];
+        const int kn = 4 * (kt + 3) + q;
+        bq[2] = (vok && kn < cols) ? in[vb * ldin + kn] : 0.0;
 #pragma unroll
         for (int j = 0; j < kApplyMtc; ++j)
           if (mt0 + j < MT) dmma_m8n8k4(d[j][0], d[j][1], sA[((mt0 + j) * KT + kt) * 32 + lane], b);

@@ -22,6 +22,7 @@ struct PeakParams {
   float* pdir;            // V x npeaks x 3 (zeros past the peaks found)
   float* pval;            // V x npeaks ODF amplitude at the peak
   float* pqa;             // V x npeaks amplitude minus the voxel's minimum amplitude (>= 0)
+  int at_in_smem;         // stage At in shared memory once per CTA (when it fits)
 };
 
 // One warp per voxel.  Amplitudes a_r = sum_k A[r][k] c_k in FP64 (lane
@@ -32,13 +33,20 @@ struct PeakParams {
 // decreasing amplitude (ties: lower index first), stopping below rel_thr x
 // the largest, skipping any within the separation angle of a kept one
 // (|cos| >= cos_sep, antipodes included), up to npeaks.
-__global__ void __launch_bounds__(256) k_odf_peaks(PeakParams p) {
+__global__ void __launch_bounds__(512) k_odf_peaks(PeakParams p) {
   extern __shared__ __align__(16) double pk_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nw = blockDim.x >> 5;
   const int K = p.K, R = p.R;
-  double* sc = pk_smem + static_cast<size_t>(warp) * (K + R);  // coefficients, then amplitudes
+  const size_t at_sz = p.at_in_smem ? static_cast<size_t>(K) * R : 0;
+  double* sat = pk_smem;                                                 // K x R (staged At), or empty
+  double* sc = pk_smem + at_sz + static_cast<size_t>(warp) * (K + R);  // coefficients, then amplitudes
   double* sa = sc + K;
+  const double* At = p.at_in_smem ? sat : p.At;
+  if (p.at_in_smem) {
+    for (size_t i = threadIdx.x; i < at_sz; i += blockDim.x) sat[i] = p.At[i];
+    __syncthreads();
+  }
   for (int64_t v = static_cast<int64_t>(blockIdx.x) * nw + warp; v < p.V; v += static_cast<int64_t>(gridDim.x) * nw) {
     const float* c = p.coeffs + p.vox[v] * K;
     __syncwarp();
@@ -49,7 +57,7 @@ __global__ void __launch_bounds__(256) k_odf_peaks(PeakParams p) {
     for (int j = 0; j < kPeakMaxRows; ++j) a[j] = 0.0;
     for (int k = 0; k < K; ++k) {
       const double ck = sc[k];
-      const double* row = p.At + static_cast<size_t>(k) * R;
+      const double* row = At + static_cast<size_t>(k) * R;
 #pragma unroll
       for (int j = 0; j < kPeakMaxRows; ++j) {
         const int r = lane + 32 * j;

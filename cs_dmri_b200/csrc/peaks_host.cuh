@@ -93,11 +93,18 @@ extern "C" int csd_shore_odf_peaks(csd_handle* h, const float* coefficients, int
     pp.pdir = o + V;
     pp.pval = o + V + 3 * npeaks * V;
     pp.pqa = o + V + 4 * npeaks * V;
-    const int warps = 8;
-    const size_t smem = sizeof(double) * static_cast<size_t>(warps) * (K + R);
+    // the amplitude matrix staged once per CTA when it fits next to the warp
+    // slices (16 warps), else read through the caches (8 warps)
+    const size_t at_bytes = sizeof(double) * static_cast<size_t>(K) * R;
+    pp.at_in_smem = at_bytes + sizeof(double) * 16 * static_cast<size_t>(K + R) <= static_cast<size_t>(h->smem_optin);
+    const int warps = pp.at_in_smem ? 16 : 8;
+    const size_t smem = (pp.at_in_smem ? at_bytes : 0) + sizeof(double) * static_cast<size_t>(warps) * (K + R);
     CSD_CUDA(cudaFuncSetAttribute(csd::k_odf_peaks, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem)));
-    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((V + warps - 1) / warps, h->num_sms * 8));
+    int per_sm = 0;
+    CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_odf_peaks, 32 * warps, smem));
+    const int64_t blocks =
+        std::max<int64_t>(1, std::min<int64_t>((V + warps - 1) / warps, h->num_sms * std::max(per_sm, 1)));
     csd::k_odf_peaks<<<static_cast<unsigned>(blocks), 32 * warps, smem, st>>>(pp);
     CSD_LAUNCH();
     std::vector<float> hs(per_v * static_cast<size_t>(V));
