@@ -251,3 +251,20 @@ def last_timing(device: int = 0) -> Timing:
     t = Timing()
     load().csd_last_timing(handle(device), C.byref(t))
     return t
+
+
+class PrivateHandle:
+    """A handle of its own (device memory, streams, set-up cache) for a user
+    that must not share scratch buffers with other calls, such as a captured
+    CUDA graph whose kernels keep pointing at them; released with the object."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        self.h = C.c_void_p()
+        err = C.create_string_buffer(1024)
+        check(self.lib.csd_create(C.byref(self.h), device, err, len(err)), err)
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.lib.csd_destroy(self.h)
+            self.h = C.c_void_p()

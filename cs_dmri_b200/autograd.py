@@ -125,11 +125,13 @@ class DifferentiableShore:
     ``radial_order``, ``zeta``, ``regularization`` ("l1" or "l2"),
     ``max_iter``, ``tol``, ``non_negative``, ``precision``; the gradient
     table is ``bvals``, ``bvecs``, ``big_delta``, ``small_delta``,
-    ``b0_threshold``.  L1 fits take a fixed alpha (one, or one per voxel)."""
+    ``b0_threshold``.  L1 fits take a fixed alpha (one, or one per voxel).
+    ``handle`` (an ``_abi.PrivateHandle``) gives the model library scratch of
+    its own instead of the device's shared handle."""
 
     def __init__(self, bvals, bvecs, *, big_delta=None, small_delta=None, b0_threshold=50.0, radial_order=6,
                  zeta=700.0, regularization="l1", max_iter=1000, tol=1e-6, non_negative=False, precision="fp64",
-                 allow_single_shell=False, device: int = 0):
+                 allow_single_shell=False, device: int = 0, handle=None):
         if regularization not in ("l1", "l2"):
             raise ValueError(f"regularization must be l1 or l2 for the differentiable fit, got {regularization!r}")
         self.regularization = regularization
@@ -149,6 +151,7 @@ class DifferentiableShore:
         self.device = torch.device("cuda", self.device_index)
         self._mats: dict = {}
         self._singular = torch.zeros(1, dtype=torch.int64, device=self.device)
+        self._private = handle  # an _abi.PrivateHandle, or None for the process-wide handle of the device
 
     # ---------------------------------------------------------------- public
     def fit(self, signals: torch.Tensor, alpha=None, *, lambda_n=None, lambda_l=None, warm=None) -> torch.Tensor:
@@ -190,7 +193,7 @@ class DifferentiableShore:
         if key not in self._mats:
             d = geodesic_sphere(6) if directions is None else np.ascontiguousarray(directions, dtype=np.float64)
             A = np.zeros((len(d), self.K))
-            _call(_abi.load().csd_shore_odf_matrix, _abi.handle(self.device_index), self.radial_order, self.zeta,
+            _call(_abi.load().csd_shore_odf_matrix, self._handle(), self.radial_order, self.zeta,
                   d.ctypes.data, len(d), A.ctypes.data)
             self._mats[key] = self._device_pair(A)
         A, At = self._mats[key]
@@ -221,6 +224,9 @@ class DifferentiableShore:
         return self._adjoint_raw(self._check_coef(coef).detach(), grad_coef, spec, signal32=False, signal64=True)
 
     # -------------------------------------------------------------- internals
+    def _handle(self):
+        return self._private.h if self._private is not None else _abi.handle(self.device_index)
+
     def _as_f64(self, v) -> torch.Tensor:
         if isinstance(v, torch.Tensor):
             return v.to(self.device, torch.float64)
@@ -257,7 +263,7 @@ class DifferentiableShore:
         alpha_v = hyper.detach().expand(V).contiguous() if self.regularization == "l1" else None
         coef = torch.empty((V, self.K), dtype=torch.float64, device=self.device)
         lib = _abi.load()
-        _call(lib.csd_shore_fit_batch_device, _abi.handle(self.device_index), s.data_ptr(), V, C.byref(self._g),
+        _call(lib.csd_shore_fit_batch_device, self._handle(), s.data_ptr(), V, C.byref(self._g),
               C.byref(spec), _ptr(alpha_v), _ptr(warm), coef.data_ptr(), None, _stream(s))
         return coef
 
@@ -267,7 +273,7 @@ class DifferentiableShore:
         gs32 = torch.empty((V, self.N), dtype=torch.float32, device=self.device) if signal32 else None
         gs64 = torch.empty((V, self.N), dtype=torch.float64, device=self.device) if signal64 else None
         gh = torch.empty((V, 2), dtype=torch.float64, device=self.device)
-        _call(_abi.load().csd_shore_fit_adjoint_device, _abi.handle(self.device_index), C.byref(self._g),
+        _call(_abi.load().csd_shore_fit_adjoint_device, self._handle(), C.byref(self._g),
               C.byref(spec), coef.contiguous().data_ptr(), g.data_ptr(), V, _ptr(gs32), _ptr(gs64),
               gh.data_ptr(), _ptr(self._singular), _stream(g))
         return (gs64 if signal64 else gs32), gh
@@ -281,14 +287,14 @@ class DifferentiableShore:
     def _apply_raw(self, At, rows, cols, x) -> torch.Tensor:
         x = x.detach().to(self.device, torch.float64).contiguous()
         out = torch.empty((x.shape[0], rows), dtype=torch.float64, device=self.device)
-        _call(_abi.load().csd_apply_rows_device, _abi.handle(self.device_index), At.data_ptr(), rows, cols,
+        _call(_abi.load().csd_apply_rows_device, self._handle(), At.data_ptr(), rows, cols,
               x.data_ptr(), x.shape[0], out.data_ptr(), _stream(x))
         return out
 
     def _rtop_raw(self, coef) -> torch.Tensor:
         c = coef.detach().contiguous()
         out = torch.empty(c.shape[0], dtype=torch.float64, device=self.device)
-        _call(_abi.load().csd_shore_rtop_device, _abi.handle(self.device_index), self.radial_order, self.zeta,
+        _call(_abi.load().csd_shore_rtop_device, self._handle(), self.radial_order, self.zeta,
               c.data_ptr(), c.shape[0], out.data_ptr(), _stream(c))
         return out
 
@@ -296,6 +302,6 @@ class DifferentiableShore:
         c = coef.detach().contiguous()
         g = grad.detach().to(self.device, torch.float64).contiguous()
         out = torch.empty_like(c)
-        _call(_abi.load().csd_shore_rtop_adjoint_device, _abi.handle(self.device_index), self.radial_order,
+        _call(_abi.load().csd_shore_rtop_adjoint_device, self._handle(), self.radial_order,
               self.zeta, c.data_ptr(), c.shape[0], g.data_ptr(), out.data_ptr(), _stream(c))
         return out

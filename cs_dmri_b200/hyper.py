@@ -26,7 +26,7 @@ import torch
 from . import _core
 from .autograd import DifferentiableShore
 
-__all__ = ["holdout_split", "HypergradientAlpha", "select_alpha_hypergradient"]
+__all__ = ["holdout_split", "HypergradientAlpha", "CapturedHypergradient", "select_alpha_hypergradient"]
 
 
 def holdout_split(bvals, fraction=0.1, seed=0, b0_threshold=50.0):
@@ -48,15 +48,25 @@ class HypergradientAlpha:
     CUDA tensors (V, N) on the full table ``bvals`` / ``bvecs``)."""
 
     def __init__(self, bvals, bvecs, *, big_delta=None, small_delta=None, b0_threshold=50.0, radial_order=6,
-                 zeta=700.0, max_iter=1000, tol=1e-6, holdout_fraction=0.1, seed=0, device: int = 0):
+                 zeta=700.0, max_iter=1000, tol=1e-6, holdout_fraction=0.1, seed=0, device: int = 0, handle=None):
+        self._args = (bvals, bvecs)
+        self._kwargs = dict(big_delta=big_delta, small_delta=small_delta, b0_threshold=b0_threshold,
+                            radial_order=radial_order, zeta=zeta, max_iter=max_iter, tol=tol,
+                            holdout_fraction=holdout_fraction, seed=seed, device=device)
         self.bvals = np.asarray(bvals, dtype=np.float64).ravel()
         self.bvecs = np.asarray(bvecs, dtype=np.float64).reshape(-1, 3)
         self.train, self.held_out = holdout_split(self.bvals, holdout_fraction, seed, b0_threshold)
         kw = dict(big_delta=big_delta, small_delta=small_delta, b0_threshold=b0_threshold,
-                  radial_order=radial_order, zeta=zeta, max_iter=max_iter, tol=tol, device=device)
+                  radial_order=radial_order, zeta=zeta, max_iter=max_iter, tol=tol, device=device, handle=handle)
         self.model = DifferentiableShore(self.bvals[self.train], self.bvecs[self.train], regularization="l1", **kw)
         self.full = DifferentiableShore(self.bvals, self.bvecs, regularization="l1", **kw)
         self.device = self.model.device
+        self._idx = None  # sample indices on the device (made once, so a captured run copies nothing from the host)
+
+    def capture(self, signals: torch.Tensor, **kw) -> "CapturedHypergradient":
+        """The whole run (``run``'s keyword arguments) as one CUDA graph
+        over ``signals``; see ``CapturedHypergradient``."""
+        return CapturedHypergradient(self, signals, **kw)
 
     def heldout_loss(self, coef: torch.Tensor, s_ho: torch.Tensor) -> torch.Tensor:
         """Per-voxel squared prediction error on the held-out samples."""
@@ -64,8 +74,11 @@ class HypergradientAlpha:
         return (pred - s_ho).square().sum(1)
 
     def split(self, signals: torch.Tensor):
-        tr = torch.as_tensor(self.train, device=signals.device)
-        ho = torch.as_tensor(self.held_out, device=signals.device)
+        """(training samples float32, held-out samples float64) of each voxel."""
+        if self._idx is None or self._idx[0].device != signals.device:
+            self._idx = (torch.as_tensor(self.train, device=signals.device),
+                         torch.as_tensor(self.held_out, device=signals.device))
+        tr, ho = self._idx
         return signals.index_select(1, tr).contiguous(), signals.index_select(1, ho).to(torch.float64)
 
     def run(self, signals: torch.Tensor, *, alpha0=0.01, steps=8, step0=0.5, alpha_range=(1e-3, 1e3)):
@@ -99,6 +112,39 @@ class HypergradientAlpha:
             prev = torch.where(agree < 0, torch.zeros_like(sgn), sgn)
             warm = c.detach()
         return best_alpha, best_loss, loss0, hist
+
+
+class CapturedHypergradient:
+    """``HypergradientAlpha.run`` captured in one CUDA graph: every fit,
+    held-out prediction, adjoint and step of the run, replayed by
+    ``replay()`` on the current contents of the signal tensor it was captured
+    with.  ``outputs`` are that run's (alpha, loss, loss at alpha0) tensors,
+    rewritten by each replay.  The run uses a library handle of its own, so
+    no other call can free or resize the scratch memory the graph's kernels
+    point at; the handle lives as long as this object."""
+
+    def __init__(self, selector: "HypergradientAlpha", signals: torch.Tensor, **kw):
+        from . import _abi
+        self._handle = _abi.PrivateHandle(selector._kwargs["device"])
+        self.selector = HypergradientAlpha(*selector._args, **selector._kwargs, handle=self._handle)
+        self.signals = signals
+        side = torch.cuda.Stream(signals.device)
+        side.wait_stream(torch.cuda.current_stream(signals.device))
+        with torch.cuda.stream(side):  # one untimed run sizes every buffer before capture
+            self.selector.run(signals, **kw)
+        torch.cuda.current_stream(signals.device).wait_stream(side)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            best, loss, loss0, _ = self.selector.run(signals, **kw)
+        self.outputs = (best, loss, loss0)
+
+    def replay(self):
+        self.graph.replay()
+        return self.outputs
+
+    def __del__(self):
+        self.graph = None  # the graph goes before the handle whose memory it uses
+        self.selector = None
 
 
 def select_alpha_hypergradient(data, bvals, bvecs, mask, *, big_delta=None, small_delta=None, b0_threshold=50.0,
