@@ -253,3 +253,28 @@ def test_zero_support_and_errors(ctx):
         m.fit(St, torch.full((3,), 0.01, dtype=torch.float64, device="cuda"))
     with pytest.raises(ValueError, match="needs alpha"):
         m.fit(St)
+
+
+@pytest.mark.parametrize("reg", ["l1", "l2"])
+def test_radial_order_8_adjoint_matches_oracle(ctx, oracle, reg):
+    """K = 145: the adjoint kernels' five-register rows and the cached-matrix
+    apply (the 259 x 145 design does not fit in shared memory)."""
+    torch = ctx["torch"]
+    ph = ctx["ph"]
+    m = model(ctx, regularization=reg, radial_order=8)
+    St = ctx["St"][:48]
+    c = m.fit(St, 0.01) if reg == "l1" else m.fit(St, lambda_n=0.05, lambda_l=0.02)
+    gc = np.random.default_rng(11).normal(size=c.shape)
+    kw = dict(alpha=0.01) if reg == "l1" else dict(lambda_n=0.05, lambda_l=0.02)
+    gs, gh = m.signal_gradient(c, torch.from_numpy(gc).cuda(), **kw)
+    gs, gh, cn = gs.cpu().numpy(), gh.cpu().numpy(), c.cpu().numpy()
+    M8 = oracle.design_matrix(ph.bvals, ph.bvecs, 8, 700.0, **ctx["kw"])
+    nd, ld = oracle.regularization(8)
+    for v in range(0, len(cn), 4):
+        if reg == "l1":
+            ws, wa, _ = oracle.l1_adjoint(M8, cn[v], gc[v])
+            np.testing.assert_allclose(gh[v, 0], wa, rtol=1e-8, atol=1e-300)
+        else:
+            ws, (wn, wl), _ = oracle.l2_adjoint(M8, cn[v], gc[v], nd, ld, 0.05, 0.02)
+            np.testing.assert_allclose(gh[v], [wn, wl], rtol=1e-8)
+        np.testing.assert_allclose(gs[v], ws, rtol=0, atol=1e-8 * np.abs(ws).max() + 1e-300)
