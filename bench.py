@@ -29,6 +29,9 @@ error of the mixed path against the FP64 path).
           forward+backward step to the forward step.
 * graddev the per-voxel-design fit (BASELINE config 3 shapes: radial order 8,
           a deviation tensor and dropped samples per voxel) on 100k voxels.
+* pipeline the hypergradient alpha selection pipeline (BASELINE config 5
+          shapes) on the same volume, host clock, with the held-out error of
+          the reference's own alpha selections beside it.
 * cpu_baseline  the CPU FP64 oracle (a restatement of the reference's rayon
           path: the Rust reference cannot be built without cargo) on all host
           threads, on a bounded sample of the same voxels.
@@ -50,6 +53,8 @@ import sys
 import threading
 import time
 from pathlib import Path
+
+import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
@@ -374,6 +379,8 @@ def run_ours(args):
     fwd_bwd = fwd_bwd_block(args, device, world)
     # ---- per-voxel designs (gradient deviation, dropped samples)
     graddev = graddev_block(args, device, world)
+    # ---- hypergradient alpha selection pipeline on the same volume
+    pipeline = pipeline_block(ph, device, world)
 
     # ---- roofline of the FISTA kernel
     flops_per_iter = 2 * K * K + 8 * K
@@ -430,6 +437,7 @@ def run_ours(args):
             "gpu_launches": launches if path == "fp64" else mix_launches,
             "fwd_bwd": fwd_bwd,
             "graddev": graddev,
+            "pipeline": pipeline,
             "paths": paths,
             "clocks": clocks.summary(),
             "iterations_per_voxel": it_launch / V,
@@ -536,6 +544,35 @@ def graddev_block(args, device: int, world: int) -> dict:
             "workload": f"graddev100k: {GRADDEV_VOXELS} voxels, radial order 8 (K = 145), N = {S.shape[1]}, "
                         "deviation tensor and 0-15 % dropped samples per voxel",
             "dtype": "f64", "iterations_per_voxel": float(out["iterations"].double().mean())}
+
+
+def pipeline_block(ph, device: int, world: int) -> dict:
+    """The hypergradient pipeline on the brain-sized volume: per-voxel alpha by
+    8 Rprop steps on the hypergradient of a held-out 10 % of the samples, the
+    final fit on every sample, 3 peaks + GFA, RTOP and MSD (host volumes in
+    and out).  One untimed run, then one run on the host clock (it includes
+    the host copies); the reference's own selections (L2-anchored, path-BIC)
+    and the fixed alpha are scored on the same held-out samples in that run."""
+    import torch
+
+    from cs_dmri_b200.hyper import select_alpha_hypergradient
+
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, device=device)
+    select_alpha_hypergradient(ph.data, ph.bvals, ph.bvecs, ph.mask, compare_reference=False, **kw)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    t = time.perf_counter()
+    out = select_alpha_hypergradient(ph.data, ph.bvals, ph.bvecs, ph.mask, compare_reference=False, **kw)
+    torch.cuda.synchronize(device)
+    dt = max_over_ranks(time.perf_counter() - t, world, torch.device("cuda", device))
+    comp = select_alpha_hypergradient(ph.data, ph.bvals, ph.bvecs, ph.mask, compare_reference=True,
+                                      **kw)["comparison"]
+    V = int(ph.mask.sum())
+    return {"metric": "hypergradient-pipeline voxels/s", "value": world * V / dt, "unit": "voxels/s",
+            "seconds": dt, "workload": f"{WORKLOAD}: {V} voxels, 8 hypergradient steps, final fit, 3 peaks, "
+                                       "GFA, RTOP, MSD (host volumes in and out)",
+            "heldout_error_median": comp,
+            "alpha_median": float(np.median(out["alpha"][ph.mask]))}
 
 
 def main():
