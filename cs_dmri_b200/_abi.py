@@ -98,6 +98,9 @@ class Timing(C.Structure):
         ("ms_mixed_kernel", C.c_float),
         ("int8_tensor_ops", C.c_double),
         ("fp64_rerun_voxels", C.c_uint64),
+        ("fista_warps", C.c_int32),
+        ("fista_tune_ms12", C.c_float),
+        ("fista_tune_ms16", C.c_float),
     ]
 
 

@@ -285,6 +285,11 @@ struct csd_handle {
   int adjconst_order = -1;
   double adjconst_zeta = 0.0;
   int sm_cap = 0;  // > 0: FISTA grids use at most this many SMs
+  // FISTA autotuning (per gradient table): warps per CTA of k_fista_v3 and
+  // the batch times of the two candidates
+  int fista_warps = 0;
+  float tune_ms[2] = {0.f, 0.f};
+  DevBuf tuneB, tuneX, tuneIt, tuneConv, tuneQ;
   double mixed_ms = 0.0, mixed_ops = 0.0;
   unsigned long long mixed_rerun = 0;
 };
@@ -294,6 +299,8 @@ namespace {
 void set_err(char* err, size_t len, const std::string& msg) {
   if (err && len > 0) std::snprintf(err, len, "%s", msg.c_str());
 }
+
+void autotune_fista(csd_handle* h);
 
 // Build (or reuse) the per-gradient-table device setup.
 void ensure_setup(csd_handle* h, const HostGtab& g, int radial_order, double zeta, bool need_chol,
@@ -382,6 +389,7 @@ void ensure_setup(csd_handle* h, const HostGtab& g, int radial_order, double zet
     h->lambda_max = sc2[1];
     h->setup_key = key;
     h->setup_valid = true;
+    autotune_fista(h);
   }
   if (need_chol) {
     uint64_t ck = fnv1a(key, &lambda_n, sizeof lambda_n);
@@ -532,12 +540,12 @@ void launch_fista_v3_t(csd_handle* h, const csd::FistaParams& p) {
 }
 
 // FISTA kernel variant: 0 = k_fista_fp64 (registers hold x, y, b); 3 / 4 =
-// k_fista_v3 with 12 / 16 warps per CTA.  CSD_FISTA_VARIANT overrides the
-// default.
-int fista_variant() {
+// k_fista_v3 with 12 / 16 warps per CTA, chosen per gradient table by
+// autotune_fista.  CSD_FISTA_VARIANT overrides the choice.
+int fista_variant(const csd_handle* h) {
   const char* e = std::getenv("CSD_FISTA_VARIANT");
   if (e && *e) return std::atoi(e);
-  return 4;
+  return (h && h->fista_warps == 12) ? 3 : 4;
 }
 
 void launch_fista(csd_handle* h, int MT, const csd::FistaParams& p);
@@ -620,7 +628,7 @@ void launch_fista(csd_handle* h, int MT, const csd::FistaParams& p) {
     CSD_LAUNCH();
     return;
   }
-  const int variant = fista_variant();
+  const int variant = fista_variant(h);
   if (variant == 3 || variant == 4) {
     switch (MT * 8 + variant) {
       case 1 * 8 + 3: launch_fista_v3_t<1, 12>(h, p); return;
@@ -911,6 +919,65 @@ double validate(const csd_shore_spec* s, const HostGtab& g, std::string& warning
 void record(csd_handle* h, int i) { CSD_CUDA(cudaEventRecord(h->ev[i], h->stream)); }
 
 // The whole-volume fit on device buffers.
+// Autotuning of the FISTA kernel's warps per CTA (12 or 16), once per
+// gradient table: both k_fista_v3 variants fit a fixed synthetic batch of
+// 73,728 voxels (four waves of slots) - single-tensor signals on the table
+// (k_tune_signal), alpha 0.01, exactly 48 iterations each (tol 0) - and the
+// faster is used for the table's fits.  Both variants compute identical
+// iterates, so the choice never changes a result.  Each candidate runs once
+// untimed, then once timed.
+void autotune_fista(csd_handle* h) {
+  h->fista_warps = 16;
+  h->tune_ms[0] = h->tune_ms[1] = 0.f;
+  const int MT = h->Kp / 8;
+  if (MT != 4 && MT != 9) return;
+  cudaStream_t st = h->stream;
+  const int64_t Vt = 73728;
+  const int its = 48;
+  const int Kp = h->Kp, N = h->N, K = h->K;
+  ensure_mom(h, its);
+  h->tuneB.ensure(sizeof(double) * Vt * Kp);
+  h->tuneX.ensure(std::max(sizeof(double) * Vt * Kp, sizeof(float) * Vt * N));
+  h->tuneIt.ensure(sizeof(uint32_t) * Vt);
+  h->tuneConv.ensure(Vt);
+  h->tuneQ.ensure(sizeof(unsigned long long));
+  float* S = h->tuneX.as<float>();  // the signals live in X until the right-hand sides are formed
+  csd::k_tune_signal<<<grid1(Vt * N), 256, 0, st>>>(h->bvals.as<double>(), h->bvecs.as<double>(), N, Vt, S);
+  CSD_LAUNCH();
+  csd::k_tune_rhs<<<grid1(Vt * Kp), 256, 0, st>>>(h->M.as<double>(), N, K, Kp, S, Vt, h->tuneB.as<double>());
+  CSD_LAUNCH();
+  csd::FistaParams p{};
+  p.B = h->tuneB.as<double>();
+  p.X = h->tuneX.as<double>();
+  p.iters = h->tuneIt.as<uint32_t>();
+  p.conv = h->tuneConv.as<uint8_t>();
+  p.V = Vt;
+  p.n_inv = 1.0 / static_cast<double>(N);
+  p.step = 1.0 / h->lipschitz;
+  p.thr = p.step * 0.01;
+  p.tol = 0.0;  // never converges: every voxel runs exactly `its` iterations
+  p.max_iter = its;
+  p.queue = h->tuneQ.as<unsigned long long>();
+  p.n_work = Vt;
+  const int saved_cap = h->sm_cap;
+  h->sm_cap = 0;
+  for (int pass = 0; pass < 2; ++pass)
+    for (int c = 0; c < 2; ++c) {
+      CSD_CUDA(cudaMemsetAsync(p.queue, 0, sizeof(unsigned long long), st));
+      CSD_CUDA(cudaEventRecord(h->ev[8], st));
+      if (MT == 4)
+        c == 0 ? launch_fista_v3_t<4, 12>(h, p) : launch_fista_v3_t<4, 16>(h, p);
+      else
+        c == 0 ? launch_fista_v3_t<9, 12>(h, p) : launch_fista_v3_t<9, 16>(h, p);
+      CSD_CUDA(cudaEventRecord(h->ev[9], st));
+      CSD_CUDA(cudaEventSynchronize(h->ev[9]));
+      float ms = 0.f;
+      if (pass == 1 && cudaEventElapsedTime(&ms, h->ev[8], h->ev[9]) == cudaSuccess) h->tune_ms[c] = ms;
+    }
+  h->sm_cap = saved_cap;
+  h->fista_warps = (h->tune_ms[0] > 0.f && h->tune_ms[0] < h->tune_ms[1]) ? 12 : 16;
+}
+
 FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64_t nvol,
                 const HostGtab& g, const csd_shore_spec* spec, double path_eps, const DevOut& out,
                 bool data_on_host = false) {
@@ -1548,7 +1615,7 @@ void csd_destroy(csd_handle* h) {
                     &h->palpha_fb, &h->pit_fb, &h->pconv_fb, &h->pcode, &h->gdig, &h->gfexp, &h->flagged,
                     &h->mixstat, &h->pcoef, &h->pmat, &h->pout, &h->pgt, &h->pgv, &h->pdir, &h->pconst,
                     &h->iota, &h->adjW, &h->adjovf, &h->adjstat, &h->adjconst,
-                    &h->gdtab, &h->gdq};
+                    &h->gdtab, &h->gdq, &h->tuneB, &h->tuneX, &h->tuneIt, &h->tuneConv, &h->tuneQ};
   for (auto s : h->pipe)
     if (s) cudaStreamSynchronize(s);
   for (DevBuf* b : bufs) b->release();
@@ -1671,7 +1738,8 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
     // coefficients requested: the pipelined path (transfers overlap the fit).
     const bool pipelined = on_host && K == 72 && spec->regularization == CSD_REG_L1 &&
                            spec->alpha_mode == CSD_ALPHA_FIXED && spec->precision == CSD_PRECISION_FP64 &&
-                           !diag && !out->coef64 && !out->converged && spec->max_iter > 0 && fista_variant() == 4;
+                           !diag && !out->coef64 && !out->converged && spec->max_iter > 0 &&
+                           (fista_variant(h) == 3 || fista_variant(h) == 4);
     FitInfo info = pipelined
                        ? run_fit_pipelined(h, d_data, h->mask.as<uint8_t>(), nvol, g, spec, d.coeffs, out->coefficients)
                        : run_fit(h, d_data, h->mask.as<uint8_t>(), nvol, g, spec, path_eps, d, on_host);
@@ -1917,6 +1985,9 @@ int csd_shore_microstructure(csd_handle* h, const float* coefficients, int64_t X
 int csd_last_timing(const csd_handle* h, csd_fit_timing* out) {
   if (!h || !out) return CSD_ERR_INVALID;
   *out = h->timing;
+  out->fista_warps = h->fista_warps;
+  out->fista_tune_ms12 = h->tune_ms[0];
+  out->fista_tune_ms16 = h->tune_ms[1];
   return CSD_OK;
 }
 

@@ -1096,6 +1096,39 @@ __global__ void k_iota(int64_t* __restrict__ a, int64_t n) {
   if (i < n) a[i] = i;
 }
 
+// Signals of the FISTA autotuning batch: one tensor per voxel on the table,
+// S0 1000 exp(-b (l_perp + (l_par - l_perp) (g . u)^2)) with l_par 1.7e-3,
+// l_perp 0.3e-3 and a direction u hashed from the voxel index - data whose
+// fits have the sparsity, and so the k-step skipping, of real ones.
+__global__ void k_tune_signal(const double* __restrict__ bvals, const double* __restrict__ bvecs, int N,
+                              int64_t V, float* __restrict__ S) {
+  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= V * N) return;
+  const int64_t v = idx / N;
+  const int i = static_cast<int>(idx % N);
+  unsigned long long z = static_cast<unsigned long long>(v) * 0x9E3779B97F4A7C15ull + 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 31)) * 0x94D049BB133111EBull;
+  z ^= z >> 29;
+  const double cz = 2.0 * static_cast<double>(z & 0xffffff) / 16777216.0 - 1.0;
+  const double ph = 6.283185307179586 * static_cast<double>((z >> 24) & 0xffffff) / 16777216.0;
+  const double sz = sqrt(fmax(1.0 - cz * cz, 0.0));
+  const double gu = bvecs[3 * i] * sz * cos(ph) + bvecs[3 * i + 1] * sz * sin(ph) + bvecs[3 * i + 2] * cz;
+  S[idx] = static_cast<float>(1000.0 * exp(-bvals[i] * (0.3e-3 + 1.4e-3 * gu * gu)));
+}
+
+// b = M^T s of the autotuning batch, one thread per (voxel, coefficient).
+__global__ void k_tune_rhs(const double* __restrict__ M, int N, int K, int Kp, const float* __restrict__ S,
+                           int64_t V, double* __restrict__ B) {
+  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= V * Kp) return;
+  const int64_t v = idx / Kp;
+  const int k = static_cast<int>(idx % Kp);
+  double acc = 0.0;
+  if (k < K)
+    for (int i = 0; i < N; ++i) acc += M[static_cast<size_t>(i) * K + k] * static_cast<double>(S[v * N + i]);
+  B[idx] = acc;
+}
+
 __global__ void k_fill_f64(double* __restrict__ a, int64_t n, double v) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < n) a[i] = v;

@@ -220,6 +220,9 @@ typedef struct csd_fit_timing {
   float ms_mixed_kernel;/* the mixed-precision FISTA kernel alone (0 in FP64) */
   double int8_tensor_ops;      /* int8 tensor-core ops it issued (2 per MAC) */
   uint64_t fp64_rerun_voxels;  /* voxels the stop-decision guard re-ran in FP64 */
+  int32_t fista_warps;         /* FISTA kernel warps per CTA the autotuner chose for the table (0: none) */
+  float fista_tune_ms12;       /* the autotuning batch's time with 12 warps per CTA */
+  float fista_tune_ms16;       /* ... and with 16 */
 } csd_fit_timing;
 
 int csd_last_timing(const csd_handle* h, csd_fit_timing* out);

@@ -353,3 +353,25 @@ def test_pipelined_host_fit_matches_the_device_fit():
     np.testing.assert_array_equal(out.numpy(), pageable["coefficients"])
     np.testing.assert_array_equal(out.numpy(), dev.cpu().numpy())
     assert got["total_iterations"] == pageable["total_iterations"]
+
+
+def test_fista_autotuner_choice_changes_nothing(monkeypatch):
+    """The per-table autotuner picks k_fista_v3's warps per CTA (12 or 16)
+    from a timed synthetic batch; both give bit-identical fits."""
+    from cs_dmri_b200 import _abi, shore_fit
+    from cs_dmri_b200.phantom import make_phantom
+    ph = make_phantom((12, 10, 8), seed=23)
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, alpha_mode="fixed", alpha=0.01,
+              return_coef64=True)
+    auto = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, **kw)
+    t = _abi.last_timing(0)
+    assert t.fista_warps in (12, 16)
+    assert t.fista_tune_ms12 > 0 and t.fista_tune_ms16 > 0
+    assert t.fista_warps == (12 if t.fista_tune_ms12 < t.fista_tune_ms16 else 16)
+    fits = {}
+    for variant in ("3", "4"):
+        monkeypatch.setenv("CSD_FISTA_VARIANT", variant)
+        fits[variant] = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, **kw)
+    for f in fits.values():
+        np.testing.assert_array_equal(f["coef64"], auto["coef64"])
+        np.testing.assert_array_equal(f["coefficients"], auto["coefficients"])
