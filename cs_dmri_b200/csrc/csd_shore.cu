@@ -289,6 +289,7 @@ struct csd_handle {
   // the batch times of the two candidates
   int fista_warps = 0;
   float tune_ms[2] = {0.f, 0.f};
+  std::map<uint64_t, std::array<float, 3>> tune_cache;  // table key -> (warps, ms12, ms16)
   DevBuf tuneB, tuneX, tuneIt, tuneConv, tuneQ;
   double mixed_ms = 0.0, mixed_ops = 0.0;
   unsigned long long mixed_rerun = 0;
@@ -931,6 +932,13 @@ void autotune_fista(csd_handle* h) {
   h->tune_ms[0] = h->tune_ms[1] = 0.f;
   const int MT = h->Kp / 8;
   if (MT != 4 && MT != 9) return;
+  const auto hit = h->tune_cache.find(h->setup_key);  // a table seen before on this handle
+  if (hit != h->tune_cache.end()) {
+    h->fista_warps = static_cast<int>(hit->second[0]);
+    h->tune_ms[0] = hit->second[1];
+    h->tune_ms[1] = hit->second[2];
+    return;
+  }
   cudaStream_t st = h->stream;
   const int64_t Vt = 73728;
   const int its = 48;
@@ -976,6 +984,7 @@ void autotune_fista(csd_handle* h) {
     }
   h->sm_cap = saved_cap;
   h->fista_warps = (h->tune_ms[0] > 0.f && h->tune_ms[0] < h->tune_ms[1]) ? 12 : 16;
+  h->tune_cache[h->setup_key] = {static_cast<float>(h->fista_warps), h->tune_ms[0], h->tune_ms[1]};
 }
 
 FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64_t nvol,
