@@ -27,11 +27,12 @@ error of the mixed path against the FP64 path).
           (fit + RTOP + 362-direction ODF, then backward to the signals and the
           hyper-parameter), voxels/s for L1 and Tikhonov, and the ratio of the
           forward+backward step to the forward step.
-* graddev the per-voxel-design fit (BASELINE config 3 shapes: radial order 8,
-          a deviation tensor and dropped samples per voxel) on 100k voxels.
-* pipeline the hypergradient alpha selection pipeline (BASELINE config 5
-          shapes) on the same volume, host clock, with the held-out error of
-          the reference's own alpha selections beside it.
+* graddev the per-voxel-design fit (radial order 8, a gradient-deviation
+          tensor and 0-15 % dropped samples per voxel) on 100k voxels.
+* pipeline the hypergradient alpha selection pipeline (8 steps on a held-out
+          10 % of the samples, final fit, peaks, RTOP / MSD) on the same
+          volume, host clock, with the held-out error of the reference's own
+          alpha selections beside it.
 * cpu_baseline  the CPU FP64 oracle (a restatement of the reference's rayon
           path: the Rust reference cannot be built without cargo) on all host
           threads, on a bounded sample of the same voxels.
