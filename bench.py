@@ -402,7 +402,7 @@ def run_ours(args):
         mk_ms = statistics.median(mix_kernel_ms)
         paths = {
             "fp64": {"value": value, "unit": "voxels/s", "ms_per_step": ms / args.steps,
-                     "kernel": "k_fista_v3<9,16> (FP64 DMMA mma.sync.m8n8k4)", "kernel_ms": statistics.median(kernel_ms),
+                     "kernel": "k_fista_v3<9,16> (FP64 DMMA mma.sync.m8n8k4), two passes", "kernel_ms": statistics.median(kernel_ms),
                      "gpu_launches": launches},
             "mixed": {"value": value_mix, "unit": "voxels/s", "ms_per_step": ms_mix / args.steps,
                       "speedup_vs_fp64": value_mix / value,
@@ -428,6 +428,9 @@ def run_ours(args):
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": dmma_peak, "unit": "TFLOP/s",
                          "frac": (achieved / dmma_peak) if dmma_peak else None, "traffic": traffic,
                          "kernel": "k_fista_v3<9,16>", "kernel_ms": k_ms,
+                         "kernel_scope": "both passes of the two-pass schedule (to iteration 80, then the "
+                                         "parked voxels slowest-first) and the bucket sort between them, "
+                                         "timed together with CUDA events",
                          "flops_per_launch": it_launch * flops_per_iter,
                          "flops_basis": "dense Gram form, executed voxel-iterations x (2K^2 + 8K)",
                          "executed_tensor_flops_per_launch": statistics.median(tensor_flops),

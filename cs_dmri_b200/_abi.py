@@ -101,6 +101,7 @@ class Timing(C.Structure):
         ("fista_warps", C.c_int32),
         ("fista_tune_ms12", C.c_float),
         ("fista_tune_ms16", C.c_float),
+        ("fista_parked", C.c_int64),
     ]
 
 
@@ -173,7 +174,7 @@ def _declare(lib: C.CDLL) -> C.CDLL:
     tail = [C.c_void_p, C.c_char_p, C.c_size_t]  # stream, err, err_len
     lib.csd_shore_fit_batch_device.restype = C.c_int
     lib.csd_shore_fit_batch_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(Gtab), C.POINTER(Spec),
-                                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + tail
+                                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + tail
     lib.csd_shore_fit_adjoint_device.restype = C.c_int
     lib.csd_shore_fit_adjoint_device.argtypes = [C.c_void_p, C.POINTER(Gtab), C.POINTER(Spec), C.c_void_p,
                                                  C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -127,11 +127,16 @@ class DifferentiableShore:
     table is ``bvals``, ``bvecs``, ``big_delta``, ``small_delta``,
     ``b0_threshold``.  L1 fits take a fixed alpha (one, or one per voxel).
     ``handle`` (an ``_abi.PrivateHandle``) gives the model library scratch of
-    its own instead of the device's shared handle."""
+    its own instead of the device's shared handle.  ``schedule="previous"``
+    (the default) has each L1 fit of a batch take its voxels up in decreasing
+    iteration count of the model's previous fit of a batch of the same size
+    (repeated fits of one batch - training loops, hypergradient steps - then
+    have no late-starting slow voxels); ``"index"`` keeps voxel order.  The
+    results are the same either way."""
 
     def __init__(self, bvals, bvecs, *, big_delta=None, small_delta=None, b0_threshold=50.0, radial_order=6,
                  zeta=700.0, regularization="l1", max_iter=1000, tol=1e-6, non_negative=False, precision="fp64",
-                 allow_single_shell=False, device: int = 0, handle=None):
+                 allow_single_shell=False, device: int = 0, handle=None, schedule="previous"):
         if regularization not in ("l1", "l2"):
             raise ValueError(f"regularization must be l1 or l2 for the differentiable fit, got {regularization!r}")
         self.regularization = regularization
@@ -152,6 +157,10 @@ class DifferentiableShore:
         self._mats: dict = {}
         self._singular = torch.zeros(1, dtype=torch.int64, device=self.device)
         self._private = handle  # an _abi.PrivateHandle, or None for the process-wide handle of the device
+        if schedule not in ("previous", "index"):
+            raise ValueError(f"schedule must be 'previous' or 'index', got {schedule!r}")
+        self.schedule = schedule
+        self._iters = None  # iteration counts of the last L1 fit (int32, one per voxel)
 
     # ---------------------------------------------------------------- public
     def fit(self, signals: torch.Tensor, alpha=None, *, lambda_n=None, lambda_l=None, warm=None) -> torch.Tensor:
@@ -262,9 +271,17 @@ class DifferentiableShore:
         V = s.shape[0]
         alpha_v = hyper.detach().expand(V).contiguous() if self.regularization == "l1" else None
         coef = torch.empty((V, self.K), dtype=torch.float64, device=self.device)
+        order = None
+        if self.regularization == "l1" and self.schedule == "previous":
+            # voxels in decreasing iteration count of this model's previous fit of a batch this size
+            if self._iters is not None and self._iters.shape[0] == V:
+                order = torch.argsort(self._iters, descending=True, stable=True)
+            else:
+                self._iters = torch.zeros(V, dtype=torch.int32, device=self.device)
         lib = _abi.load()
         _call(lib.csd_shore_fit_batch_device, self._handle(), s.data_ptr(), V, C.byref(self._g),
-              C.byref(spec), _ptr(alpha_v), _ptr(warm), coef.data_ptr(), None, _stream(s))
+              C.byref(spec), _ptr(alpha_v), _ptr(warm), _ptr(order), coef.data_ptr(),
+              _ptr(self._iters if self.schedule == "previous" and self.regularization == "l1" else None), _stream(s))
         return coef
 
     def _adjoint_raw(self, coef, grad, spec, *, signal32=True, signal64=False):

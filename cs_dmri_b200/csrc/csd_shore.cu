@@ -69,9 +69,15 @@ struct Error {
     ++h->launches;                                                                             \
   } while (0)
 
+// Device buffer that grows on demand; freed when the handle that owns it is
+// destroyed (csd_destroy makes the handle's device current first).
 struct DevBuf {
   void* p = nullptr;
   size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
   void ensure(size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (bytes <= cap) return;
@@ -285,6 +291,14 @@ struct csd_handle {
   int adjconst_order = -1;
   double adjconst_zeta = 0.0;
   int sm_cap = 0;  // > 0: FISTA grids use at most this many SMs
+  // two-pass FISTA schedule: parked state (Y), parked positions, their keys,
+  // the second pass's order, and per call slot [count, bucket counts,
+  // bucket cursors]; a call uses slot sched_slot and entries from sched_base
+  // on (the pipelined fit runs chunks concurrently, one slot each)
+  DevBuf schedY, schedPend, schedKey, schedOrder, schedCnt;
+  int sched_slot = 0;
+  int64_t sched_base = 0;
+  int sched_off = 0;  // > 0: single pass (an explicit order was given, or timing runs)
   // FISTA autotuning (per gradient table): warps per CTA of k_fista_v3 and
   // the batch times of the two candidates
   int fista_warps = 0;
@@ -519,6 +533,47 @@ void launch_fista_t(csd_handle* h, const csd::FistaParams& p) {
   CSD_LAUNCH();
 }
 
+// Two-pass schedule: a fit is split at iteration sched_cap() when it has at
+// least kSchedMinWaves voxels per FISTA slot (fewer: the slowest voxels start
+// in the first wave anyway) and max_iter is above twice the cap.  The slot
+// count of the call's grid sets the scale.  CSD_FISTA_SCHEDULE=0 turns it
+// off; a value of 2 or more sets the cap.
+constexpr int kSchedCap = 80;
+
+int sched_cap() {
+  const char* e = std::getenv("CSD_FISTA_SCHEDULE");
+  if (!e || !*e) return kSchedCap;
+  const int c = std::atoi(e);
+  return c == 0 ? 0 : std::max(c, 2);
+}
+constexpr int64_t kSchedMinWaves = 4;
+constexpr size_t kSchedSlotBytes = 4096;  // count (8 B), bucket counts, bucket cursors
+constexpr int kSchedSlots = 16;
+
+// Single-pass FISTA for the lifetime of the guard.
+struct SchedOff {
+  csd_handle* h;
+  explicit SchedOff(csd_handle* hh) : h(hh) { ++h->sched_off; }
+  ~SchedOff() { --h->sched_off; }
+  SchedOff(const SchedOff&) = delete;
+  SchedOff& operator=(const SchedOff&) = delete;
+};
+
+bool sched_enabled(const csd_handle* h, const csd::FistaParams& p, int64_t slots) {
+  const int cap = sched_cap();
+  if (cap == 0 || h->sched_off > 0 || p.cap != 0 || p.n_work_dev || p.max_iter <= 2 * cap) return false;
+  return p.n_work >= kSchedMinWaves * slots;
+}
+
+// Scratch of the two-pass schedule for fits over up to V positions.
+void ensure_sched(csd_handle* h, int64_t V) {
+  h->schedY.ensure(sizeof(double) * static_cast<size_t>(V) * h->Kp);
+  h->schedPend.ensure(sizeof(int64_t) * static_cast<size_t>(V));
+  h->schedKey.ensure(sizeof(float) * static_cast<size_t>(V));
+  h->schedOrder.ensure(sizeof(int64_t) * static_cast<size_t>(V));
+  h->schedCnt.ensure(kSchedSlotBytes * kSchedSlots);
+}
+
 template <int MT, int WARPS, bool G_IN_SMEM = true>
 void launch_fista_v3_t(csd_handle* h, const csd::FistaParams& p) {
   constexpr int KP = 8 * MT;
@@ -536,7 +591,46 @@ void launch_fista_v3_t(csd_handle* h, const csd::FistaParams& p) {
   csd::FistaParams q = p;
   q.gfrag = h->gfrag.as<double>();
   q.mom = h->mom.as<double>();
-  csd::k_fista_v3<MT, WARPS, G_IN_SMEM><<<static_cast<unsigned>(blocks), 32 * WARPS, smem, h->stream>>>(q);
+  cudaStream_t st = h->stream;
+  if (!sched_enabled(h, p, blocks * WARPS * 8)) {
+    csd::k_fista_v3<MT, WARPS, G_IN_SMEM><<<static_cast<unsigned>(blocks), 32 * WARPS, smem, st>>>(q);
+    CSD_LAUNCH();
+    return;
+  }
+  // pass 1 to the cap; order the parked voxels; pass 2 resumes them
+  if (h->sched_slot < 0 || h->sched_slot >= kSchedSlots || h->sched_base < 0 || h->sched_base + p.n_work > p.V)
+    throw Error{CSD_ERR_INVALID, "two-pass FISTA schedule: slot or base out of range"};
+  ensure_sched(h, p.V);
+  char* cnt = static_cast<char*>(h->schedCnt.p) + kSchedSlotBytes * h->sched_slot;
+  auto* n_pend = reinterpret_cast<unsigned long long*>(cnt);
+  auto* hist = reinterpret_cast<unsigned*>(cnt + 8);
+  unsigned* cursor = hist + csd::kSchedBins;
+  int64_t* pend = h->schedPend.as<int64_t>() + h->sched_base;
+  float* key = h->schedKey.as<float>() + h->sched_base;
+  int64_t* order = h->schedOrder.as<int64_t>() + h->sched_base;
+  CSD_CUDA(cudaMemsetAsync(cnt, 0, kSchedSlotBytes, st));
+  csd::FistaParams q1 = q;
+  q1.cap = sched_cap();
+  q1.resume = 0;
+  q1.Y = h->schedY.as<double>();
+  q1.pend = pend;
+  q1.pend_key = key;
+  q1.n_pend = n_pend;
+  csd::k_fista_v3<MT, WARPS, G_IN_SMEM><<<static_cast<unsigned>(blocks), 32 * WARPS, smem, st>>>(q1);
+  CSD_LAUNCH();
+  csd::k_sched_hist<<<h->num_sms, 256, 0, st>>>(key, n_pend, hist, p.iter_total ? p.iter_total + 2 : nullptr);
+  CSD_LAUNCH();
+  csd::k_sched_order<<<h->num_sms, csd::kSchedBins, 0, st>>>(pend, key, n_pend, hist, cursor, order);
+  CSD_LAUNCH();
+  CSD_CUDA(cudaMemsetAsync(p.queue, 0, sizeof(unsigned long long), st));
+  csd::FistaParams q2 = q1;
+  q2.resume = 1;
+  q2.warm = nullptr;
+  q2.list = order;
+  q2.n_work_dev = n_pend;
+  q2.pend = nullptr;
+  q2.pend_key = nullptr;
+  csd::k_fista_v3<MT, WARPS, G_IN_SMEM><<<static_cast<unsigned>(blocks), 32 * WARPS, smem, st>>>(q2);
   CSD_LAUNCH();
 }
 
@@ -939,6 +1033,7 @@ void autotune_fista(csd_handle* h) {
     h->tune_ms[1] = hit->second[2];
     return;
   }
+  SchedOff single_pass(h);  // the timed batch runs a fixed 48 iterations per voxel
   cudaStream_t st = h->stream;
   const int64_t Vt = 73728;
   const int its = 48;
@@ -1034,10 +1129,10 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   h->iters.ensure(sizeof(uint32_t) * V);
   h->conv.ensure(V);
   h->queue.ensure(sizeof(unsigned long long));
-  h->itotal.ensure(2 * sizeof(unsigned long long));
+  h->itotal.ensure(3 * sizeof(unsigned long long));
   h->resid_v.ensure(sizeof(double) * V);
   h->nnz_v.ensure(sizeof(int) * V);
-  CSD_CUDA(cudaMemsetAsync(h->itotal.p, 0, 2 * sizeof(unsigned long long), st));
+  CSD_CUDA(cudaMemsetAsync(h->itotal.p, 0, 3 * sizeof(unsigned long long), st));
 
   if (data_on_host) {
     // `d_data` aliases pinned host memory: read each masked row once over the
@@ -1301,7 +1396,7 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   record(h, 3);
 
   // executed iteration total and the alpha distribution
-  unsigned long long itot[2] = {0, 0};
+  unsigned long long itot[3] = {0, 0, 0};
   if (spec->regularization != CSD_REG_L2) {
     CSD_CUDA(cudaMemcpyAsync(itot, h->itotal.p, sizeof itot, cudaMemcpyDeviceToHost, st));
   }
@@ -1310,6 +1405,7 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   // executed FP64 tensor work of the FISTA launches: k-steps x row tiles x
   // one m8n8k4 DMMA (8 x 8 x 4 FMA)
   h->timing.tensor_flops = static_cast<double>(itot[1]) * (Kp / 8) * 512.0;
+  h->timing.fista_parked = static_cast<int64_t>(itot[2]);
   h->timing.ms_mixed_kernel = static_cast<float>(h->mixed_ms);
   h->timing.int8_tensor_ops = h->mixed_ops;
   h->timing.fp64_rerun_voxels = h->mixed_rerun;
@@ -1392,14 +1488,14 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   h->iters.ensure(sizeof(uint32_t) * V);
   h->conv.ensure(V);
   h->queue.ensure(sizeof(unsigned long long) * C);
-  h->itotal.ensure(2 * sizeof(unsigned long long));
+  h->itotal.ensure(3 * sizeof(unsigned long long));
   h->resid_v.ensure(sizeof(double) * V);
   h->sst_v.ensure(sizeof(double) * V);
   h->nnz_v.ensure(sizeof(int) * V);
   h->sig.ensure(sizeof(float) * static_cast<size_t>(V) * N);
   h->iota.ensure(sizeof(int64_t) * V);
   h->sig_compact = h->sig.as<float>();
-  CSD_CUDA(cudaMemsetAsync(h->itotal.p, 0, 2 * sizeof(unsigned long long), st));
+  CSD_CUDA(cudaMemsetAsync(h->itotal.p, 0, 3 * sizeof(unsigned long long), st));
   CSD_CUDA(cudaMemsetAsync(h->queue.p, 0, sizeof(unsigned long long) * C, st));
   csd::k_iota<<<grid1(V), 256, 0, st>>>(h->iota.as<int64_t>(), V);
   CSD_LAUNCH();
@@ -1463,8 +1559,11 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
     ~Restore() {
       h->stream = st;
       h->sm_cap = 0;
+      h->sched_slot = 0;
+      h->sched_base = 0;
     }
   } restore{h, st};
+  ensure_sched(h, V);  // before any chunk runs: chunks share the buffers
   cudaStream_t rs = h->pipe[0];
   for (int k = 0; k < C; ++k) {
     const int64_t a = c0[k], n = c0[k + 1] - c0[k];
@@ -1482,12 +1581,16 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
     CSD_CUDA(cudaStreamWaitEvent(ks, h->pev[k], 0));
     h->stream = ks;
     h->sm_cap = (k + 1 < C) ? h->num_sms - kPipeRhsCtas : 0;
+    h->sched_slot = 1 + k;
+    h->sched_base = a;
     csd::FistaParams f = fp;
     f.list = h->iota.as<int64_t>() + a;
     f.n_work = n;
     f.queue = h->queue.as<unsigned long long>() + k;
     launch_fista(h, Kp / 8, f);
     h->sm_cap = 0;
+    h->sched_slot = 0;
+    h->sched_base = 0;
     csd::EpilogueParams e = ep;
     e.list = h->iota.as<int64_t>() + a;
     e.n_work = n;
@@ -1503,7 +1606,7 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   }
   record(h, 7);
   record(h, 3);
-  unsigned long long itot[2] = {0, 0};
+  unsigned long long itot[3] = {0, 0, 0};
   CSD_CUDA(cudaMemcpyAsync(itot, h->itotal.p, sizeof itot, cudaMemcpyDeviceToHost, st));
   CSD_CUDA(cudaStreamSynchronize(st));
   info.total_iterations = itot[0];
@@ -1511,6 +1614,7 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   info.Xfinal = h->X.as<double>();
   info.conv_final = h->conv.as<uint8_t>();
   h->timing.tensor_flops = static_cast<double>(itot[1]) * (Kp / 8) * 512.0;
+  h->timing.fista_parked = static_cast<int64_t>(itot[2]);
   h->timing.ms_mixed_kernel = 0.f;
   h->timing.int8_tensor_ops = 0.0;
   h->timing.fp64_rerun_voxels = 0;
@@ -1624,7 +1728,8 @@ void csd_destroy(csd_handle* h) {
                     &h->palpha_fb, &h->pit_fb, &h->pconv_fb, &h->pcode, &h->gdig, &h->gfexp, &h->flagged,
                     &h->mixstat, &h->pcoef, &h->pmat, &h->pout, &h->pgt, &h->pgv, &h->pdir, &h->pconst,
                     &h->iota, &h->adjW, &h->adjovf, &h->adjstat, &h->adjconst,
-                    &h->gdtab, &h->gdq, &h->tuneB, &h->tuneX, &h->tuneIt, &h->tuneConv, &h->tuneQ};
+                    &h->gdtab, &h->gdq, &h->tuneB, &h->tuneX, &h->tuneIt, &h->tuneConv, &h->tuneQ,
+                    &h->schedY, &h->schedPend, &h->schedKey, &h->schedOrder, &h->schedCnt};
   for (auto s : h->pipe)
     if (s) cudaStreamSynchronize(s);
   for (DevBuf* b : bufs) b->release();

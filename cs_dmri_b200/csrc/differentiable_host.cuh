@@ -22,7 +22,8 @@ struct StreamScope {
 // b = M^T s for every row, then FISTA (fixed or per-voxel alpha, optional
 // warm start) or the Tikhonov solve; FP64 coefficients (V x K) out.
 void run_fit_batch(csd_handle* h, const float* d_sig, int64_t V, const HostGtab& g, const csd_shore_spec* spec,
-                   const double* d_alpha, const double* d_warm, double* d_coef, uint32_t* d_iters) {
+                   const double* d_alpha, const double* d_warm, const int64_t* d_order, double* d_coef,
+                   uint32_t* d_iters) {
   cudaStream_t st = h->stream;
   h->launches = 0;
   h->precision = spec->precision;
@@ -62,9 +63,15 @@ void run_fit_batch(csd_handle* h, const float* d_sig, int64_t V, const HostGtab&
     fp.max_iter = spec->max_iter;
     fp.non_negative = spec->non_negative;
     fp.queue = h->queue.as<unsigned long long>();
+    fp.list = d_order;  // the order the persistent kernel takes voxels in (nullptr: 0 .. V-1)
     fp.n_work = V;
     CSD_CUDA(cudaMemsetAsync(h->queue.p, 0, sizeof(unsigned long long), st));
-    launch_fista(h, Kp / 8, fp);
+    if (d_order) {
+      SchedOff single_pass(h);  // the caller's order replaces the two-pass schedule
+      launch_fista(h, Kp / 8, fp);
+    } else {
+      launch_fista(h, Kp / 8, fp);
+    }
     if (d_iters)
       CSD_CUDA(cudaMemcpyAsync(d_iters, h->iters.p, sizeof(uint32_t) * V, cudaMemcpyDeviceToDevice, st));
   } else {
@@ -214,7 +221,8 @@ int csd_geodesic_sphere(int32_t frequency, int32_t hemisphere, double* out, int3
 
 int csd_shore_fit_batch_device(csd_handle* h, const float* d_signals, int64_t n_voxels, const csd_gtab* gtab,
                                const csd_shore_spec* spec, const double* d_alpha, const double* d_warm,
-                               double* d_coef, uint32_t* d_iterations, void* stream, char* err, size_t err_len) {
+                               const int64_t* d_order, double* d_coef, uint32_t* d_iterations, void* stream,
+                               char* err, size_t err_len) {
   if (!h || !gtab || !spec || n_voxels < 0 || (n_voxels > 0 && (!d_signals || !d_coef))) {
     set_err(err, err_len, "invalid argument: null pointer or negative voxel count");
     return CSD_ERR_INVALID;
@@ -229,7 +237,7 @@ int csd_shore_fit_batch_device(csd_handle* h, const float* d_signals, int64_t n_
     if (spec->regularization == CSD_REG_L1 && spec->alpha_mode != CSD_ALPHA_FIXED)
       throw Error{CSD_ERR_INVALID, "the batch fit takes alpha_mode fixed (one alpha, or one per voxel)"};
     StreamScope scope(h, stream);
-    run_fit_batch(h, d_signals, n_voxels, g, spec, d_alpha, d_warm, d_coef, d_iterations);
+    run_fit_batch(h, d_signals, n_voxels, g, spec, d_alpha, d_warm, d_order, d_coef, d_iterations);
   } catch (const Error& e) {
     set_err(err, err_len, e.msg);
     return e.code;

@@ -203,9 +203,25 @@ struct FistaParams {
   unsigned long long* queue;   // next unassigned position in the work list
   const int64_t* list;         // work list of voxel positions, or nullptr (= 0..V-1)
   int64_t n_work;              // length of the work list
-  unsigned long long* iter_total;  // executed iterations, summed (nullable)
+  unsigned long long* iter_total;  // executed iterations, summed (nullable); the fit's counters
+                                   // [iterations, k-steps, voxels parked by the two-pass schedule]
   const double* mom;           // Nesterov momentum (t_k - 1) / t_{k+1}, k < max_iter
   unsigned long long* kstep_total;  // executed DMMA k-steps (each MT DMMAs), summed (nullable)
+  // Two-pass schedule (k_fista_v3 only).  Pass 1 (cap > 0, resume = 0): a
+  // voxel that has neither converged nor reached max_iter after `cap`
+  // iterations stores its exact state - x in X, the next momentum point y
+  // in Y - appends its position to `pend` with a prediction of the
+  // iterations it still needs in `pend_key`, and frees its slot.  Pass 2
+  // (resume = 1) takes such voxels (in the order of `list`, `*n_work_dev` of
+  // them) from that state at iteration `cap`.  The per-voxel arithmetic is
+  // unchanged, so the iterates are those of a single pass.
+  int cap;
+  int resume;
+  double* Y;                            // V x Kp
+  int64_t* pend;                        // positions left unfinished by pass 1
+  float* pend_key;                      // predicted remaining iterations / 2^16, in [2^-16, 1]
+  unsigned long long* n_pend;           // entries in pend
+  const unsigned long long* n_work_dev; // work-list length on the device (nullptr: n_work)
 };
 
 // One warp fits 8 voxels at a time (the 8 columns of an m8n8k4 tile).  Lane
@@ -419,6 +435,8 @@ __global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
   bool exhausted = false;
   unsigned long long executed = 0, ksteps = 0;
   const double tol2x4 = 4.0 * p.tol * p.tol;
+  float sl[2] = {0.f, 0.f}, skl[2] = {0.f, 0.f};  // pass 1: sums of log2(rel^2) and k log2(rel^2)
+  const int w0 = p.cap - p.cap / 2;                 // window of the slope fit: iterations w0+1 .. cap
 
   while (true) {
     // ---- refill (warp-aggregated queue)
@@ -431,7 +449,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
         colmask |= (((n0 >> l) & 1u) << (2 * l)) | (((n1 >> l) & 1u) << (2 * l + 1));
       const int nneed = __popc(colmask);
       if (nneed > 0) {
-        const unsigned long long V_END = static_cast<unsigned long long>(p.n_work);
+        const unsigned long long V_END = p.n_work_dev ? *p.n_work_dev : static_cast<unsigned long long>(p.n_work);
         unsigned long long base = V_END;
         if (!exhausted) {
           if (lane == 0) base = atomicAdd(p.queue, static_cast<unsigned long long>(nneed));
@@ -445,20 +463,27 @@ __global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
           const unsigned long long cand = base + __popc(colmask & ((1u << col) - 1u));
           const int64_t nv = (cand < V_END) ? (p.list ? p.list[cand] : static_cast<int64_t>(cand)) : -1;
           vid[j] = nv;
-          it[j] = 0;
+          it[j] = p.resume ? p.cap : 0;
+          sl[j] = skl[j] = 0.f;
           thr[j] = (p.alpha_v && nv >= 0) ? __dmul_rn(p.step, p.alpha_v[nv]) : p.thr;
           need[j] = false;
 #pragma unroll
           for (int mt = 0; mt < MT; ++mt) {
             const int row = 8 * mt + g;
-            double bv = 0.0, xv = 0.0;
+            double bv = 0.0, xv = 0.0, yv = 0.0;
             if (nv >= 0) {
               bv = p.B[nv * KP + row];
-              xv = p.warm ? p.warm[nv * KP + row] : 0.0;
+              if (p.resume) {
+                xv = p.X[nv * KP + row];
+                yv = p.Y[nv * KP + row];
+              } else {
+                xv = p.warm ? p.warm[nv * KP + row] : 0.0;
+                yv = xv;
+              }
             }
             x[mt][j] = xv;
             bbuf[(mt * 32 + lane) * 2 + j] = bv;
-            ybuf[row * 8 + col] = xv;
+            ybuf[row * 8 + col] = yv;
           }
         }
       }
@@ -532,6 +557,11 @@ __global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
     for (int j = 0; j < 2; ++j) {
       if (vid[j] < 0) continue;
       it[j] += 1;
+      if (p.cap > 0 && !p.resume && it[j] > w0) {
+        const float l2 = log2f(fmaxf(static_cast<float>(dx2[j] / fmax(xn2[j], 1e-24)), 1e-37f));
+        sl[j] += l2;
+        skl[j] = fmaf(static_cast<float>(it[j] - w0), l2, skl[j]);
+      }
       bool converged = false;
       if (!(dx2[j] > tol2x4 * fmax(xn2[j], 1e-24))) {
         const double rel = sqrt(dx2[j]) / fmax(sqrt(xn2[j]), 1e-12);
@@ -547,6 +577,33 @@ __global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
         }
         need[j] = true;
         vid[j] = -1;
+      } else if (it[j] == p.cap && !p.resume) {
+        // pass 1 of the two-pass schedule: park the voxel (y is this lane's
+        // own entries of the next B operand, written above)
+        const int64_t v = vid[j];
+        const int col = 2 * q + j;
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+          const int row = 8 * mt + g;
+          p.X[v * KP + row] = x[mt][j];
+          p.Y[v * KP + row] = ybuf[row * 8 + col];
+        }
+        if (g == 0) {
+          const unsigned long long slot = atomicAdd(p.n_pend, 1ull);
+          p.pend[slot] = v;
+          // remaining iterations: the least-squares line through log2(rel^2)
+          // over the window, extended to log2(tol^2) (no decrease: the most)
+          const float n = static_cast<float>(p.cap - w0), km = 0.5f * (n + 1.f);
+          const float lm = sl[j] / n;
+          const float sxx = n * (n * n - 1.f) / 12.f;
+          const float slope = (skl[j] - km * sl[j]) / sxx;
+          const float lc = lm + slope * (n - km);
+          const float target = 2.f * log2f(static_cast<float>(p.tol));
+          const float rem = slope < 0.f ? (target - lc) / slope : 65536.f;
+          p.pend_key[slot] = fminf(fmaxf(rem, 1.f), 65536.f) * (1.f / 65536.f);
+        }
+        need[j] = true;
+        vid[j] = -1;
       }
     }
     __syncwarp();
@@ -556,6 +613,74 @@ __global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
     if (lane == 0) atomicAdd(p.iter_total, executed);
   }
   if (p.kstep_total && lane == 0) atomicAdd(p.kstep_total, ksteps);
+}
+
+// Order of the second pass of the two-pass FISTA schedule: the voxels that
+// pass 1 parked, largest predicted remaining iteration count first (the ones
+// likely to need the most iterations start first instead of finishing
+// alone).  A bucket sort on the float bits of the key: 8 buckets per octave
+// from 2^-24 (smaller keys share the lowest bucket, larger ones and NaN the
+// highest); within a bucket the order is arbitrary, which changes no result.
+constexpr int kSchedBins = 256;
+constexpr unsigned kSchedBinBase = (127u - 24u) << 3;
+
+__device__ __forceinline__ int sched_bin(float key) {
+  const unsigned u = __float_as_uint(key) >> 20;  // sign 0: exponent and 3 mantissa bits
+  const int b = static_cast<int>(u) - static_cast<int>(kSchedBinBase);
+  return b < 0 ? 0 : (b >= kSchedBins ? kSchedBins - 1 : b);
+}
+
+// hist[b] += keys in bucket b (hist zeroed by the caller); the key count is
+// added to *parked_total (nullable).
+__global__ void __launch_bounds__(256) k_sched_hist(const float* __restrict__ key,
+                                                    const unsigned long long* __restrict__ n_key,
+                                                    unsigned* __restrict__ hist,
+                                                    unsigned long long* __restrict__ parked_total) {
+  __shared__ unsigned sh[kSchedBins];
+  if (parked_total && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(parked_total, *n_key);
+  for (int b = threadIdx.x; b < kSchedBins; b += blockDim.x) sh[b] = 0;
+  __syncthreads();
+  const int64_t n = static_cast<int64_t>(*n_key);
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    atomicAdd(&sh[sched_bin(key[i])], 1u);
+  __syncthreads();
+  for (int b = threadIdx.x; b < kSchedBins; b += blockDim.x)
+    if (sh[b]) atomicAdd(&hist[b], sh[b]);
+}
+
+// order[] = pend[] by bucket, highest bucket first.  Block `blk` handles one
+// contiguous segment: it reserves a run in each bucket with one atomic per
+// bucket (cursor zeroed by the caller), then places its entries.  256 threads.
+__global__ void __launch_bounds__(256) k_sched_order(const int64_t* __restrict__ pend, const float* __restrict__ key,
+                                                     const unsigned long long* __restrict__ n_key,
+                                                     const unsigned* __restrict__ hist, unsigned* __restrict__ cursor,
+                                                     int64_t* __restrict__ order) {
+  __shared__ unsigned scan[kSchedBins], base[kSchedBins], cnt[kSchedBins];
+  const int t = threadIdx.x;
+  // base[b] = entries in buckets above b (inclusive scan over reversed buckets)
+  scan[t] = hist[kSchedBins - 1 - t];
+  cnt[t] = 0;
+  __syncthreads();
+  for (int o = 1; o < kSchedBins; o <<= 1) {
+    const unsigned v = t >= o ? scan[t - o] : 0u;
+    __syncthreads();
+    scan[t] += v;
+    __syncthreads();
+  }
+  base[kSchedBins - 1 - t] = scan[t] - hist[kSchedBins - 1 - t];
+  const int64_t n = static_cast<int64_t>(*n_key);
+  const int64_t seg = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t lo = static_cast<int64_t>(blockIdx.x) * seg, hi = lo + seg < n ? lo + seg : n;
+  for (int64_t i = lo + t; i < hi; i += blockDim.x) atomicAdd(&cnt[sched_bin(key[i])], 1u);
+  __syncthreads();
+  base[t] += cnt[t] ? atomicAdd(&cursor[t], cnt[t]) : 0u;
+  cnt[t] = 0;
+  __syncthreads();
+  for (int64_t i = lo + t; i < hi; i += blockDim.x) {
+    const int b = sched_bin(key[i]);
+    order[base[b] + atomicAdd(&cnt[b], 1u)] = pend[i];
+  }
 }
 
 // max_iter == 0: every voxel of the work list keeps its starting point.

@@ -5,6 +5,10 @@ on the device at most):
     python -m cs_dmri_b200.profile_cases graddev2k   # k_graddev_fit, 2,000 voxels, radial order 8
     python -m cs_dmri_b200.profile_cases diff50k     # differentiable fit step: k_l1_adjoint, k_apply_dmma, ...
     python -m cs_dmri_b200.profile_cases peaks108k   # k_odf_peaks on a 60 x 60 x 30 coefficient volume
+    python -m cs_dmri_b200.profile_cases fista125k   # the two-pass FISTA schedule on 125,000 voxels
+
+fista125k runs its measured fit inside an NVTX range of that name
+(``ncu --nvtx --nvtx-include "fista125k/"`` selects its launches).
 """
 
 from __future__ import annotations
@@ -48,7 +52,31 @@ def peaks108k() -> None:
     print("peaks108k: mean GFA", float(out["gfa"].mean()))
 
 
-CASES = {"graddev2k": graddev2k, "diff50k": diff50k, "peaks108k": peaks108k}
+def fista125k() -> None:
+    """A fixed-alpha fit of a 50^3 phantom (125,000 voxels, K = 72) through the
+    device entry point: enough voxels per FISTA slot for the two-pass
+    schedule (pass 1 to iteration 80, bucket sort, pass 2).  A first fit
+    (gradient-table set-up, autotuning) runs outside the NVTX range."""
+    import torch
+
+    from . import _abi
+    from ._core import shore_fit_device
+    from .phantom import make_phantom
+    ph = make_phantom((50, 50, 50), seed=6)
+    d = torch.from_numpy(ph.data).cuda()
+    m = torch.from_numpy(ph.mask).cuda()
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, alpha_mode="fixed", alpha=0.01)
+    shore_fit_device(d, m, ph.bvals, ph.bvecs, **kw)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("fista125k")
+    shore_fit_device(d, m, ph.bvals, ph.bvecs, **kw)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    t = _abi.last_timing(0)
+    print(f"fista125k: solve {t.ms_solve_kernel:.3f} ms, parked {t.fista_parked} of {int(ph.mask.sum())} voxels")
+
+
+CASES = {"graddev2k": graddev2k, "diff50k": diff50k, "peaks108k": peaks108k, "fista125k": fista125k}
 
 if __name__ == "__main__":
     if len(sys.argv) != 2 or sys.argv[1] not in CASES:

@@ -223,6 +223,8 @@ typedef struct csd_fit_timing {
   int32_t fista_warps;         /* FISTA kernel warps per CTA the autotuner chose for the table (0: none) */
   float fista_tune_ms12;       /* the autotuning batch's time with 12 warps per CTA */
   float fista_tune_ms16;       /* ... and with 16 */
+  int64_t fista_parked;        /* voxels the two-pass FISTA schedule stopped at the cap and resumed,
+                                  slowest-first, in its second pass (0: single pass) */
 } csd_fit_timing;
 
 int csd_last_timing(const csd_handle* h, csd_fit_timing* out);
@@ -293,11 +295,17 @@ int csd_shore_odf_peaks(csd_handle* h, const float* coefficients, int64_t X, int
  * with alpha_mode FIXED (spec->alpha, or one alpha per voxel in `d_alpha`,
  * nullable) and an optional warm start `d_warm` (n_voxels, K), or L2.
  * FP64 coefficients (n_voxels, K) out; `d_iterations` (n_voxels) nullable.
- * The per-voxel arithmetic is that of csd_shore_fit_volume. */
+ * `d_order` (nullable) is a permutation of 0 .. n_voxels-1: the order in which
+ * the persistent FISTA kernel takes the voxels up.  Putting the voxels that
+ * need the most iterations first (known, for instance, from the previous fit
+ * of the same batch) keeps them from starting late and finishing alone; the
+ * results do not depend on the order.  The per-voxel arithmetic is that of
+ * csd_shore_fit_volume. */
 int csd_shore_fit_batch_device(csd_handle* h, const float* d_signals, int64_t n_voxels,
                                const csd_gtab* gtab, const csd_shore_spec* spec,
-                               const double* d_alpha, const double* d_warm, double* d_coef,
-                               uint32_t* d_iterations, void* stream, char* err, size_t err_len);
+                               const double* d_alpha, const double* d_warm, const int64_t* d_order,
+                               double* d_coef, uint32_t* d_iterations, void* stream, char* err,
+                               size_t err_len);
 
 /* Adjoint of that fit at the coefficients `d_coef` (n_voxels, K) for the
  * upstream gradient `d_grad_coef` (n_voxels, K).  L1: implicit derivative on

@@ -237,6 +237,29 @@ def test_end_to_end_backward(ctx, oracle):
     np.testing.assert_allclose(float(alpha.grad), ga_want, rtol=1e-8)
 
 
+def test_previous_iteration_schedule_changes_nothing(ctx):
+    """Repeated L1 fits of one batch take the voxels up slowest first (the
+    previous fit's iteration counts); coefficients stay bit-identical to the
+    fits in voxel order, at a fixed alpha and across alpha and warm-start
+    changes."""
+    torch = ctx["torch"]
+    St = ctx["St"]
+    ref, sch = model(ctx, schedule="index"), model(ctx)
+    assert sch.schedule == "previous"
+    warm = None
+    for a in (0.01, 0.01, 0.03, 0.01):
+        want = ref.fit(St, a, warm=warm).cpu().numpy()
+        got = sch.fit(St, a, warm=warm).cpu().numpy()
+        np.testing.assert_array_equal(got, want)
+        warm = torch.from_numpy(want).cuda()
+    it = sch._iters.cpu().numpy()
+    assert it.min() >= 1 and it.max() > it.min()  # counts recorded for the next fit's order
+    half = sch.fit(St[:100], 0.01).cpu().numpy()  # another batch size: voxel order again
+    np.testing.assert_array_equal(half, ref.fit(St[:100], 0.01).cpu().numpy())
+    with pytest.raises(ValueError, match="schedule"):
+        model(ctx, schedule="fastest")
+
+
 def test_zero_support_and_errors(ctx):
     torch = ctx["torch"]
     m = model(ctx)

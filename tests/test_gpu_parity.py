@@ -375,3 +375,36 @@ def test_fista_autotuner_choice_changes_nothing(monkeypatch):
     for f in fits.values():
         np.testing.assert_array_equal(f["coef64"], auto["coef64"])
         np.testing.assert_array_equal(f["coefficients"], auto["coefficients"])
+
+
+def test_two_pass_fista_schedule_changes_nothing(monkeypatch):
+    """With at least four voxels per FISTA slot a fit runs in two passes:
+    every voxel up to iteration 80, then the unfinished ones resumed from
+    their exact state, largest predicted remaining iteration count first.  The
+    coefficients, iteration counts and convergence flags are bit-identical to
+    a single pass (CSD_FISTA_SCHEDULE=0), on the device-buffer path and on the
+    pipelined host path (whose larger chunks take the two passes)."""
+    import torch
+    from cs_dmri_b200 import _abi, shore_fit
+    from cs_dmri_b200.phantom import make_phantom
+    ph = make_phantom((64, 64, 50), seed=31)  # 204,800 voxels
+    V = int(ph.mask.sum())
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, alpha_mode="fixed", alpha=0.01)
+    two = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, return_coef64=True, diagnostics=True, **kw)
+    parked = _abi.last_timing(0).fista_parked
+    assert 0.5 * V < parked <= V
+    monkeypatch.setenv("CSD_FISTA_SCHEDULE", "0")
+    one = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, return_coef64=True, diagnostics=True, **kw)
+    assert _abi.last_timing(0).fista_parked == 0
+    for k in ("coef64", "coefficients", "iterations", "converged"):
+        np.testing.assert_array_equal(two[k], one[k])
+    assert two["total_iterations"] == one["total_iterations"]
+    monkeypatch.delenv("CSD_FISTA_SCHEDULE")
+    pin = torch.empty(ph.data.shape, dtype=torch.float32, pin_memory=True)
+    pin.numpy()[...] = ph.data
+    out = torch.full(ph.data.shape[:3] + (72,), float("nan"), dtype=torch.float32, pin_memory=True)
+    got = shore_fit(pin.numpy(), ph.bvals, ph.bvecs, ph.mask, coefficients_out=out.numpy(), **kw)
+    t = _abi.last_timing(0)
+    assert t.ms_rhs == 0.0 and 0 < t.fista_parked < V  # pipelined; its two larger chunks took two passes
+    np.testing.assert_array_equal(out.numpy(), one["coefficients"])
+    assert got["total_iterations"] == one["total_iterations"]
