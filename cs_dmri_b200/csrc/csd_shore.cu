@@ -282,7 +282,7 @@ struct csd_handle {
   DevBuf flagged, mixstat;  // guard re-run list; [n_flagged, batches, error]
   DevBuf pcoef, pmat, pout, pgt, pgv, pdir, pconst;  // post-fit maps
   // pipelined host-buffer fit: rhs stream + two compute streams, chunk events
-  cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};
+  cudaStream_t pipe[4] = {nullptr, nullptr, nullptr, nullptr};  // rhs, two solve streams, output zero-fill
   cudaEvent_t pev[20] = {};
   DevBuf iota;
   // differentiable fit: adjoint solution w, overflow list and its count, RTOP constants
@@ -291,6 +291,9 @@ struct csd_handle {
   int adjconst_order = -1;
   double adjconst_zeta = 0.0;
   int sm_cap = 0;  // > 0: FISTA grids use at most this many SMs
+  // device-side call order (HandleOrder): recorded at the end of each call
+  cudaEvent_t order_ev = nullptr;
+  bool order_recorded = false;
   // two-pass FISTA schedule: parked state (Y), parked positions, their keys,
   // the second pass's order, and per call slot [count, bucket counts,
   // bucket cursors]; a call uses slot sched_slot and entries from sched_base
@@ -310,6 +313,34 @@ struct csd_handle {
 };
 
 namespace {
+
+// Device-side call order on a handle.  Every call shares the handle's buffers
+// (table set-up, scratch); the device entry points return with their work
+// still queued on the caller's stream, and the other calls run on the
+// handle's own stream.  So each call makes its stream wait for the event the
+// previous call recorded when it ended, and records it in turn: calls on one
+// handle run on the device in the order they were made, whatever streams
+// they use.  Inside a stream capture the graph's order applies and the event
+// is neither waited on nor recorded.  Declare it once the call's stream is
+// in h->stream; it records on that stream when the call returns.
+struct HandleOrder {
+  csd_handle* h;
+  bool active = false;
+  explicit HandleOrder(csd_handle* hh) : h(hh) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(h->stream, &cs) != cudaSuccess) {
+      cudaGetLastError();
+      return;  // status unknown (another stream captures in global mode): leave the order alone
+    }
+    active = cs == cudaStreamCaptureStatusNone;
+    if (active && h->order_recorded) CSD_CUDA(cudaStreamWaitEvent(h->stream, h->order_ev, 0));
+  }
+  ~HandleOrder() {
+    if (active && cudaEventRecord(h->order_ev, h->stream) == cudaSuccess) h->order_recorded = true;
+  }
+  HandleOrder(const HandleOrder&) = delete;
+  HandleOrder& operator=(const HandleOrder&) = delete;
+};
 
 void set_err(char* err, size_t len, const std::string& msg) {
   if (err && len > 0) std::snprintf(err, len, "%s", msg.c_str());
@@ -833,11 +864,15 @@ void launch_resid_dmma_t(csd_handle* h, const csd::ResidParams& r) {
 // Residual / R^2 / BIC / scatter pass.  With the M tiles in shared memory the
 // residuals run on the FP64 tensor cores (k_resid_dmma) and a light per-voxel
 // pass scatters the results (k_finalize); otherwise k_epilogue does both.
+// The residuals ||s - M c|| feed only the R^2, residual and BIC maps and the
+// explicit per-voxel output (resid_out); a scatter of coefficients alone
+// (diagnostics off) skips them.
 void launch_epilogue(csd_handle* h, const csd::EpilogueParams& p) {
   if (!h->dmma_resid || p.n_work == 0) {
     if (p.n_work > 0) launch_epilogue_ffma(h, p);
     return;
   }
+  const bool need_resid = !p.scatter || p.resid_out || p.r2 || p.resid || p.bic_map;
   const int64_t V = p.V;
   h->resid_v.ensure(sizeof(double) * V);
   h->sst_v.ensure(sizeof(double) * V);
@@ -853,11 +888,13 @@ void launch_epilogue(csd_handle* h, const csd::EpilogueParams& p) {
   r.X = p.X;
   r.resid_out = p.resid_out ? p.resid_out : h->resid_v.as<double>();
   r.sst_out = (p.scatter && p.r2) ? h->sst_v.as<double>() : nullptr;
-  switch (h->Kp) {
-    case 8: launch_resid_dmma_t<8>(h, r); break;
-    case 32: launch_resid_dmma_t<32>(h, r); break;
-    case 72: launch_resid_dmma_t<72>(h, r); break;
-    default: throw Error{CSD_ERR_INVALID, "unsupported coefficient count"};
+  if (need_resid) {
+    switch (h->Kp) {
+      case 8: launch_resid_dmma_t<8>(h, r); break;
+      case 32: launch_resid_dmma_t<32>(h, r); break;
+      case 72: launch_resid_dmma_t<72>(h, r); break;
+      default: throw Error{CSD_ERR_INVALID, "unsupported coefficient count"};
+    }
   }
   if (!p.scatter && !p.nnz_out) return;
   csd::FinalizeParams f{};
@@ -868,8 +905,8 @@ void launch_epilogue(csd_handle* h, const csd::EpilogueParams& p) {
   f.K = p.K;
   f.Kp = p.Kp;
   f.X = p.X;
-  f.resid = r.resid_out;
-  f.sst = r.sst_out;
+  f.resid = need_resid ? r.resid_out : nullptr;
+  f.sst = need_resid ? r.sst_out : nullptr;
   f.iters = p.iters;
   f.zero_v = p.zero_v;
   f.alpha_v = p.alpha_v;
@@ -1439,24 +1476,70 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
 
 // Fixed-alpha L1 fit of a page-locked host volume with the transfers
 // overlapped.  The masked voxels are cut into chunks (kPipePlan: fractions of
-// the voxels).  Three streams, ordered by events only (no kernel waits on
+// the voxels).  Streams ordered by events only (no kernel waits on
 // another):
 //   rhs:     right-hand side of chunk 0 on every SM (it reads its rows over
 //            the bus, in place), then of the later chunks, one after another,
 //            on kPipeRhsCtas SMs while the earlier chunks iterate on the rest;
-//   solve:   chunks alternate between two streams, each running its FISTA,
-//            residual / scatter and the copy of the slab of the coefficient
+//   solve:   chunks alternate between two streams, each running its FISTA
+//            and scatter, then the copy of the slab of the coefficient
 //            volume it covers back to the host.  Chunk k starts once its
 //            right-hand side is done, so its CTAs take the SMs that chunk
 //            k-1's tail frees; it leaves kPipeRhsCtas SMs free while a later
 //            right-hand side may still be running.
+//   output:  with a page-locked, mapped output volume the last chunk's
+//            slab is written in place instead of copied back after it: a
+//            fourth stream zero-fills that slab from the zeroed device volume
+//            once the last right-hand side has read its rows (so the fill
+//            does not compete with those reads on the bus), and the last
+//            chunk's scatter, ordered after the fill, writes its voxels' rows
+//            over the bus.  The drain is then the scatter alone.
 // A small first chunk shortens the fill (the first right-hand side runs
-// alone); a small last chunk shortens the drain (its copy back runs alone).
+// alone).
 // Results are those of run_fit (same kernels, same per-voxel arithmetic).
-constexpr int kPipeRhsCtas = 16;
-constexpr double kPipePlan[] = {0.2, 0.4, 0.4};
+constexpr int kPipeRhsCtas = 8;
+constexpr double kPipePlan[] = {0.15, 0.425, 0.425};
 constexpr int kPipeChunks = sizeof(kPipePlan) / sizeof(kPipePlan[0]);
-static_assert(kPipeChunks <= 15, "pipeline events");
+constexpr int kPipeMaxChunks = 15;  // events pev[0..14]; two-pass schedule slots 1..15
+static_assert(kPipeChunks <= kPipeMaxChunks, "pipeline events");
+
+// The chunk plan and the right-hand-side SM count; CSD_PIPE_PLAN ("0.2,0.4,0.4":
+// at most 15 fractions, each at least 0.02, summing to 1) and
+// CSD_PIPE_RHS_CTAS override them (invalid values are ignored).
+struct PipePlan {
+  std::vector<double> frac;
+  int rhs_ctas;
+};
+
+PipePlan pipe_plan(int num_sms) {
+  PipePlan p{std::vector<double>(kPipePlan, kPipePlan + kPipeChunks), kPipeRhsCtas};
+  if (const char* e = std::getenv("CSD_PIPE_PLAN"); e && *e) {
+    std::vector<double> f;
+    double sum = 0.0;
+    const char* s = e;
+    while (*s) {
+      char* end = nullptr;
+      const double v = std::strtod(s, &end);
+      if (end == s || !(v >= 0.02)) {
+        f.clear();
+        break;
+      }
+      f.push_back(v);
+      sum += v;
+      s = (*end == ',') ? end + 1 : end;
+      if (end == s && *s) {
+        f.clear();
+        break;
+      }
+    }
+    if (!f.empty() && static_cast<int>(f.size()) <= kPipeMaxChunks && std::fabs(sum - 1.0) < 1e-6) p.frac = f;
+  }
+  if (const char* e = std::getenv("CSD_PIPE_RHS_CTAS"); e && *e) {
+    const int v = std::atoi(e);
+    if (v >= 1 && v < num_sms) p.rhs_ctas = v;
+  }
+  return p;
+}
 
 FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64_t nvol,
                           const HostGtab& g, const csd_shore_spec* spec, float* d_coeffs, float* host_coeffs) {
@@ -1482,7 +1565,8 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
     CSD_CUDA(cudaStreamSynchronize(st));
     return info;
   }
-  const int C = V >= 65536 ? kPipeChunks : 1;
+  const PipePlan plan = pipe_plan(h->num_sms);
+  const int C = V >= 65536 ? static_cast<int>(plan.frac.size()) : 1;
   h->B.ensure(sizeof(double) * V * Kp);
   h->X.ensure(sizeof(double) * V * Kp);
   h->iters.ensure(sizeof(uint32_t) * V);
@@ -1507,7 +1591,7 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   c0[C] = V;
   double acc = 0.0;
   for (int k = 1; k < C; ++k) {
-    acc += kPipePlan[k - 1];
+    acc += plan.frac[static_cast<size_t>(k - 1)];
     c0[k] = std::min<int64_t>(V, static_cast<int64_t>(acc * static_cast<double>(V)) & ~int64_t(7));
   }
   for (int k = 1; k < C; ++k)
@@ -1520,6 +1604,15 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   CSD_CUDA(cudaStreamSynchronize(st));  // boundaries on the host; set-up done
   record(h, 2);
   record(h, 6);
+  float* d_out_host = nullptr;  // device view of a page-locked, mapped output volume
+  {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, host_coeffs) == cudaSuccess && attr.type == cudaMemoryTypeHost &&
+        attr.devicePointer)
+      d_out_host = static_cast<float*>(attr.devicePointer);
+    cudaGetLastError();  // a pageable pointer may leave an error code behind
+  }
+  if (C < 2) d_out_host = nullptr;  // one chunk: a single copy back
 
   const size_t rhs_smem = sizeof(double) * static_cast<size_t>(h->Np) * Kp + sizeof(float) * 8 * 8 * (h->Np + 4);
   CSD_CUDA(cudaFuncSetAttribute(csd::k_rhs_dmma<72>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1568,19 +1661,27 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   for (int k = 0; k < C; ++k) {
     const int64_t a = c0[k], n = c0[k + 1] - c0[k];
     const int64_t groups = (n + 7) / 8;
-    const int rhs_grid = static_cast<int>(std::min<int64_t>(k == 0 ? h->num_sms : kPipeRhsCtas, (groups + 7) / 8));
+    const int rhs_grid = static_cast<int>(std::min<int64_t>(k == 0 ? h->num_sms : plan.rhs_ctas, (groups + 7) / 8));
     csd::k_rhs_dmma<72><<<std::max(rhs_grid, 1), 256, rhs_smem, rs>>>(
         d_data, h->vox.as<int64_t>() + a, n, N, h->Np, h->mtfrag.as<double>(), h->B.as<double>() + a * Kp,
         h->sig.as<float>() + a * N);
     CSD_LAUNCH();
     CSD_CUDA(cudaEventRecord(h->pev[k], rs));
   }
+  if (d_out_host) {
+    // zero-fill the last chunk's slab in the host volume once every row has been read
+    const int64_t lo = vb[C - 1];
+    CSD_CUDA(cudaStreamWaitEvent(h->pipe[3], h->pev[C - 1], 0));
+    CSD_CUDA(cudaMemcpyAsync(host_coeffs + lo * K, d_coeffs + lo * K, sizeof(float) * static_cast<size_t>(nvol - lo) * K,
+                             cudaMemcpyDeviceToHost, h->pipe[3]));
+    CSD_CUDA(cudaEventRecord(h->pev[18], h->pipe[3]));
+  }
   for (int k = 0; k < C; ++k) {
     const int64_t a = c0[k], n = c0[k + 1] - c0[k];
     cudaStream_t ks = h->pipe[1 + (k & 1)];
     CSD_CUDA(cudaStreamWaitEvent(ks, h->pev[k], 0));
     h->stream = ks;
-    h->sm_cap = (k + 1 < C) ? h->num_sms - kPipeRhsCtas : 0;
+    h->sm_cap = (k + 1 < C) ? h->num_sms - plan.rhs_ctas : 0;
     h->sched_slot = 1 + k;
     h->sched_base = a;
     csd::FistaParams f = fp;
@@ -1594,12 +1695,20 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
     csd::EpilogueParams e = ep;
     e.list = h->iota.as<int64_t>() + a;
     e.n_work = n;
+    const bool direct = d_out_host && k == C - 1;
+    if (direct) {
+      e.coeffs = d_out_host;
+      CSD_CUDA(cudaStreamWaitEvent(ks, h->pev[18], 0));  // after the slab's zero-fill
+    }
     launch_epilogue(h, e);
     h->stream = st;
-    const int64_t lo = vb[k], hi = vb[k + 1];
-    CSD_CUDA(cudaMemcpyAsync(host_coeffs + lo * K, d_coeffs + lo * K, sizeof(float) * static_cast<size_t>(hi - lo) * K,
-                             cudaMemcpyDeviceToHost, ks));
+    if (!direct) {
+      const int64_t lo = vb[k], hi = vb[k + 1];
+      CSD_CUDA(cudaMemcpyAsync(host_coeffs + lo * K, d_coeffs + lo * K,
+                               sizeof(float) * static_cast<size_t>(hi - lo) * K, cudaMemcpyDeviceToHost, ks));
+    }
   }
+  if (d_out_host) CSD_CUDA(cudaStreamWaitEvent(st, h->pev[18], 0));
   for (int j = 1; j <= 2; ++j) {
     CSD_CUDA(cudaEventRecord(h->pev[15 + j], h->pipe[j]));
     CSD_CUDA(cudaStreamWaitEvent(st, h->pev[15 + j], 0));
@@ -1706,6 +1815,7 @@ int csd_create(csd_handle** out, int32_t device, char* err, size_t err_len) {
     h->smem_optin = static_cast<int>(prop.sharedMemPerBlockOptin);
     CSD_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     for (auto& e : h->ev) CSD_CUDA(cudaEventCreate(&e));
+    CSD_CUDA(cudaEventCreateWithFlags(&h->order_ev, cudaEventDisableTiming));
   } catch (const Error& e) {
     set_err(err, err_len, e.msg);
     delete h;
@@ -1735,6 +1845,7 @@ void csd_destroy(csd_handle* h) {
   for (DevBuf* b : bufs) b->release();
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
+  if (h->order_ev) cudaEventDestroy(h->order_ev);
   for (auto& e : h->pev)
     if (e) cudaEventDestroy(e);
   for (auto s : h->pipe)
@@ -1769,6 +1880,7 @@ int csd_shore_fit_volume_device(csd_handle* h, const float* d_data, const uint8_
       ~StreamSwap() { h->stream = saved; }
     } swap{h, h->stream};
     if (stream) h->stream = static_cast<cudaStream_t>(stream);
+    HandleOrder call_order(h);
     DevOut d{out->coefficients, out->r2,  out->residual_l2, out->alpha, out->bic, out->rss_l2,
              out->iterations,   out->regularization_kind};
     FitInfo info = run_fit(h, d_data, d_mask, X * Y * Z, g, spec, path_eps, d);
@@ -1798,6 +1910,7 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
   }
   try {
     CSD_CUDA(cudaSetDevice(h->device));
+    HandleOrder call_order(h);
     HostGtab g = make_gtab(gtab);
     std::string warnings;
     const double path_eps = validate(spec, g, warnings);
@@ -1900,6 +2013,7 @@ int csd_shore_design_matrix(csd_handle* h, const csd_gtab* gtab, int32_t radial_
   }
   try {
     CSD_CUDA(cudaSetDevice(h->device));
+    HandleOrder call_order(h);
     HostGtab g = make_gtab(gtab);
     ensure_setup(h, g, radial_order, zeta, false, 0.0, 0.0);
     CSD_CUDA(cudaMemcpyAsync(out, h->M.p, sizeof(double) * h->N * h->K, cudaMemcpyDeviceToHost, h->stream));
@@ -1969,6 +2083,7 @@ int csd_shore_predict(csd_handle* h, const float* coefficients, int64_t X, int64
   try {
     check_coeff_args(X, Y, Z, radial_order);
     CSD_CUDA(cudaSetDevice(h->device));
+    HandleOrder call_order(h);
     cudaStream_t st = h->stream;
     HostGtab g = make_gtab(target);
     const int N = static_cast<int>(g.bvals.size());
@@ -2007,6 +2122,7 @@ int csd_shore_odf_sh(csd_handle* h, const float* coefficients, int64_t X, int64_
       throw Error{CSD_ERR_INVALID, "lmax must be even and \xe2\x89\xa4 radial_order (" + std::to_string(radial_order) +
                                        "), got " + std::to_string(lmax)};
     CSD_CUDA(cudaSetDevice(h->device));
+    HandleOrder call_order(h);
     cudaStream_t st = h->stream;
     const int K = n_coeffs(radial_order);
     const int R = (lmax + 1) * (lmax + 2) / 2;
@@ -2045,6 +2161,7 @@ int csd_shore_microstructure(csd_handle* h, const float* coefficients, int64_t X
     check_coeff_args(X, Y, Z, radial_order);
     if (units != 0 && units != 1) throw Error{CSD_ERR_INVALID, "units must be 0 (um) or 1 (mm)"};
     CSD_CUDA(cudaSetDevice(h->device));
+    HandleOrder call_order(h);
     cudaStream_t st = h->stream;
     const int K = n_coeffs(radial_order);
     for (float* m : maps)

@@ -237,6 +237,7 @@ int csd_shore_fit_batch_device(csd_handle* h, const float* d_signals, int64_t n_
     if (spec->regularization == CSD_REG_L1 && spec->alpha_mode != CSD_ALPHA_FIXED)
       throw Error{CSD_ERR_INVALID, "the batch fit takes alpha_mode fixed (one alpha, or one per voxel)"};
     StreamScope scope(h, stream);
+    HandleOrder call_order(h);
     run_fit_batch(h, d_signals, n_voxels, g, spec, d_alpha, d_warm, d_order, d_coef, d_iterations);
   } catch (const Error& e) {
     set_err(err, err_len, e.msg);
@@ -259,6 +260,7 @@ int csd_shore_fit_adjoint_device(csd_handle* h, const csd_gtab* gtab, const csd_
     if (spec->regularization == CSD_REG_NONNEG)
       throw Error{CSD_ERR_INVALID, "the adjoint covers regularization l1 and l2"};
     StreamScope scope(h, stream);
+    HandleOrder call_order(h);
     const bool is_l1 = spec->regularization == CSD_REG_L1;
     h->launches = 0;
     ensure_setup(h, g, spec->radial_order, spec->zeta, !is_l1, spec->lambda_n, spec->lambda_l);
@@ -308,6 +310,7 @@ int csd_apply_rows_device(csd_handle* h, const double* d_At, int32_t rows, int32
   try {
     CSD_CUDA(cudaSetDevice(h->device));
     StreamScope scope(h, stream);
+    HandleOrder call_order(h);
     h->launches = 0;
     if (n_voxels > 0) launch_apply64(h, d_At, rows, cols, d_in, cols, n_voxels, d_out, nullptr, rows);
   } catch (const Error& e) {
@@ -325,6 +328,7 @@ int csd_shore_odf_matrix(csd_handle* h, int32_t radial_order, double zeta, const
   }
   try {
     CSD_CUDA(cudaSetDevice(h->device));
+    HandleOrder call_order(h);
     const int K = n_coeffs(radial_order);
     cudaStream_t st = h->stream;
     h->pdir.ensure(sizeof(double) * 3 * n_dirs);
@@ -353,6 +357,7 @@ int csd_shore_rtop_device(csd_handle* h, int32_t radial_order, double zeta, cons
   try {
     CSD_CUDA(cudaSetDevice(h->device));
     StreamScope scope(h, stream);
+    HandleOrder call_order(h);
     h->launches = 0;
     const csd::MicroConsts* mc = micro_consts(h, radial_order, zeta);
     if (n_voxels > 0) {
@@ -376,6 +381,7 @@ int csd_shore_rtop_adjoint_device(csd_handle* h, int32_t radial_order, double ze
   try {
     CSD_CUDA(cudaSetDevice(h->device));
     StreamScope scope(h, stream);
+    HandleOrder call_order(h);
     h->launches = 0;
     const csd::MicroConsts* mc = micro_consts(h, radial_order, zeta);
     const int K = n_coeffs(radial_order);

@@ -23,6 +23,7 @@ extern "C" int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signal
     if (spec->radial_order != 6 && spec->radial_order != 8)
       throw Error{CSD_ERR_INVALID, "the per-voxel-design fit is built for radial orders 6 and 8"};
     StreamScope scope(h, stream);
+    HandleOrder call_order(h);
     cudaStream_t st = h->stream;
     h->launches = 0;
     const int N = static_cast<int>(g.bvals.size());

@@ -23,6 +23,7 @@ extern "C" int csd_shore_odf_peaks(csd_handle* h, const float* coefficients, int
     if (!(min_separation_angle_deg >= 0.0 && min_separation_angle_deg <= 90.0))
       throw Error{CSD_ERR_INVALID, "min_separation_angle must be in [0, 90] degrees"};
     CSD_CUDA(cudaSetDevice(h->device));
+    HandleOrder call_order(h);
     cudaStream_t st = h->stream;
     h->launches = 0;
     const int K = n_coeffs(radial_order);

@@ -1152,7 +1152,7 @@ struct FinalizeParams {
   int64_t n_work;
   int N, K, Kp;
   const double* X;          // V x Kp
-  const double* resid;      // V (from k_resid_dmma)
+  const double* resid;      // V (from k_resid_dmma), or nullptr when no map needs it
   const double* sst;        // V, or nullptr (only needed with maps)
   const uint32_t* iters;    // V or nullptr (iteration count 1)
   const uint8_t* zero_v;    // V or nullptr
@@ -1186,7 +1186,7 @@ __global__ void __launch_bounds__(256) k_finalize(FinalizeParams p) {
       if (p.nnz_out) p.nnz_out[v] = nnz;
       if (p.scatter) {
         const bool zero = p.zero_v && p.zero_v[v];
-        const double resid = zero ? 0.0 : p.resid[v];
+        const double resid = (zero || !p.resid) ? 0.0 : p.resid[v];
         const double ss_res = resid * resid;
         const double sst = p.sst ? p.sst[v] : 0.0;
         if (p.r2) p.r2[li] = static_cast<float>(sst > 0.0 ? 1.0 - ss_res / sst : 0.0);

@@ -260,6 +260,29 @@ def test_previous_iteration_schedule_changes_nothing(ctx):
         model(ctx, schedule="fastest")
 
 
+def test_calls_on_one_handle_run_in_call_order():
+    """The batch fit returns with its work queued on the caller's stream; a
+    call that then switches the handle's gradient table on the handle's own
+    stream (here the design matrix of another table) must not reach the
+    shared set-up before the queued fit has used it.  100,000 voxels, so the
+    fit runs the two-pass schedule and its second pass starts late."""
+    import torch
+    from cs_dmri_b200 import design_matrix
+    from cs_dmri_b200.autograd import DifferentiableShore
+    from cs_dmri_b200.phantom import make_phantom
+    ph = make_phantom((50, 50, 40), seed=12)
+    S = torch.from_numpy(ph.data.reshape(-1, ph.data.shape[-1])).cuda()
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta)
+    a = torch.full((S.shape[0],), 0.01, dtype=torch.float64, device="cuda")
+    ref = DifferentiableShore(ph.bvals, ph.bvecs, **kw).fit(S, a)
+    torch.cuda.synchronize()
+    other = np.arange(0, len(ph.bvals), 2)
+    for _ in range(2):
+        c = DifferentiableShore(ph.bvals, ph.bvecs, **kw).fit(S, a)  # queued, not waited for
+        design_matrix(ph.bvals[other], ph.bvecs[other], **kw)       # another table on the same handle
+        assert torch.equal(c, ref)
+
+
 def test_zero_support_and_errors(ctx):
     torch = ctx["torch"]
     m = model(ctx)

@@ -339,7 +339,7 @@ def test_pipelined_host_fit_matches_the_device_fit():
     from cs_dmri_b200.phantom import make_phantom
     rng = np.random.default_rng(2)
     mask = rng.random((48, 48, 48)) < 0.9
-    ph = make_phantom((48, 48, 48), mask=mask, seed=5)   # ~99.5 k voxels -> 3 chunks (0.2 / 0.4 / 0.4)
+    ph = make_phantom((48, 48, 48), mask=mask, seed=5)   # ~99.5 k voxels -> 3 chunks (0.15 / 0.425 / 0.425)
     kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, alpha_mode="fixed", alpha=0.01)
     pin = torch.empty(ph.data.shape, dtype=torch.float32, pin_memory=True)
     pin.numpy()[...] = ph.data
@@ -353,6 +353,12 @@ def test_pipelined_host_fit_matches_the_device_fit():
     np.testing.assert_array_equal(out.numpy(), pageable["coefficients"])
     np.testing.assert_array_equal(out.numpy(), dev.cpu().numpy())
     assert got["total_iterations"] == pageable["total_iterations"]
+    # a page-locked output is written in place by the scatter kernels; a
+    # pageable one gets the slab copies
+    out2 = np.full(ph.data.shape[:3] + (72,), np.nan, np.float32)
+    shore_fit(pin.numpy(), ph.bvals, ph.bvecs, ph.mask, coefficients_out=out2, **kw)
+    assert _abi.last_timing(0).ms_rhs == 0.0
+    np.testing.assert_array_equal(out2, pageable["coefficients"])
 
 
 def test_fista_autotuner_choice_changes_nothing(monkeypatch):
