@@ -215,13 +215,17 @@ def barrier(world: int):
         dist.barrier()
 
 
-def traffic_from_profile():
-    """Per-launch DRAM bytes of the FISTA kernel from the committed ncu summary."""
-    p = ROOT / "profiles" / "k_fista_v3_brain300k.md"
+def traffic_from_profile(voxels: int, parked: float):
+    """DRAM bytes of one fit's FISTA passes from the committed ncu summary of
+    the two-pass schedule: a per-voxel figure plus one per parked voxel (its
+    state written at the cap and read back), times this run's counts."""
+    p = ROOT / "profiles" / "k_fista_v3_twopass_fista125k.md"
     if not p.exists():
         return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
-    return float(m.group(1)) if m else None
+    t = p.read_text()
+    a = re.search(r"traffic_bytes_per_voxel:\s*([0-9.eE+]+)", t)
+    b = re.search(r"traffic_bytes_per_parked_voxel:\s*([0-9.eE+]+)", t)
+    return float(a.group(1)) * voxels + float(b.group(1)) * parked if a and b else None
 
 
 def fp64_peak_tflops(device: int):
@@ -300,7 +304,7 @@ def run_ours(args):
     barrier(world)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    kernel_ms, tensor_flops, launches, iters = [], [], 0, []
+    kernel_ms, tensor_flops, launches, iters, parked = [], [], 0, [], []
     with ClockSampler(device) as clocks:
         torch.cuda.synchronize(device)
         ev0.record(stream)
@@ -309,6 +313,7 @@ def run_ours(args):
             tm = _abi.last_timing(device)
             kernel_ms.append(tm.ms_solve_kernel)
             tensor_flops.append(tm.tensor_flops)
+            parked.append(tm.fista_parked)
             iters.append(res.total_iterations)
             launches += tm.launches
         ev1.record(stream)
@@ -390,7 +395,7 @@ def run_ours(args):
     achieved = it_launch * flops_per_iter / (k_ms * 1e-3) / 1e12
     executed = statistics.median(tensor_flops) / (k_ms * 1e-3) / 1e12
     dmma_peak, dfma_peak = fp64_peak_tflops(device)
-    traffic = traffic_from_profile()
+    traffic = traffic_from_profile(V, statistics.median(parked))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -431,6 +436,9 @@ def run_ours(args):
                          "kernel_scope": "both passes of the two-pass schedule (to iteration 80, then the "
                                          "parked voxels slowest-first) and the bucket sort between them, "
                                          "timed together with CUDA events",
+                         "parked_voxels": statistics.median(parked),
+                         "traffic_basis": "ncu per-voxel and per-parked-voxel DRAM bytes of the two passes "
+                                          "(fista125k capture) x this run's voxel and parked counts",
                          "flops_per_launch": it_launch * flops_per_iter,
                          "flops_basis": "dense Gram form, executed voxel-iterations x (2K^2 + 8K)",
                          "executed_tensor_flops_per_launch": statistics.median(tensor_flops),
