@@ -304,7 +304,7 @@ def run_ours(args):
     barrier(world)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    kernel_ms, tensor_flops, launches, iters, parked = [], [], 0, [], []
+    kernel_ms, tensor_flops, launches, iters, parked, warps = [], [], 0, [], [], set()
     with ClockSampler(device) as clocks:
         torch.cuda.synchronize(device)
         ev0.record(stream)
@@ -314,6 +314,7 @@ def run_ours(args):
             kernel_ms.append(tm.ms_solve_kernel)
             tensor_flops.append(tm.tensor_flops)
             parked.append(tm.fista_parked)
+            warps.add(tm.fista_warps)
             iters.append(res.total_iterations)
             launches += tm.launches
         ev1.record(stream)
@@ -396,6 +397,8 @@ def run_ours(args):
     executed = statistics.median(tensor_flops) / (k_ms * 1e-3) / 1e12
     dmma_peak, dfma_peak = fp64_peak_tflops(device)
     traffic = traffic_from_profile(V, statistics.median(parked))
+    # warps per CTA the per-table autotuner chose (12 or 16)
+    fista_kernel = "k_fista_v3<9," + "/".join(str(w) for w in sorted(warps)) + ">"
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -407,7 +410,7 @@ def run_ours(args):
         mk_ms = statistics.median(mix_kernel_ms)
         paths = {
             "fp64": {"value": value, "unit": "voxels/s", "ms_per_step": ms / args.steps,
-                     "kernel": "k_fista_v3<9,16> (FP64 DMMA mma.sync.m8n8k4), two passes", "kernel_ms": statistics.median(kernel_ms),
+                     "kernel": f"{fista_kernel} (FP64 DMMA mma.sync.m8n8k4), two passes", "kernel_ms": statistics.median(kernel_ms),
                      "gpu_launches": launches},
             "mixed": {"value": value_mix, "unit": "voxels/s", "ms_per_step": ms_mix / args.steps,
                       "speedup_vs_fp64": value_mix / value,
@@ -432,7 +435,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": dmma_peak, "unit": "TFLOP/s",
                          "frac": (achieved / dmma_peak) if dmma_peak else None, "traffic": traffic,
-                         "kernel": "k_fista_v3<9,16>", "kernel_ms": k_ms,
+                         "kernel": fista_kernel, "kernel_ms": k_ms,
                          "kernel_scope": "both passes of the two-pass schedule (to iteration 80, then the "
                                          "parked voxels slowest-first) and the bucket sort between them, "
                                          "timed together with CUDA events",
