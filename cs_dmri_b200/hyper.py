@@ -165,16 +165,23 @@ def select_alpha_hypergradient(data, bvals, bvecs, mask, *, big_delta=None, smal
     sel = HypergradientAlpha(bvals, bvecs, big_delta=big_delta, small_delta=small_delta, b0_threshold=b0_threshold,
                              radial_order=radial_order, zeta=zeta, holdout_fraction=holdout_fraction, seed=seed,
                              device=device)
-    S = torch.from_numpy(np.ascontiguousarray(data[mask], dtype=np.float32)).to(sel.device)
+    rows = np.flatnonzero(mask.ravel())  # masked voxels in x-y-z order
+    S = torch.from_numpy(np.ascontiguousarray(np.take(data.reshape(-1, N), rows, axis=0), dtype=np.float32))
+    S = S.to(sel.device)
     alpha, loss, loss0, _ = sel.run(S, alpha0=alpha0, steps=steps)
     coef = sel.full.fit(S, alpha).detach()
     K = coef.shape[1]
-    vol = np.zeros((X, Y, Z, K), np.float32)
-    vol[mask] = coef.cpu().numpy().astype(np.float32)
-    out = {"alpha": np.zeros((X, Y, Z), np.float32), "heldout_loss": np.zeros((X, Y, Z), np.float32),
+    # the volumes are assembled on the device and copied back once each
+    idx = torch.from_numpy(rows).to(sel.device)
+
+    def volume(v: torch.Tensor, width: int) -> np.ndarray:
+        full = torch.zeros((X * Y * Z, width), dtype=torch.float32, device=sel.device)
+        full.index_copy_(0, idx, v.reshape(-1, width).to(torch.float32))
+        return full.cpu().numpy().reshape((X, Y, Z) + ((width,) if width > 1 else ()))
+
+    vol = volume(coef, K)
+    out = {"alpha": volume(alpha, 1), "heldout_loss": volume(loss, 1),
            "coefficients": vol, "train_samples": sel.train, "heldout_samples": sel.held_out}
-    out["alpha"][mask] = alpha.cpu().numpy()
-    out["heldout_loss"][mask] = loss.cpu().numpy()
     pk = _core.shore_odf_peaks(vol, radial_order, zeta, mask, npeaks=npeaks, device=device)
     out.update(gfa=pk["gfa"], peak_dirs=pk["peak_dirs"], peak_values=pk["peak_values"])
     micro = _core.shore_microstructure(vol, radial_order, zeta, mask, units="mm", outlier_factor=None,
