@@ -299,6 +299,7 @@ struct csd_handle {
   // bucket cursors]; a call uses slot sched_slot and entries from sched_base
   // on (the pipelined fit runs chunks concurrently, one slot each)
   DevBuf schedY, schedPend, schedKey, schedOrder, schedCnt;
+  DevBuf schedD, schedU, schedN;  // the mixed kernel's parked d and u rows and guard flags
   int sched_slot = 0;
   int64_t sched_base = 0;
   int sched_off = 0;  // > 0: single pass (an explicit order was given, or timing runs)
@@ -717,8 +718,52 @@ void launch_fista_mixed(csd_handle* h, const csd::FistaParams& p) {
   const int64_t tiles = (p.n_work + TILE - 1) / TILE;
   const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(h->num_sms, tiles)));
   CSD_CUDA(cudaEventRecord(h->ev[8], st));
-  csd::k_fista_i8<<<grid, THREADS, smem, st>>>(q);
-  CSD_LAUNCH();
+  if (!sched_enabled(h, p, static_cast<int64_t>(grid) * TILE)) {
+    csd::k_fista_i8<<<grid, THREADS, smem, st>>>(q);
+    CSD_LAUNCH();
+  } else {
+    // two passes, as launch_fista_v3_t: every voxel to the cap, the parked
+    // ones (x, d, u and the guard flag kept) resumed slowest-first
+    if (h->sched_slot < 0 || h->sched_slot >= kSchedSlots || h->sched_base < 0 || h->sched_base + p.n_work > p.V)
+      throw Error{CSD_ERR_INVALID, "two-pass FISTA schedule: slot or base out of range"};
+    ensure_sched(h, p.V);
+    h->schedD.ensure(sizeof(double) * static_cast<size_t>(p.V) * KC);
+    h->schedU.ensure(sizeof(double) * static_cast<size_t>(p.V) * KC);
+    h->schedN.ensure(static_cast<size_t>(p.V));
+    char* cnt = static_cast<char*>(h->schedCnt.p) + kSchedSlotBytes * h->sched_slot;
+    auto* n_pend = reinterpret_cast<unsigned long long*>(cnt);
+    auto* hist = reinterpret_cast<unsigned*>(cnt + 8);
+    unsigned* cursor = hist + csd::kSchedBins;
+    int64_t* pend = h->schedPend.as<int64_t>() + h->sched_base;
+    float* key = h->schedKey.as<float>() + h->sched_base;
+    int64_t* order = h->schedOrder.as<int64_t>() + h->sched_base;
+    CSD_CUDA(cudaMemsetAsync(cnt, 0, kSchedSlotBytes, st));
+    csd::MixedParams q1 = q;
+    q1.cap = sched_cap();
+    q1.Xp = h->schedY.as<double>();
+    q1.Dp = h->schedD.as<double>();
+    q1.Up = h->schedU.as<double>();
+    q1.Np = h->schedN.as<uint8_t>();
+    q1.pend = pend;
+    q1.pend_key = key;
+    q1.n_pend = n_pend;
+    csd::k_fista_i8<<<grid, THREADS, smem, st>>>(q1);
+    CSD_LAUNCH();
+    csd::k_sched_hist<<<h->num_sms, 256, 0, st>>>(key, n_pend, hist, p.iter_total ? p.iter_total + 2 : nullptr);
+    CSD_LAUNCH();
+    csd::k_sched_order<<<h->num_sms, csd::kSchedBins, 0, st>>>(pend, key, n_pend, hist, cursor, order);
+    CSD_LAUNCH();
+    CSD_CUDA(cudaMemsetAsync(p.queue, 0, sizeof(unsigned long long), st));
+    csd::MixedParams q2 = q1;
+    q2.resume = 1;
+    q2.warm = nullptr;
+    q2.list = order;
+    q2.n_work_dev = n_pend;
+    q2.pend = nullptr;
+    q2.pend_key = nullptr;
+    csd::k_fista_i8<<<grid, THREADS, smem, st>>>(q2);
+    CSD_LAUNCH();
+  }
   CSD_CUDA(cudaEventRecord(h->ev[9], st));
   unsigned long long hs[3] = {0, 0, 0};
   CSD_CUDA(cudaMemcpyAsync(hs, stat, sizeof hs, cudaMemcpyDeviceToHost, st));
@@ -1839,7 +1884,8 @@ void csd_destroy(csd_handle* h) {
                     &h->mixstat, &h->pcoef, &h->pmat, &h->pout, &h->pgt, &h->pgv, &h->pdir, &h->pconst,
                     &h->iota, &h->adjW, &h->adjovf, &h->adjstat, &h->adjconst,
                     &h->gdtab, &h->gdq, &h->tuneB, &h->tuneX, &h->tuneIt, &h->tuneConv, &h->tuneQ,
-                    &h->schedY, &h->schedPend, &h->schedKey, &h->schedOrder, &h->schedCnt};
+                    &h->schedY, &h->schedPend, &h->schedKey, &h->schedOrder, &h->schedCnt,
+                    &h->schedD, &h->schedU, &h->schedN};
   for (auto s : h->pipe)
     if (s) cudaStreamSynchronize(s);
   for (DevBuf* b : bufs) b->release();

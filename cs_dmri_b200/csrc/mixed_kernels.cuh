@@ -53,12 +53,13 @@ constexpr uint64_t kWaitNs = 2000000000ull;    // give up on one MMA batch after
 constexpr int RING = 16;                       // prefetched voxels per CTA
 constexpr int MOM_SMEM = 1024;                 // momentum factors held in shared memory
 constexpr int PRODUCER_WARP = 7;               // tops the prefetch ring up while the MMAs run
-// dynamic shared memory: A, B, u [KC][TILE], prefetch ring (b and warm rows),
+// dynamic shared memory: A, B, u [KC][TILE], prefetch ring (b and warm rows;
+// u, x and d rows of resumed voxels),
 // momentum table, column exponents, per-voxel state
-constexpr size_t kSmem = A_BYTES + B_BYTES + sizeof(double) * KC * TILE + sizeof(double) * 2 * RING * KC +
+constexpr size_t kSmem = A_BYTES + B_BYTES + sizeof(double) * KC * TILE + sizeof(double) * 3 * RING * KC +
                          sizeof(double) * MOM_SMEM + sizeof(double) * RING + sizeof(int64_t) * RING +
                          sizeof(int) * NB + sizeof(double) * 5 * TILE + sizeof(int64_t) * 2 * TILE +
-                         sizeof(unsigned) * 2 * TILE + sizeof(int) * 4 * TILE;
+                         sizeof(unsigned) * 2 * TILE + sizeof(int) * 5 * TILE + sizeof(int) * RING;
 
 // Byte offset of digit plane s, coefficient j of voxel row r in the A operand
 // (canonical K-major, no swizzle: 8 rows x 16 bytes per core matrix).
@@ -129,6 +130,24 @@ struct MixedParams {
   unsigned long long* n_flagged;
   unsigned long long* batches; // MMA batches issued (36 MMAs each), summed
   int* error;                  // set to 1 when a tensor-core wait gives up
+  // Two-pass schedule (as FistaParams).  Pass 1 (cap > 0, resume = 0): a
+  // voxel neither finished nor flagged after `cap` iterations stores its
+  // exact state - x, d and u rows in Xp, Dp, Up and its guard-band flag in
+  // Np - appends its position to `pend` with a prediction of the iterations
+  // it still needs in `pend_key`, and frees its slot; its X row stays
+  // untouched (a flagged voxel's FP64 re-run starts from the original
+  // point).  Pass 2 (resume = 1) takes those voxels (the order of `list`,
+  // `*n_work_dev` of them) from that state at iteration `cap`.
+  int cap;
+  int resume;
+  double* Xp;
+  double* Dp;
+  double* Up;
+  uint8_t* Np;
+  int64_t* pend;
+  float* pend_key;
+  unsigned long long* n_pend;
+  const unsigned long long* n_work_dev;
 };
 
 namespace i8 {
@@ -233,7 +252,8 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
   double* sU = reinterpret_cast<double*>(sB + B_BYTES);          // [KC][TILE]
   double* rB = sU + KC * TILE;                                   // [RING][KC] prefetched b rows
   double* rW = rB + RING * KC;                                   // [RING][KC] prefetched warm rows
-  double* sMom = rW + RING * KC;                                 // [MOM_SMEM]
+  double* rD = rW + RING * KC;                                   // [RING][KC] d rows of resumed voxels
+  double* sMom = rD + RING * KC;                                 // [MOM_SMEM]
   double* rThr = sMom + MOM_SMEM;                                // [RING]
   int64_t* rVid = reinterpret_cast<int64_t*>(rThr + RING);       // [RING]
   int* sF = reinterpret_cast<int*>(rVid + RING);                 // [NB]
@@ -247,6 +267,8 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
   int* sNear = sIt + TILE;                                       // [TILE]
   int* sFin = sNear + TILE;                                      // [TILE] 1: slot emptied this pass
   int* sSrc = sFin + TILE;                                       // [TILE] ring entry of a new voxel, -1: direct
+  int* sPark = sSrc + TILE;                                      // [TILE] 1: the emptied slot's voxel is parked
+  int* rNear = sPark + TILE;                                     // [RING] guard flag of a resumed voxel
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_slot;
   __shared__ int s_abort, s_head, s_tail, s_exhausted;
@@ -270,6 +292,7 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
     sNear[tid] = 0;
     sFin[tid] = 0;
     sSrc[tid] = -1;
+    sPark[tid] = 0;
     sThr[tid] = p.thr;
   }
   if (warp == 0) {
@@ -304,6 +327,12 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
   // square-root form can only matter inside the band, where the FP64 kernel
   // decides anyway.
   const double tol2 = tol * tol, lo2 = lo_band * lo_band, hi2 = hi_band * hi_band;
+  const unsigned long long nwork =
+      p.n_work_dev ? *p.n_work_dev : static_cast<unsigned long long>(p.n_work);  // work-list length
+  // pass 1 of the two-pass schedule: sums of log2(rel^2) and k log2(rel^2)
+  // over iterations w0+1 .. cap of this thread's slot (part-0 threads)
+  const int w0 = p.cap - p.cap / 2;
+  float ksl = 0.f, kskl = 0.f;
 
   while (true) {
     const int64_t vid = sVid[r];
@@ -356,7 +385,7 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
     // ---- stopping rule, guard and refill decision (one thread per voxel)
     if (part == 0) {
       const int64_t v = sVid[r];
-      bool finish = false, write_out = true;
+      bool finish = false, write_out = true, park = false;
       if (have_p && v >= 0) {
         ++executed;
         const int it = sIt[r] + 1;
@@ -386,9 +415,31 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
           finish = true;
           write_out = false;
         }
+        if (p.cap > 0 && !p.resume && !finish) {
+          if (it > w0) {
+            const float l2 = log2f(fmaxf(static_cast<float>(dx2 / ref2), 1e-37f));
+            ksl += l2;
+            kskl = fmaf(static_cast<float>(it - w0), l2, kskl);
+          }
+          if (it == p.cap) {
+            // park: remaining iterations predicted by the least-squares line
+            // through log2(rel^2) over the window, extended to log2(tol^2)
+            const float n = static_cast<float>(p.cap - w0), km = 0.5f * (n + 1.f);
+            const float slope = (kskl - km * ksl) / (n * (n * n - 1.f) / 12.f);
+            const float lc = ksl / n + slope * (n - km);
+            const float rem = slope < 0.f ? (2.f * log2f(static_cast<float>(tol)) - lc) / slope : 65536.f;
+            const unsigned long long k = atomicAdd(p.n_pend, 1ull);
+            p.pend[k] = v;
+            p.pend_key[k] = fminf(fmaxf(rem, 1.f), 65536.f) * (1.f / 65536.f);
+            p.Np[v] = static_cast<uint8_t>(sNear[r]);
+            finish = true;
+            park = true;
+          }
+        }
       }
       sFin[r] = finish ? 1 : 0;
-      sOld[r] = (finish && write_out) ? v : -1;
+      sPark[r] = park ? 1 : 0;
+      sOld[r] = (finish && (write_out || park)) ? v : -1;
       // refill: the next prefetched voxel, else straight from the work queue
       const bool need = finish || v < 0;
       const unsigned m = __ballot_sync(0xffffffffu, need);
@@ -408,7 +459,7 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
             thr = rThr[src];
           } else if (!*reinterpret_cast<volatile int*>(&s_exhausted)) {
             const unsigned long long k = atomicAdd(p.queue, 1ull);
-            if (k < static_cast<unsigned long long>(p.n_work)) {
+            if (k < nwork) {
               nv = p.list ? p.list[k] : static_cast<int64_t>(k);
               if (p.alpha_v) thr = p.step * p.alpha_v[nv];
             } else {
@@ -417,9 +468,10 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
           }
           sVid[r] = nv;
           sSrc[r] = src;
-          sIt[r] = 0;
-          sNear[r] = 0;
+          sIt[r] = p.resume ? p.cap : 0;
+          sNear[r] = (p.resume && nv >= 0) ? (src >= 0 ? rNear[src] : static_cast<int>(p.Np[nv])) : 0;
           sThr[r] = thr;
+          ksl = kskl = 0.f;
         }
       }
     }
@@ -430,8 +482,18 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
     {
       if (sFin[r] && sOld[r] >= 0) {
         const int64_t ov = sOld[r];
+        if (sPark[r]) {
 #pragma unroll
-        for (int i = 0; i < CPT; ++i) p.X[ov * KC + coef_of(part, i)] = x[i];
+          for (int i = 0; i < CPT; ++i) {
+            const int j = coef_of(part, i);
+            p.Xp[ov * KC + j] = x[i];
+            p.Dp[ov * KC + j] = d[i];
+            p.Up[ov * KC + j] = sU[j * TILE + r];
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < CPT; ++i) p.X[ov * KC + coef_of(part, i)] = x[i];
+        }
       }
       const int64_t nv = sVid[r];
       const bool fresh = nv >= 0 && (sFin[r] || vid < 0);
@@ -445,7 +507,27 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
           d[i] = __longlong_as_double(0ll);
         }
       }
-      if (fresh) {
+      if (fresh && p.resume) {
+        // a parked voxel: its x, d and u rows as pass 1 left them
+        const int src = sSrc[r];
+        if (src >= 0) {
+#pragma unroll
+          for (int i = 0; i < CPT; ++i) {
+            const int j = coef_of(part, i);
+            sU[j * TILE + r] = rB[src * KC + j];
+            x[i] = rW[src * KC + j];
+            d[i] = rD[src * KC + j];
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < CPT; ++i) {
+            const int j = coef_of(part, i);
+            sU[j * TILE + r] = p.Up[nv * KC + j];
+            x[i] = p.Xp[nv * KC + j];
+            d[i] = p.Dp[nv * KC + j];
+          }
+        }
+      } else if (fresh) {
         // u = -b for the new voxel.  A warm start x_0 enters as d = x_0, so the
         // first product gives u_0 = G x_0 - b and the first update sees y_0 = x_0.
         const int src = sSrc[r];
@@ -538,16 +620,25 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(p.queue, static_cast<unsigned long long>(space));
         base = __shfl_sync(0xffffffffu, base, 0);
-        const unsigned long long nw = static_cast<unsigned long long>(p.n_work);
+        const unsigned long long nw = nwork;
         const int ok = base >= nw ? 0 : static_cast<int>(min(static_cast<unsigned long long>(space), nw - base));
         if (lane < ok) {
           const int e = (tail + lane) % RING;
           const int64_t nv = p.list ? p.list[base + lane] : static_cast<int64_t>(base + lane);
           rVid[e] = nv;
           rThr[e] = p.alpha_v ? p.step * p.alpha_v[nv] : p.thr;
-          for (int c = 0; c < KC / 2; ++c) {
-            cp_async16(rB + e * KC + 2 * c, p.B + nv * KC + 2 * c);
-            if (p.warm) cp_async16(rW + e * KC + 2 * c, p.warm + nv * KC + 2 * c);
+          if (p.resume) {
+            rNear[e] = static_cast<int>(p.Np[nv]);
+            for (int c = 0; c < KC / 2; ++c) {
+              cp_async16(rB + e * KC + 2 * c, p.Up + nv * KC + 2 * c);
+              cp_async16(rW + e * KC + 2 * c, p.Xp + nv * KC + 2 * c);
+              cp_async16(rD + e * KC + 2 * c, p.Dp + nv * KC + 2 * c);
+            }
+          } else {
+            for (int c = 0; c < KC / 2; ++c) {
+              cp_async16(rB + e * KC + 2 * c, p.B + nv * KC + 2 * c);
+              if (p.warm) cp_async16(rW + e * KC + 2 * c, p.warm + nv * KC + 2 * c);
+            }
           }
         }
         cp_async_commit();

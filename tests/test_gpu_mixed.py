@@ -130,3 +130,27 @@ def test_mixed_larger_volume_against_fp64_gpu():
     assert glob <= 1e-6, glob
     assert per.max() <= 1e-5, per.max()
     assert np.percentile(per, 99) <= 1e-6
+
+
+def test_two_pass_schedule_changes_nothing_in_the_mixed_path(monkeypatch):
+    """The mixed kernel's two-pass schedule parks a voxel's x, d, u rows and
+    guard flag at iteration 80 and resumes them slowest-first: coefficients,
+    iteration counts, convergence flags and the voxels re-run in FP64 are
+    those of a single pass (CSD_FISTA_SCHEDULE=0)."""
+    from cs_dmri_b200 import _abi, shore_fit
+    from cs_dmri_b200.phantom import make_phantom
+    ph = make_phantom((64, 64, 50), seed=31)  # 204,800 voxels: two passes
+    V = int(ph.mask.sum())
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, alpha_mode="fixed", alpha=0.01,
+              precision="mixed", return_coef64=True, diagnostics=True)
+    two = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, **kw)
+    t2 = _abi.last_timing(0)
+    assert 0.5 * V < t2.fista_parked <= V
+    monkeypatch.setenv("CSD_FISTA_SCHEDULE", "0")
+    one = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, **kw)
+    t1 = _abi.last_timing(0)
+    assert t1.fista_parked == 0
+    assert t1.fp64_rerun_voxels == t2.fp64_rerun_voxels
+    for k in ("coef64", "coefficients", "iterations", "converged"):
+        np.testing.assert_array_equal(two[k], one[k])
+    assert two["total_iterations"] == one["total_iterations"]
