@@ -414,7 +414,7 @@ def run_ours(args):
                      "gpu_launches": launches},
             "mixed": {"value": value_mix, "unit": "voxels/s", "ms_per_step": ms_mix / args.steps,
                       "speedup_vs_fp64": value_mix / value,
-                      "kernel": "k_fista_i8 (tcgen05.mma kind::i8, 36 MMAs 128x80x32 per iteration)",
+                      "kernel": "k_fista_i8 (tcgen05.mma kind::i8, 36 MMAs 128x80x32 per iteration), two passes",
                       "kernel_ms": mk_ms, "int8_tensor_ops_per_launch": statistics.median(mix_ops),
                       "executed_int8_tops": statistics.median(mix_ops) / (mk_ms * 1e-3) / 1e12 if mk_ms else None,
                       "fp64_rerun_voxels": statistics.median(mix_rerun),
