@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--profile-case", choices=["graddev2k", "diff50k", "peaks108k", "fista125k", "kkt64k"],
+                    help="run one small profiling workload instead of the benchmark")
     ap.add_argument("--workload", choices=["brain300k", "grid64k"], default="brain300k",
                     help="brain300k: the benchmark volume; grid64k: 40^3 fully masked (profiling case)")
     return ap.parse_args()
@@ -412,6 +414,8 @@ def run_ours(args):
     h2d = V * N * 4 + ph.mask.nbytes
     d2h = out["coefficients"].nbytes
 
+    # ---- the converged-optimum paths on the same volume
+    optimum = optimum_block(args, ph, d_data, d_mask, stream, device, world, ms / args.steps)
     # ---- fwd+bwd: differentiable fit of 50k voxels
     fwd_bwd = fwd_bwd_block(args, device, world)
     # ---- per-voxel designs (gradient deviation, dropped samples)
@@ -483,6 +487,7 @@ def run_ours(args):
             "graddev": graddev,
             "pipeline": pipeline,
             "paths": paths,
+            "optimum": optimum,
             "clocks": clocks.summary(),
             "iterations_per_voxel": it_launch / V,
         }
@@ -493,6 +498,102 @@ def run_ours(args):
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def timed_fits(args, fit, stream, device, world):
+    """Device ms per fit over args.steps fits after args.warmup untimed ones
+    (CUDA events on the fit stream, max over ranks), with the clock samples."""
+    import torch
+
+    for _ in range(args.warmup):
+        fit()
+    torch.cuda.synchronize(device)
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clocks:
+        torch.cuda.synchronize(device)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fit()
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+    return max_over_ranks(e0.elapsed_time(e1) / args.steps, world, torch.device("cuda", device)), clocks.summary()
+
+
+def optimum_block(args, ph, d_data, d_mask, stream, device: int, world: int, fp64_ms: float) -> dict:
+    """The LASSO optimum itself (precision "mixed-kkt": TF32 tensor-core FISTA
+    iterations find the support, an FP64 active-set polish solves on it and
+    certifies every voxel by its KKT conditions) against three FP64 GPU
+    references on the same volume:
+      fp64       the reference stopping rule (tol 1e-6) - the parity path,
+                 whose output is not the optimum;
+      fp64-kkt   the same support identification with FP64 iterations;
+      fp64-tight the reference FISTA with tol 1e-9 and max_iter 20000, the
+                 plain FP64 path run far enough to approach the optimum.
+    Errors are per-voxel relative L2 against the certified optimum, whole
+    volume; KKT residuals in the form of the reference's
+    tests/common/mod.rs:127-153."""
+    import torch
+
+    from cs_dmri_b200 import _abi, shore_fit, shore_fit_device
+
+    V = int(ph.mask.sum())
+    base = dict(fit_kwargs(), big_delta=ph.big_delta, small_delta=ph.small_delta, device=device)
+    tight = dict(base, tol=1e-9, max_iter=20000)
+
+    def dev(precision, kw):
+        return lambda: shore_fit_device(d_data, d_mask, ph.bvals, ph.bvecs, stream=stream, precision=precision,
+                                        **kw)
+
+    out = {"metric": "converged-optimum L1-fit voxels/s", "unit": "voxels/s", "workload": f"{WORKLOAD}: {V} voxels",
+           "certificate": "every off-support |M_j^T (M c - s)| / n <= alpha (1 + 1e-9), signs consistent on the "
+                          "support"}
+    ms_kkt, clk = timed_fits(args, dev("mixed-kkt", base), stream, device, world)
+    t = _abi.last_timing(device)
+    out["mixed_kkt"] = {"value": world * V / (ms_kkt * 1e-3), "ms_per_step": ms_kkt,
+                        "speedup_vs_fp64_reference_rule": fp64_ms / ms_kkt,
+                        "ms_iterate": t.ms_kkt_iterate, "ms_polish": t.ms_kkt_polish,
+                        "ms_fallback": t.ms_kkt_fallback, "ms_rhs": t.ms_rhs,
+                        "fallback_voxels": t.kkt_fallback_voxels, "uncertified_voxels": t.kkt_uncertified,
+                        "polish_rounds_per_voxel": t.kkt_rounds / V, "kkt_max": t.kkt_max,
+                        "tf32_tensor_tflops_executed": t.tf32_tensor_flops / (t.ms_kkt_iterate * 1e-3) / 1e12
+                        if t.ms_kkt_iterate else None,
+                        "kernels": "k_fista_tf32 (tcgen05.mma kind::tf32, 128 voxels x 80 x 72 per iteration), "
+                                   "k_l1_polish (FP64, warp per voxel)",
+                        "clocks": clk}
+    ms_f, clk = timed_fits(args, dev("fp64-kkt", base), stream, device, world)
+    t = _abi.last_timing(device)
+    out["fp64_kkt"] = {"value": world * V / (ms_f * 1e-3), "ms_per_step": ms_f, "ms_iterate": t.ms_kkt_iterate,
+                       "ms_polish": t.ms_kkt_polish, "uncertified_voxels": t.kkt_uncertified, "clocks": clk}
+    targs = argparse.Namespace(warmup=1, steps=max(1, min(args.steps, 3)))
+    ms_t, clk = timed_fits(targs, dev("fp64", tight), stream, device, world)
+    out["fp64_tight"] = {"value": world * V / (ms_t * 1e-3), "ms_per_step": ms_t, "tol": 1e-9, "max_iter": 20000,
+                         "steps": targs.steps, "clocks": clk}
+    out["mixed_kkt"]["speedup_vs_fp64_kkt"] = ms_f / ms_kkt
+    out["mixed_kkt"]["speedup_vs_fp64_tight"] = ms_t / ms_kkt
+
+    # errors against the certified optimum, whole volume (FP64 outputs)
+    common = dict(return_coef64=True, diagnostics=True)
+    opt = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, precision="mixed-kkt", **common, **base)
+    ok = opt["converged"]
+    c_opt = opt["coef64"]
+    nrm = np.linalg.norm(c_opt, axis=1)
+    sel = ok & (nrm > 0)
+
+    def errs(c):
+        r = np.linalg.norm(c[sel] - c_opt[sel], axis=1) / nrm[sel]
+        return {"median": float(np.median(r)), "p99": float(np.percentile(r, 99)), "max": float(r.max()),
+                "frac_above_1e-5": float(np.mean(r > 1e-5))}
+
+    out["certified_fraction"] = float(ok.mean())
+    out["fp64"] = {"value": world * V / (fp64_ms * 1e-3), "ms_per_step": fp64_ms,
+                   "note": "the FP64 path of paths.fp64 (reference stopping rule)"}
+    for name, kw, prec in (("fp64_kkt", base, "fp64-kkt"), ("fp64", base, "fp64"), ("fp64_tight", tight, "fp64")):
+        res = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, precision=prec, **common, **kw)
+        out[name]["coef_rel_err_vs_optimum"] = errs(res["coef64"])
+        del res
+    del opt, c_opt
+    return out
 
 
 def fwd_bwd_block(args, device: int, world: int) -> dict:
@@ -619,8 +720,102 @@ def pipeline_block(ph, device: int, world: int) -> dict:
             "alpha_median": float(np.median(out["alpha"][ph.mask]))}
 
 
+# ------------------------------------------------------------------ profiling cases
+#
+# Small, fixed workloads that run one pass of a kernel family, for profiling
+# under ncu (a few launches of each kernel of interest, a few hundred MB on
+# the device at most): python bench.py --profile-case NAME.
+
+def case_graddev2k() -> None:
+    import torch
+
+    from cs_dmri_b200.graddev import graddev_phantom, shore_fit_graddev
+    S, bvals, bvecs, T, keep, big, small = graddev_phantom(2000, seed=3)
+    out = shore_fit_graddev(S, bvals, bvecs, T, keep, alpha=0.01, radial_order=8, big_delta=big, small_delta=small)
+    torch.cuda.synchronize()
+    print("graddev2k: mean iterations", float(out["iterations"].double().mean()))
+
+
+def case_diff50k() -> None:
+    import torch
+
+    from cs_dmri_b200.autograd import DifferentiableShore
+    from cs_dmri_b200.phantom import make_phantom
+    ph = make_phantom((50, 50, 20), seed=4)
+    S = torch.from_numpy(ph.data.reshape(-1, ph.data.shape[-1])).cuda().requires_grad_(True)
+    m = DifferentiableShore(ph.bvals, ph.bvecs, big_delta=ph.big_delta, small_delta=ph.small_delta)
+    a = torch.tensor(0.01, dtype=torch.float64, device="cuda", requires_grad=True)
+    c = m.fit(S, a)
+    (m.rtop(c).sum() + 1e-3 * m.odf(c).square().sum()).backward()
+    torch.cuda.synchronize()
+    print("diff50k: d loss / d alpha", float(a.grad))
+
+
+def case_peaks108k() -> None:
+    from cs_dmri_b200._core import shore_odf_peaks
+    rng = np.random.default_rng(1)
+    vol = rng.normal(size=(60, 60, 30, 72)).astype(np.float32)
+    vol[..., 0] = np.abs(vol[..., 0]) + 5.0
+    out = shore_odf_peaks(vol, 6, 700.0)
+    print("peaks108k: mean GFA", float(out["gfa"].mean()))
+
+
+def case_fista125k() -> None:
+    """A fixed-alpha fit of a 50^3 phantom (125,000 voxels, K = 72) through the
+    device entry point: enough voxels per FISTA slot for the two-pass
+    schedule (pass 1 to iteration 80, bucket sort, pass 2).  A first fit
+    (gradient-table set-up, autotuning) runs outside the NVTX range."""
+    import torch
+
+    from cs_dmri_b200 import _abi
+    from cs_dmri_b200._core import shore_fit_device
+    from cs_dmri_b200.phantom import make_phantom
+    ph = make_phantom((50, 50, 50), seed=6)
+    d = torch.from_numpy(ph.data).cuda()
+    m = torch.from_numpy(ph.mask).cuda()
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, alpha_mode="fixed", alpha=0.01)
+    shore_fit_device(d, m, ph.bvals, ph.bvecs, **kw)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("fista125k")
+    shore_fit_device(d, m, ph.bvals, ph.bvecs, **kw)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    t = _abi.last_timing(0)
+    print(f"fista125k: solve {t.ms_solve_kernel:.3f} ms, parked {t.fista_parked} of {int(ph.mask.sum())} voxels")
+
+
+def case_kkt64k() -> None:
+    """The converged-optimum fit (precision "mixed-kkt") of the 40^3 phantom
+    (64,000 voxels, K = 72) through the device entry point: one launch each of
+    k_fista_tf32 and k_l1_polish per fit.  A first fit (set-up) runs before
+    the measured one."""
+    import torch
+
+    from cs_dmri_b200 import _abi
+    from cs_dmri_b200._core import shore_fit_device
+    from cs_dmri_b200.phantom import config_phantom
+    ph = config_phantom("grid64k")
+    d = torch.from_numpy(ph.data).cuda()
+    m = torch.from_numpy(ph.mask).cuda()
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, alpha_mode="fixed", alpha=0.01,
+              precision="mixed-kkt")
+    shore_fit_device(d, m, ph.bvals, ph.bvecs, **kw)
+    shore_fit_device(d, m, ph.bvals, ph.bvecs, **kw)
+    torch.cuda.synchronize()
+    t = _abi.last_timing(0)
+    print(f"kkt64k: iterate {t.ms_kkt_iterate:.3f} ms, polish {t.ms_kkt_polish:.3f} ms, "
+          f"fallback voxels {t.kkt_fallback_voxels}, uncertified {t.kkt_uncertified}")
+
+
+PROFILE_CASES = {"graddev2k": case_graddev2k, "diff50k": case_diff50k, "peaks108k": case_peaks108k,
+                 "fista125k": case_fista125k, "kkt64k": case_kkt64k}
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        PROFILE_CASES[args.profile_case]()
+        return 0
     select_workload(args.workload)
     if args.impl == "reference":
         return run_reference(args)

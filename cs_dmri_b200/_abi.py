@@ -16,7 +16,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libcsdshore.so"
 OK, ERR_INVALID, ERR_FIT_REFUSED, ERR_NUMERICAL, ERR_CUDA, ERR_TIMEOUT = range(6)
 REG_L1, REG_L2, REG_NONNEG = 1, 2, 3
 ALPHA_FIXED, ALPHA_RATIO, ALPHA_PATH_BIC, ALPHA_L2_ANCHORED = range(4)
-PRECISION_FP64, PRECISION_MIXED = 0, 1
+PRECISION_FP64, PRECISION_MIXED, PRECISION_MIXED_KKT, PRECISION_FP64_KKT = 0, 1, 2, 3
 
 
 class Gtab(C.Structure):
@@ -102,7 +102,23 @@ class Timing(C.Structure):
         ("fista_tune_ms12", C.c_float),
         ("fista_tune_ms16", C.c_float),
         ("fista_parked", C.c_int64),
+        ("ms_kkt_iterate", C.c_float),
+        ("ms_kkt_polish", C.c_float),
+        ("ms_kkt_fallback", C.c_float),
+        ("kkt_fallback_voxels", C.c_int64),
+        ("kkt_uncertified", C.c_int64),
+        ("kkt_rounds", C.c_uint64),
+        ("tf32_tensor_flops", C.c_double),
+        ("kkt_max", C.c_double),
     ]
+
+
+# csd_set_option options
+OPT_FISTA_SHAPE = 1
+OPT_FISTA_SCHEDULE = 2
+OPT_KKT_ITERATIONS = 3
+OPT_TENSOR_WAIT_NS = 4
+OPT_KKT_ROUNDS = 5
 
 
 # Every symbol include/csd_shore.h declares, for load checks.
@@ -117,6 +133,7 @@ EXPORTS = (
     "csd_shore_fit_volume_device",
     "csd_shore_design_matrix",
     "csd_last_timing",
+    "csd_set_option",
     "csd_shore_fista_batch_noalloc",
     "csd_shore_predict",
     "csd_shore_odf_sh",
@@ -160,6 +177,8 @@ def _declare(lib: C.CDLL) -> C.CDLL:
                                             C.c_void_p, C.c_char_p, C.c_size_t]
     lib.csd_last_timing.restype = C.c_int
     lib.csd_last_timing.argtypes = [C.c_void_p, C.POINTER(Timing)]
+    lib.csd_set_option.restype = C.c_int
+    lib.csd_set_option.argtypes = [C.c_void_p, C.c_int32, C.c_int64]
     lib.csd_shore_fista_batch_noalloc.restype = C.c_int
     lib.csd_shore_fista_batch_noalloc.argtypes = [C.POINTER(Gtab), C.POINTER(Spec), C.c_void_p, C.c_int64,
                                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]
@@ -249,6 +268,12 @@ def default_spec() -> Spec:
     s = Spec()
     load().csd_default_spec(C.byref(s))
     return s
+
+
+def set_option(option: int, value: int, device: int = 0) -> None:
+    """Set a tuning option of the device's shared handle (csd_set_option)."""
+    if load().csd_set_option(handle(device), int(option), int(value)) != OK:
+        raise ValueError(f"invalid option {option} or value {value}")
 
 
 def last_timing(device: int = 0) -> Timing:

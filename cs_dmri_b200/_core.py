@@ -22,7 +22,8 @@ from . import _abi
 TORTOISE_DEFAULT_GMAX = 80e-3  # src/qspace.rs:262
 
 _REGS = {"l1": _abi.REG_L1, "l2": _abi.REG_L2, "nonneg": _abi.REG_NONNEG}
-_PRECISIONS = {"fp64": _abi.PRECISION_FP64, "mixed": _abi.PRECISION_MIXED}
+_PRECISIONS = {"fp64": _abi.PRECISION_FP64, "mixed": _abi.PRECISION_MIXED,
+               "mixed-kkt": _abi.PRECISION_MIXED_KKT, "fp64-kkt": _abi.PRECISION_FP64_KKT}
 _MODES = {"fixed": _abi.ALPHA_FIXED, "alpha-ratio": _abi.ALPHA_RATIO,
           "path-bic": _abi.ALPHA_PATH_BIC, "l2-anchored": _abi.ALPHA_L2_ANCHORED}
 
@@ -72,7 +73,7 @@ def build_spec(*, radial_order=6, zeta=700.0, regularization="l1", alpha_mode="l
     s.diagnostics = int(bool(diagnostics))
     s.allow_single_shell = int(bool(allow_single_shell))
     if precision not in _PRECISIONS:
-        raise ValueError(f"precision must be fp64 or mixed, got {precision!r}")
+        raise ValueError(f"precision must be fp64, mixed, mixed-kkt or fp64-kkt, got {precision!r}")
     s.precision = _PRECISIONS[precision]
     return s
 
@@ -168,6 +169,11 @@ def shore_fit(data, bvals, bvecs, mask, *, big_delta=None, small_delta=None, b0_
     read in place, masked voxels only.  ``precision="mixed"`` (radial order 6)
     runs the L1 iterations with int8 digit-slice tensor-core Gram products and
     FP64 state; the default ``"fp64"`` is the reference arithmetic.
+    ``"mixed-kkt"`` and ``"fp64-kkt"`` (fixed alpha or alpha ratio, radial
+    order <= 6) return the KKT-certified LASSO optimum instead of the
+    reference's early-stopped iterate: support identification by TF32
+    tensor-core (or FP64) FISTA iterations, then an FP64 active-set polish;
+    ``converged`` is the certificate.
     """
     if bvec_frame not in ("image-axis", "world-ras"):
         raise ValueError(f"bvec_frame must be 'image-axis' or 'world-ras', got {bvec_frame!r}")

@@ -39,6 +39,7 @@
 #include "solve_kernels.cuh"
 #include "icls_kernels.cuh"
 #include "mixed_kernels.cuh"
+#include "tf32_kernels.cuh"
 #include "epilogue_kernels.cuh"
 #include "adjoint_kernels.cuh"
 #include "odf_kernels.cuh"
@@ -311,6 +312,23 @@ struct csd_handle {
   DevBuf tuneB, tuneX, tuneIt, tuneConv, tuneQ;
   double mixed_ms = 0.0, mixed_ops = 0.0;
   unsigned long long mixed_rerun = 0;
+  // converged-optimum modes: the TF32 B operand (per table), the iterate,
+  // per-voxel KKT residuals, overflow / failure lists, counters
+  // [batches, error, n_overflow, n_failed, rounds, kkt max bits, n_failed2]
+  DevBuf gtf32, x32, kktv, kktovf, kktfail, kktstat;
+  uint64_t gtf32_key = 0;
+  bool gtf32_valid = false;
+  cudaEvent_t kev[5] = {};
+  // tuning options (csd_set_option); -1 / 0 = default
+  int opt_shape = 0;
+  int opt_schedule = -1;
+  int opt_kkt_iters = 64;
+  int opt_kkt_rounds = 48;
+  unsigned long long opt_wait_ns = 2000000000ull;  // tensor-core completion waits
+  unsigned long long kkt_batches = 0, kkt_fallback = 0, kkt_rounds = 0, kkt_uncertified = 0, kkt_iter_add = 0;
+  double kkt_max = 0.0;
+  float kkt_ms[3] = {0.f, 0.f, 0.f};  // iterate, first polish, fallback (FISTA + last polish)
+  float kkt_ms_last_polish = 0.f;
 };
 
 namespace {
@@ -568,15 +586,14 @@ void launch_fista_t(csd_handle* h, const csd::FistaParams& p) {
 // Two-pass schedule: a fit is split at iteration sched_cap() when it has at
 // least kSchedMinWaves voxels per FISTA slot (fewer: the slowest voxels start
 // in the first wave anyway) and max_iter is above twice the cap.  The slot
-// count of the call's grid sets the scale.  CSD_FISTA_SCHEDULE=0 turns it
-// off; a value of 2 or more sets the cap.
+// count of the call's grid sets the scale.  The handle option
+// CSD_OPT_FISTA_SCHEDULE turns it off (0) or sets the cap (>= 2).
 constexpr int kSchedCap = 80;
 
-int sched_cap() {
-  const char* e = std::getenv("CSD_FISTA_SCHEDULE");
-  if (!e || !*e) return kSchedCap;
-  const int c = std::atoi(e);
-  return c == 0 ? 0 : std::max(c, 2);
+int sched_cap(const csd_handle* h) {
+  const int o = h->opt_schedule;
+  if (o < 0 || o == 1) return kSchedCap;
+  return o == 0 ? 0 : o;
 }
 constexpr int64_t kSchedMinWaves = 4;
 constexpr size_t kSchedSlotBytes = 4096;  // count (8 B), bucket counts, bucket cursors
@@ -592,7 +609,7 @@ struct SchedOff {
 };
 
 bool sched_enabled(const csd_handle* h, const csd::FistaParams& p, int64_t slots) {
-  const int cap = sched_cap();
+  const int cap = sched_cap(h);
   if (cap == 0 || h->sched_off > 0 || p.cap != 0 || p.n_work_dev || p.max_iter <= 2 * cap) return false;
   return p.n_work >= kSchedMinWaves * slots;
 }
@@ -642,7 +659,7 @@ void launch_fista_v3_t(csd_handle* h, const csd::FistaParams& p) {
   int64_t* order = h->schedOrder.as<int64_t>() + h->sched_base;
   CSD_CUDA(cudaMemsetAsync(cnt, 0, kSchedSlotBytes, st));
   csd::FistaParams q1 = q;
-  q1.cap = sched_cap();
+  q1.cap = sched_cap(h);
   q1.resume = 0;
   q1.Y = h->schedY.as<double>();
   q1.pend = pend;
@@ -668,10 +685,13 @@ void launch_fista_v3_t(csd_handle* h, const csd::FistaParams& p) {
 
 // FISTA kernel variant: 0 = k_fista_fp64 (registers hold x, y, b); 3 / 4 =
 // k_fista_v3 with 12 / 16 warps per CTA, chosen per gradient table by
-// autotune_fista.  CSD_FISTA_VARIANT overrides the choice.
+// autotune_fista.  The handle option CSD_OPT_FISTA_SHAPE overrides the choice.
 int fista_variant(const csd_handle* h) {
-  const char* e = std::getenv("CSD_FISTA_VARIANT");
-  if (e && *e) return std::atoi(e);
+  if (h) {
+    if (h->opt_shape == 1) return 0;
+    if (h->opt_shape == 12) return 3;
+    if (h->opt_shape == 16) return 4;
+  }
   return (h && h->fista_warps == 12) ? 3 : 4;
 }
 
@@ -712,6 +732,7 @@ void launch_fista_mixed(csd_handle* h, const csd::FistaParams& p) {
   q.n_flagged = stat;
   q.batches = stat + 1;
   q.error = reinterpret_cast<int*>(stat + 2);
+  q.wait_ns = h->opt_wait_ns;
   const size_t smem = csd::kMixedSmem;
   CSD_CUDA(cudaFuncSetAttribute(csd::k_fista_i8, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem)));
@@ -739,7 +760,7 @@ void launch_fista_mixed(csd_handle* h, const csd::FistaParams& p) {
     int64_t* order = h->schedOrder.as<int64_t>() + h->sched_base;
     CSD_CUDA(cudaMemsetAsync(cnt, 0, kSchedSlotBytes, st));
     csd::MixedParams q1 = q;
-    q1.cap = sched_cap();
+    q1.cap = sched_cap(h);
     q1.Xp = h->schedY.as<double>();
     q1.Dp = h->schedD.as<double>();
     q1.Up = h->schedU.as<double>();
@@ -787,7 +808,244 @@ void launch_fista_mixed(csd_handle* h, const csd::FistaParams& p) {
   }
 }
 
+// Converged-optimum L1 fit (precision MIXED_KKT / FP64_KKT, radial order
+// <= 6): support identification by a fixed number of FISTA iterations (TF32
+// tensor cores, or the FP64 kernel), the FP64 active-set polish with its KKT
+// certificate, a second polish for supports larger than the warp slice, and
+// the FP64 FISTA path with the reference stopping rule followed by a last
+// polish for the voxels the first polish could not certify.
+constexpr double kKktKappa = 1e-9;   // certificate: off-support |g_j| <= alpha (1 + kappa)
+constexpr int kKktRounds = 48;       // rounds of the first polish (default of CSD_OPT_KKT_ROUNDS)
+constexpr int kKktRoundsFallback = 64;
+constexpr int kPolishCap = 32;       // support held by the first polish's warp slice
+
+template <int K, bool NONNEG>
+void launch_fista_tf32_nt(csd_handle* h, const csd::Tf32Params& q) {
+  using S = csd::tf::Shape<K>;
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_fista_tf32<K, NONNEG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(S::SMEM)));
+  const int64_t tiles = (q.n_work + csd::tf::TILE - 1) / csd::tf::TILE;
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(2LL * h->num_sms, tiles)));
+  csd::k_fista_tf32<K, NONNEG><<<grid, csd::tf::THREADS, S::SMEM, h->stream>>>(q);
+  CSD_LAUNCH();
+}
+
+template <int K>
+void launch_fista_tf32_t(csd_handle* h, const csd::Tf32Params& q) {
+  if (q.non_negative)
+    launch_fista_tf32_nt<K, true>(h, q);
+  else
+    launch_fista_tf32_nt<K, false>(h, q);
+}
+
+template <int K>
+void build_gtf32_t(csd_handle* h, double scale) {
+  using S = csd::tf::Shape<K>;
+  h->gtf32.ensure(S::B_BYTES);
+  const int n = S::NB * S::KA;
+  csd::k_gtf32<K><<<(n + 255) / 256, 256, 0, h->stream>>>(h->G.as<double>(), h->Kp, scale, h->gtf32.as<float>());
+  CSD_LAUNCH();
+}
+
+// `items` bounds the grid (a device-side list length may be shorter).
+template <int RPL, int RPS>
+void launch_polish_t(csd_handle* h, const csd::PolishParams& q, int warps, int64_t items) {
+  const size_t smem = sizeof(double) * static_cast<size_t>(warps) * csd::polish_warp_doubles(q.cap, q.Kp);
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_l1_polish<RPL, RPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  int per_sm = 0;
+  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_l1_polish<RPL, RPS>, 32 * warps, smem));
+  const int64_t need = (std::max<int64_t>(items, 1) + warps - 1) / warps;
+  const int blocks = static_cast<int>(std::max<int64_t>(
+      1, std::min<int64_t>(static_cast<int64_t>(h->num_sms) * std::max(per_sm, 1), need)));
+  csd::k_l1_polish<RPL, RPS><<<blocks, 32 * warps, smem, h->stream>>>(q);
+  CSD_LAUNCH();
+}
+
+// Supports of up to 32 coefficients keep their vectors in one register per
+// lane; the passes with room for all K coefficients take ceil(K / 32).
+void launch_polish(csd_handle* h, const csd::PolishParams& q, int warps, int64_t items) {
+  const int rpl = (q.K + 31) / 32;
+  const bool small = q.cap <= 32;
+  if (rpl == 1) {
+    launch_polish_t<1, 1>(h, q, warps, items);
+  } else if (rpl == 3) {
+    if (small)
+      launch_polish_t<3, 1>(h, q, warps, items);
+    else
+      launch_polish_t<3, 3>(h, q, warps, items);
+  } else {
+    throw Error{CSD_ERR_INVALID, "the converged-optimum polish is built for radial orders <= 6"};
+  }
+}
+
+void launch_fista_kkt(csd_handle* h, int MT, const csd::FistaParams& p) {
+  cudaStream_t st = h->stream;
+  const int K = h->K, Kp = h->Kp;
+  const int64_t V = p.V;
+  const int k1 = h->opt_kkt_iters;
+  h->kktstat.ensure(8 * sizeof(unsigned long long));
+  auto* stat = h->kktstat.as<unsigned long long>();
+  CSD_CUDA(cudaMemsetAsync(stat, 0, 8 * sizeof(unsigned long long), st));
+  h->kktv.ensure(sizeof(double) * std::max<int64_t>(V, 1));
+  h->kktovf.ensure(sizeof(int64_t) * std::max<int64_t>(p.n_work, 1));
+  h->kktfail.ensure(sizeof(int64_t) * std::max<int64_t>(p.n_work, 1));
+  for (auto& e : h->kev)
+    if (!e) CSD_CUDA(cudaEventCreate(&e));
+  CSD_CUDA(cudaEventRecord(h->kev[0], st));
+
+  const bool tf32 = h->precision == CSD_PRECISION_MIXED_KKT;
+  if (tf32) {
+    if (!(h->gtf32_valid && h->gtf32_key == h->setup_key)) {
+      const double scale = p.step * p.n_inv;  // G / (n L)
+      switch (K) {
+        case 8: build_gtf32_t<8>(h, scale); break;
+        case 29: build_gtf32_t<29>(h, scale); break;
+        case 72: build_gtf32_t<72>(h, scale); break;
+        default: throw Error{CSD_ERR_INVALID, "precision 'mixed-kkt' is built for radial orders 2, 4 and 6"};
+      }
+      h->gtf32_key = h->setup_key;
+      h->gtf32_valid = true;
+    }
+    h->x32.ensure(sizeof(float) * static_cast<size_t>(V) * Kp);
+    csd::Tf32Params q{};
+    q.gop = h->gtf32.as<float>();
+    q.B = p.B;
+    q.Kp = Kp;
+    q.X32 = h->x32.as<float>();
+    q.c_step = p.step * p.n_inv;
+    q.step = p.step;
+    q.thr = p.thr;
+    q.alpha_v = p.alpha_v;
+    q.iters = k1;
+    q.mom = h->mom.as<double>();
+    q.non_negative = p.non_negative;
+    q.list = p.list;
+    q.n_work = p.n_work;
+    q.queue = p.queue;
+    q.batches = stat;
+    q.error = reinterpret_cast<int*>(stat + 1);
+    q.wait_ns = h->opt_wait_ns;
+    CSD_CUDA(cudaMemsetAsync(p.queue, 0, sizeof(unsigned long long), st));
+    switch (K) {
+      case 8: launch_fista_tf32_t<8>(h, q); break;
+      case 29: launch_fista_tf32_t<29>(h, q); break;
+      case 72: launch_fista_tf32_t<72>(h, q); break;
+      default: break;
+    }
+  } else {
+    // FP64 iterations of the same count: tol 0 never stops a voxel early
+    csd::FistaParams f = p;
+    f.max_iter = k1;
+    f.tol = 0.0;
+    f.warm = nullptr;
+    f.iter_total = nullptr;
+    CSD_CUDA(cudaMemsetAsync(p.queue, 0, sizeof(unsigned long long), st));
+    const int saved = h->precision;
+    h->precision = CSD_PRECISION_FP64;
+    launch_fista(h, MT, f);
+    h->precision = saved;
+  }
+  CSD_CUDA(cudaEventRecord(h->kev[1], st));
+
+  csd::PolishParams pp{};
+  pp.G = h->G.as<double>();
+  pp.B = p.B;
+  pp.S32 = tf32 ? h->x32.as<float>() : nullptr;
+  pp.S64 = tf32 ? nullptr : p.X;
+  pp.X = p.X;
+  pp.iters = p.iters;
+  pp.conv = p.conv;
+  pp.kkt = h->kktv.as<double>();
+  pp.K = K;
+  pp.Kp = Kp;
+  pp.n_samples = 1.0 / p.n_inv;
+  pp.alpha = p.thr / p.step;
+  pp.alpha_v = p.alpha_v;
+  pp.non_negative = p.non_negative;
+  pp.kappa = kKktKappa;
+  pp.rounds = h->opt_kkt_rounds;
+  pp.it_base = k1;
+  pp.cap = std::min(kPolishCap, K);
+  pp.list = p.list;
+  pp.n_work = p.n_work;
+  pp.overflow = h->kktovf.as<int64_t>();
+  pp.n_overflow = stat + 2;
+  pp.failed = h->kktfail.as<int64_t>();
+  pp.n_failed = stat + 3;
+  pp.round_total = stat + 4;
+  pp.kkt_max_bits = stat + 5;
+  pp.n_uncertified = stat + 6;  // non-finite inputs (failures go to the fallback list)
+  launch_polish(h, pp, 8, p.n_work);
+  // supports that outgrew the warp slice: again with room for all K
+  csd::PolishParams po = pp;
+  po.cap = K;
+  po.list = h->kktovf.as<int64_t>();
+  po.list_len = stat + 2;
+  po.overflow = h->kktovf.as<int64_t>();  // unused: cap = K cannot overflow
+  po.n_overflow = stat + 7;
+  launch_polish(h, po, 4, p.n_work);
+  CSD_CUDA(cudaEventRecord(h->kev[2], st));
+  unsigned long long hs[6] = {0, 0, 0, 0, 0, 0};
+  CSD_CUDA(cudaMemcpyAsync(hs, stat, sizeof hs, cudaMemcpyDeviceToHost, st));
+  CSD_CUDA(cudaStreamSynchronize(st));
+  if (static_cast<int>(hs[1]) != 0)
+    throw Error{CSD_ERR_TIMEOUT, "TF32 FISTA: a tensor-core completion wait gave up"};
+  h->kkt_batches = hs[0];
+  h->kkt_fallback = hs[3];
+  if (hs[3] > 0) {
+    // the FP64 FISTA path with the reference stopping rule, then a last polish
+    csd::FistaParams r = p;
+    r.list = h->kktfail.as<int64_t>();
+    r.n_work = static_cast<int64_t>(hs[3]);
+    r.warm = nullptr;
+    CSD_CUDA(cudaMemsetAsync(p.queue, 0, sizeof(unsigned long long), st));
+    const int saved = h->precision;
+    h->precision = CSD_PRECISION_FP64;
+    launch_fista(h, MT, r);
+    h->precision = saved;
+    CSD_CUDA(cudaEventRecord(h->kev[3], st));
+    csd::PolishParams pf = pp;
+    pf.S32 = nullptr;
+    pf.S64 = p.X;
+    pf.cap = K;
+    pf.rounds = kKktRoundsFallback;
+    pf.it_add = 1;
+    pf.keep_on_fail = 1;
+    pf.list = h->kktfail.as<int64_t>();
+    pf.list_len = nullptr;
+    pf.n_work = static_cast<int64_t>(hs[3]);
+    pf.failed = nullptr;
+    pf.n_failed = nullptr;
+    pf.overflow = h->kktovf.as<int64_t>();
+    pf.n_overflow = stat + 7;
+    pf.n_uncertified = stat + 6;
+    launch_polish(h, pf, 4, r.n_work);
+  }
+  CSD_CUDA(cudaEventRecord(h->kev[4], st));
+  unsigned long long hs2[3] = {0, 0, 0};
+  CSD_CUDA(cudaMemcpyAsync(hs2, stat + 4, sizeof hs2, cudaMemcpyDeviceToHost, st));
+  CSD_CUDA(cudaStreamSynchronize(st));
+  h->kkt_rounds = hs2[0];
+  double mx = 0.0;
+  std::memcpy(&mx, &hs2[1], sizeof mx);
+  h->kkt_max = mx;
+  h->kkt_uncertified = hs2[2];
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]) == cudaSuccess) h->kkt_ms[0] += ms;
+  if (cudaEventElapsedTime(&ms, h->kev[1], h->kev[2]) == cudaSuccess) h->kkt_ms[1] += ms;
+  if (hs[3] > 0 && cudaEventElapsedTime(&ms, h->kev[2], h->kev[4]) == cudaSuccess) h->kkt_ms[2] += ms;
+  if (hs[3] > 0 && cudaEventElapsedTime(&ms, h->kev[3], h->kev[4]) == cudaSuccess) h->kkt_ms_last_polish = ms;
+  // executed FISTA iterations: k1 per voxel in the first phase (the fallback
+  // fit counted its own)
+  h->kkt_iter_add += static_cast<unsigned long long>(p.n_work) * static_cast<unsigned long long>(k1);
+}
+
 void launch_fista(csd_handle* h, int MT, const csd::FistaParams& p) {
+  if ((h->precision == CSD_PRECISION_MIXED_KKT || h->precision == CSD_PRECISION_FP64_KKT) && p.max_iter > 0) {
+    launch_fista_kkt(h, MT, p);
+    return;
+  }
   if (h->precision == CSD_PRECISION_MIXED && MT * 8 == csd::i8::KC && p.max_iter > 0) {
     launch_fista_mixed(h, p);
     return;
@@ -1027,8 +1285,16 @@ double validate(const csd_shore_spec* s, const HostGtab& g, std::string& warning
   if (s->radial_order <= 0 || s->radial_order % 2 != 0)
     throw Error{CSD_ERR_INVALID,
                 "radial_order must be a positive even number, got " + std::to_string(s->radial_order)};
-  if (s->precision != CSD_PRECISION_FP64 && s->precision != CSD_PRECISION_MIXED)
+  if (s->precision < CSD_PRECISION_FP64 || s->precision > CSD_PRECISION_FP64_KKT)
     throw Error{CSD_ERR_INVALID, "unknown precision"};
+  if ((s->precision == CSD_PRECISION_MIXED_KKT || s->precision == CSD_PRECISION_FP64_KKT) &&
+      s->regularization == CSD_REG_L1) {
+    if (s->radial_order > 6)
+      throw Error{CSD_ERR_INVALID, "the converged-optimum precisions are built for radial orders 2, 4 and 6, got " +
+                                       std::to_string(s->radial_order)};
+    if (s->alpha_mode != CSD_ALPHA_FIXED && s->alpha_mode != CSD_ALPHA_RATIO)
+      throw Error{CSD_ERR_INVALID, "the converged-optimum precisions take alpha_mode fixed or alpha-ratio"};
+  }
   if (s->precision == CSD_PRECISION_MIXED && s->regularization == CSD_REG_L1 && s->radial_order != 6)
     throw Error{CSD_ERR_INVALID, "precision 'mixed' is built for radial order 6, got " +
                                      std::to_string(s->radial_order)};
@@ -1175,6 +1441,9 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   h->mixed_ms = 0.0;
   h->mixed_ops = 0.0;
   h->mixed_rerun = 0;
+  h->kkt_batches = h->kkt_fallback = h->kkt_rounds = h->kkt_uncertified = h->kkt_iter_add = 0;
+  h->kkt_max = 0.0;
+  h->kkt_ms[0] = h->kkt_ms[1] = h->kkt_ms[2] = 0.f;
   const bool is_l1 = spec->regularization == CSD_REG_L1;
   const int mode = spec->alpha_mode;
   const bool need_chol = spec->regularization == CSD_REG_L2 || (is_l1 && mode == CSD_ALPHA_L2_ANCHORED);
@@ -1254,7 +1523,7 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   fp.iter_total = h->itotal.as<unsigned long long>();
   fp.kstep_total = h->itotal.as<unsigned long long>() + 1;
   fp.n_work = V;
-  if (is_l1) ensure_mom(h, spec->max_iter);
+  if (is_l1) ensure_mom(h, std::max(spec->max_iter, h->opt_kkt_iters));
 
   const double* Xfinal = h->X.as<double>();
   const uint32_t* it_final = h->iters.as<uint32_t>();
@@ -1483,7 +1752,7 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
     CSD_CUDA(cudaMemcpyAsync(itot, h->itotal.p, sizeof itot, cudaMemcpyDeviceToHost, st));
   }
   CSD_CUDA(cudaStreamSynchronize(st));
-  if (spec->regularization != CSD_REG_L2) info.total_iterations = itot[0];
+  if (spec->regularization != CSD_REG_L2) info.total_iterations = itot[0] + h->kkt_iter_add;
   // executed FP64 tensor work of the FISTA launches: k-steps x row tiles x
   // one m8n8k4 DMMA (8 x 8 x 4 FMA)
   h->timing.tensor_flops = static_cast<double>(itot[1]) * (Kp / 8) * 512.0;
@@ -1491,6 +1760,19 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   h->timing.ms_mixed_kernel = static_cast<float>(h->mixed_ms);
   h->timing.int8_tensor_ops = h->mixed_ops;
   h->timing.fp64_rerun_voxels = h->mixed_rerun;
+  h->timing.ms_kkt_iterate = h->kkt_ms[0];
+  h->timing.ms_kkt_polish = h->kkt_ms[1];
+  h->timing.ms_kkt_fallback = h->kkt_ms[2];
+  h->timing.kkt_fallback_voxels = static_cast<int64_t>(h->kkt_fallback);
+  h->timing.kkt_uncertified = static_cast<int64_t>(h->kkt_uncertified);
+  h->timing.kkt_rounds = h->kkt_rounds;
+  h->timing.kkt_max = h->kkt_max;
+  if (h->precision == CSD_PRECISION_MIXED_KKT && K <= 80) {
+    const int ks = (K + 7) / 8, nb = 16 * ((K + 15) / 16);
+    h->timing.tf32_tensor_flops = static_cast<double>(h->kkt_batches) * ks * 2.0 * 128 * nb * 8;
+  } else {
+    h->timing.tf32_tensor_flops = 0.0;
+  }
   if (is_l1 && mode != CSD_ALPHA_FIXED) {
     // median / p10 / p90 by nearest rank (src/fit.rs:334-352)
     std::vector<double> a(V);
@@ -1548,42 +1830,15 @@ constexpr int kPipeChunks = sizeof(kPipePlan) / sizeof(kPipePlan[0]);
 constexpr int kPipeMaxChunks = 15;  // events pev[0..14]; two-pass schedule slots 1..15
 static_assert(kPipeChunks <= kPipeMaxChunks, "pipeline events");
 
-// The chunk plan and the right-hand-side SM count; CSD_PIPE_PLAN ("0.2,0.4,0.4":
-// at most 15 fractions, each at least 0.02, summing to 1) and
-// CSD_PIPE_RHS_CTAS override them (invalid values are ignored).
+// The chunk plan (fractions of the masked voxels) and the right-hand-side SM
+// count.
 struct PipePlan {
   std::vector<double> frac;
   int rhs_ctas;
 };
 
 PipePlan pipe_plan(int num_sms) {
-  PipePlan p{std::vector<double>(kPipePlan, kPipePlan + kPipeChunks), kPipeRhsCtas};
-  if (const char* e = std::getenv("CSD_PIPE_PLAN"); e && *e) {
-    std::vector<double> f;
-    double sum = 0.0;
-    const char* s = e;
-    while (*s) {
-      char* end = nullptr;
-      const double v = std::strtod(s, &end);
-      if (end == s || !(v >= 0.02)) {
-        f.clear();
-        break;
-      }
-      f.push_back(v);
-      sum += v;
-      s = (*end == ',') ? end + 1 : end;
-      if (end == s && *s) {
-        f.clear();
-        break;
-      }
-    }
-    if (!f.empty() && static_cast<int>(f.size()) <= kPipeMaxChunks && std::fabs(sum - 1.0) < 1e-6) p.frac = f;
-  }
-  if (const char* e = std::getenv("CSD_PIPE_RHS_CTAS"); e && *e) {
-    const int v = std::atoi(e);
-    if (v >= 1 && v < num_sms) p.rhs_ctas = v;
-  }
-  return p;
+  return PipePlan{std::vector<double>(kPipePlan, kPipePlan + kPipeChunks), std::min(kPipeRhsCtas, num_sms - 1)};
 }
 
 FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64_t nvol,
@@ -1596,6 +1851,9 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   h->mixed_ms = 0.0;
   h->mixed_ops = 0.0;
   h->mixed_rerun = 0;
+  h->kkt_batches = h->kkt_fallback = h->kkt_rounds = h->kkt_uncertified = h->kkt_iter_add = 0;
+  h->kkt_max = 0.0;
+  h->kkt_ms[0] = h->kkt_ms[1] = h->kkt_ms[2] = 0.f;
   record(h, 0);
   ensure_setup(h, g, spec->radial_order, spec->zeta, false, 0.0, 0.0);
   const int N = h->N, K = h->K, Kp = h->Kp;
@@ -1885,7 +2143,8 @@ void csd_destroy(csd_handle* h) {
                     &h->iota, &h->adjW, &h->adjovf, &h->adjstat, &h->adjconst,
                     &h->gdtab, &h->gdq, &h->tuneB, &h->tuneX, &h->tuneIt, &h->tuneConv, &h->tuneQ,
                     &h->schedY, &h->schedPend, &h->schedKey, &h->schedOrder, &h->schedCnt,
-                    &h->schedD, &h->schedU, &h->schedN};
+                    &h->schedD, &h->schedU, &h->schedN, &h->gtf32, &h->x32, &h->kktv, &h->kktovf,
+                    &h->kktfail, &h->kktstat};
   for (auto s : h->pipe)
     if (s) cudaStreamSynchronize(s);
   for (DevBuf* b : bufs) b->release();
@@ -1893,6 +2152,8 @@ void csd_destroy(csd_handle* h) {
     if (e) cudaEventDestroy(e);
   if (h->order_ev) cudaEventDestroy(h->order_ev);
   for (auto& e : h->pev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : h->kev)
     if (e) cudaEventDestroy(e);
   for (auto s : h->pipe)
     if (s) cudaStreamDestroy(s);
@@ -2259,6 +2520,34 @@ int csd_shore_microstructure(csd_handle* h, const float* coefficients, int64_t X
   return CSD_OK;
 }
 
+int csd_set_option(csd_handle* h, int32_t option, int64_t value) {
+  if (!h) return CSD_ERR_INVALID;
+  switch (option) {
+    case CSD_OPT_FISTA_SHAPE:
+      if (value != 0 && value != 1 && value != 12 && value != 16) return CSD_ERR_INVALID;
+      h->opt_shape = static_cast<int>(value);
+      return CSD_OK;
+    case CSD_OPT_FISTA_SCHEDULE:
+      if (value < 0 || value > 100000) return CSD_ERR_INVALID;
+      h->opt_schedule = static_cast<int>(value);
+      return CSD_OK;
+    case CSD_OPT_KKT_ITERATIONS:
+      if (value < 1 || value > 100000) return CSD_ERR_INVALID;
+      h->opt_kkt_iters = static_cast<int>(value);
+      return CSD_OK;
+    case CSD_OPT_KKT_ROUNDS:
+      if (value < 1 || value > 4096) return CSD_ERR_INVALID;
+      h->opt_kkt_rounds = static_cast<int>(value);
+      return CSD_OK;
+    case CSD_OPT_TENSOR_WAIT_NS:
+      if (value < 1 || value > 2000000000LL) return CSD_ERR_INVALID;
+      h->opt_wait_ns = static_cast<unsigned long long>(value);
+      return CSD_OK;
+    default:
+      return CSD_ERR_INVALID;
+  }
+}
+
 int csd_last_timing(const csd_handle* h, csd_fit_timing* out) {
   if (!h || !out) return CSD_ERR_INVALID;
   *out = h->timing;
@@ -2337,7 +2626,10 @@ std::mutex g_noalloc_mutex;
 unsigned char* g_noalloc_addr[256] = {};
 
 // Device address of the scratch array on the current device, looked up once
-// per device (with that device current) and cached.
+// per device (with that device current) and cached for the life of the
+// process.  cudaDeviceReset unloads the module that holds the array, so the
+// cached address is not valid across a reset: this entry point must not be
+// called after the process has reset a device.
 unsigned char* noalloc_scratch(int device) {
   if (device < 0 || device >= 256) throw Error{CSD_ERR_INVALID, "device index out of range"};
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
@@ -2391,6 +2683,8 @@ extern "C" int csd_shore_fista_batch_noalloc(const csd_gtab* gtab, const csd_sho
   try {
     if (spec->regularization != CSD_REG_L1 || spec->alpha_mode != CSD_ALPHA_FIXED)
       throw Error{CSD_ERR_INVALID, "the allocation-free batch fit supports L1 with a fixed alpha only"};
+    if (spec->precision != CSD_PRECISION_FP64)
+      throw Error{CSD_ERR_INVALID, "the allocation-free batch fit runs in FP64 only (precision fp64)"};
     if (spec->radial_order > 6)
       throw Error{CSD_ERR_INVALID, "the allocation-free batch fit supports radial order <= 6 (K <= 72), got " +
                                        std::to_string(spec->radial_order)};

@@ -236,6 +236,8 @@ int csd_shore_fit_batch_device(csd_handle* h, const float* d_signals, int64_t n_
       throw Error{CSD_ERR_INVALID, "the batch fit takes regularization l1 or l2"};
     if (spec->regularization == CSD_REG_L1 && spec->alpha_mode != CSD_ALPHA_FIXED)
       throw Error{CSD_ERR_INVALID, "the batch fit takes alpha_mode fixed (one alpha, or one per voxel)"};
+    if (spec->precision == CSD_PRECISION_MIXED_KKT || spec->precision == CSD_PRECISION_FP64_KKT)
+      throw Error{CSD_ERR_INVALID, "the batch fit takes precision fp64 or mixed"};
     StreamScope scope(h, stream);
     HandleOrder call_order(h);
     run_fit_batch(h, d_signals, n_voxels, g, spec, d_alpha, d_warm, d_order, d_coef, d_iterations);

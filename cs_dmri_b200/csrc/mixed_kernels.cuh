@@ -130,6 +130,8 @@ struct MixedParams {
   unsigned long long* n_flagged;
   unsigned long long* batches; // MMA batches issued (36 MMAs each), summed
   int* error;                  // set to 1 when a tensor-core wait gives up
+  unsigned long long wait_ns;  // limit of one wait for the tensor cores (the drain after a
+                               // give-up keeps its own kWaitNs bound)
   // Two-pass schedule (as FistaParams).  Pass 1 (cap > 0, resume = 0): a
   // voxel neither finished nor flagged after `cap` iterations stores its
   // exact state - x, d and u rows in Xp, Dp, Up and its guard-band flag in
@@ -652,7 +654,7 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
     // ---- wait for the products (bounded)
     uint32_t done = 0;
     const uint64_t t_start = globaltimer_ns();
-    while (!done && globaltimer_ns() - t_start < kWaitNs) done = try_wait(&mbar, phase);
+    while (!done && globaltimer_ns() - t_start < p.wait_ns) done = try_wait(&mbar, phase);
     if (!done) {
       s_abort = 1;
       atomicExch(p.error, 1);

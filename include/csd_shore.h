@@ -28,7 +28,7 @@
  *   0 ok, 1 invalid argument / dimension mismatch (CsDmriError::Dimension,
  *   ::Other), 2 fit refused (CsDmriError::Fit, shell guard src/fit.rs:691-717),
  *   3 numerical (a normal matrix that is not positive definite; the reference
- *   panics at src/solver/tikhonov.rs:326), 4 CUDA error, 5 timeout (a bounded
+ *   panics at src/solver/tikhonov.rs:44), 4 CUDA error, 5 timeout (a bounded
  *   device wait gave up).  A message is written to `err` (NUL-terminated,
  *   truncated to err_len).  Per-voxel non-convergence is not an error: it is
  *   reported through the iterations map and the converged flags.
@@ -80,7 +80,25 @@ enum csd_alpha_mode {
  * tol are re-fitted in FP64. */
 enum csd_precision {
   CSD_PRECISION_FP64 = 0,
-  CSD_PRECISION_MIXED = 1
+  CSD_PRECISION_MIXED = 1,
+  /* The two converged-optimum modes (fixed alpha or alpha ratio, radial
+   * order <= 6) return the LASSO minimiser of (1/(2n)) ||M c - s||^2 +
+   * alpha ||c||_1 itself, certified per voxel by its KKT conditions (the
+   * witness of the reference's tests/common/mod.rs:127-153), instead of the
+   * iterate the reference's stopping rule leaves (fista.rs:120-127), which
+   * sits a relative 1e-5 .. 1e-2 from it.  A fixed number of FISTA
+   * iterations (csd_set_option CSD_OPT_KKT_ITERATIONS, default 64) finds
+   * the support; an FP64 active-set polish (Lawson-Hanson style, with signs
+   * in place of non-negativity) solves G_SS c_S = b_S - n alpha sign(c_S) on
+   * it, moving coefficients in and out until no sign disagrees and every
+   * off-support |M_j^T (M c - s)| / n <= alpha (1 + 1e-9); voxels it has not
+   * certified within its round limit are fitted by the FP64 FISTA path with
+   * the reference stopping rule and polished again.  The iterations map counts the FISTA
+   * iterations plus the polish rounds, and the converged flag is the
+   * certificate.  MIXED_KKT runs the iterations in TF32 on the tensor cores
+   * (FP32 accumulation); FP64_KKT runs them in FP64, as a reference for it. */
+  CSD_PRECISION_MIXED_KKT = 2,
+  CSD_PRECISION_FP64_KKT = 3
 };
 
 /* Gradient table (src/qspace.rs:90-130).  big_delta / small_delta in seconds;
@@ -225,9 +243,50 @@ typedef struct csd_fit_timing {
   float fista_tune_ms16;       /* ... and with 16 */
   int64_t fista_parked;        /* voxels the two-pass FISTA schedule stopped at the cap and resumed,
                                   slowest-first, in its second pass (0: single pass) */
+  /* converged-optimum modes (zero otherwise) */
+  float ms_kkt_iterate;        /* support identification: the TF32 tensor-core (or FP64) FISTA iterations */
+  float ms_kkt_polish;         /* first FP64 polish and certificate */
+  float ms_kkt_fallback;       /* FP64 FISTA of the voxels it left uncertified and their last polish */
+  int64_t kkt_fallback_voxels; /* voxels the first polish did not certify (fitted again in FP64) */
+  int64_t kkt_uncertified;     /* voxels left without a certificate */
+  uint64_t kkt_rounds;         /* polish rounds, summed over voxels and passes */
+  double tf32_tensor_flops;    /* TF32 tensor-core FLOPs issued (2 per multiply-add) */
+  double kkt_max;              /* largest KKT residual of a certified voxel */
 } csd_fit_timing;
 
 int csd_last_timing(const csd_handle* h, csd_fit_timing* out);
+
+/* Tuning options of a handle (they never change a result's meaning):
+ *   CSD_OPT_FISTA_SHAPE     FP64 FISTA kernel: 0 = the per-table autotuned
+ *                           choice (default), 12 or 16 warps per CTA of the
+ *                           DMMA kernel, 1 = the register kernel; every
+ *                           shape computes the same iterates
+ *   CSD_OPT_FISTA_SCHEDULE  0 = single-pass FISTA; 1 = the two-pass
+ *                           schedule where it applies (default); a value
+ *                           >= 2 also sets its cap (iteration of the first
+ *                           pass' end, default 80)
+ *   CSD_OPT_KKT_ITERATIONS  FISTA iterations of the converged-optimum
+ *                           modes' support identification (1 .. 100000,
+ *                           default 64)
+ *   CSD_OPT_KKT_ROUNDS      solves the first polish of the converged-optimum
+ *                           modes may take per voxel before the voxel goes
+ *                           to the FP64 FISTA fallback (1 .. 4096, default 48)
+ *   CSD_OPT_TENSOR_WAIT_NS  how long a tensor-core kernel (MIXED, MIXED_KKT)
+ *                           waits for one batch of its products before it
+ *                           gives up, lets the products in flight land (a
+ *                           separate 2 s bound), frees its tensor memory and
+ *                           makes the call return CSD_ERR_TIMEOUT
+ *                           (1 .. 2e9 ns, default 2e9); a tiny value makes
+ *                           that failure path testable
+ * Returns CSD_ERR_INVALID for an unknown option or value. */
+enum csd_option {
+  CSD_OPT_FISTA_SHAPE = 1,
+  CSD_OPT_FISTA_SCHEDULE = 2,
+  CSD_OPT_KKT_ITERATIONS = 3,
+  CSD_OPT_TENSOR_WAIT_NS = 4,
+  CSD_OPT_KKT_ROUNDS = 5
+};
+int csd_set_option(csd_handle* h, int32_t option, int64_t value);
 
 /* ---- post-fit maps over a coefficient volume (X, Y, Z, K) f32, C order;
  * host buffers in and out; the radial order fixes K. */
@@ -384,15 +443,20 @@ int csd_geodesic_sphere(int32_t frequency, int32_t hemisphere, double* out, int3
  * Inputs and outputs are caller-owned DEVICE memory on the current device:
  * `d_signals` float32 (n_voxels, N) row-major, `d_coeffs` float32
  * (n_voxels, K), `d_iterations` uint32 (n_voxels) or NULL.  `spec` must ask
- * for L1 with a fixed alpha; the result is the same as csd_shore_fit_volume's
- * for those voxels.  Limits: n_voxels <= 8192, N <= 1024, radial order <= 6;
- * larger requests return CSD_ERR_INVALID with a message.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress) with
- * that device current; make that first call before any stream capture.  All
- * calls share the one array and it keeps the last call's contents (each call
- * rebuilds what it reads and zeroes its work counter): calls that overlap on
- * the GPU race.  Work is queued on `stream` (a cudaStream_t, NULL = the
- * legacy default stream) and the call returns after that stream finishes. */
+ * for L1 with a fixed alpha and precision FP64 (anything else returns
+ * CSD_ERR_INVALID); the result is the same as csd_shore_fit_volume's FP64
+ * fit for those voxels.  Limits: n_voxels <= 8192, N <= 1024, radial order
+ * <= 6; larger requests return CSD_ERR_INVALID with a message.  The first
+ * call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current and keeps it for the life
+ * of the process; make that first call before any stream capture, and do not
+ * call this entry point after the process has reset the device
+ * (cudaDeviceReset unloads the array).  All calls share the one array and it
+ * keeps the last call's contents (each call rebuilds what it reads and
+ * zeroes its work counter): calls that overlap on the GPU race.  Work is
+ * queued on `stream` (a cudaStream_t, NULL = the legacy default stream); the
+ * call copies the Lipschitz constant of the table to the host and waits for
+ * `stream` to finish before it returns. */
 int csd_shore_fista_batch_noalloc(const csd_gtab* gtab, const csd_shore_spec* spec,
                                   const float* d_signals, int64_t n_voxels, float* d_coeffs,
                                   uint32_t* d_iterations, void* stream, char* err,

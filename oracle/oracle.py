@@ -426,6 +426,20 @@ def lasso_polish(M, s, alpha, c0, non_negative=False, margin=1e-6):
     return c, ok
 
 
+def lasso_optimum_rows(M, S, alpha, C0, non_negative=False, margin=0.0):
+    """Row-wise lasso_polish: the exact minimiser of every voxel (rows of the
+    signals S) on the support and signs of its approximate solution C0, and
+    whether its KKT conditions certify it.  alpha may be one value per row.
+    Returns (C, certified)."""
+    S, C0 = _f64(S), _f64(C0)
+    a = np.broadcast_to(np.asarray(alpha, np.float64), (S.shape[0],))
+    out = np.zeros_like(C0)
+    ok = np.zeros(S.shape[0], bool)
+    for v in range(S.shape[0]):
+        out[v], ok[v] = lasso_polish(M, S[v], float(a[v]), C0[v], non_negative=non_negative, margin=margin)
+    return out, ok
+
+
 def geodesic_sphere(frequency, hemisphere=False):
     """Class I geodesic sphere: each icosahedron face cut into f^2 triangles on
     a flat barycentric grid, the points projected on the unit sphere and the

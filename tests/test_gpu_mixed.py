@@ -132,11 +132,11 @@ def test_mixed_larger_volume_against_fp64_gpu():
     assert np.percentile(per, 99) <= 1e-6
 
 
-def test_two_pass_schedule_changes_nothing_in_the_mixed_path(monkeypatch):
+def test_two_pass_schedule_changes_nothing_in_the_mixed_path():
     """The mixed kernel's two-pass schedule parks a voxel's x, d, u rows and
     guard flag at iteration 80 and resumes them slowest-first: coefficients,
     iteration counts, convergence flags and the voxels re-run in FP64 are
-    those of a single pass (CSD_FISTA_SCHEDULE=0)."""
+    those of a single pass (handle option CSD_OPT_FISTA_SCHEDULE = 0)."""
     from cs_dmri_b200 import _abi, shore_fit
     from cs_dmri_b200.phantom import make_phantom
     ph = make_phantom((64, 64, 50), seed=31)  # 204,800 voxels: two passes
@@ -146,11 +146,37 @@ def test_two_pass_schedule_changes_nothing_in_the_mixed_path(monkeypatch):
     two = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, **kw)
     t2 = _abi.last_timing(0)
     assert 0.5 * V < t2.fista_parked <= V
-    monkeypatch.setenv("CSD_FISTA_SCHEDULE", "0")
-    one = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, **kw)
-    t1 = _abi.last_timing(0)
+    _abi.set_option(_abi.OPT_FISTA_SCHEDULE, 0)
+    try:
+        one = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, **kw)
+        t1 = _abi.last_timing(0)
+    finally:
+        _abi.set_option(_abi.OPT_FISTA_SCHEDULE, 1)
     assert t1.fista_parked == 0
     assert t1.fp64_rerun_voxels == t2.fp64_rerun_voxels
     for k in ("coef64", "coefficients", "iterations", "converged"):
         np.testing.assert_array_equal(two[k], one[k])
     assert two["total_iterations"] == one["total_iterations"]
+
+
+@pytest.mark.parametrize("precision", ["mixed", "mixed-kkt"])
+def test_tensor_core_wait_gives_up_and_the_handle_recovers(ph, precision):
+    """The tensor-core kernels bound every wait for their products.  With the
+    limit set to 1 ns (handle option CSD_OPT_TENSOR_WAIT_NS) the first wait
+    gives up: the kernel flags the error, lets the products in flight land,
+    frees its tensor memory and returns, and the call reports CSD_ERR_TIMEOUT
+    (status 5).  The next fit on the same handle succeeds and equals a fit
+    that never timed out."""
+    from cs_dmri_b200 import _abi
+    kw = dict(alpha_mode="fixed", alpha=0.01)
+    before = fit(ph, precision, **kw)
+    _abi.set_option(_abi.OPT_TENSOR_WAIT_NS, 1)
+    try:
+        with pytest.raises(_abi.CsdError) as e:
+            fit(ph, precision, **kw)
+        assert e.value.code == 5 and "gave up" in str(e.value)
+    finally:
+        _abi.set_option(_abi.OPT_TENSOR_WAIT_NS, 2_000_000_000)
+    after = fit(ph, precision, **kw)
+    for k in ("coef64", "coefficients", "iterations", "converged"):
+        np.testing.assert_array_equal(before[k], after[k])

@@ -1,6 +1,6 @@
 """Parity of the CUDA library with the CPU oracle on identical seeded inputs.
 
-Tolerances.  The FP64 path runs the reference's iteration (fista.rs:121-194)
+Tolerances.  The FP64 path runs the reference's iteration (fista.rs:70-143)
 in Gram form on FP64 tensor cores, so iterates differ from the oracle only by
 rounding; the stopping rule ||dx|| < tol ||x|| can then end a voxel's loop
 one iteration earlier or later, which moves its coefficients by about
@@ -12,10 +12,25 @@ lambda = 0.05 and through the reference's normal-equation residual at the
 default lambda = 1e-8.
 """
 
+from contextlib import contextmanager
+
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+OPT_FISTA_SHAPE, OPT_FISTA_SCHEDULE = 1, 2  # csd_set_option
+
+
+@contextmanager
+def handle_option(option, value, default):
+    """A tuning option of the shared device-0 handle for the block's calls."""
+    from cs_dmri_b200 import _abi
+    _abi.set_option(option, value)
+    try:
+        yield
+    finally:
+        _abi.set_option(option, default)
 
 
 @pytest.fixture(scope="module")
@@ -215,18 +230,18 @@ def test_shore_model_interface(ph, oracle):
     assert sp[0] == 0.0 and sp[1:].min() > 0.9 and "256 voxels" in repr(fit)
 
 
-@pytest.mark.parametrize("variant", ["0", "3", "4"])
-def test_fista_kernel_variants_match_oracle(ph, oracle, variant, monkeypatch):
-    """Every FISTA kernel variant (k_fista_fp64; k_fista_v3 with 12 or 16
+@pytest.mark.parametrize("shape", [1, 12, 16])
+def test_fista_kernel_variants_match_oracle(ph, oracle, shape):
+    """Every FISTA kernel shape (k_fista_fp64; k_fista_v3 with 12 or 16
     warps per CTA) runs the same per-voxel iteration."""
-    monkeypatch.setenv("CSD_FISTA_VARIANT", variant)
-    for mode in ("fixed", "l2-anchored"):
-        gpu, ref = both(ph, oracle, alpha_mode=mode, alpha=0.01)
+    with handle_option(OPT_FISTA_SHAPE, shape, 0):
+        fits = {mode: both(ph, oracle, alpha_mode=mode, alpha=0.01) for mode in ("fixed", "l2-anchored")}
+    for mode, (gpu, ref) in fits.items():
         same = np.isclose(gpu["alpha"][ph.mask], ref["alpha"][ph.mask], rtol=1e-9, atol=0)
         assert same.mean() >= 0.98
         r = rel_rows(gpu["coef64"], ref["coef64"])
         nz = np.linalg.norm(ref["coef64"], axis=1) > 0
-        assert r[same & nz].max() <= 1e-5, (variant, mode, r[same & nz].max())
+        assert r[same & nz].max() <= 1e-5, (shape, mode, r[same & nz].max())
         it_g = gpu["iterations"][ph.mask].astype(int)
         it_o = ref["iterations"][ph.mask].astype(int)
         assert np.abs(it_g - it_o)[same].max() <= 1
@@ -361,7 +376,7 @@ def test_pipelined_host_fit_matches_the_device_fit():
     np.testing.assert_array_equal(out2, pageable["coefficients"])
 
 
-def test_fista_autotuner_choice_changes_nothing(monkeypatch):
+def test_fista_autotuner_choice_changes_nothing():
     """The per-table autotuner picks k_fista_v3's warps per CTA (12 or 16)
     from a timed synthetic batch; both give bit-identical fits."""
     from cs_dmri_b200 import _abi, shore_fit
@@ -375,20 +390,20 @@ def test_fista_autotuner_choice_changes_nothing(monkeypatch):
     assert t.fista_tune_ms12 > 0 and t.fista_tune_ms16 > 0
     assert t.fista_warps == (12 if t.fista_tune_ms12 < t.fista_tune_ms16 else 16)
     fits = {}
-    for variant in ("3", "4"):
-        monkeypatch.setenv("CSD_FISTA_VARIANT", variant)
-        fits[variant] = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, **kw)
+    for shape in (12, 16):
+        with handle_option(OPT_FISTA_SHAPE, shape, 0):
+            fits[shape] = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, **kw)
     for f in fits.values():
         np.testing.assert_array_equal(f["coef64"], auto["coef64"])
         np.testing.assert_array_equal(f["coefficients"], auto["coefficients"])
 
 
-def test_two_pass_fista_schedule_changes_nothing(monkeypatch):
+def test_two_pass_fista_schedule_changes_nothing():
     """With at least four voxels per FISTA slot a fit runs in two passes:
     every voxel up to iteration 80, then the unfinished ones resumed from
     their exact state, largest predicted remaining iteration count first.  The
     coefficients, iteration counts and convergence flags are bit-identical to
-    a single pass (CSD_FISTA_SCHEDULE=0), on the device-buffer path and on the
+    a single pass (handle option CSD_OPT_FISTA_SCHEDULE = 0), on the device-buffer path and on the
     pipelined host path (whose larger chunks take the two passes)."""
     import torch
     from cs_dmri_b200 import _abi, shore_fit
@@ -399,13 +414,12 @@ def test_two_pass_fista_schedule_changes_nothing(monkeypatch):
     two = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, return_coef64=True, diagnostics=True, **kw)
     parked = _abi.last_timing(0).fista_parked
     assert 0.5 * V < parked <= V
-    monkeypatch.setenv("CSD_FISTA_SCHEDULE", "0")
-    one = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, return_coef64=True, diagnostics=True, **kw)
-    assert _abi.last_timing(0).fista_parked == 0
+    with handle_option(OPT_FISTA_SCHEDULE, 0, 1):
+        one = shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, return_coef64=True, diagnostics=True, **kw)
+        assert _abi.last_timing(0).fista_parked == 0
     for k in ("coef64", "coefficients", "iterations", "converged"):
         np.testing.assert_array_equal(two[k], one[k])
     assert two["total_iterations"] == one["total_iterations"]
-    monkeypatch.delenv("CSD_FISTA_SCHEDULE")
     pin = torch.empty(ph.data.shape, dtype=torch.float32, pin_memory=True)
     pin.numpy()[...] = ph.data
     out = torch.full(ph.data.shape[:3] + (72,), float("nan"), dtype=torch.float32, pin_memory=True)

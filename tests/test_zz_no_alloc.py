@@ -28,7 +28,10 @@ def _noalloc(lib, gtab, spec, sig, out, its, stream):
     return code, err.value.decode()
 
 
-def test_noalloc_batch_matches_volume_fit():
+@pytest.mark.parametrize("order", [2, 4, 6])
+def test_noalloc_batch_matches_volume_fit(order):
+    """Radial orders 2, 4 and 6 (K = 8, 29, 72): the 8- and 32-row padded
+    layouts of the right-hand sides and iterates, and the 72-row one."""
     import torch
 
     from cs_dmri_b200 import _abi, shore_fit
@@ -36,7 +39,8 @@ def test_noalloc_batch_matches_volume_fit():
     from cs_dmri_b200.phantom import make_phantom
 
     lib = _abi.load()
-    kw = dict(alpha_mode="fixed", alpha=0.01)
+    kw = dict(alpha_mode="fixed", alpha=0.01, radial_order=order)
+    K = lib.csd_shore_n_coeffs(order)
     stream = torch.cuda.current_stream().cuda_stream
     first = None
     for seed, shape in ((21, (12, 10, 8)), (22, (16, 16, 5)), (21, (12, 10, 8))):
@@ -45,7 +49,7 @@ def test_noalloc_batch_matches_volume_fit():
                         return_coef64=True, diagnostics=True, **kw)
         V = ph.n_voxels
         sig = torch.from_numpy(np.ascontiguousarray(ph.data.reshape(V, -1))).cuda()
-        out = torch.full((V, 72), float("nan"), dtype=torch.float32, device="cuda")
+        out = torch.full((V, K), float("nan"), dtype=torch.float32, device="cuda")
         its = torch.zeros(V, dtype=torch.int32, device="cuda")
         gtab, keep = build_gtab(ph.bvals, ph.bvecs, 50.0, ph.big_delta, ph.small_delta)
         spec = build_spec(**kw)
@@ -83,3 +87,6 @@ def test_noalloc_rejects_oversize_batches():
     code, msg = _noalloc(lib, gtab, build_spec(alpha_mode="fixed", alpha=0.01, radial_order=8), sig[:4], out[:4],
                          its[:4], 0)
     assert code == _abi.ERR_INVALID and "radial order" in msg
+    code, msg = _noalloc(lib, gtab, build_spec(alpha_mode="fixed", alpha=0.01, precision="mixed"), sig[:4],
+                         out[:4], its[:4], 0)
+    assert code == _abi.ERR_INVALID and "FP64 only" in msg
