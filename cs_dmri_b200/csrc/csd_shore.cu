@@ -546,7 +546,7 @@ int64_t compact(csd_handle* h, const uint8_t* d_flags, int64_t n, DevBuf& out) {
 inline unsigned grid1(int64_t n, int bs = 256) { return static_cast<unsigned>((n + bs - 1) / bs); }
 
 // Momentum of FISTA iteration k, (t_k - 1) / t_{k+1} with t_0 = 1 and
-// t_{k+1} = (1 + sqrt(1 + 4 t_k^2)) / 2 (src/solver/fista.rs:161-163).  It
+// t_{k+1} = (1 + sqrt(1 + 4 t_k^2)) / 2 (src/solver/fista.rs:110-112).  It
 // depends on k only; the table is built once per max_iter with the same IEEE
 // operations the reference performs inside its loop.
 void ensure_mom(csd_handle* h, int max_iter) {
@@ -1052,7 +1052,7 @@ void launch_fista(csd_handle* h, int MT, const csd::FistaParams& p) {
   }
   if (p.max_iter <= 0) {
     // An empty iteration loop: the warm start (or zero) is the result, with
-    // 0 iterations and not converged (fista.rs:126-140 with max_iter = 0).
+    // 0 iterations and not converged (fista.rs:89-143 with max_iter = 0).
     csd::k_fista_noop<<<grid1(p.n_work * (h->Kp + 1)), 256, 0, h->stream>>>(p, h->Kp);
     CSD_LAUNCH();
     return;

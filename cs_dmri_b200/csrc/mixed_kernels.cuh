@@ -3,7 +3,7 @@
 // (tcgen05.mma kind::i8, int32 accumulators in tensor memory) and every other
 // piece of state stays FP64.
 //
-// The FISTA update needs G y - b (fista.rs:141-160 in Gram form).  Written
+// The FISTA update needs G y - b (fista.rs:90-107 in Gram form).  Written
 // incrementally, with d_k = x_k - x_{k-1}, u_k = G x_k - b and P_k = G d_k,
 //
 //     G y_k - b = u_k + mom_{k-1} P_k,     u_k = u_{k-1} + P_k,
@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(i8::THREADS, 1) k_fista_i8(MixedParams p) {
   unsigned long long executed = 0, n_batches = 0;
   const double tol = p.tol;
   const double lo_band = tol * (1.0 - p.band), hi_band = tol * (1.0 + p.band);
-  // The stopping rule ||dx|| < tol max(||x||, 1e-12) (fista.rs:166-179) and
+  // The stopping rule ||dx|| < tol max(||x||, 1e-12) (fista.rs:115-127) and
   // the guard band, compared in squares: a rounding-level difference from the
   // square-root form can only matter inside the band, where the FP64 kernel
   // decides anyway.

@@ -9,7 +9,7 @@
 // with alpha_max = ||M^T s||_inf / n and the zero result for alpha_max == 0.
 // The path is walked one point at a time over the whole volume: each point is
 // one FISTA launch over the voxels still in play, warm-started in place from
-// the previous point (fista.rs:216-230), then one residual pass and the
+// the previous point (fista.rs:164-178), then one residual pass and the
 // selection update below.  Under PathL2Anchored a voxel leaves the work list
 // as soon as it is selected: the later points of its path cannot change the
 // result, so they are not computed.

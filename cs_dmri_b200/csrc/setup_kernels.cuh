@@ -164,7 +164,7 @@ __global__ void k_lipschitz(const double* __restrict__ G, int Kp, int N, int max
 
 // In-place right-looking Cholesky A = L L^T of the leading K x K block of a
 // Kp x Kp matrix, one CTA.  Writes 0 to *ok_out if A is not positive definite
-// (the reference panics there, src/solver/tikhonov.rs:326).  The accumulation
+// (the reference panics there, src/solver/tikhonov.rs:44).  The accumulation
 // order of every entry is the left-looking order k = 0, 1, ..., so results
 // match a sequential LL^T factorisation.
 __global__ void k_cholesky(double* __restrict__ A, int K, int Kp, int* __restrict__ ok_out) {

@@ -3,13 +3,13 @@
 //   k_mask_count / k_scan_blocks / k_mask_compact
 //       masked voxel list in canonical x-y-z order (src/voxel_loop.rs:28-42)
 //   k_rhs         b_v = M^T s_v for every masked voxel (the A^T s of every
-//                 solver: fista.rs:142-144 in Gram form, tikhonov.rs:343,
+//                 solver: fista.rs:90-93 in Gram form, tikhonov.rs:62,
 //                 alpha.rs:51)
-//   k_fista_fp64  warm-startable FISTA iterations (src/solver/fista.rs:121-194)
+//   k_fista_fp64  warm-startable FISTA iterations (src/solver/fista.rs:70-143)
 //                 in Gram form on FP64 DMMA tensor cores, 8 voxels per warp,
 //                 slots refilled from a device work queue as voxels converge
 //   k_tikhonov    L L^T c = b by forward/back substitution
-//                 (src/solver/tikhonov.rs:342-357)
+//                 (src/solver/tikhonov.rs:60-76)
 //   k_epilogue    residual ||s - M c||, R^2, BIC, diagnostic maps and the
 //                 scatter into the (X, Y, Z, K) coefficient volume
 //                 (src/fit.rs:115-155, 264-318)
@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(256) k_fista_fp64(FistaParams p) {
     }
     __syncwarp();
 
-    // ---- proximal gradient step and momentum (fista.rs:141-173)
+    // ---- proximal gradient step and momentum (fista.rs:95-113)
     double tn[2], mom[2], dx2[2] = {0.0, 0.0}, xn2[2] = {0.0, 0.0};
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(256) k_fista_fp64(FistaParams p) {
       }
     }
 
-    // ---- per-voxel stopping rule (fista.rs:166-179) and write-out
+    // ---- per-voxel stopping rule (fista.rs:115-127) and write-out
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       if (vid[j] < 0) continue;
@@ -512,7 +512,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
     }
     __syncwarp();
 
-    // ---- proximal gradient step and momentum (fista.rs:141-173)
+    // ---- proximal gradient step and momentum (fista.rs:95-113)
     double mom[2], dx2[2] = {0.0, 0.0}, xn2[2] = {0.0, 0.0};
 #pragma unroll
     for (int j = 0; j < 2; ++j) mom[j] = (vid[j] >= 0) ? p.mom[it[j]] : 0.0;
@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_fista_v3(FistaParams p) {
       }
     }
 
-    // ---- per-voxel stopping rule (fista.rs:166-179) and write-out
+    // ---- per-voxel stopping rule (fista.rs:115-127) and write-out
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       if (vid[j] < 0) continue;

@@ -649,7 +649,7 @@ struct Fista {
       for (int j = 0; j < M.cols; ++j) mt(j, i) = M(i, j);
   }
 
-  // fit_with_warm_start (fista.rs:121-194).
+  // fit_with_warm_start (fista.rs:70-143).
   Diag fit(const double* s, const double* warm, double* x_out) const {
     const int K = design->cols, N = design->rows;
     Vec x(K, 0.0), y, xn(K), yn(K), my(N), res(N), grad(K);
@@ -1349,7 +1349,7 @@ int oracle_shore_fit_volume(const float* data, const uint8_t* mask, int64_t X, i
           f.alpha = a_used;
           d = f.fit(s.data(), nullptr, c);
         } else {
-          // fit_path, warm-started descending (fista.rs:216-230).
+          // fit_path, warm-started descending (fista.rs:164-178).
           Vec alphas = log_path(amax, spec->path_n_alphas, path_eps);
           const int P = spec->path_n_alphas;
           std::vector<Vec> cs(P, Vec(K));

@@ -1,7 +1,7 @@
 """Regenerate the golden fixtures under tests/golden/.
 
-Run in a container that holds the cs_dmri reference at REFERENCE (default
-/root/reference).  Two sets are written:
+Run where a checkout of the cs_dmri reference is available, giving its path
+as the first argument or in CS_DMRI_REFERENCE.  Two sets are written:
 
 1. lasso_fixtures.npz - the reference's eight scikit-learn LASSO fixtures
    (tests/data/lasso_fixtures/*.bin, format of tests/optimization_sklearn.rs:
@@ -27,7 +27,12 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
-REFERENCE = Path(os.environ.get("CS_DMRI_REFERENCE", "/root/reference"))
+def reference_root() -> Path:
+    """The reference checkout: argv[1], else $CS_DMRI_REFERENCE."""
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CS_DMRI_REFERENCE")
+    if not root:
+        sys.exit("usage: python tests/golden/make_golden.py <cs_dmri checkout> (or set CS_DMRI_REFERENCE)")
+    return Path(root)
 
 
 def decode_bin(raw: bytes) -> dict:
@@ -44,8 +49,8 @@ def decode_bin(raw: bytes) -> dict:
                 objective=obj, positive=bool(positive))
 
 
-def lasso_fixtures() -> None:
-    src = REFERENCE / "tests" / "data" / "lasso_fixtures"
+def lasso_fixtures(reference: Path) -> None:
+    src = reference / "tests" / "data" / "lasso_fixtures"
     names = json.loads((src / "manifest.json").read_text())
     arrays = {}
     for fname in names:
@@ -85,5 +90,5 @@ def shore_lasso() -> None:
 
 
 if __name__ == "__main__":
-    lasso_fixtures()
+    lasso_fixtures(reference_root())
     shore_lasso()

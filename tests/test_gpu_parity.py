@@ -151,7 +151,7 @@ def test_partial_mask_zeros_outside(ph, oracle):
 
 def test_nan_voxel_matches_reference_semantics(ph, oracle):
     """A NaN sample makes every soft-threshold comparison false, so the
-    reference's prox falls through to 0.0 (src/solver/fista.rs:151-157): the
+    reference's prox falls through to 0.0 (src/solver/fista.rs:99-107): the
     voxel converges to zero coefficients at iteration 1.  Other voxels are
     unaffected."""
     data = ph.data.copy()

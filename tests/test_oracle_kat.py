@@ -195,7 +195,7 @@ def test_hemisphere_is_321_unit_directions(oracle):
     assert d.min() > -1 + 1e-9
 
 
-def test_fista_recovers_sparse_signal(oracle):  # src/solver/fista.rs:239-266
+def test_fista_recovers_sparse_signal(oracle):  # src/solver/fista.rs:188-216
     m = np.array([1.0, 0.0, 0.5, -0.2, 0.0, 1.0, -0.1, 0.3, -0.3, 0.4, 1.0, 0.0, 0.2, -0.1, 0.0, 1.0,
                   0.5, 0.5, 0.5, 0.5, -0.5, 0.5, -0.5, 0.5, 0.5, -0.5, 0.5, -0.5, 0.1, 0.2, -0.3, 0.4]).reshape(8, 4)
     c = np.array([2.0, 0.0, -1.5, 0.0])
@@ -203,7 +203,7 @@ def test_fista_recovers_sparse_signal(oracle):  # src/solver/fista.rs:239-266
     assert abs(coef[0] - 2) < 0.05 and abs(coef[1]) < 0.05 and abs(coef[2] + 1.5) < 0.05 and abs(coef[3]) < 0.05
 
 
-def test_fista_zero_alpha_is_least_squares(oracle):  # src/solver/fista.rs:268-281
+def test_fista_zero_alpha_is_least_squares(oracle):  # src/solver/fista.rs:217-231
     m = np.array([1.0, 0.0, 0.0, 1.0, 1.0, 1.0, 1.0, -1.0]).reshape(4, 2)
     coef, *_ = oracle.fista_fit(m, m @ np.array([2.0, -3.0]), 0.0, 5000, 1e-12)
     assert abs(coef[0] - 2) < 1e-3 and abs(coef[1] + 3) < 1e-3
@@ -248,7 +248,7 @@ def test_bic_formula(oracle):  # src/solver/alpha.rs:96-103
     assert math.isfinite(oracle.bic(10, 0.0, 0))
 
 
-def test_tikhonov_unregularized(oracle):  # src/solver/tikhonov.rs:366-387
+def test_tikhonov_unregularized(oracle):  # src/solver/tikhonov.rs:85-106
     m = np.array([1.0, 0.0, 0.0, 1.0, 1.0, 1.0, 1.0, -1.0]).reshape(4, 2)
     c, _ = oracle.tikhonov_fit(m, m @ np.array([2.0, -3.0]), np.zeros(2), np.zeros(2), 1e-12, 0.0)
     assert np.allclose(c, [2.0, -3.0], atol=1e-6)
