@@ -28,7 +28,7 @@ error of the mixed path against the FP64 path).
           hyper-parameter), voxels/s for L1 and Tikhonov, and the ratio of the
           forward+backward step to the forward step.
 * graddev the per-voxel-design fit (radial order 8, a gradient-deviation
-          tensor and 0-15 % dropped samples per voxel) on 100k voxels.
+          tensor and 0-15 % dropped samples per voxel) on 300k voxels.
 * pipeline the hypergradient alpha selection pipeline (8 steps on a held-out
           10 % of the samples, final fit, peaks, RTOP / MSD) on the same
           volume, host clock, with the held-out error of the reference's own
@@ -38,8 +38,11 @@ error of the mixed path against the FP64 path).
           threads, on a bounded sample of the same voxels.
 
 ``--impl reference`` times that CPU path alone, as the reference arm.
-Multi-GPU (torchrun): every rank fits its own copy of the volume (independent
-subjects; weak scaling, no collective in the data path).
+Multi-GPU: `--gpus N` runs N ranks (under torchrun, or launched by this
+script itself when no launcher set WORLD_SIZE).  The line's `value` is weak
+scaling: every rank fits its own copy of the volume (independent subjects; no
+collective in the data path).  The `sharded` block is strong scaling: one
+volume split across the ranks, and the row gather that reassembles it.
 """
 
 from __future__ import annotations
@@ -48,6 +51,7 @@ import argparse
 import json
 import os
 import re
+import socket
 import statistics
 import subprocess
 import sys
@@ -62,7 +66,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "SHORE L1-fit voxels/s, mixed vs FP64 GPU at \u22641e-5 rel err; fwd+bwd voxels/s"
 FWD_BWD_GRID = (50, 50, 20)  # the differentiable-fit workload: 50,000 voxels, radial order 6
-GRADDEV_VOXELS = 100_000     # per-voxel-design workload (radial order 8), a third of the 300k volume
+GRADDEV_VOXELS = 300_000     # per-voxel-design workload (radial order 8): configuration 3's size
 WORKLOAD = "brain300k"
 
 
@@ -410,12 +414,46 @@ def run_ours(args):
             e2e_t.append(dt)
     e2e_s = max_over_ranks(sum(e2e_t), world, torch.device("cuda", device))
     e2e_value = world * V * args.steps / e2e_s
+    # the drop-in's usual call: a pageable numpy volume and a new output array
+    # (the masked rows are gathered into the library's page-locked staging
+    # volume on host threads), warm and cold (a new library handle: table
+    # set-up, autotuning and allocations included)
+    pg_t = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize(device)
+        barrier(world)
+        t = time.perf_counter()
+        shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, big_delta=ph.big_delta, small_delta=ph.small_delta,
+                  device=device, precision=path, **kw)
+        if i >= args.warmup:
+            pg_t.append(time.perf_counter() - t)
+    pg_s = max_over_ranks(sum(pg_t), world, torch.device("cuda", device))
+    cold_t = []
+    for _ in range(2):
+        _abi.reset_handle(device)
+        torch.cuda.synchronize(device)
+        barrier(world)
+        t = time.perf_counter()
+        shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, big_delta=ph.big_delta, small_delta=ph.small_delta,
+                  device=device, precision=path, **kw)
+        cold_t.append(time.perf_counter() - t)
+    cold_s = max_over_ranks(statistics.median(cold_t), world, torch.device("cuda", device))
+    e2e_variants = {"pageable": {"value": world * V * args.steps / pg_s, "unit": "voxels/s",
+                                 "ms_per_step": 1e3 * pg_s / args.steps,
+                                 "input": "pageable numpy volume, new output array each call"},
+                    "cold": {"value": world * V / cold_s, "unit": "voxels/s", "ms_per_step": 1e3 * cold_s,
+                             "input": "pageable numpy volume on a new library handle (set-up, autotuning and "
+                                      "allocations included), median of 2"}}
     # page-locked input: the library reads the masked rows in place (V x N x 4 B) plus the mask
     h2d = V * N * 4 + ph.mask.nbytes
     d2h = out["coefficients"].nbytes
 
     # ---- the converged-optimum paths on the same volume
     optimum = optimum_block(args, ph, d_data, d_mask, stream, device, world, ms / args.steps)
+    # ---- configuration 2's other fits: Tikhonov and the positivity QP
+    config2 = config2_block(args, ph, d_data, d_mask, stream, device, world)
+    # ---- one volume across the ranks (strong scaling), when there are several
+    sharded = sharded_block(args, ph, d_data, stream, device, world) if world > 1 else None
     # ---- fwd+bwd: differentiable fit of 50k voxels
     fwd_bwd = fwd_bwd_block(args, device, world)
     # ---- per-voxel designs (gradient deviation, dropped samples)
@@ -465,7 +503,8 @@ def run_ours(args):
             "data": "synthetic (seeded CS-DSI multi-tensor phantom, S0 1000, SNR 25)",
             "config": bench_config(ph), "path": path,
             "parallelism": f"{world} independent volume(s), one per GPU",
-            "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e_value, "unit": "voxels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "input": "page-locked volume and output", **e2e_variants},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": dmma_peak, "unit": "TFLOP/s",
                          "frac": (achieved / dmma_peak) if dmma_peak else None, "traffic": traffic,
                          "kernel": fista_kernel, "kernel_ms": k_ms,
@@ -488,6 +527,8 @@ def run_ours(args):
             "pipeline": pipeline,
             "paths": paths,
             "optimum": optimum,
+            "sharded": sharded,
+            "config2": config2,
             "clocks": clocks.summary(),
             "iterations_per_voxel": it_launch / V,
         }
@@ -518,6 +559,78 @@ def timed_fits(args, fit, stream, device, world):
         e1.record(stream)
         torch.cuda.synchronize(device)
     return max_over_ranks(e0.elapsed_time(e1) / args.steps, world, torch.device("cuda", device)), clocks.summary()
+
+
+def sharded_block(args, ph, d_data, stream, device: int, world: int) -> dict:
+    """The same volume split across the ranks (strong scaling): rank r fits
+    its contiguous chunk of the masked voxels (cs_dmri_b200.distributed.shard_mask)
+    from the device-resident volume; device time per fit, max over ranks.
+    Then one cs_dmri_b200.distributed.fit_sharded call from the host volume -
+    fit, gather of every shard's rows to rank 0, reassembly - on the host
+    clock."""
+    import torch
+
+    from cs_dmri_b200 import shore_fit_device
+    from cs_dmri_b200.distributed import fit_sharded, shard_mask
+
+    rank = int(os.environ.get("RANK", "0"))
+    V = int(ph.mask.sum())
+    local = torch.from_numpy(shard_mask(ph.mask, rank, world)).to(f"cuda:{device}")
+    kw = dict(fit_kwargs(), big_delta=ph.big_delta, small_delta=ph.small_delta, device=device)
+
+    def fit():
+        return shore_fit_device(d_data, local, ph.bvals, ph.bvecs, stream=stream, **kw)
+
+    ms_step, clk = timed_fits(args, fit, stream, device, world)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    t = time.perf_counter()
+    fit_sharded(ph.data, ph.bvals, ph.bvecs, ph.mask, **kw)
+    dt = max_over_ranks(time.perf_counter() - t, world, torch.device("cuda", device))
+    return {"metric": "voxels/s of one volume across all ranks", "scaling": "strong", "value": V / (ms_step * 1e-3),
+            "unit": "voxels/s", "ms_per_step": ms_step, "voxels_per_rank": V // world, "clocks": clk,
+            "fit_sharded_host_s": dt, "fit_sharded_voxels_per_s": V / dt}
+
+
+def config2_block(args, ph, d_data, d_mask, stream, device: int, world: int) -> dict:
+    """The brain-sized volume's other two fits of configuration 2, device
+    buffers in and out:
+      l2      Tikhonov, lambda_n = lambda_l = 0.05: c = P s with the solution
+              operator P = H^-1 M^T (built once per table from the Cholesky
+              factor of H, src/solver/tikhonov.rs:26-76), one FP64 DMMA
+              product per 8 voxels (k_rhs_dmma with P in place of M^T);
+              algorithmic work 2 N K FLOP and 4 N + 8 K bytes per voxel;
+      nonneg  the amplitude-positivity QP (Goldfarb-Idnani, k_icls), credited
+              with iterations x (2 m K + 2 K^2) FLOP, m = 321 constraints."""
+    from cs_dmri_b200 import _abi, shore_fit_device
+
+    V = int(ph.mask.sum())
+    N, K, m = ph.data.shape[-1], 72, 321
+    base = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, device=device, radial_order=6, zeta=700.0)
+    out = {}
+    for name, kw in (("l2", dict(regularization="l2", lambda_n=0.05, lambda_l=0.05)),
+                     ("nonneg", dict(regularization="nonneg"))):
+        def fit():
+            return shore_fit_device(d_data, d_mask, ph.bvals, ph.bvecs, stream=stream, **base, **kw)
+        ms_step, clk = timed_fits(args, fit, stream, device, world)
+        coef, res = fit()
+        t = _abi.last_timing(device)
+        blk = {"value": world * V / (ms_step * 1e-3), "unit": "voxels/s", "ms_per_step": ms_step, "clocks": clk}
+        if name == "l2":
+            k_ms = t.ms_rhs  # the operator product is the whole solve
+            flops = 2.0 * N * K * V
+            byts = (4.0 * N + 8.0 * K) * V
+            blk.update({"kernel": "k_rhs_dmma<72> with the Tikhonov operator (FP64 DMMA)", "kernel_ms": k_ms,
+                        "achieved_tflops": flops / (k_ms * 1e-3) / 1e12,
+                        "achieved_gbs": byts / (k_ms * 1e-3) / 1e9})
+        else:
+            k_ms = t.ms_solve_kernel
+            it = res.total_iterations / V
+            flops = res.total_iterations * (2.0 * m * K + 2.0 * K * K)
+            blk.update({"kernel": "k_icls (FP64, warp per voxel)", "kernel_ms": k_ms,
+                        "iterations_per_voxel": it, "achieved_tflops": flops / (k_ms * 1e-3) / 1e12})
+        out[name] = blk
+    return out
 
 
 def optimum_block(args, ph, d_data, d_mask, stream, device: int, world: int, fp64_ms: float) -> dict:
@@ -658,11 +771,11 @@ def fwd_bwd_block(args, device: int, world: int) -> dict:
 
 
 def graddev_block(args, device: int, world: int) -> dict:
-    """L1 fit on a design per voxel: 100,000 voxels of the phantom, each with
+    """L1 fit on a design per voxel: 300,000 voxels of the phantom, each with
     its own gradient-deviation tensor (I + N(0, 0.02)) and 0-15 % of its
     samples dropped, radial order 8 (K = 145), alpha 0.01, the reference's
     FISTA.  CUDA events on the fit stream, max over ranks; min(steps, 3)
-    timed steps (each builds 100k Gram matrices of 145 x 145)."""
+    timed steps (each builds 300k Gram matrices of 145 x 145)."""
     import torch
 
     from cs_dmri_b200.graddev import graddev_phantom, shore_fit_graddev
@@ -671,7 +784,7 @@ def graddev_block(args, device: int, world: int) -> dict:
     dev = f"cuda:{device}"
     St, Tt, Kt = (torch.from_numpy(a).to(dev) for a in (S, T, keep))
     kw = dict(alpha=0.01, radial_order=8, big_delta=big, small_delta=small, device=device)
-    for _ in range(args.warmup):
+    for _ in range(min(args.warmup, 1)):  # each step is a second of work
         out = shore_fit_graddev(St, bvals, bvecs, Tt, Kt, **kw)
     steps = max(1, min(args.steps, 3))
     torch.cuda.synchronize(device)
@@ -686,7 +799,7 @@ def graddev_block(args, device: int, world: int) -> dict:
     ms = max_over_ranks(e0.elapsed_time(e1) / steps, world, torch.device("cuda", device))
     return {"metric": "per-voxel-design L1-fit voxels/s", "value": world * GRADDEV_VOXELS / (ms * 1e-3),
             "unit": "voxels/s", "ms_per_step": ms, "steps": steps,
-            "workload": f"graddev100k: {GRADDEV_VOXELS} voxels, radial order 8 (K = 145), N = {S.shape[1]}, "
+            "workload": f"graddev300k: {GRADDEV_VOXELS} voxels, radial order 8 (K = 145), N = {S.shape[1]}, "
                         "deviation tensor and 0-15 % dropped samples per voxel",
             "dtype": "f64", "iterations_per_voxel": float(out["iterations"].double().mean())}
 
@@ -811,11 +924,24 @@ PROFILE_CASES = {"graddev2k": case_graddev2k, "diff50k": case_diff50k, "peaks108
                  "fista125k": case_fista125k, "kkt64k": case_kkt64k}
 
 
+def launch_ranks(args) -> int:
+    """`--gpus N` without a launcher: run this script under torchrun with N
+    ranks on this node (rendezvous on 127.0.0.1); rank 0 prints the line."""
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve()), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
     if args.profile_case:
         PROFILE_CASES[args.profile_case]()
         return 0
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args)
     select_workload(args.workload)
     if args.impl == "reference":
         return run_reference(args)

@@ -264,6 +264,17 @@ def handle(device: int = 0) -> C.c_void_p:
     return h
 
 
+def reset_handle(device: int = 0) -> None:
+    """Destroy the process-wide handle of `device`: the next call creates a
+    new one and pays the per-table set-up, the autotuning and the buffer
+    allocations again (a cold start)."""
+    lib = load()
+    with _lock:
+        h = _handles.pop(device, None)
+    if h is not None and h.value:
+        lib.csd_destroy(h)
+
+
 def default_spec() -> Spec:
     s = Spec()
     load().csd_default_spec(C.byref(s))

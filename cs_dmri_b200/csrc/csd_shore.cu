@@ -30,6 +30,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/csd_shore.h"
@@ -263,6 +264,10 @@ struct csd_handle {
     // k_rhs_dmma holds up to 9 samples per lane (N_pad <= 288)
     return (kp == 8 || kp == 32 || kp == 72) && np <= 288 && bytes <= static_cast<size_t>(smem_optin);
   }
+  // Tikhonov solution operator P = H^-1 M^T in DMMA fragment order (as
+  // mtfrag), so an L2 fit is the single product c = P s; built with the factor
+  DevBuf pfrag, ptmp;
+  bool pfrag_valid = false;
   DevBuf mom;      // Nesterov momentum table (t_k - 1) / t_{k+1}
   int mom_len = 0;
   // amplitude-ICLS setup: constraint C (m x K), factor of M^T M + eps I, W = L^{-1} C^T
@@ -322,8 +327,12 @@ struct csd_handle {
   // tuning options (csd_set_option); -1 / 0 = default
   int opt_shape = 0;
   int opt_schedule = -1;
-  int opt_kkt_iters = 64;
+  int opt_kkt_iters = 32;
   int opt_kkt_rounds = 48;
+  // page-locked, mapped staging volume for pageable host inputs: the masked
+  // rows are gathered into it on host threads and read in place by the device
+  float* stage = nullptr;
+  size_t stage_bytes = 0;
   unsigned long long opt_wait_ns = 2000000000ull;  // tensor-core completion waits
   unsigned long long kkt_batches = 0, kkt_fallback = 0, kkt_rounds = 0, kkt_uncertified = 0, kkt_iter_add = 0;
   double kkt_max = 0.0;
@@ -366,6 +375,7 @@ void set_err(char* err, size_t len, const std::string& msg) {
 }
 
 void autotune_fista(csd_handle* h);
+void launch_tikhonov(csd_handle* h, const double* B, double* X, int64_t V);
 
 // Build (or reuse) the per-gradient-table device setup.
 void ensure_setup(csd_handle* h, const HostGtab& g, int radial_order, double zeta, bool need_chol,
@@ -382,6 +392,7 @@ void ensure_setup(csd_handle* h, const HostGtab& g, int radial_order, double zet
   if (!(h->setup_valid && h->setup_key == key)) {
     h->setup_valid = false;
     h->chol_valid = false;
+    h->pfrag_valid = false;
     h->icls_valid = false;
     h->N = N;
     h->K = K;
@@ -475,6 +486,22 @@ void ensure_setup(csd_handle* h, const HostGtab& g, int radial_order, double zet
       if (!okv) throw Error{CSD_ERR_NUMERICAL, "normal-equations matrix should be PD"};
       h->chol_key = ck;
       h->chol_valid = true;
+      // P^T = rows H^-1 m_n of the design rows m_n, by the factor's solves,
+      // then packed like M^T for the right-hand-side kernel
+      h->pfrag_valid = false;
+      if (h->dmma_rhs) {
+        h->ptmp.ensure(2 * sizeof(double) * static_cast<size_t>(N) * Kp);
+        double* mpad = h->ptmp.as<double>();
+        double* pt = mpad + static_cast<size_t>(N) * Kp;
+        csd::k_pad_rows<<<(N * Kp + 255) / 256, 256, 0, st>>>(h->M.as<double>(), N, K, Kp, mpad);
+        CSD_LAUNCH();
+        launch_tikhonov(h, mpad, pt, N);
+        h->pfrag.ensure(sizeof(double) * static_cast<size_t>(h->Np) * Kp);
+        csd::k_pack_afrag<<<(h->Np * Kp + 255) / 256, 256, 0, st>>>(pt, N, K, Kp, 1, Kp, h->Np,
+                                                                    h->pfrag.as<double>());
+        CSD_LAUNCH();
+        h->pfrag_valid = true;
+      }
     }
   }
 }
@@ -1094,26 +1121,33 @@ void launch_rhs_t(csd_handle* h, const float* d_data, int64_t V) {
 }
 
 template <int KP>
-void launch_rhs_dmma_t(csd_handle* h, const float* d_data, int64_t V, float* sig_out) {
+void launch_rhs_dmma_t(csd_handle* h, const float* d_data, int64_t V, float* sig_out, const double* frag,
+                       double* out) {
   const size_t smem = sizeof(double) * static_cast<size_t>(h->Np) * KP + sizeof(float) * 8 * 8 * (h->Np + 4);
   CSD_CUDA(cudaFuncSetAttribute(csd::k_rhs_dmma<KP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(smem)));
   const int64_t groups = (V + 7) / 8;
   const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(h->num_sms, (groups + 7) / 8)));
-  csd::k_rhs_dmma<KP><<<blocks, 256, smem, h->stream>>>(d_data, h->vox.as<int64_t>(), V, h->N, h->Np,
-                                                        h->mtfrag.as<double>(), h->B.as<double>(), sig_out);
+  csd::k_rhs_dmma<KP><<<blocks, 256, smem, h->stream>>>(d_data, h->vox.as<int64_t>(), V, h->N, h->Np, frag, out,
+                                                        sig_out);
   CSD_LAUNCH();
 }
 
-void launch_rhs(csd_handle* h, const float* d_data, int64_t V, float* sig_out = nullptr) {
+// b = M^T s for every masked voxel into h->B; or, with `frag` / `out` set (the
+// packed Tikhonov operator, DMMA path only), c = P s into `out`.
+void launch_rhs(csd_handle* h, const float* d_data, int64_t V, float* sig_out = nullptr,
+                const double* frag = nullptr, double* out = nullptr) {
   if (h->dmma_rhs) {
+    const double* f = frag ? frag : h->mtfrag.as<double>();
+    double* o = out ? out : h->B.as<double>();
     switch (h->Kp) {
-      case 8: launch_rhs_dmma_t<8>(h, d_data, V, sig_out); return;
-      case 32: launch_rhs_dmma_t<32>(h, d_data, V, sig_out); return;
-      case 72: launch_rhs_dmma_t<72>(h, d_data, V, sig_out); return;
+      case 8: launch_rhs_dmma_t<8>(h, d_data, V, sig_out, f, o); return;
+      case 32: launch_rhs_dmma_t<32>(h, d_data, V, sig_out, f, o); return;
+      case 72: launch_rhs_dmma_t<72>(h, d_data, V, sig_out, f, o); return;
       default: break;
     }
   }
+  if (frag) throw Error{CSD_ERR_INVALID, "the Tikhonov operator product needs the DMMA right-hand-side kernel"};
   switch (h->Kp) {
     case 8: launch_rhs_t<8>(h, d_data, V); break;
     case 32: launch_rhs_t<32>(h, d_data, V); break;
@@ -1485,14 +1519,18 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   h->nnz_v.ensure(sizeof(int) * V);
   CSD_CUDA(cudaMemsetAsync(h->itotal.p, 0, 3 * sizeof(unsigned long long), st));
 
+  // Tikhonov with the DMMA product: c = P s directly into X (no b)
+  const bool l2_operator = spec->regularization == CSD_REG_L2 && h->dmma_rhs && h->pfrag_valid;
+  const double* rhs_frag = l2_operator ? h->pfrag.as<double>() : nullptr;
+  double* rhs_out = l2_operator ? h->X.as<double>() : nullptr;
   if (data_on_host) {
     // `d_data` aliases pinned host memory: read each masked row once over the
     // bus and keep a compact device copy for every later pass.
     h->sig.ensure(sizeof(float) * static_cast<size_t>(V) * N);
-    launch_rhs(h, d_data, V, h->sig.as<float>());
+    launch_rhs(h, d_data, V, h->sig.as<float>(), rhs_frag, rhs_out);
     h->sig_compact = h->sig.as<float>();
   } else {
-    launch_rhs(h, d_data, V);
+    launch_rhs(h, d_data, V, nullptr, rhs_frag, rhs_out);
   }
   record(h, 2);
 
@@ -1573,7 +1611,7 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   } else if (spec->regularization == CSD_REG_L2) {
     kind = 2;
     record(h, 6);
-    launch_tikhonov(h, h->B.as<double>(), h->X.as<double>(), V);
+    if (!l2_operator) launch_tikhonov(h, h->B.as<double>(), h->X.as<double>(), V);
     record(h, 7);
     it_final = nullptr;
     CSD_CUDA(cudaMemsetAsync(h->conv.p, 1, V, st));
@@ -2155,10 +2193,41 @@ void csd_destroy(csd_handle* h) {
     if (e) cudaEventDestroy(e);
   for (auto& e : h->kev)
     if (e) cudaEventDestroy(e);
+  if (h->stage) cudaFreeHost(h->stage);
   for (auto s : h->pipe)
     if (s) cudaStreamDestroy(s);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
+}
+
+// Masked rows of a pageable (X, Y, Z, N) volume copied into the handle's
+// page-locked, mapped staging volume of the same shape, on up to 16 host
+// threads (each takes a contiguous range of voxels); returns the staging
+// volume's device address.
+static const float* stage_masked_rows(csd_handle* h, const float* data, const uint8_t* mask, int64_t nvol, int N) {
+  const size_t bytes = sizeof(float) * static_cast<size_t>(nvol) * N;
+  if (h->stage_bytes < bytes) {
+    if (h->stage) CSD_CUDA(cudaFreeHost(h->stage));
+    h->stage = nullptr;
+    h->stage_bytes = 0;
+    void* p = nullptr;
+    CSD_CUDA(cudaHostAlloc(&p, bytes, cudaHostAllocMapped | cudaHostAllocPortable));
+    h->stage = static_cast<float*>(p);
+    h->stage_bytes = bytes;
+  }
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int64_t T = std::min<int64_t>(std::min<unsigned>(hw, 16u), std::max<int64_t>(1, nvol / 4096));
+  auto copy_range = [&](int64_t lo, int64_t hi) {
+    for (int64_t v = lo; v < hi; ++v)
+      if (mask[v]) std::memcpy(h->stage + v * N, data + v * N, sizeof(float) * N);
+  };
+  std::vector<std::thread> pool;
+  for (int64_t t = 1; t < T; ++t) pool.emplace_back(copy_range, nvol * t / T, nvol * (t + 1) / T);
+  copy_range(0, nvol / T);
+  for (auto& th : pool) th.join();
+  void* dp = nullptr;
+  CSD_CUDA(cudaHostGetDevicePointer(&dp, h->stage, 0));
+  return static_cast<const float*>(dp);
 }
 
 static int check_common(csd_handle* h, const void* data, const void* mask, int64_t X, int64_t Y, int64_t Z,
@@ -2240,6 +2309,14 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
         on_host = true;
       }
       cudaGetLastError();  // a pageable pointer may leave an error code behind
+    }
+    if (!on_host && h->dmma_rhs_possible(N, K)) {
+      // A pageable volume: its masked rows are gathered on host threads into
+      // the handle's page-locked staging volume, which the device then reads
+      // in place like a page-locked input (masked rows only; the other rows
+      // of the staging volume are never read).
+      d_data = stage_masked_rows(h, data, mask, nvol, N);
+      on_host = true;
     }
     if (!on_host) {
       h->data.ensure(sizeof(float) * static_cast<size_t>(nvol) * N);

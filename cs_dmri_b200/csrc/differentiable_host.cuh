@@ -39,7 +39,10 @@ void run_fit_batch(csd_handle* h, const float* d_sig, int64_t V, const HostGtab&
   h->queue.ensure(sizeof(unsigned long long));
   csd::k_iota<<<grid1(V), 256, 0, st>>>(h->vox.as<int64_t>(), V);
   CSD_LAUNCH();
-  launch_rhs(h, d_sig, V);
+  // Tikhonov with the DMMA product c = P s, as the volume fit does
+  const bool l2_operator = !is_l1 && h->dmma_rhs && h->pfrag_valid;
+  launch_rhs(h, d_sig, V, nullptr, l2_operator ? h->pfrag.as<double>() : nullptr,
+             l2_operator ? h->X.as<double>() : nullptr);
   if (is_l1) {
     ensure_mom(h, spec->max_iter);
     if (d_warm) {
@@ -75,7 +78,7 @@ void run_fit_batch(csd_handle* h, const float* d_sig, int64_t V, const HostGtab&
     if (d_iters)
       CSD_CUDA(cudaMemcpyAsync(d_iters, h->iters.p, sizeof(uint32_t) * V, cudaMemcpyDeviceToDevice, st));
   } else {
-    launch_tikhonov(h, h->B.as<double>(), h->X.as<double>(), V);
+    if (!l2_operator) launch_tikhonov(h, h->B.as<double>(), h->X.as<double>(), V);
     if (d_iters) {
       csd::k_fill_u32<<<grid1(V), 256, 0, st>>>(d_iters, V, 1u);
       CSD_LAUNCH();

@@ -211,4 +211,12 @@ __global__ void k_pack_gfrag(const double* __restrict__ G, int Kp, double* __res
   frag[idx] = G[(8 * mt + lane / 4) * Kp + 4 * kt + (lane & 3)];
 }
 
+// Rows of an N x K matrix copied into N x Kp rows with zero padding.
+__global__ void k_pad_rows(const double* __restrict__ src, int N, int K, int Kp, double* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N * Kp) return;
+  const int r = i / Kp, c = i % Kp;
+  dst[i] = c < K ? src[r * K + c] : 0.0;
+}
+
 }  // namespace csd

@@ -5,9 +5,12 @@ the solve: rank r fits a contiguous chunk of the masked voxels (canonical
 x-y-z order, src/voxel_loop.rs:28-42) on its own GPU.  Two collectives
 assemble the result, both outside the solve:
 
-* the coefficient volumes and maps are sum-reduced to the destination rank -
-  every rank's output is exactly zero outside its own shard, so the sum is the
-  single-GPU result bit for bit;
+* each rank's rows - the coefficients and diagnostic values of its own
+  masked voxels, V_r x (K + maps) - are gathered to the destination rank,
+  which places them into the volume by the mask (the shards are contiguous
+  runs of the canonical order, so the rows arrive in order); the result is
+  the single-GPU result bit for bit, and only V x (K + maps) values cross the
+  interconnect, not world x the volume;
 * the per-voxel alphas are gathered so the alpha distribution (median, p10,
   p90 by nearest rank, src/fit.rs:334-352) is taken over the whole mask.
 
@@ -19,6 +22,14 @@ from __future__ import annotations
 import numpy as np
 
 __all__ = ["shard_mask", "fit_sharded", "alpha_distribution"]
+
+
+def _torch_dtype(dt: np.dtype):
+    import torch
+    return {np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64,
+            np.dtype(np.uint32): torch.int64, np.dtype(np.uint8): torch.uint8,
+            np.dtype(np.int32): torch.int32, np.dtype(np.int64): torch.int64}[np.dtype(dt)]
+
 
 _MAPS = ("r2", "rmse", "residual_l2", "iterations", "regularization_kind", "alpha", "bic", "rss_l2")
 
@@ -75,19 +86,37 @@ def fit_sharded(data, bvals, bvecs, mask, *, group=None, dst: int = 0, fit_fn=No
     out = fit_fn(data, bvals, bvecs, local, **dict(kw, diagnostics=diag or per_voxel_alpha))
     backend = dist.get_backend(group)
     dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+    sel = local.ravel()
+    counts_all = [int(shard_mask(mask, r, world).sum()) for r in range(world)]  # the same on every rank
+    n_max = max(1, max(counts_all))
 
-    def reduce_array(a: np.ndarray) -> np.ndarray:
-        t = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
-        if t.dtype in (torch.uint8, torch.uint32):  # one non-zero shard per voxel: the sum stays in range
-            t = t.to(torch.int64)
-        dist.reduce(t, dst=dst, op=dist.ReduceOp.SUM, group=group)
-        return t.cpu().numpy().astype(a.dtype, copy=False)
+    def gather_rows(a: np.ndarray, width: int) -> np.ndarray | None:
+        """This rank's masked rows of `a` (flattened to (voxels, width)),
+        gathered on `dst` in rank order: (V, width), or None elsewhere."""
+        rows = np.asarray(a).reshape(-1, width)[sel]
+        buf = torch.zeros((n_max, width), dtype=_torch_dtype(rows.dtype), device=dev)
+        send = rows.astype(np.int64) if rows.dtype == np.uint32 else rows  # no uint32 collectives
+        buf[: rows.shape[0]] = torch.from_numpy(np.ascontiguousarray(send)).to(dev)
+        parts = [torch.empty_like(buf) for _ in range(world)] if rank == dst else None
+        dist.gather(buf, gather_list=parts, dst=dst, group=group)
+        if rank != dst:
+            return None
+        return np.concatenate([p[:c].cpu().numpy() for p, c in zip(parts, counts_all)]).astype(rows.dtype, copy=False)
 
-    result = {"coefficients": reduce_array(out["coefficients"])}
+    def place(rows: np.ndarray | None, like: np.ndarray) -> np.ndarray | None:
+        if rows is None:
+            return None
+        full = np.zeros_like(like)
+        flat = full.reshape(len(sel), -1)
+        flat[np.asarray(mask, dtype=bool).ravel()] = rows.reshape(rows.shape[0], -1)
+        return full
+
+    K = out["coefficients"].shape[-1]
+    result = {"coefficients": place(gather_rows(out["coefficients"], K), out["coefficients"])}
     if diag:
         for k in _MAPS:
             if out.get(k) is not None:
-                result[k] = reduce_array(out[k])
+                result[k] = place(gather_rows(out[k], 1), out[k])
     counts = torch.tensor([out.get("total_iterations", 0), out.get("n_voxels", int(local.sum()))],
                           dtype=torch.int64, device=dev)
     dist.all_reduce(counts, op=dist.ReduceOp.SUM, group=group)

@@ -87,7 +87,7 @@ enum csd_precision {
    * witness of the reference's tests/common/mod.rs:127-153), instead of the
    * iterate the reference's stopping rule leaves (fista.rs:120-127), which
    * sits a relative 1e-5 .. 1e-2 from it.  A fixed number of FISTA
-   * iterations (csd_set_option CSD_OPT_KKT_ITERATIONS, default 64) finds
+   * iterations (csd_set_option CSD_OPT_KKT_ITERATIONS, default 32) finds
    * the support; an FP64 active-set polish (Lawson-Hanson style, with signs
    * in place of non-negativity) solves G_SS c_S = b_S - n alpha sign(c_S) on
    * it, moving coefficients in and out until no sign disagrees and every
@@ -267,7 +267,7 @@ int csd_last_timing(const csd_handle* h, csd_fit_timing* out);
  *                           pass' end, default 80)
  *   CSD_OPT_KKT_ITERATIONS  FISTA iterations of the converged-optimum
  *                           modes' support identification (1 .. 100000,
- *                           default 64)
+ *                           default 32)
  *   CSD_OPT_KKT_ROUNDS      solves the first polish of the converged-optimum
  *                           modes may take per voxel before the voxel goes
  *                           to the FP64 FISTA fallback (1 .. 4096, default 48)

@@ -15,7 +15,8 @@ configurations themselves:
   - the mixed-precision device fit,
   - Tikhonov (lambda_n = lambda_l = 0.05) and the amplitude-positivity QP
     on the same sample;
-* per-voxel designs at radial order 8 on 1,024 voxels.
+* per-voxel designs at radial order 8 on 1,024 voxels: coefficients, and
+  the RTOP and GFA computed from them.
 
 Tolerances are the parity bounds of the FP64 path: per-voxel coefficient
 relative L2 <= 1e-5 for L1 (a stopping decision within rounding of tol may
@@ -281,3 +282,16 @@ def test_graddev_order8_per_voxel(oracle):
     np.testing.assert_allclose(lip, wl, rtol=1e-12)
     check_l1(c, want, "graddev order 8")
     assert np.abs(it - wit).max() <= 1 and np.mean(it == wit) >= 0.99
+    # the outputs derived from the coefficients: RTOP (GPU map kernel on the
+    # GPU fit, the oracle's on the oracle fit) and GFA (GPU ODF sampling
+    # against the oracle's), each within the coefficients' 1e-5
+    from cs_dmri_b200 import shore_microstructure, shore_odf_peaks
+    vol_g = c.astype(np.float32).reshape(V, 1, 1, -1)
+    vol_o = want.astype(np.float32).reshape(V, 1, 1, -1)
+    m = np.ones((V, 1, 1), bool)
+    rt_g = shore_microstructure(vol_g, 8, 700.0, m, outlier_factor=None)["rtop"].ravel()
+    rt_o = oracle.shore_microstructure(vol_o, 8, 700.0, m, outlier_factor=None)["rtop"].ravel()
+    np.testing.assert_allclose(rt_g, rt_o, rtol=1e-5, atol=1e-6 * np.abs(rt_o).max())
+    gfa_g = shore_odf_peaks(vol_g[:256], 8, 700.0)["gfa"].ravel()
+    gfa_o = np.array([oracle.odf_peaks(w, 8, 700.0)[0] for w in want[:256]])
+    np.testing.assert_allclose(gfa_g, gfa_o, rtol=1e-5, atol=1e-6)

@@ -30,7 +30,7 @@ def kkt_iterations(k):
     try:
         yield
     finally:
-        _abi.set_option(_abi.OPT_KKT_ITERATIONS, 64)
+        _abi.set_option(_abi.OPT_KKT_ITERATIONS, 32)
 
 
 @pytest.fixture(scope="module")
