@@ -78,7 +78,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--profile-case", choices=["graddev2k", "diff50k", "peaks108k", "fista125k", "kkt64k"],
+    ap.add_argument("--profile-case", choices=["graddev2k", "diff50k", "peaks108k", "fista125k", "kkt64k",
+                                               "icls64k", "tikhonov64k"],
                     help="run one small profiling workload instead of the benchmark")
     ap.add_argument("--workload", choices=["brain300k", "grid64k"], default="brain300k",
                     help="brain300k: the benchmark volume; grid64k: 40^3 fully masked (profiling case)")
@@ -427,6 +428,7 @@ def run_ours(args):
                   device=device, precision=path, **kw)
         if i >= args.warmup:
             pg_t.append(time.perf_counter() - t)
+    pg_host = _abi.last_timing(device)
     pg_s = max_over_ranks(sum(pg_t), world, torch.device("cuda", device))
     cold_t = []
     for _ in range(2):
@@ -440,7 +442,9 @@ def run_ours(args):
     cold_s = max_over_ranks(statistics.median(cold_t), world, torch.device("cuda", device))
     e2e_variants = {"pageable": {"value": world * V * args.steps / pg_s, "unit": "voxels/s",
                                  "ms_per_step": 1e3 * pg_s / args.steps,
-                                 "input": "pageable numpy volume, new output array each call"},
+                                 "input": "pageable numpy volume, new output array each call",
+                                 "ms_host_gather": pg_host.ms_host_gather,
+                                 "ms_host_copy_out": pg_host.ms_host_copy_out},
                     "cold": {"value": world * V / cold_s, "unit": "voxels/s", "ms_per_step": 1e3 * cold_s,
                              "input": "pageable numpy volume on a new library handle (set-up, autotuning and "
                                       "allocations included), median of 2"}}
@@ -773,35 +777,50 @@ def fwd_bwd_block(args, device: int, world: int) -> dict:
 def graddev_block(args, device: int, world: int) -> dict:
     """L1 fit on a design per voxel: 300,000 voxels of the phantom, each with
     its own gradient-deviation tensor (I + N(0, 0.02)) and 0-15 % of its
-    samples dropped, radial order 8 (K = 145), alpha 0.01, the reference's
-    FISTA.  CUDA events on the fit stream, max over ranks; min(steps, 3)
-    timed steps (each builds 300k Gram matrices of 145 x 145)."""
+    samples dropped, radial order 8 (K = 145), alpha 0.01: the reference's
+    FISTA (`value`), and the certified optimum of each voxel's design
+    (precision "fp64-kkt": 32 FISTA iterations, the polish on the voxel's own
+    Gram matrix, the KKT certificate).  CUDA events on the fit stream, max
+    over ranks; min(steps, 3) timed steps (each builds 300k Gram matrices of
+    145 x 145)."""
     import torch
 
+    from cs_dmri_b200 import _abi
     from cs_dmri_b200.graddev import graddev_phantom, shore_fit_graddev
 
     S, bvals, bvecs, T, keep, big, small = graddev_phantom(GRADDEV_VOXELS, seed=3)
     dev = f"cuda:{device}"
     St, Tt, Kt = (torch.from_numpy(a).to(dev) for a in (S, T, keep))
-    kw = dict(alpha=0.01, radial_order=8, big_delta=big, small_delta=small, device=device)
-    for _ in range(min(args.warmup, 1)):  # each step is a second of work
-        out = shore_fit_graddev(St, bvals, bvecs, Tt, Kt, **kw)
     steps = max(1, min(args.steps, 3))
-    torch.cuda.synchronize(device)
-    barrier(world)
-    st = torch.cuda.current_stream(device)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    for _ in range(steps):
-        out = shore_fit_graddev(St, bvals, bvecs, Tt, Kt, **kw)
-    e1.record(st)
-    torch.cuda.synchronize(device)
-    ms = max_over_ranks(e0.elapsed_time(e1) / steps, world, torch.device("cuda", device))
+
+    def timed(precision):
+        kw = dict(alpha=0.01, radial_order=8, big_delta=big, small_delta=small, device=device, precision=precision)
+        out = shore_fit_graddev(St, bvals, bvecs, Tt, Kt, **kw)  # one untimed fit: each is a second of work
+        torch.cuda.synchronize(device)
+        barrier(world)
+        st = torch.cuda.current_stream(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            out = shore_fit_graddev(St, bvals, bvecs, Tt, Kt, **kw)
+        e1.record(st)
+        torch.cuda.synchronize(device)
+        return max_over_ranks(e0.elapsed_time(e1) / steps, world, torch.device("cuda", device)), out
+
+    ms, out = timed("fp64")
+    it = float(out["iterations"].double().mean())
+    ms_k, out_k = timed("fp64-kkt")
+    t = _abi.last_timing(device)
     return {"metric": "per-voxel-design L1-fit voxels/s", "value": world * GRADDEV_VOXELS / (ms * 1e-3),
             "unit": "voxels/s", "ms_per_step": ms, "steps": steps,
             "workload": f"graddev300k: {GRADDEV_VOXELS} voxels, radial order 8 (K = 145), N = {S.shape[1]}, "
                         "deviation tensor and 0-15 % dropped samples per voxel",
-            "dtype": "f64", "iterations_per_voxel": float(out["iterations"].double().mean())}
+            "dtype": "f64", "iterations_per_voxel": it,
+            "kkt": {"value": world * GRADDEV_VOXELS / (ms_k * 1e-3), "ms_per_step": ms_k,
+                    "speedup_vs_reference_rule": ms / ms_k, "uncertified_voxels": t.kkt_uncertified,
+                    "polish_rounds_per_voxel": t.kkt_rounds / GRADDEV_VOXELS,
+                    "support_iterations": t.kkt_iterations,
+                    "certified_fraction": float(out_k["converged"].double().mean())}}
 
 
 def pipeline_block(ph, device: int, world: int) -> dict:
@@ -900,8 +919,8 @@ def case_fista125k() -> None:
 def case_kkt64k() -> None:
     """The converged-optimum fit (precision "mixed-kkt") of the 40^3 phantom
     (64,000 voxels, K = 72) through the device entry point: one launch each of
-    k_fista_tf32 and k_l1_polish per fit.  A first fit (set-up) runs before
-    the measured one."""
+    k_fista_tf32, k_l1_polish_tpv and the two k_l1_polish passes per fit.  A
+    first fit (set-up) runs before the measured one."""
     import torch
 
     from cs_dmri_b200 import _abi
@@ -920,8 +939,40 @@ def case_kkt64k() -> None:
           f"fallback voxels {t.kkt_fallback_voxels}, uncertified {t.kkt_uncertified}")
 
 
+def _case_grid64k(name: str, **fit_kw) -> None:
+    """One fit of the 40^3 phantom (64,000 voxels, K = 72) through the device
+    entry point after a set-up fit of the same kind."""
+    import torch
+
+    from cs_dmri_b200 import _abi
+    from cs_dmri_b200._core import shore_fit_device
+    from cs_dmri_b200.phantom import config_phantom
+    ph = config_phantom("grid64k")
+    d = torch.from_numpy(ph.data).cuda()
+    m = torch.from_numpy(ph.mask).cuda()
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, **fit_kw)
+    shore_fit_device(d, m, ph.bvals, ph.bvecs, **kw)
+    shore_fit_device(d, m, ph.bvals, ph.bvecs, **kw)
+    torch.cuda.synchronize()
+    t = _abi.last_timing(0)
+    print(f"{name}: solve kernel {t.ms_solve_kernel:.3f} ms, right-hand side {t.ms_rhs:.3f} ms, "
+          f"total {t.ms_total:.3f} ms")
+
+
+def case_icls64k() -> None:
+    """The amplitude-positivity QP (k_icls) on the 40^3 phantom."""
+    _case_grid64k("icls64k", regularization="nonneg")
+
+
+def case_tikhonov64k() -> None:
+    """The Tikhonov fit (lambda_n = lambda_l = 0.05): one k_rhs_dmma launch
+    with the solution operator on the 40^3 phantom."""
+    _case_grid64k("tikhonov64k", regularization="l2", lambda_n=0.05, lambda_l=0.05)
+
+
 PROFILE_CASES = {"graddev2k": case_graddev2k, "diff50k": case_diff50k, "peaks108k": case_peaks108k,
-                 "fista125k": case_fista125k, "kkt64k": case_kkt64k}
+                 "fista125k": case_fista125k, "kkt64k": case_kkt64k, "icls64k": case_icls64k,
+                 "tikhonov64k": case_tikhonov64k}
 
 
 def launch_ranks(args) -> int:

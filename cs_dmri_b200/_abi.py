@@ -110,6 +110,11 @@ class Timing(C.Structure):
         ("kkt_rounds", C.c_uint64),
         ("tf32_tensor_flops", C.c_double),
         ("kkt_max", C.c_double),
+        ("ms_host_gather", C.c_float),
+        ("ms_host_copy_out", C.c_float),
+        ("kkt_iterations", C.c_int32),
+        ("kkt_tune_ms", C.c_float * 4),
+        ("kkt_overflow", C.c_int64 * 2),
     ]
 
 
@@ -119,6 +124,8 @@ OPT_FISTA_SCHEDULE = 2
 OPT_KKT_ITERATIONS = 3
 OPT_TENSOR_WAIT_NS = 4
 OPT_KKT_ROUNDS = 5
+OPT_POLISH = 6
+OPT_ICLS = 7
 
 
 # Every symbol include/csd_shore.h declares, for load checks.

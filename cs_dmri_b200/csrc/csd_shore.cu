@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <map>
 #include <set>
@@ -275,6 +276,11 @@ struct csd_handle {
   uint64_t icls_key = 0;
   int icls_m = 0, icls_m_pad = 0, icls_lmax = 0, icls_qmax = 0;
   DevBuf dirs, Cmat, Le, Wi, Q1, ovf;
+  // Gram form of the amplitude ICLS (active sets <= 32): W^T W, W^T, C = Y P
+  DevBuf icls_gam, icls_wt, icls_y, icls_pf, icls_jcol;
+  bool icls_gram = false;  // the Gram-form kernel serves this table
+  int icls_nsh = 0;
+  int opt_icls = 0;        // 0 = Gram form where it applies, 1 = the Q1 form
   // int8 digit planes of G for the mixed-precision FISTA (radial order 6)
   DevBuf gdig, gfexp;
   int precision = CSD_PRECISION_FP64;  // precision of the current fit
@@ -314,27 +320,37 @@ struct csd_handle {
   int fista_warps = 0;
   float tune_ms[2] = {0.f, 0.f};
   std::map<uint64_t, std::array<float, 3>> tune_cache;  // table key -> (warps, ms12, ms16)
+  // converged-optimum modes: the support-identification iteration count the
+  // autotuner chose per (table, mode), and its candidates' batch times
+  std::map<uint64_t, std::array<float, 5>> kkt_tune_cache;  // -> (iterations, ms at 16, 24, 32, 48)
+  int kkt_iters_used = 0;
+  float kkt_tune_ms[4] = {0.f, 0.f, 0.f, 0.f};
+  bool kkt_tuning = false;
   DevBuf tuneB, tuneX, tuneIt, tuneConv, tuneQ;
   double mixed_ms = 0.0, mixed_ops = 0.0;
   unsigned long long mixed_rerun = 0;
   // converged-optimum modes: the TF32 B operand (per table), the iterate,
   // per-voxel KKT residuals, overflow / failure lists, counters
   // [batches, error, n_overflow, n_failed, rounds, kkt max bits, n_failed2]
-  DevBuf gtf32, x32, kktv, kktovf, kktfail, kktstat;
+  DevBuf gtf32, x32, kktv, kktovf, kktovf2, kktfail, kktstat;
   uint64_t gtf32_key = 0;
   bool gtf32_valid = false;
   cudaEvent_t kev[5] = {};
   // tuning options (csd_set_option); -1 / 0 = default
   int opt_shape = 0;
   int opt_schedule = -1;
-  int opt_kkt_iters = 32;
+  int opt_kkt_iters = 0;  // 0: the autotuner's choice per table
   int opt_kkt_rounds = 48;
+  int opt_polish = 0;  // first polish pass: 0 = thread per voxel, 1 = warp per voxel
   // page-locked, mapped staging volume for pageable host inputs: the masked
   // rows are gathered into it on host threads and read in place by the device
   float* stage = nullptr;
   size_t stage_bytes = 0;
+  float* ostage = nullptr;  // page-locked output volume for pageable outputs of the pipelined fit
+  size_t ostage_bytes = 0;
   unsigned long long opt_wait_ns = 2000000000ull;  // tensor-core completion waits
   unsigned long long kkt_batches = 0, kkt_fallback = 0, kkt_rounds = 0, kkt_uncertified = 0, kkt_iter_add = 0;
+  unsigned long long kkt_overflow[2] = {0, 0};
   double kkt_max = 0.0;
   float kkt_ms[3] = {0.f, 0.f, 0.f};  // iterate, first polish, fallback (FISTA + last polish)
   float kkt_ms_last_polish = 0.f;
@@ -369,6 +385,31 @@ struct HandleOrder {
   HandleOrder(const HandleOrder&) = delete;
   HandleOrder& operator=(const HandleOrder&) = delete;
 };
+
+// A page-locked, mapped host buffer of at least `bytes`, kept across calls.
+static float* ensure_pinned(float*& buf, size_t& cap, size_t bytes) {
+  if (cap < bytes) {
+    if (buf) CSD_CUDA(cudaFreeHost(buf));
+    buf = nullptr;
+    cap = 0;
+    void* p = nullptr;
+    CSD_CUDA(cudaHostAlloc(&p, bytes, cudaHostAllocMapped | cudaHostAllocPortable));
+    buf = static_cast<float*>(p);
+    cap = bytes;
+  }
+  return buf;
+}
+
+// fn(lo, hi) over [0, n) split into contiguous ranges on up to 32 host threads.
+template <class F>
+static void host_parallel(int64_t n, int64_t grain, F fn) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int64_t T = std::min<int64_t>(std::min<unsigned>(hw, 32u), std::max<int64_t>(1, n / grain));
+  std::vector<std::thread> pool;
+  for (int64_t t = 1; t < T; ++t) pool.emplace_back(fn, n * t / T, n * (t + 1) / T);
+  fn(0, n / T);
+  for (auto& th : pool) th.join();
+}
 
 void set_err(char* err, size_t len, const std::string& msg) {
   if (err && len > 0) std::snprintf(err, len, "%s", msg.c_str());
@@ -506,6 +547,8 @@ void ensure_setup(csd_handle* h, const HostGtab& g, int radial_order, double zet
   }
 }
 
+constexpr int kIclsGramCpl = 11;  // constraint slots per lane of k_icls_gram (321 directions, m_pad 352)
+
 // Setup of the amplitude-positivity fit (src/solver/shore_icls.rs:41-71,
 // src/solver/icls.rs:183-222): constraint matrix on the hemisphere, Cholesky
 // factor of M^T M + eps I and W = L^{-1} C^T.  Cached per table and epsilon.
@@ -545,6 +588,27 @@ void ensure_icls_setup(csd_handle* h, int radial_order, double zeta, double eps)
   csd::k_icls_w<<<(m_pad + 127) / 128, 128, 0, st>>>(h->Le.as<double>(), K, Kp, h->Cmat.as<double>(), m, m_pad,
                                                       h->Wi.as<double>());
   CSD_LAUNCH();
+  // the Gram form: active sets one entry per lane (nsh <= 32), 11 constraint
+  // slots per lane (m_pad = 352), x~ in <= 3 registers per lane
+  h->icls_nsh = h->icls_qmax;
+  h->icls_gram = h->icls_nsh <= 32 && m_pad == 32 * kIclsGramCpl && Kp <= 96 &&
+                 csd::icls_gram_smem(h->icls_nsh, m_pad) <= static_cast<size_t>(h->smem_optin);
+  if (h->icls_gram) {
+    const int64_t n_set = static_cast<int64_t>(m_pad) * m_pad + static_cast<int64_t>(m_pad) * Kp;
+    h->icls_gam.ensure(sizeof(double) * static_cast<size_t>(m_pad) * m_pad);
+    h->icls_wt.ensure(sizeof(double) * static_cast<size_t>(m_pad) * Kp);
+    csd::k_icls_gram_setup<<<static_cast<unsigned>((n_set + 255) / 256), 256, 0, st>>>(
+        h->Wi.as<double>(), K, Kp, m_pad, h->icls_gam.as<double>(), h->icls_wt.as<double>());
+    CSD_LAUNCH();
+    const int ny = h->icls_nsh * m_pad;
+    h->icls_y.ensure(sizeof(double) * static_cast<size_t>(ny));
+    h->icls_pf.ensure(sizeof(double) * K);
+    h->icls_jcol.ensure(sizeof(int) * K);
+    csd::k_constraint_factors<<<(std::max(ny, K) + 255) / 256, 256, 0, st>>>(
+        h->dirs.as<double>(), m, m_pad, K, radial_order, lmax, zeta, h->icls_y.as<double>(),
+        h->icls_pf.as<double>(), h->icls_jcol.as<int>());
+    CSD_LAUNCH();
+  }
   h->icls_key = key;
   h->icls_valid = true;
 }
@@ -842,7 +906,6 @@ void launch_fista_mixed(csd_handle* h, const csd::FistaParams& p) {
 // the FP64 FISTA path with the reference stopping rule followed by a last
 // polish for the voxels the first polish could not certify.
 constexpr double kKktKappa = 1e-9;   // certificate: off-support |g_j| <= alpha (1 + kappa)
-constexpr int kKktRounds = 48;       // rounds of the first polish (default of CSD_OPT_KKT_ROUNDS)
 constexpr int kKktRoundsFallback = 64;
 constexpr int kPolishCap = 32;       // support held by the first polish's warp slice
 
@@ -906,16 +969,125 @@ void launch_polish(csd_handle* h, const csd::PolishParams& q, int warps, int64_t
   }
 }
 
+// The thread-per-voxel first polish: one CTA of kTpvWarps warps per SM (its
+// shared memory holds each lane's factor), lanes taking voxels from `queue`.
+template <int RPL>
+void launch_polish_tpv_t(csd_handle* h, const csd::PolishParams& q, unsigned long long* queue) {
+  const size_t smem = sizeof(double) * static_cast<size_t>(csd::kTpvWarps) * csd::kTpvWarpDoubles;
+  CSD_CUDA(cudaFuncSetAttribute(csd::k_l1_polish_tpv<RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)));
+  int per_sm = 0;
+  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_l1_polish_tpv<RPL>, 32 * csd::kTpvWarps,
+                                                         smem));
+  if (per_sm < 1) throw Error{CSD_ERR_CUDA, "thread-per-voxel polish: no CTA fits an SM"};
+  const int64_t lanes = 32 * csd::kTpvWarps;
+  const int blocks = static_cast<int>(std::max<int64_t>(
+      1, std::min<int64_t>(static_cast<int64_t>(h->num_sms) * per_sm, (std::max<int64_t>(q.n_work, 1) + lanes - 1) / lanes)));
+  CSD_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), h->stream));
+  csd::k_l1_polish_tpv<RPL><<<blocks, 32 * csd::kTpvWarps, smem, h->stream>>>(q, queue);
+  CSD_LAUNCH();
+}
+
+void launch_fista_kkt(csd_handle* h, int MT, const csd::FistaParams& p);
+
+// Autotuning of the converged-optimum modes' support-identification
+// iteration count, once per gradient table and mode: the whole path (its
+// iterations, the polish and any fallback) fits the FISTA autotuner's
+// synthetic batch (73,728 single-tensor voxels on the table's own b-values,
+// alpha 0.01) with 16, 24, 32 and 48 iterations, once untimed and once timed,
+// and the fastest count serves the table's fits.  Every count ends at the
+// certified optimum, so the choice changes the time, not the result.
+void autotune_kkt(csd_handle* h, int MT, bool non_negative) {
+  static constexpr int kCand[4] = {16, 24, 32, 48};
+  const uint64_t key = h->setup_key ^ (0x9E3779B97F4A7C15ull * (1 + h->precision + 4 * (non_negative ? 1 : 0)));
+  const auto hit = h->kkt_tune_cache.find(key);
+  if (hit != h->kkt_tune_cache.end()) {
+    h->kkt_iters_used = static_cast<int>(hit->second[0]);
+    for (int i = 0; i < 4; ++i) h->kkt_tune_ms[i] = hit->second[1 + i];
+    return;
+  }
+  h->kkt_tuning = true;
+  cudaStream_t st = h->stream;
+  const int64_t Vt = 73728;
+  const int Kp = h->Kp, N = h->N, K = h->K;
+  ensure_mom(h, kCand[3]);
+  h->tuneB.ensure(sizeof(double) * Vt * Kp);
+  h->tuneX.ensure(std::max(sizeof(double) * Vt * Kp, sizeof(float) * Vt * N));
+  h->tuneIt.ensure(sizeof(uint32_t) * Vt);
+  h->tuneConv.ensure(Vt);
+  h->tuneQ.ensure(sizeof(unsigned long long));
+  float* S = h->tuneX.as<float>();
+  csd::k_tune_signal<<<grid1(Vt * N), 256, 0, st>>>(h->bvals.as<double>(), h->bvecs.as<double>(), N, Vt, S);
+  CSD_LAUNCH();
+  csd::k_tune_rhs<<<grid1(Vt * Kp), 256, 0, st>>>(h->M.as<double>(), N, K, Kp, S, Vt, h->tuneB.as<double>());
+  CSD_LAUNCH();
+  csd::FistaParams q{};
+  q.gfrag = h->gfrag.as<double>();
+  q.B = h->tuneB.as<double>();
+  q.X = h->tuneX.as<double>();
+  q.iters = h->tuneIt.as<uint32_t>();
+  q.conv = h->tuneConv.as<uint8_t>();
+  q.V = Vt;
+  q.n_inv = 1.0 / static_cast<double>(N);
+  q.step = 1.0 / h->lipschitz;
+  q.thr = q.step * 0.01;
+  q.tol = 1e-6;
+  q.max_iter = 1000;
+  q.non_negative = non_negative ? 1 : 0;
+  q.queue = h->tuneQ.as<unsigned long long>();
+  q.n_work = Vt;
+  ensure_mom(h, q.max_iter);
+  const int saved = h->opt_kkt_iters;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CSD_CUDA(cudaEventCreate(&e0));
+  CSD_CUDA(cudaEventCreate(&e1));
+  float best = 0.f;
+  int best_k = 32;
+  for (int c = 0; c < 4; ++c) {
+    h->opt_kkt_iters = kCand[c];
+    float ms = 0.f;
+    for (int pass = 0; pass < 2; ++pass) {
+      CSD_CUDA(cudaEventRecord(e0, st));
+      launch_fista_kkt(h, MT, q);
+      CSD_CUDA(cudaEventRecord(e1, st));
+      CSD_CUDA(cudaEventSynchronize(e1));
+      if (pass == 1 && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) ms = 0.f;
+    }
+    h->kkt_tune_ms[c] = ms;
+    if (ms > 0.f && (best == 0.f || ms < best)) {
+      best = ms;
+      best_k = kCand[c];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->opt_kkt_iters = saved;
+  h->kkt_iters_used = best_k;
+  h->kkt_tuning = false;
+  h->kkt_tune_cache[key] = {static_cast<float>(best_k), h->kkt_tune_ms[0], h->kkt_tune_ms[1], h->kkt_tune_ms[2],
+                            h->kkt_tune_ms[3]};
+}
+
 void launch_fista_kkt(csd_handle* h, int MT, const csd::FistaParams& p) {
   cudaStream_t st = h->stream;
   const int K = h->K, Kp = h->Kp;
   const int64_t V = p.V;
-  const int k1 = h->opt_kkt_iters;
-  h->kktstat.ensure(8 * sizeof(unsigned long long));
+  if (h->opt_kkt_iters <= 0 && !h->kkt_tuning) {
+    autotune_kkt(h, MT, p.non_negative != 0);
+    h->kkt_ms[0] = h->kkt_ms[1] = h->kkt_ms[2] = 0.f;  // the tuning batch's time is not this fit's
+    h->kkt_iter_add = 0;
+  }
+  const int k1 = h->opt_kkt_iters > 0 ? h->opt_kkt_iters : h->kkt_iters_used;
+  // stat: [0] tensor batches, [1] tensor error, [2] first-pass overflows,
+  // [3] failures (the fallback's list), [4] rounds, [5] largest KKT residual
+  // (bits), [6] uncertified, [7] unused overflow count, [8] second-pass
+  // overflows
+  h->kktstat.ensure(10 * sizeof(unsigned long long));
   auto* stat = h->kktstat.as<unsigned long long>();
-  CSD_CUDA(cudaMemsetAsync(stat, 0, 8 * sizeof(unsigned long long), st));
+  CSD_CUDA(cudaMemsetAsync(stat, 0, 10 * sizeof(unsigned long long), st));
   h->kktv.ensure(sizeof(double) * std::max<int64_t>(V, 1));
   h->kktovf.ensure(sizeof(int64_t) * std::max<int64_t>(p.n_work, 1));
+  h->kktovf2.ensure(sizeof(int64_t) * std::max<int64_t>(p.n_work, 1));
   h->kktfail.ensure(sizeof(int64_t) * std::max<int64_t>(p.n_work, 1));
   for (auto& e : h->kev)
     if (!e) CSD_CUDA(cudaEventCreate(&e));
@@ -1003,23 +1175,46 @@ void launch_fista_kkt(csd_handle* h, int MT, const csd::FistaParams& p) {
   pp.round_total = stat + 4;
   pp.kkt_max_bits = stat + 5;
   pp.n_uncertified = stat + 6;  // non-finite inputs (failures go to the fallback list)
-  launch_polish(h, pp, 8, p.n_work);
+  csd::PolishParams po = pp;    // the pass over the supports that outgrew the first
+  if (h->opt_polish == 0) {
+    // thread per voxel (supports <= kTpvCap), then a warp per voxel for the
+    // supports that outgrew it, then room for all K
+    pp.cap = csd::kTpvCap;
+    if ((K + 31) / 32 == 1)
+      launch_polish_tpv_t<1>(h, pp, p.queue);
+    else if ((K + 31) / 32 == 3)
+      launch_polish_tpv_t<3>(h, pp, p.queue);
+    else
+      throw Error{CSD_ERR_INVALID, "the converged-optimum polish is built for radial orders <= 6"};
+    csd::PolishParams pw = pp;
+    pw.cap = std::min(kPolishCap, K);
+    pw.list = h->kktovf.as<int64_t>();
+    pw.list_len = stat + 2;
+    pw.overflow = h->kktovf2.as<int64_t>();
+    pw.n_overflow = stat + 8;
+    launch_polish(h, pw, 8, p.n_work);
+    po.list = h->kktovf2.as<int64_t>();
+    po.list_len = stat + 8;
+  } else {
+    launch_polish(h, pp, 8, p.n_work);
+    po.list = h->kktovf.as<int64_t>();
+    po.list_len = stat + 2;
+  }
   // supports that outgrew the warp slice: again with room for all K
-  csd::PolishParams po = pp;
   po.cap = K;
-  po.list = h->kktovf.as<int64_t>();
-  po.list_len = stat + 2;
   po.overflow = h->kktovf.as<int64_t>();  // unused: cap = K cannot overflow
   po.n_overflow = stat + 7;
   launch_polish(h, po, 4, p.n_work);
   CSD_CUDA(cudaEventRecord(h->kev[2], st));
-  unsigned long long hs[6] = {0, 0, 0, 0, 0, 0};
+  unsigned long long hs[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   CSD_CUDA(cudaMemcpyAsync(hs, stat, sizeof hs, cudaMemcpyDeviceToHost, st));
   CSD_CUDA(cudaStreamSynchronize(st));
   if (static_cast<int>(hs[1]) != 0)
     throw Error{CSD_ERR_TIMEOUT, "TF32 FISTA: a tensor-core completion wait gave up"};
   h->kkt_batches = hs[0];
   h->kkt_fallback = hs[3];
+  h->kkt_overflow[0] = hs[2];
+  h->kkt_overflow[1] = h->opt_polish == 0 ? hs[8] : 0;
   if (hs[3] > 0) {
     // the FP64 FISTA path with the reference stopping rule, then a last polish
     csd::FistaParams r = p;
@@ -1282,7 +1477,52 @@ void launch_icls_t(csd_handle* h, csd::IclsParams p) {
   CSD_LAUNCH();
 }
 
+template <int RPL>
+void launch_icls_gram_t(csd_handle* h, const csd::IclsParams& p) {
+  csd::IclsGramParams g{};
+  g.B = p.B;
+  g.L = p.L;
+  g.Gam = h->icls_gam.as<double>();
+  g.WT = h->icls_wt.as<double>();
+  g.Y = h->icls_y.as<double>();
+  g.pf = h->icls_pf.as<double>();
+  g.jcol = h->icls_jcol.as<int>();
+  g.X = p.X;
+  g.iters = p.iters;
+  g.conv = p.conv;
+  g.V = p.V;
+  g.K = p.K;
+  g.Kp = p.Kp;
+  g.m = p.m;
+  g.m_pad = p.m_pad;
+  g.nsh = h->icls_nsh;
+  g.max_iter = p.max_iter;
+  g.tol = p.tol;
+  g.queue = p.queue;
+  g.overflow = p.overflow;
+  g.iter_total = p.iter_total;
+  const size_t smem = csd::icls_gram_smem(g.nsh, g.m_pad);
+  auto* kern = csd::k_icls_gram<RPL, kIclsGramCpl>;
+  CSD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  int per_sm = 0;
+  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * csd::kIclsGramWarps, smem));
+  if (per_sm < 1) throw Error{CSD_ERR_CUDA, "Gram-form ICLS: no CTA fits an SM"};
+  const int64_t blocks = std::max<int64_t>(
+      1, std::min<int64_t>(static_cast<int64_t>(h->num_sms) * per_sm,
+                           (p.V + csd::kIclsGramWarps - 1) / csd::kIclsGramWarps));
+  kern<<<static_cast<unsigned>(blocks), 32 * csd::kIclsGramWarps, smem, h->stream>>>(g);
+  CSD_LAUNCH();
+}
+
 void launch_icls(csd_handle* h, const csd::IclsParams& p) {
+  if (h->icls_gram && h->opt_icls == 0) {
+    switch ((h->K + 31) / 32) {
+      case 1: launch_icls_gram_t<1>(h, p); return;
+      case 2: launch_icls_gram_t<2>(h, p); return;
+      case 3: launch_icls_gram_t<3>(h, p); return;
+      default: break;
+    }
+  }
   switch ((h->K + 31) / 32) {
     case 1: launch_icls_t<1>(h, p); break;
     case 2: launch_icls_t<2>(h, p); break;
@@ -1476,6 +1716,7 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   h->mixed_ops = 0.0;
   h->mixed_rerun = 0;
   h->kkt_batches = h->kkt_fallback = h->kkt_rounds = h->kkt_uncertified = h->kkt_iter_add = 0;
+  h->kkt_overflow[0] = h->kkt_overflow[1] = 0;
   h->kkt_max = 0.0;
   h->kkt_ms[0] = h->kkt_ms[1] = h->kkt_ms[2] = 0.f;
   const bool is_l1 = spec->regularization == CSD_REG_L1;
@@ -1805,6 +2046,11 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   h->timing.kkt_uncertified = static_cast<int64_t>(h->kkt_uncertified);
   h->timing.kkt_rounds = h->kkt_rounds;
   h->timing.kkt_max = h->kkt_max;
+  h->timing.kkt_iterations = (h->precision == CSD_PRECISION_MIXED_KKT || h->precision == CSD_PRECISION_FP64_KKT)
+                                 ? (h->opt_kkt_iters > 0 ? h->opt_kkt_iters : h->kkt_iters_used)
+                                 : 0;
+  for (int i = 0; i < 4; ++i) h->timing.kkt_tune_ms[i] = h->kkt_tune_ms[i];
+  for (int i = 0; i < 2; ++i) h->timing.kkt_overflow[i] = static_cast<int64_t>(h->kkt_overflow[i]);
   if (h->precision == CSD_PRECISION_MIXED_KKT && K <= 80) {
     const int ks = (K + 7) / 8, nb = 16 * ((K + 15) / 16);
     h->timing.tf32_tensor_flops = static_cast<double>(h->kkt_batches) * ks * 2.0 * 128 * nb * 8;
@@ -1879,8 +2125,28 @@ PipePlan pipe_plan(int num_sms) {
   return PipePlan{std::vector<double>(kPipePlan, kPipePlan + kPipeChunks), std::min(kPipeRhsCtas, num_sms - 1)};
 }
 
+// A pageable host volume whose masked rows the pipelined fit gathers into
+// the page-locked staging volume chunk by chunk, each chunk just before its
+// right-hand side is queued, so that the gather of chunk k + 1 on the host
+// overlaps the device's work on chunk k.
+struct HostGather {
+  const float* data = nullptr;   // pageable (X, Y, Z, N) volume
+  const uint8_t* mask = nullptr; // host mask
+  float* stage = nullptr;        // page-locked staging volume, same shape
+  int N = 0;
+};
+
+void gather_rows(const HostGather& hg, int64_t lo, int64_t hi) {
+  const int N = hg.N;
+  host_parallel(hi - lo, 4096, [&](int64_t a, int64_t b) {
+    for (int64_t v = lo + a; v < lo + b; ++v)
+      if (hg.mask[v]) std::memcpy(hg.stage + v * N, hg.data + v * N, sizeof(float) * N);
+  });
+}
+
 FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64_t nvol,
-                          const HostGtab& g, const csd_shore_spec* spec, float* d_coeffs, float* host_coeffs) {
+                          const HostGtab& g, const csd_shore_spec* spec, float* d_coeffs, float* host_coeffs,
+                          const HostGather* hg = nullptr) {
   FitInfo info;
   h->sig_compact = nullptr;
   cudaStream_t st = h->stream;
@@ -1890,6 +2156,7 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   h->mixed_ops = 0.0;
   h->mixed_rerun = 0;
   h->kkt_batches = h->kkt_fallback = h->kkt_rounds = h->kkt_uncertified = h->kkt_iter_add = 0;
+  h->kkt_overflow[0] = h->kkt_overflow[1] = 0;
   h->kkt_max = 0.0;
   h->kkt_ms[0] = h->kkt_ms[1] = h->kkt_ms[2] = 0.f;
   record(h, 0);
@@ -1999,7 +2266,7 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   } restore{h, st};
   ensure_sched(h, V);  // before any chunk runs: chunks share the buffers
   cudaStream_t rs = h->pipe[0];
-  for (int k = 0; k < C; ++k) {
+  auto queue_rhs = [&](int k) {
     const int64_t a = c0[k], n = c0[k + 1] - c0[k];
     const int64_t groups = (n + 7) / 8;
     const int rhs_grid = static_cast<int>(std::min<int64_t>(k == 0 ? h->num_sms : plan.rhs_ctas, (groups + 7) / 8));
@@ -2008,16 +2275,29 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
         h->sig.as<float>() + a * N);
     CSD_LAUNCH();
     CSD_CUDA(cudaEventRecord(h->pev[k], rs));
-  }
-  if (d_out_host) {
-    // zero-fill the last chunk's slab in the host volume once every row has been read
-    const int64_t lo = vb[C - 1];
-    CSD_CUDA(cudaStreamWaitEvent(h->pipe[3], h->pev[C - 1], 0));
-    CSD_CUDA(cudaMemcpyAsync(host_coeffs + lo * K, d_coeffs + lo * K, sizeof(float) * static_cast<size_t>(nvol - lo) * K,
-                             cudaMemcpyDeviceToHost, h->pipe[3]));
-    CSD_CUDA(cudaEventRecord(h->pev[18], h->pipe[3]));
-  }
+    if (k == C - 1 && d_out_host) {
+      // zero-fill the last chunk's slab in the host volume once every row has been read
+      const int64_t lo = vb[C - 1];
+      CSD_CUDA(cudaStreamWaitEvent(h->pipe[3], h->pev[C - 1], 0));
+      CSD_CUDA(cudaMemcpyAsync(host_coeffs + lo * K, d_coeffs + lo * K,
+                               sizeof(float) * static_cast<size_t>(nvol - lo) * K, cudaMemcpyDeviceToHost,
+                               h->pipe[3]));
+      CSD_CUDA(cudaEventRecord(h->pev[18], h->pipe[3]));
+    }
+  };
+  // Without a host gather every right-hand side is queued first; with one,
+  // chunk k's rows are gathered and its right-hand side queued just before
+  // its iterations, so the next chunk's gather overlaps them.
+  if (!hg)
+    for (int k = 0; k < C; ++k) queue_rhs(k);
   for (int k = 0; k < C; ++k) {
+    if (hg) {
+      const auto t0 = std::chrono::steady_clock::now();
+      gather_rows(*hg, vb[k], vb[k + 1]);
+      h->timing.ms_host_gather +=
+          std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      queue_rhs(k);
+    }
     const int64_t a = c0[k], n = c0[k + 1] - c0[k];
     cudaStream_t ks = h->pipe[1 + (k & 1)];
     CSD_CUDA(cudaStreamWaitEvent(ks, h->pev[k], 0));
@@ -2171,6 +2451,7 @@ void csd_destroy(csd_handle* h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   DevBuf* bufs[] = {&h->bvals, &h->bvecs, &h->M, &h->Mt, &h->G, &h->A, &h->gfrag, &h->mfrag, &h->mtfrag, &h->sst_v, &h->mom, &h->scal, &h->ok, &h->dirs, &h->Cmat, &h->Le, &h->Wi, &h->Q1, &h->ovf,
+                    &h->icls_gam, &h->icls_wt, &h->icls_y, &h->icls_pf, &h->icls_jcol,
                     &h->data, &h->mask, &h->coeffs, &h->r2, &h->resid, &h->iters_map, &h->kind_map,
                     &h->alpha_map, &h->bic_map, &h->rss_map, &h->blk, &h->total, &h->vox, &h->B, &h->X, &h->sig,
                     &h->iters, &h->conv, &h->queue, &h->itotal, &h->resid_v, &h->nnz_v, &h->amax,
@@ -2181,7 +2462,7 @@ void csd_destroy(csd_handle* h) {
                     &h->iota, &h->adjW, &h->adjovf, &h->adjstat, &h->adjconst,
                     &h->gdtab, &h->gdq, &h->tuneB, &h->tuneX, &h->tuneIt, &h->tuneConv, &h->tuneQ,
                     &h->schedY, &h->schedPend, &h->schedKey, &h->schedOrder, &h->schedCnt,
-                    &h->schedD, &h->schedU, &h->schedN, &h->gtf32, &h->x32, &h->kktv, &h->kktovf,
+                    &h->schedD, &h->schedU, &h->schedN, &h->gtf32, &h->x32, &h->kktv, &h->kktovf, &h->kktovf2,
                     &h->kktfail, &h->kktstat};
   for (auto s : h->pipe)
     if (s) cudaStreamSynchronize(s);
@@ -2194,40 +2475,11 @@ void csd_destroy(csd_handle* h) {
   for (auto& e : h->kev)
     if (e) cudaEventDestroy(e);
   if (h->stage) cudaFreeHost(h->stage);
+  if (h->ostage) cudaFreeHost(h->ostage);
   for (auto s : h->pipe)
     if (s) cudaStreamDestroy(s);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
-}
-
-// Masked rows of a pageable (X, Y, Z, N) volume copied into the handle's
-// page-locked, mapped staging volume of the same shape, on up to 16 host
-// threads (each takes a contiguous range of voxels); returns the staging
-// volume's device address.
-static const float* stage_masked_rows(csd_handle* h, const float* data, const uint8_t* mask, int64_t nvol, int N) {
-  const size_t bytes = sizeof(float) * static_cast<size_t>(nvol) * N;
-  if (h->stage_bytes < bytes) {
-    if (h->stage) CSD_CUDA(cudaFreeHost(h->stage));
-    h->stage = nullptr;
-    h->stage_bytes = 0;
-    void* p = nullptr;
-    CSD_CUDA(cudaHostAlloc(&p, bytes, cudaHostAllocMapped | cudaHostAllocPortable));
-    h->stage = static_cast<float*>(p);
-    h->stage_bytes = bytes;
-  }
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const int64_t T = std::min<int64_t>(std::min<unsigned>(hw, 16u), std::max<int64_t>(1, nvol / 4096));
-  auto copy_range = [&](int64_t lo, int64_t hi) {
-    for (int64_t v = lo; v < hi; ++v)
-      if (mask[v]) std::memcpy(h->stage + v * N, data + v * N, sizeof(float) * N);
-  };
-  std::vector<std::thread> pool;
-  for (int64_t t = 1; t < T; ++t) pool.emplace_back(copy_range, nvol * t / T, nvol * (t + 1) / T);
-  copy_range(0, nvol / T);
-  for (auto& th : pool) th.join();
-  void* dp = nullptr;
-  CSD_CUDA(cudaHostGetDevicePointer(&dp, h->stage, 0));
-  return static_cast<const float*>(dp);
 }
 
 static int check_common(csd_handle* h, const void* data, const void* mask, int64_t X, int64_t Y, int64_t Z,
@@ -2310,13 +2562,21 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
       }
       cudaGetLastError();  // a pageable pointer may leave an error code behind
     }
+    h->timing.ms_host_gather = 0.f;
+    h->timing.ms_host_copy_out = 0.f;
+    bool staged = false;
     if (!on_host && h->dmma_rhs_possible(N, K)) {
       // A pageable volume: its masked rows are gathered on host threads into
       // the handle's page-locked staging volume, which the device then reads
       // in place like a page-locked input (masked rows only; the other rows
-      // of the staging volume are never read).
-      d_data = stage_masked_rows(h, data, mask, nvol, N);
+      // of the staging volume are never read).  The pipelined fit gathers
+      // chunk by chunk (below); other fits gather everything first.
+      float* stage = ensure_pinned(h->stage, h->stage_bytes, sizeof(float) * static_cast<size_t>(nvol) * N);
+      void* dp = nullptr;
+      CSD_CUDA(cudaHostGetDevicePointer(&dp, stage, 0));
+      d_data = static_cast<const float*>(dp);
       on_host = true;
+      staged = true;
     }
     if (!on_host) {
       h->data.ensure(sizeof(float) * static_cast<size_t>(nvol) * N);
@@ -2351,8 +2611,37 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
                            spec->alpha_mode == CSD_ALPHA_FIXED && spec->precision == CSD_PRECISION_FP64 &&
                            !diag && !out->coef64 && !out->converged && spec->max_iter > 0 &&
                            (fista_variant(h) == 3 || fista_variant(h) == 4);
+    // A pageable output of the pipelined fit: the fit writes the handle's
+    // page-locked output volume (in place and by slab copies, as for a
+    // page-locked output) and host threads copy it out afterwards.
+    float* host_out = out->coefficients;
+    bool out_staged = false;
+    if (pipelined) {
+      cudaPointerAttributes attr{};
+      const bool pinned_out = cudaPointerGetAttributes(&attr, out->coefficients) == cudaSuccess &&
+                              attr.type == cudaMemoryTypeHost && attr.devicePointer;
+      cudaGetLastError();
+      if (!pinned_out) {
+        host_out = ensure_pinned(h->ostage, h->ostage_bytes, sizeof(float) * static_cast<size_t>(nvol) * K);
+        out_staged = true;
+      }
+    }
+    HostGather hg;
+    if (staged) {
+      hg.data = data;
+      hg.mask = mask;
+      hg.stage = h->stage;
+      hg.N = N;
+      if (!pipelined) {
+        const auto t0 = std::chrono::steady_clock::now();
+        gather_rows(hg, 0, nvol);
+        h->timing.ms_host_gather =
+            std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      }
+    }
     FitInfo info = pipelined
-                       ? run_fit_pipelined(h, d_data, h->mask.as<uint8_t>(), nvol, g, spec, d.coeffs, out->coefficients)
+                       ? run_fit_pipelined(h, d_data, h->mask.as<uint8_t>(), nvol, g, spec, d.coeffs, host_out,
+                                           staged ? &hg : nullptr)
                        : run_fit(h, d_data, h->mask.as<uint8_t>(), nvol, g, spec, path_eps, d, on_host);
     if (!pipelined)
       CSD_CUDA(cudaMemcpyAsync(out->coefficients, d.coeffs, sizeof(float) * static_cast<size_t>(nvol) * K,
@@ -2379,6 +2668,15 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
     if (out->converged && info.V > 0)
       CSD_CUDA(cudaMemcpyAsync(out->converged, info.conv_final, info.V, cudaMemcpyDeviceToHost, st));
     CSD_CUDA(cudaStreamSynchronize(st));
+    if (out_staged) {
+      const auto t0 = std::chrono::steady_clock::now();
+      const size_t row = sizeof(float) * static_cast<size_t>(K);
+      host_parallel(nvol, 4096, [&](int64_t lo, int64_t hi) {
+        std::memcpy(out->coefficients + lo * K, host_out + lo * K, row * static_cast<size_t>(hi - lo));
+      });
+      h->timing.ms_host_copy_out =
+          std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
     fill_scalars(g, info, spec, out);
     warnings += info.warnings;
     std::snprintf(out->warnings, sizeof out->warnings, "%s", warnings.c_str());
@@ -2609,7 +2907,7 @@ int csd_set_option(csd_handle* h, int32_t option, int64_t value) {
       h->opt_schedule = static_cast<int>(value);
       return CSD_OK;
     case CSD_OPT_KKT_ITERATIONS:
-      if (value < 1 || value > 100000) return CSD_ERR_INVALID;
+      if (value < 0 || value > 100000) return CSD_ERR_INVALID;
       h->opt_kkt_iters = static_cast<int>(value);
       return CSD_OK;
     case CSD_OPT_KKT_ROUNDS:
@@ -2619,6 +2917,14 @@ int csd_set_option(csd_handle* h, int32_t option, int64_t value) {
     case CSD_OPT_TENSOR_WAIT_NS:
       if (value < 1 || value > 2000000000LL) return CSD_ERR_INVALID;
       h->opt_wait_ns = static_cast<unsigned long long>(value);
+      return CSD_OK;
+    case CSD_OPT_POLISH:
+      if (value != 0 && value != 1) return CSD_ERR_INVALID;
+      h->opt_polish = static_cast<int>(value);
+      return CSD_OK;
+    case CSD_OPT_ICLS:
+      if (value != 0 && value != 1) return CSD_ERR_INVALID;
+      h->opt_icls = static_cast<int>(value);
       return CSD_OK;
     default:
       return CSD_ERR_INVALID;

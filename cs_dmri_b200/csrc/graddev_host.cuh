@@ -22,6 +22,13 @@ extern "C" int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signal
       throw Error{CSD_ERR_INVALID, "the per-voxel-design fit takes regularization l1 with alpha_mode fixed"};
     if (spec->radial_order != 6 && spec->radial_order != 8)
       throw Error{CSD_ERR_INVALID, "the per-voxel-design fit is built for radial orders 6 and 8"};
+    if (spec->precision == CSD_PRECISION_MIXED)
+      throw Error{CSD_ERR_INVALID, "the per-voxel-design fit takes precision fp64, fp64-kkt or mixed-kkt"};
+    // converged-optimum modes: the support-identification iterations run in
+    // FP64 here (each voxel has its own Gram matrix, so there is no shared
+    // tensor-core operand); the polish and certificate are those of the
+    // shared-design path
+    const bool kkt = spec->precision == CSD_PRECISION_MIXED_KKT || spec->precision == CSD_PRECISION_FP64_KKT;
     StreamScope scope(h, stream);
     HandleOrder call_order(h);
     cudaStream_t st = h->stream;
@@ -37,9 +44,10 @@ extern "C" int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signal
     CSD_CUDA(cudaMemcpyAsync(h->gdtab.p, g.bvals.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st));
     CSD_CUDA(cudaMemcpyAsync(h->gdtab.as<double>() + N, g.bvecs.data(), sizeof(double) * 3 * N,
                              cudaMemcpyHostToDevice, st));
-    ensure_mom(h, spec->max_iter);
-    h->gdq.ensure(2 * sizeof(unsigned long long));
-    CSD_CUDA(cudaMemsetAsync(h->gdq.p, 0, 2 * sizeof(unsigned long long), st));
+    const int kkt_iters = h->opt_kkt_iters > 0 ? h->opt_kkt_iters : 32;
+    ensure_mom(h, std::max(spec->max_iter, kkt_iters));
+    h->gdq.ensure(4 * sizeof(unsigned long long));
+    CSD_CUDA(cudaMemsetAsync(h->gdq.p, 0, 4 * sizeof(unsigned long long), st));
     csd::GraddevParams p{};
     p.S = d_signals;
     p.T = d_graddev;
@@ -66,6 +74,12 @@ extern "C" int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signal
     p.lipschitz = d_lipschitz;
     p.n_rows = d_n_rows;
     p.iter_total = h->gdq.as<unsigned long long>() + 1;
+    p.kkt = kkt ? 1 : 0;
+    p.kkt_iters = kkt_iters;
+    p.kkt_rounds = h->opt_kkt_rounds;
+    p.kappa = kKktKappa;
+    p.n_uncertified = h->gdq.as<unsigned long long>() + 2;
+    p.round_total = h->gdq.as<unsigned long long>() + 3;
     auto go = [&](auto kern) {
       CSD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(lay.total_bytes)));
@@ -77,6 +91,14 @@ extern "C" int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signal
       go(csd::k_graddev_fit<9>);
     else
       go(csd::k_graddev_fit<19>);
+    if (kkt) {  // the certificate counters (this mode waits for its work)
+      unsigned long long c[2] = {0, 0};
+      CSD_CUDA(cudaMemcpyAsync(c, h->gdq.as<unsigned long long>() + 2, sizeof c, cudaMemcpyDeviceToHost, st));
+      CSD_CUDA(cudaStreamSynchronize(st));
+      h->timing.kkt_uncertified = static_cast<int64_t>(c[0]);
+      h->timing.kkt_rounds = c[1];
+      h->timing.kkt_iterations = kkt_iters;
+    }
   } catch (const Error& e) {
     set_err(err, err_len, e.msg);
     return e.code;

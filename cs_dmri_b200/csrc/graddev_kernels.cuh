@@ -49,6 +49,15 @@ struct GraddevParams {
   double* lipschitz;        // V (nullable)
   int* n_rows;              // V (nullable): samples kept
   unsigned long long* iter_total;  // executed FISTA iterations, summed (nullable)
+  // converged-optimum mode (kkt != 0): kkt_iters FISTA iterations find the
+  // support, one warp polishes on G_v and certifies (polish_warp); a voxel it
+  // cannot certify gets the reference FISTA from zero, uncertified
+  int kkt;
+  int kkt_iters, kkt_rounds;
+  double kappa;
+  double* kkt_out;                   // V (nullable): largest KKT residual, NaN when uncertified
+  unsigned long long* n_uncertified; // (nullable)
+  unsigned long long* round_total;   // polish solves, summed (nullable)
 };
 
 // Shared-memory plan (doubles unless noted), shared by host and device.
@@ -170,6 +179,11 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
   __shared__ int s_n;
   __shared__ double s_lmax;
   __shared__ int s_first;
+  __shared__ uint16_t gd_tri[kTriTable];  // (row, col) of a packed triangle, for the polish
+  for (int e = threadIdx.x; e < kTriTable; e += blockDim.x) {
+    const int r = tri_row(e);
+    gd_tri[e] = static_cast<uint16_t>((r << 8) | (e - pk_row(r)));
+  }
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, q = lane & 3;
 
@@ -465,63 +479,126 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
     // ---- 4. FISTA (src/solver/fista.rs:70-143), Gram form
     const double n_inv = (n > 0) ? 1.0 / nv : 0.0;
     const double step = (n > 0) ? 1.0 / lip : 0.0;
-    const double thr = __dmul_rn(step, p.alpha_v ? p.alpha_v[v] : p.alpha);
-    for (int i = tid; i < Kp; i += blockDim.x) {
-      vx[i] = 0.0;
-      vy[i] = 0.0;
-    }
-    __syncthreads();
-    int it = 0;
-    bool converged = false;
-    while (n > 0 && it < p.max_iter) {
-      gd_gemv(G, LDG, K, vy, vgy);
-      __syncthreads();
-      const double mom = p.mom[it];
-      double dx2 = 0.0, xn2 = 0.0;
-      if (tid < K) {
-        const int i = tid;
-        const double grad = __dmul_rn(__dsub_rn(vgy[i], vb[i]), n_inv);
-        const double cand = __dsub_rn(vy[i], __dmul_rn(step, grad));
-        double sv;
-        if (cand > thr)
-          sv = __dsub_rn(cand, thr);
-        else if (cand < -thr)
-          sv = __dadd_rn(cand, thr);
-        else
-          sv = 0.0;
-        const double xn = p.non_negative ? fmax(sv, 0.0) : sv;
-        const double d = __dsub_rn(xn, vx[i]);
-        vy[i] = __dadd_rn(xn, __dmul_rn(mom, d));
-        vx[i] = xn;
-        dx2 = __dmul_rn(d, d);
-        xn2 = __dmul_rn(xn, xn);
+    const double alpha_v = p.alpha_v ? p.alpha_v[v] : p.alpha;
+    const double thr = __dmul_rn(step, alpha_v);
+    // `max_it` iterations from zero, stopping early below `tol` (never with tol 0)
+    auto run_fista = [&](int max_it, double tol, bool& converged) -> int {
+      for (int i = tid; i < Kp; i += blockDim.x) {
+        vx[i] = 0.0;
+        vy[i] = 0.0;
       }
+      __syncthreads();
+      int it = 0;
+      converged = false;
+      while (n > 0 && it < max_it) {
+        gd_gemv(G, LDG, K, vy, vgy);
+        __syncthreads();
+        const double mom = p.mom[it];
+        double dx2 = 0.0, xn2 = 0.0;
+        if (tid < K) {
+          const int i = tid;
+          const double grad = __dmul_rn(__dsub_rn(vgy[i], vb[i]), n_inv);
+          const double cand = __dsub_rn(vy[i], __dmul_rn(step, grad));
+          double sv;
+          if (cand > thr)
+            sv = __dsub_rn(cand, thr);
+          else if (cand < -thr)
+            sv = __dadd_rn(cand, thr);
+          else
+            sv = 0.0;
+          const double xn = p.non_negative ? fmax(sv, 0.0) : sv;
+          const double d = __dsub_rn(xn, vx[i]);
+          vy[i] = __dadd_rn(xn, __dmul_rn(mom, d));
+          vx[i] = xn;
+          dx2 = __dmul_rn(d, d);
+          xn2 = __dmul_rn(xn, xn);
+        }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        dx2 += __shfl_xor_sync(kFull, dx2, o);
-        xn2 += __shfl_xor_sync(kFull, xn2, o);
+        for (int o = 16; o > 0; o >>= 1) {
+          dx2 += __shfl_xor_sync(kFull, dx2, o);
+          xn2 += __shfl_xor_sync(kFull, xn2, o);
+        }
+        if (lane == 0) {
+          red[2 * warp] = dx2;
+          red[2 * warp + 1] = xn2;
+        }
+        __syncthreads();
+        double sdx = 0.0, sxn = 0.0;
+        for (int w = 0; w < 8; ++w) {
+          sdx += red[2 * w];
+          sxn += red[2 * w + 1];
+        }
+        ++it;
+        const double rel = sqrt(sdx) / fmax(sqrt(sxn), 1e-12);
+        __syncthreads();  // red and vy are rewritten next iteration
+        if (rel < tol) {
+          converged = true;
+          break;
+        }
       }
-      if (lane == 0) {
-        red[2 * warp] = dx2;
-        red[2 * warp + 1] = xn2;
+      return it;
+    };
+    bool converged = false;
+    int it = run_fista(p.kkt ? p.kkt_iters : p.max_iter, p.kkt ? 0.0 : p.tol, converged);
+    double kkt_val = 0.0;
+    int rounds = 0;
+    if (p.kkt) {
+      // polish on G_v by warp 0, its scratch in the vectors FISTA no longer
+      // needs (y, G y, the Lanczos vectors and the reduction / tridiagonal
+      // slots: 5 Kp + 160 doubles; b and x stay)
+      constexpr int RPL = (8 * MT + 31) / 32;
+      const int cap = (K > 72) ? 32 : 24;
+      if (warp == 0 && n > 0) {
+        double* T = vy;
+        double* zw = T + cap * (cap + 1) / 2;
+        double* zj = zw + cap;
+        int* sidx = reinterpret_cast<int*>(zj + Kp);
+        int* fl = sidx + Kp;
+        double c[RPL];
+#pragma unroll
+        for (int qq = 0; qq < RPL; ++qq) {
+          const int j = lane + 32 * qq;
+          const double x0 = j < K ? vx[j] : 0.0;
+          int f = x0 > 0.0 ? 1 : (x0 < 0.0 ? -1 : 0);
+          if (p.non_negative && f < 0) f = 0;
+          c[qq] = f != 0 ? x0 : 0.0;
+          if (j < Kp) fl[j] = f;
+        }
+        __syncwarp();
+        bool ovf = false;
+        const bool cert = polish_warp<RPL, 1>(G, LDG, K, Kp, cap, vb, fl, c, T, zw, zj, sidx, gd_tri, nv, n_inv,
+                                              alpha_v, p.non_negative, p.kappa, p.kkt_rounds, rounds, kkt_val,
+                                              ovf);
+        if (cert) {
+#pragma unroll
+          for (int qq = 0; qq < RPL; ++qq)
+            if (lane + 32 * qq < K) vx[lane + 32 * qq] = c[qq];
+        }
+        if (lane == 0) {
+          s_first = cert ? 1 : 0;
+          s_lmax = cert ? kkt_val : 0.0;
+          ta[0] = static_cast<double>(rounds);
+        }
       }
       __syncthreads();
-      double sdx = 0.0, sxn = 0.0;
-      for (int w = 0; w < 8; ++w) {
-        sdx += red[2 * w];
-        sxn += red[2 * w + 1];
+      const bool cert = n > 0 && s_first == 1;
+      rounds = (n > 0) ? static_cast<int>(ta[0]) : 0;
+      kkt_val = s_lmax;
+      __syncthreads();
+      if (!cert && n > 0) {  // the reference FISTA from zero, reported uncertified
+        bool conv_ref = false;
+        it += run_fista(p.max_iter, p.tol, conv_ref);
       }
-      ++it;
-      const double rel = sqrt(sdx) / fmax(sqrt(sxn), 1e-12);
-      __syncthreads();  // red and vy are rewritten next iteration
-      if (rel < p.tol) {
-        converged = true;
-        break;
+      converged = cert || n == 0;
+      if (tid == 0) {
+        if (p.kkt_out) p.kkt_out[v] = cert || n == 0 ? kkt_val : __longlong_as_double(0x7ff8000000000000ll);
+        if (!cert && n > 0 && p.n_uncertified) atomicAdd(p.n_uncertified, 1ull);
+        if (p.round_total) atomicAdd(p.round_total, static_cast<unsigned long long>(rounds));
       }
     }
     for (int i = tid; i < K; i += blockDim.x) p.X[v * K + i] = vx[i];
     if (tid == 0) {
-      p.iters[v] = static_cast<uint32_t>(it);
+      p.iters[v] = static_cast<uint32_t>(it + rounds);
       p.conv[v] = converged ? 1 : 0;
       if (p.lipschitz) p.lipschitz[v] = lip;
       if (p.n_rows) p.n_rows[v] = n;

@@ -54,18 +54,13 @@ __device__ __forceinline__ double dev_radial_factor(unsigned n, unsigned l, doub
   return c_nl * g_nl * f_nl;
 }
 
-// C[p, col] = Y_T(dir_p)[j] * (radial_factor(n, l) * sign) where column col
-// (BrainSuite block position k of degree l) projects onto Tournier SH index j
-// with `sign` (src/odf.rs:57-102); Y_T is the MRtrix real SH at the
-// direction, rounded through float32 as the reference receives it
-// (src/solver/shore_icls.rs:52-64).  Only one Tournier row of the projection
-// is non-zero per SHORE column, so this is the matrix product Y P.
-__global__ void k_constraint(const double* __restrict__ dirs, int m, int K, int radial_order, double zeta,
-                             double* __restrict__ C) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= m * K) return;
-  const int p = idx / K, col = idx % K;
-  int n = 0, l = 0, k = 0;
+// Degree l, Tournier order m_T and sign of SHORE column col (BrainSuite
+// block position k of degree l): cosine m = l - k, m = 0, sine m = -(k - l)
+// with sign (-1)^(j+1) on the sine block (src/odf.rs:57-102).
+__device__ __forceinline__ void shore_column_sh(int col, int radial_order, int& n, int& l, int& mT,
+                                                double& sign) {
+  int k = 0;
+  n = l = 0;
   {
     int c = 0;
     bool found = false;
@@ -81,10 +76,7 @@ __global__ void k_constraint(const double* __restrict__ dirs, int m, int K, int 
         c += 2 * ll + 1;
       }
   }
-  // BrainSuite column k -> physical order m_T (cosine m = l - k, m = 0, sine
-  // m = -(k - l)) and sign (-1)^(j+1) on the sine block.
-  int mT;
-  double sign = 1.0;
+  sign = 1.0;
   if (k < l) {
     mT = l - k;
   } else if (k == l) {
@@ -94,6 +86,11 @@ __global__ void k_constraint(const double* __restrict__ dirs, int m, int K, int 
     mT = -j;
     sign = (j % 2 == 1) ? 1.0 : -1.0;
   }
+}
+
+// The MRtrix real SH of degree l, order m_T at direction p, rounded through
+// float32 as the reference receives it (src/solver/shore_icls.rs:52-64).
+__device__ __forceinline__ double sh_amplitude32(const double* __restrict__ dirs, int p, int l, int mT) {
   const double x = dirs[3 * p], y = dirs[3 * p + 1], z = dirs[3 * p + 2];
   const double r = sqrt(x * x + y * y + z * z);
   const double theta = atan2(y, x);
@@ -108,8 +105,47 @@ __global__ void k_constraint(const double* __restrict__ dirs, int m, int K, int 
     yv = pl;
   else
     yv = sqrt(2.0) * pl * cos(am * theta);
-  const double y32 = static_cast<double>(static_cast<float>(yv));
-  C[idx] = y32 * (dev_radial_factor(n, l, zeta) * sign);
+  return static_cast<double>(static_cast<float>(yv));
+}
+
+// C[p, col] = Y_T(dir_p)[j] * (radial_factor(n, l) * sign) where column col
+// projects onto Tournier SH index j with `sign` (src/odf.rs:57-102).  Only
+// one Tournier row of the projection is non-zero per SHORE column, so this
+// is the matrix product Y P.
+__global__ void k_constraint(const double* __restrict__ dirs, int m, int K, int radial_order, double zeta,
+                             double* __restrict__ C) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= m * K) return;
+  const int p = idx / K, col = idx % K;
+  int n, l, mT;
+  double sign;
+  shore_column_sh(col, radial_order, n, l, mT, sign);
+  C[idx] = sh_amplitude32(dirs, p, l, mT) * (dev_radial_factor(n, l, zeta) * sign);
+}
+
+// The factors of C = Y P: Y[j][p] (nsh x m_pad, zero past m) the amplitude
+// of Tournier SH j = l (l + 1) / 2 + m_T at direction p, and column col of
+// P as its one non-zero pf[col] in row jcol[col]; C[p, col] = Y[jcol[col]][p]
+// * pf[col] holds bit for bit.
+__global__ void k_constraint_factors(const double* __restrict__ dirs, int m, int m_pad, int K, int radial_order,
+                                     int lmax, double zeta, double* __restrict__ Y, double* __restrict__ pf,
+                                     int* __restrict__ jcol) {
+  const int nsh = (lmax + 1) * (lmax + 2) / 2;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx < nsh * m_pad) {
+    const int j = idx / m_pad, p = idx % m_pad;
+    int l = 0;
+    while ((l + 2) * (l + 3) / 2 - (l + 2) <= j) l += 2;  // j in [l(l+1)/2 - l, l(l+1)/2 + l]
+    const int mT = j - l * (l + 1) / 2;
+    Y[idx] = p < m ? sh_amplitude32(dirs, p, l, mT) : 0.0;
+  }
+  if (idx < K) {
+    int n, l, mT;
+    double sign;
+    shore_column_sh(idx, radial_order, n, l, mT, sign);
+    pf[idx] = dev_radial_factor(n, l, zeta) * sign;
+    jcol[idx] = l * (l + 1) / 2 + mT;
+  }
 }
 
 // A[i, i] += eps for i < K (G + eps I of src/solver/icls.rs:204-207).
@@ -421,6 +457,345 @@ __global__ void __launch_bounds__(32 * kIclsWarps) k_icls(IclsParams p) {
         const int row = lane + 32 * c;
         if (row < p.Kp) p.X[v * p.Kp + row] = (row < K) ? rv[c] : 0.0;
       }
+    }
+    if (lane == 0) {
+      p.iters[v] = static_cast<uint32_t>(iters - 1);
+      p.conv[v] = converged ? 1 : 0;
+      if (overflow) atomicAdd(p.overflow, 1);
+    }
+    __syncwarp();
+  }
+  if (p.iter_total && lane == 0) atomicAdd(p.iter_total, executed);
+}
+
+// ------------------------------------------------------------ Gram form
+//
+// The same method with the constraint values carried instead of recomputed.
+// With Gamma = W^T W (Gamma[c][p] = w_c . w_p, once per table) every
+// quantity of a step is a product with Gamma:
+//   d1 = Q1^T w_p = R^-T Gamma[A, p]      (Q1 = W_A R^-1 is never formed),
+//   z . n_p = |v|^2 = Gamma[p, p] - |d1|^2,   r = R^-1 d1,
+//   v = w_p - W_A r,  so the constraint values s = W^T x~ move by
+//   t (Gamma[:, p] - Gamma[:, A] r) and x~ by t (w_p - W_A r).
+// A step therefore costs (q + 1) columns of Gamma instead of the K-wide
+// products with Q1, and the scan for the most violated constraint reads s
+// from registers instead of recomputing W^T x~ (m x K) every iteration.  The
+// first s = C x0 (x0 the unconstrained minimiser) comes from C = Y P: z0 = P x0
+// (one term per column) and s = Y z0, with Y (nsh x m) in shared memory.
+// The reference's multiplier rule is kept as is (a full step pushes t for
+// the new constraint), so drops follow its iteration path; the carried s
+// and x~ differ from recomputed ones by rounding only.  Active sets of up to
+// 32 are held one entry per lane (rank C = nsh <= 28 for lmax <= 6).
+
+__global__ void k_icls_gram_setup(const double* __restrict__ W, int K, int Kp, int m_pad, double* __restrict__ Gam,
+                                  double* __restrict__ WT) {
+  const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t n2 = static_cast<int64_t>(m_pad) * m_pad;
+  if (idx < n2) {
+    const int c = static_cast<int>(idx / m_pad), q = static_cast<int>(idx % m_pad);
+    double a = 0.0;
+    for (int k = 0; k < K; ++k)
+      a = fma(W[static_cast<size_t>(k) * m_pad + c], W[static_cast<size_t>(k) * m_pad + q], a);
+    Gam[idx] = a;
+  } else if (idx < n2 + static_cast<int64_t>(m_pad) * Kp) {
+    const int64_t e = idx - n2;
+    const int c = static_cast<int>(e / Kp), k = static_cast<int>(e % Kp);
+    WT[e] = k < K ? W[static_cast<size_t>(k) * m_pad + c] : 0.0;
+  }
+}
+
+struct IclsGramParams {
+  const double* B;      // V x Kp: M^T s
+  const double* L;      // Kp x Kp: Cholesky factor of M^T M + eps I
+  const double* Gam;    // m_pad x m_pad: W^T W
+  const double* WT;     // m_pad x Kp: row c = w_c
+  const double* Y;      // nsh x m_pad: C = Y P
+  const double* pf;     // K: the non-zero of column col of P ...
+  const int* jcol;      // K: ... and its row
+  double* X;            // V x Kp out
+  uint32_t* iters;      // V
+  uint8_t* conv;        // V
+  int64_t V;
+  int K, Kp, m, m_pad, nsh, max_iter;
+  double tol;
+  unsigned long long* queue;
+  int* overflow;
+  unsigned long long* iter_total;
+};
+
+constexpr int kIclsGramWarps = 16;
+constexpr int kIclsGramRs = 33;                     // row stride of R (conflict-free rows and columns)
+// Per warp: R (32 x 33); at the start of a voxel, before R is in use, its
+// first K entries hold x0 and entries 1024.. hold z0.
+constexpr int kIclsGramWarpDoubles = 32 * kIclsGramRs;
+
+__host__ __device__ inline size_t icls_gram_smem(int nsh, int m_pad) {
+  return sizeof(double) * (static_cast<size_t>(nsh) * m_pad + static_cast<size_t>(kIclsGramWarps) * kIclsGramWarpDoubles);
+}
+
+// One warp per voxel, voxels from an atomic queue.  Constraint c lives on
+// lane c % 32 (slot c / 32): its value s and active flag in registers; entry
+// i < q of the active set (its constraint, multiplier, d1, r) on lane i.
+template <int RPL, int CPL>  // ceil(K / 32); m_pad / 32
+__global__ void __launch_bounds__(32 * kIclsGramWarps, 1) k_icls_gram(IclsGramParams p) {
+  extern __shared__ __align__(16) double gsm[];
+  const int K = p.K, Kp = p.Kp, m = p.m, mp = p.m_pad, nsh = p.nsh;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* Ysh = gsm;  // [nsh][m_pad]
+  for (int e = threadIdx.x; e < nsh * mp; e += blockDim.x) Ysh[e] = p.Y[e];
+  __syncthreads();
+  double* R = gsm + static_cast<size_t>(nsh) * mp + static_cast<size_t>(warp) * kIclsGramWarpDoubles;
+  double* x0s = R;          // [K], K <= 1024
+  double* z0 = R + 1024;    // [32]
+  const int qcap = nsh < 32 ? nsh : 32;
+  unsigned long long executed = 0;
+
+  while (true) {
+    unsigned long long vq = 0;
+    if (lane == 0) vq = atomicAdd(p.queue, 1ull);
+    vq = __shfl_sync(kFull, vq, 0);
+    if (vq >= static_cast<unsigned long long>(p.V)) break;
+    const int64_t v = static_cast<int64_t>(vq);
+
+    // x~0 = L^-1 M^T s, then x0 = L^-T x~0 (icls.rs:271-273)
+    double xt[RPL], x0[RPL];
+#pragma unroll
+    for (int c = 0; c < RPL; ++c) {
+      const int row = lane + 32 * c;
+      xt[c] = (row < K) ? p.B[v * Kp + row] : 0.0;
+    }
+    for (int i = 0; i < K; ++i) {
+      const int owner = i & 31, oc = i >> 5;
+      double xi = 0.0;
+#pragma unroll
+      for (int c = 0; c < RPL; ++c)
+        if (c == oc && lane == owner) xi = xt[c] / __ldg(p.L + i * Kp + i);
+      xi = __shfl_sync(kFull, xi, owner);
+#pragma unroll
+      for (int c = 0; c < RPL; ++c) {
+        const int row = lane + 32 * c;
+        if (row > i && row < K) xt[c] -= __ldg(p.L + row * Kp + i) * xi;
+        if (row == i) xt[c] = xi;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < RPL; ++c) x0[c] = xt[c];
+    for (int i = K - 1; i >= 0; --i) {
+      const int owner = i & 31, oc = i >> 5;
+      double xi = 0.0;
+#pragma unroll
+      for (int c = 0; c < RPL; ++c)
+        if (c == oc && lane == owner) xi = x0[c] / __ldg(p.L + i * Kp + i);
+      xi = __shfl_sync(kFull, xi, owner);
+#pragma unroll
+      for (int c = 0; c < RPL; ++c) {
+        const int row = lane + 32 * c;
+        if (row < i) x0[c] -= __ldg(p.L + i * Kp + row) * xi;
+        if (row == i) x0[c] = xi;
+      }
+    }
+    // s = C x0 = Y (P x0): z0[j] sums its columns in index order
+#pragma unroll
+    for (int c = 0; c < RPL; ++c) {
+      const int row = lane + 32 * c;
+      if (row < K) x0s[row] = x0[c];
+    }
+    __syncwarp();
+    if (lane < nsh) {
+      double zj = 0.0;
+      for (int col = 0; col < K; ++col)
+        if (__ldg(p.jcol + col) == lane) zj = fma(__ldg(p.pf + col), x0s[col], zj);
+      z0[lane] = zj;
+    }
+    __syncwarp();
+    double s[CPL];
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) s[c] = 0.0;
+    for (int j = 0; j < nsh; ++j) {
+      const double zj = z0[j];
+#pragma unroll
+      for (int c = 0; c < CPL; ++c) s[c] = fma(Ysh[j * mp + lane + 32 * c], zj, s[c]);
+    }
+    __syncwarp();
+
+    unsigned actbits = 0u;  // bit c: constraint lane + 32 c is active
+    int q = 0, a_i = -1;    // active set size; this lane's active constraint (lane < q)
+    double u_i = 0.0;       // its multiplier
+    int iters = 0;
+    bool converged = false, overflow = false;
+    while (true) {
+      iters += 1;
+      if (iters > p.max_iter) break;
+      // most violated inactive constraint (icls.rs:298-317): smallest value
+      // below -tol, first index on ties
+      double best = -p.tol;
+      int bestp = -1;
+#pragma unroll
+      for (int c = 0; c < CPL; ++c) {
+        const int ci = lane + 32 * c;
+        if (ci < m && !((actbits >> c) & 1u) && s[c] < best) {
+          best = s[c];
+          bestp = ci;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(kFull, best, o);
+        const int op = __shfl_xor_sync(kFull, bestp, o);
+        if (op >= 0 && (bestp < 0 || ob < best || (ob == best && op < bestp))) {
+          best = ob;
+          bestp = op;
+        }
+      }
+      if (bestp < 0) {
+        converged = true;
+        break;
+      }
+      double sp = best;
+      const double gpp = __ldg(p.Gam + static_cast<size_t>(bestp) * mp + bestp);
+      bool stop = false;
+      while (true) {  // inner loop: drop blocking constraints until p is added
+        // d1 = R^-T Gamma[A, p] (forward substitution by columns of R^T)
+        double d1 = (lane < q) ? __ldg(p.Gam + static_cast<size_t>(a_i) * mp + bestp) : 0.0;
+        for (int k = 0; k < q; ++k) {
+          const double dk = __shfl_sync(kFull, d1, k) / R[k * kIclsGramRs + k];
+          if (lane == k) d1 = dk;
+          else if (lane > k && lane < q) d1 = fma(-R[k * kIclsGramRs + lane], dk, d1);
+        }
+        double dd = d1 * d1;
+        for (int o = 16; o > 0; o >>= 1) dd += __shfl_xor_sync(kFull, dd, o);
+        const double zn = gpp - dd;  // z . n_p = |v|^2
+        // r = R^-1 d1 (back substitution by columns, icls.rs:331-341)
+        double rr = d1;
+        for (int i = q - 1; i >= 0; --i) {
+          const double ri = __shfl_sync(kFull, rr, i) / R[i * kIclsGramRs + i];
+          if (lane == i) rr = ri;
+          else if (lane < i) rr = fma(-R[lane * kIclsGramRs + i], ri, rr);
+        }
+        // step lengths (icls.rs:343-368)
+        double t1 = INFINITY;
+        int drop = -1;
+        if (lane < q && rr > p.tol) {
+          t1 = u_i / rr;
+          drop = lane;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ot = __shfl_xor_sync(kFull, t1, o);
+          const int od = __shfl_xor_sync(kFull, drop, o);
+          if (od >= 0 && (drop < 0 || ot < t1 || (ot == t1 && od < drop))) {
+            t1 = ot;
+            drop = od;
+          }
+        }
+        const double t2 = (zn > p.tol) ? -sp / zn : INFINITY;
+        const double t = fmin(t1, t2);
+        if (!isfinite(t)) {
+          stop = true;  // infeasible
+          break;
+        }
+        if (lane < q) u_i -= t * rr;
+        // s += t (Gamma[:, p] - Gamma[:, A] r), x~ += t (w_p - W_A r)
+        {
+          double ds[CPL], dx[RPL];
+          const double* gp = p.Gam + static_cast<size_t>(bestp) * mp + lane;
+          const double* wp = p.WT + static_cast<size_t>(bestp) * Kp + lane;
+#pragma unroll
+          for (int c = 0; c < CPL; ++c) ds[c] = __ldg(gp + 32 * c);
+#pragma unroll
+          for (int c = 0; c < RPL; ++c) dx[c] = (lane + 32 * c < Kp) ? __ldg(wp + 32 * c) : 0.0;
+          for (int i = 0; i < q; ++i) {
+            const double ri = __shfl_sync(kFull, rr, i);
+            const int ai = __shfl_sync(kFull, a_i, i);
+            const double* ga = p.Gam + static_cast<size_t>(ai) * mp + lane;
+            const double* wa = p.WT + static_cast<size_t>(ai) * Kp + lane;
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) ds[c] = fma(-ri, __ldg(ga + 32 * c), ds[c]);
+#pragma unroll
+            for (int c = 0; c < RPL; ++c)
+              if (lane + 32 * c < Kp) dx[c] = fma(-ri, __ldg(wa + 32 * c), dx[c]);
+          }
+#pragma unroll
+          for (int c = 0; c < CPL; ++c) s[c] = fma(t, ds[c], s[c]);
+#pragma unroll
+          for (int c = 0; c < RPL; ++c) xt[c] = fma(t, dx[c], xt[c]);
+        }
+        if (isfinite(t2) && t == t2) {
+          // full step: constraint p joins the active set
+          if (q >= qcap) {
+            overflow = true;
+            stop = true;
+            break;
+          }
+          if (lane < q) R[lane * kIclsGramRs + q] = d1;
+          if (lane == q) {
+            R[q * kIclsGramRs + q] = sqrt(zn);
+            a_i = bestp;
+            u_i = t;
+          }
+          if (lane == (bestp & 31)) actbits |= 1u << (bestp >> 5);
+          __syncwarp();
+          q += 1;
+          break;
+        }
+        // partial step: the blocking constraint leaves (icls.rs:385-398, 465-501)
+        sp += t * zn;
+        const int kd = drop;
+        const int dropped = __shfl_sync(kFull, a_i, kd);
+        if (lane < q) {  // each lane shifts its own row of R left past column kd
+          for (int col = kd; col < q - 1; ++col) R[lane * kIclsGramRs + col] = R[lane * kIclsGramRs + col + 1];
+          R[lane * kIclsGramRs + q - 1] = 0.0;
+        }
+        __syncwarp();
+        for (int i = kd; i < q - 1; ++i) {
+          const double aa = R[i * kIclsGramRs + i], bb = R[(i + 1) * kIclsGramRs + i];
+          if (bb == 0.0) continue;
+          const double rn = sqrt(aa * aa + bb * bb);
+          const double cg = aa / rn, sg = bb / rn;
+          __syncwarp();
+          for (int col = i + lane; col < q - 1; col += 32) {
+            const double ri = R[i * kIclsGramRs + col], rj = R[(i + 1) * kIclsGramRs + col];
+            R[i * kIclsGramRs + col] = cg * ri + sg * rj;
+            R[(i + 1) * kIclsGramRs + col] = -sg * ri + cg * rj;
+          }
+          __syncwarp();
+        }
+        {  // entry kd leaves the active list and the multipliers
+          const double un = __shfl_down_sync(kFull, u_i, 1);
+          const int an = __shfl_down_sync(kFull, a_i, 1);
+          if (lane >= kd && lane < q - 1) {
+            u_i = un;
+            a_i = an;
+          } else if (lane == q - 1) {
+            u_i = 0.0;
+            a_i = -1;
+          }
+        }
+        if (lane == (dropped & 31)) actbits &= ~(1u << (dropped >> 5));
+        __syncwarp();
+        q -= 1;
+      }
+      if (stop) break;
+    }
+    executed += static_cast<unsigned long long>(iters - 1);
+
+    // x = L^-T x~ (back substitution)
+    for (int i = K - 1; i >= 0; --i) {
+      const int owner = i & 31, oc = i >> 5;
+      double xi = 0.0;
+#pragma unroll
+      for (int c = 0; c < RPL; ++c)
+        if (c == oc && lane == owner) xi = xt[c] / __ldg(p.L + i * Kp + i);
+      xi = __shfl_sync(kFull, xi, owner);
+#pragma unroll
+      for (int c = 0; c < RPL; ++c) {
+        const int row = lane + 32 * c;
+        if (row < i) xt[c] -= __ldg(p.L + i * Kp + row) * xi;
+        if (row == i) xt[c] = xi;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < RPL; ++c) {
+      const int row = lane + 32 * c;
+      if (row < Kp) p.X[v * Kp + row] = (row < K) ? xt[c] : 0.0;
     }
     if (lane == 0) {
       p.iters[v] = static_cast<uint32_t>(iters - 1);

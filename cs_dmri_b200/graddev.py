@@ -47,13 +47,16 @@ def graddev_phantom(n_voxels, seed=3, sigma=0.02, drop_max=0.15):
 
 def shore_fit_graddev(signals, bvals, bvecs, graddev=None, sample_mask=None, *, alpha=0.01, radial_order=8,
                       zeta=700.0, big_delta=None, small_delta=None, b0_threshold=50.0, max_iter=1000, tol=1e-6,
-                      non_negative=False, device: int = 0) -> dict:
+                      non_negative=False, device: int = 0, precision: str = "fp64") -> dict:
     """L1 fit (fixed alpha, one per voxel allowed) of ``signals`` (V, N) on
     per-voxel designs.  ``graddev`` (V, 3, 3) deviation tensors (None =
     identity), ``sample_mask`` (V, N) bool of the samples each voxel keeps
     (None = all).  Inputs may be numpy arrays or CUDA tensors; outputs are
     CUDA tensors: ``coefficients`` (V, K) float64, ``iterations``,
-    ``converged``, ``lipschitz`` (sigma_max(M_v)^2 / n_v) and ``n_samples``."""
+    ``converged``, ``lipschitz`` (sigma_max(M_v)^2 / n_v) and ``n_samples``.
+    ``precision="fp64-kkt"`` (or "mixed-kkt") returns every voxel's
+    KKT-certified LASSO optimum on its own design instead of the reference
+    FISTA's stopped iterate; ``converged`` is then the certificate."""
     import torch
 
     dev = torch.device("cuda", device)
@@ -79,7 +82,8 @@ def shore_fit_graddev(signals, bvals, bvecs, graddev=None, sample_mask=None, *, 
             raise ValueError("alpha must be a scalar or one value per voxel")
         alpha = 0.0
     spec = _core.build_spec(radial_order=radial_order, zeta=zeta, regularization="l1", alpha_mode="fixed",
-                            alpha=float(alpha), max_iter=max_iter, tol=tol, non_negative=non_negative)
+                            alpha=float(alpha), max_iter=max_iter, tol=tol, non_negative=non_negative,
+                            precision=precision)
     K = _abi.load().csd_shore_n_coeffs(int(radial_order))
     out = {"coefficients": torch.empty((V, max(K, 0)), dtype=torch.float64, device=dev),
            "iterations": torch.empty(V, dtype=torch.int32, device=dev),

@@ -87,7 +87,8 @@ enum csd_precision {
    * witness of the reference's tests/common/mod.rs:127-153), instead of the
    * iterate the reference's stopping rule leaves (fista.rs:120-127), which
    * sits a relative 1e-5 .. 1e-2 from it.  A fixed number of FISTA
-   * iterations (csd_set_option CSD_OPT_KKT_ITERATIONS, default 32) finds
+   * iterations (chosen per table by a timed autotuning batch among 16, 24, 32 and 48,
+   * or fixed with csd_set_option CSD_OPT_KKT_ITERATIONS) finds
    * the support; an FP64 active-set polish (Lawson-Hanson style, with signs
    * in place of non-negativity) solves G_SS c_S = b_S - n alpha sign(c_S) on
    * it, moving coefficients in and out until no sign disagrees and every
@@ -252,6 +253,14 @@ typedef struct csd_fit_timing {
   uint64_t kkt_rounds;         /* polish rounds, summed over voxels and passes */
   double tf32_tensor_flops;    /* TF32 tensor-core FLOPs issued (2 per multiply-add) */
   double kkt_max;              /* largest KKT residual of a certified voxel */
+  /* host buffers of csd_shore_fit_volume (host clock; zero when unused) */
+  float ms_host_gather;        /* pageable input: masked rows gathered into page-locked staging (the
+                                  pipelined fit gathers chunk by chunk, overlapped with the device) */
+  float ms_host_copy_out;      /* pageable output: the page-locked output volume copied out */
+  int32_t kkt_iterations;      /* converged-optimum modes: support-identification iterations used */
+  float kkt_tune_ms[4];        /* the autotuner's batch times with 16, 24, 32 and 48 of them */
+  int64_t kkt_overflow[2];     /* voxels whose support outgrew the first polish pass (16 or 32
+                                  coefficients) and the second (32; 0 without one) */
 } csd_fit_timing;
 
 int csd_last_timing(const csd_handle* h, csd_fit_timing* out);
@@ -266,8 +275,9 @@ int csd_last_timing(const csd_handle* h, csd_fit_timing* out);
  *                           >= 2 also sets its cap (iteration of the first
  *                           pass' end, default 80)
  *   CSD_OPT_KKT_ITERATIONS  FISTA iterations of the converged-optimum
- *                           modes' support identification (1 .. 100000,
- *                           default 32)
+ *                           modes' support identification (1 .. 100000;
+ *                           0, the default, = the autotuner's choice per
+ *                           gradient table among 16, 24, 32 and 48)
  *   CSD_OPT_KKT_ROUNDS      solves the first polish of the converged-optimum
  *                           modes may take per voxel before the voxel goes
  *                           to the FP64 FISTA fallback (1 .. 4096, default 48)
@@ -278,13 +288,26 @@ int csd_last_timing(const csd_handle* h, csd_fit_timing* out);
  *                           makes the call return CSD_ERR_TIMEOUT
  *                           (1 .. 2e9 ns, default 2e9); a tiny value makes
  *                           that failure path testable
+ *   CSD_OPT_POLISH          first pass of the converged-optimum modes'
+ *                           active-set polish: 0 = one voxel per thread for
+ *                           supports of up to 16 (default), 1 = one voxel
+ *                           per warp for supports of up to 32; both take the
+ *                           same steps in the same order, and the supports
+ *                           that outgrow them go on to the wider passes
+ *   CSD_OPT_ICLS            amplitude-positivity QP kernel: 0 = the Gram
+ *                           form (constraint values carried through
+ *                           Gamma = W^T W; radial orders <= 6, the default),
+ *                           1 = the orthogonal-basis form (any order); both
+ *                           follow the reference's iteration path
  * Returns CSD_ERR_INVALID for an unknown option or value. */
 enum csd_option {
   CSD_OPT_FISTA_SHAPE = 1,
   CSD_OPT_FISTA_SCHEDULE = 2,
   CSD_OPT_KKT_ITERATIONS = 3,
   CSD_OPT_TENSOR_WAIT_NS = 4,
-  CSD_OPT_KKT_ROUNDS = 5
+  CSD_OPT_KKT_ROUNDS = 5,
+  CSD_OPT_POLISH = 6,
+  CSD_OPT_ICLS = 7
 };
 int csd_set_option(csd_handle* h, int32_t option, int64_t value);
 
@@ -416,7 +439,13 @@ int csd_shore_rtop_adjoint_device(csd_handle* h, int32_t radial_order, double ze
  * voxel: G_v = M_v^T M_v, L_v = sigma_max(M_v)^2 / n_v and the FISTA of
  * src/solver/fista.rs:70-143.  Radial orders 6 and 8.  Outputs (device):
  * coefficients (n_voxels, K) FP64, iterations, converged, and (nullable) L_v
- * and the kept sample count.  Asynchronous like the entry points above. */
+ * and the kept sample count.  Asynchronous like the entry points above.
+ * With precision FP64_KKT or MIXED_KKT each voxel's fit is its certified
+ * LASSO optimum (as for csd_shore_fit_volume; the support-identification
+ * iterations run in FP64 on the voxel's own Gram matrix, then one warp
+ * polishes and certifies): converged = certified, and the call waits for its
+ * work and reports the uncertified count and the polish rounds through
+ * csd_last_timing. */
 int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signals, int64_t n_voxels,
                                  const csd_gtab* gtab, const csd_shore_spec* spec,
                                  const double* d_graddev, const uint8_t* d_keep,

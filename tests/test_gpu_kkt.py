@@ -30,7 +30,7 @@ def kkt_iterations(k):
     try:
         yield
     finally:
-        _abi.set_option(_abi.OPT_KKT_ITERATIONS, 32)
+        _abi.set_option(_abi.OPT_KKT_ITERATIONS, 0)
 
 
 @pytest.fixture(scope="module")
@@ -195,3 +195,47 @@ def test_argument_errors(ph):
                   alpha=0.01, radial_order=8, **kw)
     with pytest.raises(ValueError, match="precision must be"):
         shore_fit(ph.data, ph.bvals, ph.bvecs, ph.mask, precision="tf32", **kw)
+
+
+def test_autotuned_support_identification(ph):
+    """With no fixed count the handle times the whole path on a synthetic
+    batch with 16, 24, 32 and 48 TF32 iterations, once per table, and uses
+    the fastest; a fixed count gives the same certified optimum."""
+    kw = dict(alpha_mode="fixed", alpha=0.01)
+    auto, t = fit(ph, "mixed-kkt", **kw)
+    times = list(t.kkt_tune_ms)
+    assert t.kkt_iterations in (16, 24, 32, 48) and all(x > 0 for x in times)
+    assert t.kkt_iterations == (16, 24, 32, 48)[int(np.argmin(times))]
+    other = 48 if t.kkt_iterations != 48 else 16
+    with kkt_iterations(other):
+        fixed, t2 = fit(ph, "mixed-kkt", **kw)
+    assert t2.kkt_iterations == other
+    both = auto["converged"] & fixed["converged"]
+    assert both.mean() >= 0.99
+    assert rel(auto["coef64"][both], fixed["coef64"][both]).max() <= 1e-6
+
+
+@pytest.mark.parametrize("k", [1, 32])
+def test_thread_and_warp_polish_take_the_same_steps(ph, k):
+    """The first polish pass one voxel per thread (supports up to 16, the
+    default) and one voxel per warp (up to 32) take the same steps in the same
+    order, so coefficients, iteration counts and certificates agree bit for
+    bit; with one support-identification iteration the starting supports are
+    wide and the voxels that outgrow 16 go on to the warp pass."""
+    from cs_dmri_b200 import _abi
+    kw = dict(alpha_mode="fixed", alpha=0.01)
+    with kkt_iterations(k):
+        a, ta = fit(ph, "mixed-kkt", **kw)
+        _abi.set_option(_abi.OPT_POLISH, 1)
+        try:
+            b, tb = fit(ph, "mixed-kkt", **kw)
+        finally:
+            _abi.set_option(_abi.OPT_POLISH, 0)
+    assert np.array_equal(a["coef64"], b["coef64"])
+    assert np.array_equal(a["iterations"], b["iterations"])
+    assert np.array_equal(a["converged"], b["converged"])
+    assert ta.kkt_overflow[0] >= tb.kkt_overflow[0] and tb.kkt_overflow[1] == 0
+    if k == 1:
+        assert ta.kkt_overflow[0] > 0
+    with pytest.raises(ValueError, match="invalid option"):
+        _abi.set_option(_abi.OPT_POLISH, 2)
