@@ -114,7 +114,7 @@ class Timing(C.Structure):
         ("ms_host_copy_out", C.c_float),
         ("kkt_iterations", C.c_int32),
         ("kkt_tune_ms", C.c_float * 4),
-        ("kkt_overflow", C.c_int64 * 2),
+        ("kkt_overflow", C.c_int64),
     ]
 
 
@@ -124,8 +124,7 @@ OPT_FISTA_SCHEDULE = 2
 OPT_KKT_ITERATIONS = 3
 OPT_TENSOR_WAIT_NS = 4
 OPT_KKT_ROUNDS = 5
-OPT_POLISH = 6
-OPT_ICLS = 7
+OPT_ICLS = 6
 
 
 # Every symbol include/csd_shore.h declares, for load checks.

@@ -332,7 +332,7 @@ struct csd_handle {
   // converged-optimum modes: the TF32 B operand (per table), the iterate,
   // per-voxel KKT residuals, overflow / failure lists, counters
   // [batches, error, n_overflow, n_failed, rounds, kkt max bits, n_failed2]
-  DevBuf gtf32, x32, kktv, kktovf, kktovf2, kktfail, kktstat;
+  DevBuf gtf32, x32, kktv, kktovf, kktfail, kktstat;
   uint64_t gtf32_key = 0;
   bool gtf32_valid = false;
   cudaEvent_t kev[5] = {};
@@ -341,7 +341,6 @@ struct csd_handle {
   int opt_schedule = -1;
   int opt_kkt_iters = 0;  // 0: the autotuner's choice per table
   int opt_kkt_rounds = 48;
-  int opt_polish = 0;  // first polish pass: 0 = thread per voxel, 1 = warp per voxel
   // page-locked, mapped staging volume for pageable host inputs: the masked
   // rows are gathered into it on host threads and read in place by the device
   float* stage = nullptr;
@@ -350,7 +349,7 @@ struct csd_handle {
   size_t ostage_bytes = 0;
   unsigned long long opt_wait_ns = 2000000000ull;  // tensor-core completion waits
   unsigned long long kkt_batches = 0, kkt_fallback = 0, kkt_rounds = 0, kkt_uncertified = 0, kkt_iter_add = 0;
-  unsigned long long kkt_overflow[2] = {0, 0};
+  unsigned long long kkt_overflow = 0;  // supports that outgrew the first polish pass
   double kkt_max = 0.0;
   float kkt_ms[3] = {0.f, 0.f, 0.f};  // iterate, first polish, fallback (FISTA + last polish)
   float kkt_ms_last_polish = 0.f;
@@ -969,25 +968,6 @@ void launch_polish(csd_handle* h, const csd::PolishParams& q, int warps, int64_t
   }
 }
 
-// The thread-per-voxel first polish: one CTA of kTpvWarps warps per SM (its
-// shared memory holds each lane's factor), lanes taking voxels from `queue`.
-template <int RPL>
-void launch_polish_tpv_t(csd_handle* h, const csd::PolishParams& q, unsigned long long* queue) {
-  const size_t smem = sizeof(double) * static_cast<size_t>(csd::kTpvWarps) * csd::kTpvWarpDoubles;
-  CSD_CUDA(cudaFuncSetAttribute(csd::k_l1_polish_tpv<RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(smem)));
-  int per_sm = 0;
-  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_l1_polish_tpv<RPL>, 32 * csd::kTpvWarps,
-                                                         smem));
-  if (per_sm < 1) throw Error{CSD_ERR_CUDA, "thread-per-voxel polish: no CTA fits an SM"};
-  const int64_t lanes = 32 * csd::kTpvWarps;
-  const int blocks = static_cast<int>(std::max<int64_t>(
-      1, std::min<int64_t>(static_cast<int64_t>(h->num_sms) * per_sm, (std::max<int64_t>(q.n_work, 1) + lanes - 1) / lanes)));
-  CSD_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), h->stream));
-  csd::k_l1_polish_tpv<RPL><<<blocks, 32 * csd::kTpvWarps, smem, h->stream>>>(q, queue);
-  CSD_LAUNCH();
-}
-
 void launch_fista_kkt(csd_handle* h, int MT, const csd::FistaParams& p);
 
 // Autotuning of the converged-optimum modes' support-identification
@@ -1080,14 +1060,12 @@ void launch_fista_kkt(csd_handle* h, int MT, const csd::FistaParams& p) {
   const int k1 = h->opt_kkt_iters > 0 ? h->opt_kkt_iters : h->kkt_iters_used;
   // stat: [0] tensor batches, [1] tensor error, [2] first-pass overflows,
   // [3] failures (the fallback's list), [4] rounds, [5] largest KKT residual
-  // (bits), [6] uncertified, [7] unused overflow count, [8] second-pass
-  // overflows
-  h->kktstat.ensure(10 * sizeof(unsigned long long));
+  // (bits), [6] uncertified, [7] unused overflow count
+  h->kktstat.ensure(8 * sizeof(unsigned long long));
   auto* stat = h->kktstat.as<unsigned long long>();
-  CSD_CUDA(cudaMemsetAsync(stat, 0, 10 * sizeof(unsigned long long), st));
+  CSD_CUDA(cudaMemsetAsync(stat, 0, 8 * sizeof(unsigned long long), st));
   h->kktv.ensure(sizeof(double) * std::max<int64_t>(V, 1));
   h->kktovf.ensure(sizeof(int64_t) * std::max<int64_t>(p.n_work, 1));
-  h->kktovf2.ensure(sizeof(int64_t) * std::max<int64_t>(p.n_work, 1));
   h->kktfail.ensure(sizeof(int64_t) * std::max<int64_t>(p.n_work, 1));
   for (auto& e : h->kev)
     if (!e) CSD_CUDA(cudaEventCreate(&e));
@@ -1175,46 +1153,24 @@ void launch_fista_kkt(csd_handle* h, int MT, const csd::FistaParams& p) {
   pp.round_total = stat + 4;
   pp.kkt_max_bits = stat + 5;
   pp.n_uncertified = stat + 6;  // non-finite inputs (failures go to the fallback list)
-  csd::PolishParams po = pp;    // the pass over the supports that outgrew the first
-  if (h->opt_polish == 0) {
-    // thread per voxel (supports <= kTpvCap), then a warp per voxel for the
-    // supports that outgrew it, then room for all K
-    pp.cap = csd::kTpvCap;
-    if ((K + 31) / 32 == 1)
-      launch_polish_tpv_t<1>(h, pp, p.queue);
-    else if ((K + 31) / 32 == 3)
-      launch_polish_tpv_t<3>(h, pp, p.queue);
-    else
-      throw Error{CSD_ERR_INVALID, "the converged-optimum polish is built for radial orders <= 6"};
-    csd::PolishParams pw = pp;
-    pw.cap = std::min(kPolishCap, K);
-    pw.list = h->kktovf.as<int64_t>();
-    pw.list_len = stat + 2;
-    pw.overflow = h->kktovf2.as<int64_t>();
-    pw.n_overflow = stat + 8;
-    launch_polish(h, pw, 8, p.n_work);
-    po.list = h->kktovf2.as<int64_t>();
-    po.list_len = stat + 8;
-  } else {
-    launch_polish(h, pp, 8, p.n_work);
-    po.list = h->kktovf.as<int64_t>();
-    po.list_len = stat + 2;
-  }
+  launch_polish(h, pp, 8, p.n_work);
+  csd::PolishParams po = pp;
+  po.list = h->kktovf.as<int64_t>();
+  po.list_len = stat + 2;
   // supports that outgrew the warp slice: again with room for all K
   po.cap = K;
   po.overflow = h->kktovf.as<int64_t>();  // unused: cap = K cannot overflow
   po.n_overflow = stat + 7;
   launch_polish(h, po, 4, p.n_work);
   CSD_CUDA(cudaEventRecord(h->kev[2], st));
-  unsigned long long hs[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long hs[6] = {0, 0, 0, 0, 0, 0};
   CSD_CUDA(cudaMemcpyAsync(hs, stat, sizeof hs, cudaMemcpyDeviceToHost, st));
   CSD_CUDA(cudaStreamSynchronize(st));
   if (static_cast<int>(hs[1]) != 0)
     throw Error{CSD_ERR_TIMEOUT, "TF32 FISTA: a tensor-core completion wait gave up"};
   h->kkt_batches = hs[0];
   h->kkt_fallback = hs[3];
-  h->kkt_overflow[0] = hs[2];
-  h->kkt_overflow[1] = h->opt_polish == 0 ? hs[8] : 0;
+  h->kkt_overflow = hs[2];
   if (hs[3] > 0) {
     // the FP64 FISTA path with the reference stopping rule, then a last polish
     csd::FistaParams r = p;
@@ -1716,7 +1672,7 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
   h->mixed_ops = 0.0;
   h->mixed_rerun = 0;
   h->kkt_batches = h->kkt_fallback = h->kkt_rounds = h->kkt_uncertified = h->kkt_iter_add = 0;
-  h->kkt_overflow[0] = h->kkt_overflow[1] = 0;
+  h->kkt_overflow = 0;
   h->kkt_max = 0.0;
   h->kkt_ms[0] = h->kkt_ms[1] = h->kkt_ms[2] = 0.f;
   const bool is_l1 = spec->regularization == CSD_REG_L1;
@@ -2050,7 +2006,7 @@ FitInfo run_fit(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64
                                  ? (h->opt_kkt_iters > 0 ? h->opt_kkt_iters : h->kkt_iters_used)
                                  : 0;
   for (int i = 0; i < 4; ++i) h->timing.kkt_tune_ms[i] = h->kkt_tune_ms[i];
-  for (int i = 0; i < 2; ++i) h->timing.kkt_overflow[i] = static_cast<int64_t>(h->kkt_overflow[i]);
+  h->timing.kkt_overflow = static_cast<int64_t>(h->kkt_overflow);
   if (h->precision == CSD_PRECISION_MIXED_KKT && K <= 80) {
     const int ks = (K + 7) / 8, nb = 16 * ((K + 15) / 16);
     h->timing.tf32_tensor_flops = static_cast<double>(h->kkt_batches) * ks * 2.0 * 128 * nb * 8;
@@ -2156,7 +2112,7 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   h->mixed_ops = 0.0;
   h->mixed_rerun = 0;
   h->kkt_batches = h->kkt_fallback = h->kkt_rounds = h->kkt_uncertified = h->kkt_iter_add = 0;
-  h->kkt_overflow[0] = h->kkt_overflow[1] = 0;
+  h->kkt_overflow = 0;
   h->kkt_max = 0.0;
   h->kkt_ms[0] = h->kkt_ms[1] = h->kkt_ms[2] = 0.f;
   record(h, 0);
@@ -2462,7 +2418,7 @@ void csd_destroy(csd_handle* h) {
                     &h->iota, &h->adjW, &h->adjovf, &h->adjstat, &h->adjconst,
                     &h->gdtab, &h->gdq, &h->tuneB, &h->tuneX, &h->tuneIt, &h->tuneConv, &h->tuneQ,
                     &h->schedY, &h->schedPend, &h->schedKey, &h->schedOrder, &h->schedCnt,
-                    &h->schedD, &h->schedU, &h->schedN, &h->gtf32, &h->x32, &h->kktv, &h->kktovf, &h->kktovf2,
+                    &h->schedD, &h->schedU, &h->schedN, &h->gtf32, &h->x32, &h->kktv, &h->kktovf,
                     &h->kktfail, &h->kktstat};
   for (auto s : h->pipe)
     if (s) cudaStreamSynchronize(s);
@@ -2917,10 +2873,6 @@ int csd_set_option(csd_handle* h, int32_t option, int64_t value) {
     case CSD_OPT_TENSOR_WAIT_NS:
       if (value < 1 || value > 2000000000LL) return CSD_ERR_INVALID;
       h->opt_wait_ns = static_cast<unsigned long long>(value);
-      return CSD_OK;
-    case CSD_OPT_POLISH:
-      if (value != 0 && value != 1) return CSD_ERR_INVALID;
-      h->opt_polish = static_cast<int>(value);
       return CSD_OK;
     case CSD_OPT_ICLS:
       if (value != 0 && value != 1) return CSD_ERR_INVALID;

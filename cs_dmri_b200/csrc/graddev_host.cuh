@@ -17,7 +17,13 @@ extern "C" int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signal
     CSD_CUDA(cudaSetDevice(h->device));
     HostGtab g = make_gtab(gtab);
     std::string warnings;
-    validate(spec, g, warnings);
+    if (spec->precision < CSD_PRECISION_FP64 || spec->precision > CSD_PRECISION_FP64_KKT)
+      throw Error{CSD_ERR_INVALID, "unknown precision"};
+    // the shared checks; the precisions this fit takes are checked below (its
+    // converged-optimum mode also serves radial order 8)
+    csd_shore_spec shared = *spec;
+    shared.precision = CSD_PRECISION_FP64;
+    validate(&shared, g, warnings);
     if (spec->regularization != CSD_REG_L1 || spec->alpha_mode != CSD_ALPHA_FIXED)
       throw Error{CSD_ERR_INVALID, "the per-voxel-design fit takes regularization l1 with alpha_mode fixed"};
     if (spec->radial_order != 6 && spec->radial_order != 8)

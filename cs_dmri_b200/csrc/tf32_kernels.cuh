@@ -678,287 +678,4 @@ __global__ void __launch_bounds__(256, 4) k_l1_polish(PolishParams p) {
   if (p.round_total && lane == 0) atomicAdd(p.round_total, rounds_sum);  // every lane holds the warp's count
 }
 
-// ---------------------------------------------------------- thread per voxel
-
-constexpr int kTpvCap = 16;                          // support held per thread
-constexpr int kTpvTri = kTpvCap * (kTpvCap + 1) / 2;
-constexpr int kTpvWarps = 5;                         // warps per CTA (one CTA per SM)
-// Per-warp shared memory in doubles: the packed factor, z and the current
-// point by support position ([entry][lane], conflict-free), then the
-// support indices and signs (bytes) and the per-slot gradient results.
-constexpr int kTpvWarpDoubles = (kTpvTri + 2 * kTpvCap) * 32 + (2 * kTpvCap * 32) / 8 + 2 * 32 + 32;
-
-// The same active-set method as k_l1_polish, one voxel per THREAD: each lane
-// factors and solves its own voxel's G_SS (supports up to kTpvCap) in its own
-// column of the warp's shared memory, and the warp computes the 72-wide
-// gradient of the KKT check together, one voxel at a time (lanes over the
-// coefficients).  Lanes that finish a voxel take the next from a device
-// counter.  Supports that outgrow kTpvCap go to the `overflow` list, voxels
-// not certified within the round limit (or with a G_SS that is not positive
-// definite) to `failed`; both are finished by k_l1_polish.
-template <int RPL>
-__global__ void __launch_bounds__(32 * kTpvWarps, 1) k_l1_polish_tpv(PolishParams p, unsigned long long* queue) {
-  extern __shared__ __align__(16) double tpv_smem[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* base = tpv_smem + static_cast<size_t>(warp) * kTpvWarpDoubles;
-  double* T = base;                                   // [kTpvTri][32]
-  double* zz = T + kTpvTri * 32;                      // [cap][32]
-  double* cc = zz + kTpvCap * 32;                     // [cap][32]
-  uint8_t* si = reinterpret_cast<uint8_t*>(cc + kTpvCap * 32);  // [cap][32] coefficient index
-  int8_t* sg = reinterpret_cast<int8_t*>(si + kTpvCap * 32);    // [cap][32] sign
-  double* r_best = cc + kTpvCap * 32 + (2 * kTpvCap * 32) / 8;  // [32] worst violation
-  double* r_act = r_best + 32;                        // [32] largest active residual
-  int* r_j = reinterpret_cast<int*>(r_act + 32);      // [32] its coefficient | sign << 16
-  const unsigned full = 0xffffffffu;
-  const int K = p.K, Kp = p.Kp;
-  const double n = p.n_samples, n_inv = 1.0 / p.n_samples;
-  const double nan = __longlong_as_double(0x7ff8000000000000ll);
-  const int64_t n_items = p.list_len ? static_cast<int64_t>(*p.list_len) : p.n_work;
-  auto at = [&](double* a, int e) -> double& { return a[e * 32 + lane]; };
-
-  // lane state
-  int64_t v = -1;
-  double alpha = 0.0;
-  int s = 0, round = 0;
-  bool need_solve = false, need_grad = false, drained = false;
-  unsigned long long rounds_sum = 0;
-
-  // The end of a lane's voxel, written as k_l1_polish writes it: certified,
-  // not certified (round limit, or a G_SS that is not positive definite), or
-  // handed to the overflow list.
-  auto finish = [&](bool certified, double kkt_val, bool overflowed) {
-    if (overflowed) {
-      p.overflow[atomicAdd(p.n_overflow, 1ull)] = v;
-    } else {
-      if (certified || !p.keep_on_fail) {
-        for (int j = 0; j < Kp; ++j) p.X[v * Kp + j] = 0.0;
-        if (certified)
-          for (int i = 0; i < s; ++i) p.X[v * Kp + si[i * 32 + lane]] = at(cc, i);
-      }
-      p.conv[v] = certified ? 1 : 0;
-      p.iters[v] = (p.it_add ? p.iters[v] : static_cast<uint32_t>(p.it_base)) + static_cast<uint32_t>(round);
-      if (p.kkt) p.kkt[v] = certified ? kkt_val : nan;
-      if (!certified && p.failed) p.failed[atomicAdd(p.n_failed, 1ull)] = v;
-      if (!certified && !p.failed && p.n_uncertified) atomicAdd(p.n_uncertified, 1ull);
-      if (certified && p.kkt_max_bits)
-        atomicMax(p.kkt_max_bits, static_cast<unsigned long long>(__double_as_longlong(kkt_val)));
-    }
-    rounds_sum += static_cast<unsigned long long>(round);
-    v = -1;
-    need_solve = need_grad = false;
-  };
-
-  while (true) {
-    // ---- take a new voxel into an empty lane
-    if (v < 0 && !drained) {
-      const unsigned long long it = atomicAdd(queue, 1ull);
-      drained = it >= static_cast<unsigned long long>(n_items);
-      if (!drained) {
-        v = p.list ? p.list[it] : static_cast<int64_t>(it);
-        alpha = p.alpha_v ? p.alpha_v[v] : p.alpha;
-        s = 0;
-        round = 0;
-        bool finite = true;
-        for (int j = 0; j < K; ++j) {
-          const double b = p.B[v * Kp + j];
-          const double x0 = p.S32 ? static_cast<double>(p.S32[v * Kp + j]) : p.S64[v * Kp + j];
-          finite = finite && isfinite(b) && isfinite(x0);
-          int f = x0 > 0.0 ? 1 : (x0 < 0.0 ? -1 : 0);
-          if (p.non_negative && f < 0) f = 0;
-          if (f != 0) {
-            if (s < kTpvCap) {
-              si[s * 32 + lane] = static_cast<uint8_t>(j);
-              sg[s * 32 + lane] = static_cast<int8_t>(f);
-              at(cc, s) = x0;
-            }
-            ++s;
-          }
-        }
-        if (!finite) {
-          for (int j = 0; j < Kp; ++j) p.X[v * Kp + j] = 0.0;
-          p.conv[v] = 0;
-          p.iters[v] = p.it_add ? p.iters[v] : static_cast<uint32_t>(p.it_base);
-          if (p.kkt) p.kkt[v] = nan;
-          if (p.n_uncertified) atomicAdd(p.n_uncertified, 1ull);
-          v = -1;
-        } else if (s > kTpvCap) {
-          finish(false, 0.0, true);
-        } else {
-          need_solve = true;
-        }
-      }
-    }
-    if (!__any_sync(full, v >= 0)) break;
-    // ---- one solve per lane that needs one (a round)
-    if (need_solve) {
-      if (round >= p.rounds) {
-        finish(false, 0.0, false);
-      } else {
-        ++round;
-        for (int i = 0; i < s; ++i) {
-          const int gi = si[i * 32 + lane];
-          const double* grow = p.G + gi * Kp;
-          for (int k = 0; k <= i; ++k) at(T, pk_row(i) + k) = grow[si[k * 32 + lane]];
-          at(zz, i) = p.B[v * Kp + gi] - n * alpha * static_cast<double>(sg[i * 32 + lane]);
-        }
-        bool pd = true;
-        for (int j = 0; j < s; ++j) {  // Cholesky by columns; the diagonal keeps 1 / L_jj
-          const double d = at(T, pk_row(j) + j);
-          if (!(d > 0.0)) {
-            pd = false;
-            break;
-          }
-          const double r = rsqrt(d);
-          at(T, pk_row(j) + j) = r;
-          for (int i = j + 1; i < s; ++i) at(T, pk_row(i) + j) *= r;
-          for (int i = j + 1; i < s; ++i) {
-            const double lij = at(T, pk_row(i) + j);
-            for (int k = j + 1; k <= i; ++k) at(T, pk_row(i) + k) = fma(-lij, at(T, pk_row(k) + j), at(T, pk_row(i) + k));
-          }
-        }
-        if (!pd) {
-          finish(false, 0.0, false);
-        } else {
-          for (int i = 0; i < s; ++i) {  // L y = rhs
-            double y = at(zz, i);
-            for (int k = 0; k < i; ++k) y = fma(-at(T, pk_row(i) + k), at(zz, k), y);
-            at(zz, i) = y * at(T, pk_row(i) + i);
-          }
-          for (int i = s - 1; i >= 0; --i) {  // L^T z = y, in k_l1_polish's order
-            double z = at(zz, i);
-            for (int k = s - 1; k > i; --k) z = fma(-at(T, pk_row(k) + i), at(zz, k), z);
-            at(zz, i) = z * at(T, pk_row(i) + i);
-          }
-          double tmin = 2.0;
-          for (int i = 0; i < s; ++i) {
-            const double z = at(zz, i), c = at(cc, i);
-            if (z * static_cast<double>(sg[i * 32 + lane]) <= 0.0) tmin = fmin(tmin, c / (c - z));
-          }
-          if (tmin < 1.0) {  // move to the first zero crossing; drop what reaches zero
-            int w = 0;
-            for (int i = 0; i < s; ++i) {
-              const double z = at(zz, i), c = at(cc, i);
-              const int sgi = sg[i * 32 + lane];
-              bool drop = false;
-              if (z * static_cast<double>(sgi) <= 0.0) drop = c / (c - z) <= tmin * (1.0 + 1e-12);
-              const double cn = fma(tmin, z - c, c);
-              if (cn * static_cast<double>(sgi) <= 0.0) drop = true;
-              if (!drop) {
-                si[w * 32 + lane] = si[i * 32 + lane];
-                sg[w * 32 + lane] = static_cast<int8_t>(sgi);
-                at(cc, w) = cn;
-                ++w;
-              }
-            }
-            s = w;
-          } else {
-            for (int i = 0; i < s; ++i) at(cc, i) = at(zz, i);
-            need_solve = false;
-            need_grad = true;
-          }
-        }
-      }
-    }
-    __syncwarp();
-    // ---- the KKT gradient of each lane whose solve kept its signs, the warp
-    // together: lanes over the coefficients, G symmetric (row S_i)
-    unsigned gm = __ballot_sync(full, need_grad);
-    while (gm) {
-      const int w = __ffs(gm) - 1;
-      gm &= gm - 1;
-      const int sw = __shfl_sync(full, s, w);
-      const int64_t vw = __shfl_sync(full, v, w);
-      const double aw = __shfl_sync(full, alpha, w);
-      double gq[RPL];
-      int inq[RPL];
-#pragma unroll
-      for (int q = 0; q < RPL; ++q) {
-        gq[q] = 0.0;
-        inq[q] = 0;
-      }
-      for (int i = 0; i < sw; ++i) {
-        const int jj = si[i * 32 + w];
-        const double ci = cc[i * 32 + w];
-        const int sgi = sg[i * 32 + w];
-        const double* grow = p.G + jj * Kp;
-#pragma unroll
-        for (int q = 0; q < RPL; ++q) {
-          const int j = lane + 32 * q;
-          if (j < K) {
-            gq[q] = fma(grow[j], ci, gq[q]);
-            if (j == jj) inq[q] = sgi;
-          }
-        }
-      }
-      double best = -INFINITY, act = 0.0;
-      int bj = 0x7fff, bsg = 0;
-#pragma unroll
-      for (int q = 0; q < RPL; ++q) {
-        const int j = lane + 32 * q;
-        if (j < K) {
-          const double g = (gq[q] - p.B[vw * Kp + j]) * n_inv;
-          if (inq[q] != 0) {
-            act = fmax(act, fabs(g + aw * static_cast<double>(inq[q])));
-          } else {
-            const double exc = p.non_negative ? -g - aw : fabs(g) - aw;
-            if (exc > best) {
-              best = exc;
-              bj = j;
-              bsg = (p.non_negative || g < 0.0) ? 1 : -1;
-            }
-          }
-        }
-      }
-      for (int o = 16; o > 0; o >>= 1) {  // arg-max over the warp, ties to the lowest index
-        const double ob = __shfl_xor_sync(full, best, o);
-        const int oj = __shfl_xor_sync(full, bj, o);
-        const int os = __shfl_xor_sync(full, bsg, o);
-        if (ob > best || (ob == best && oj < bj)) {
-          best = ob;
-          bj = oj;
-          bsg = os;
-        }
-        act = fmax(act, __shfl_xor_sync(full, act, o));
-      }
-      if (lane == 0) {
-        r_best[w] = best;
-        r_act[w] = act;
-        r_j[w] = bj | ((bsg > 0 ? 1 : 0) << 16);
-      }
-    }
-    __syncwarp();
-    if (need_grad) {
-      need_grad = false;
-      const double best = r_best[lane];
-      const int bj = r_j[lane] & 0xFFFF;
-      const int bsg = (r_j[lane] >> 16) ? 1 : -1;
-      if (best > p.kappa * alpha && bj < K) {
-        if (s + 1 > kTpvCap) {
-          finish(false, 0.0, true);
-        } else {  // bj joins at zero, in index order
-          int pos = s;
-          while (pos > 0 && si[(pos - 1) * 32 + lane] > bj) {
-            si[pos * 32 + lane] = si[(pos - 1) * 32 + lane];
-            sg[pos * 32 + lane] = sg[(pos - 1) * 32 + lane];
-            at(cc, pos) = at(cc, pos - 1);
-            --pos;
-          }
-          si[pos * 32 + lane] = static_cast<uint8_t>(bj);
-          sg[pos * 32 + lane] = static_cast<int8_t>(bsg);
-          at(cc, pos) = 0.0;
-          ++s;
-          need_solve = true;
-        }
-      } else {
-        finish(true, fmax(r_act[lane], fmax(best, 0.0)), false);
-      }
-    }
-    __syncwarp();
-  }
-  if (p.round_total) {
-    for (int o = 16; o > 0; o >>= 1) rounds_sum += __shfl_xor_sync(full, rounds_sum, o);
-    if (lane == 0) atomicAdd(p.round_total, rounds_sum);
-  }
-}
-
 }  // namespace csd

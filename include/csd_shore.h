@@ -259,8 +259,7 @@ typedef struct csd_fit_timing {
   float ms_host_copy_out;      /* pageable output: the page-locked output volume copied out */
   int32_t kkt_iterations;      /* converged-optimum modes: support-identification iterations used */
   float kkt_tune_ms[4];        /* the autotuner's batch times with 16, 24, 32 and 48 of them */
-  int64_t kkt_overflow[2];     /* voxels whose support outgrew the first polish pass (16 or 32
-                                  coefficients) and the second (32; 0 without one) */
+  int64_t kkt_overflow;        /* voxels whose support outgrew the first polish pass (32 coefficients) */
 } csd_fit_timing;
 
 int csd_last_timing(const csd_handle* h, csd_fit_timing* out);
@@ -288,12 +287,6 @@ int csd_last_timing(const csd_handle* h, csd_fit_timing* out);
  *                           makes the call return CSD_ERR_TIMEOUT
  *                           (1 .. 2e9 ns, default 2e9); a tiny value makes
  *                           that failure path testable
- *   CSD_OPT_POLISH          first pass of the converged-optimum modes'
- *                           active-set polish: 0 = one voxel per thread for
- *                           supports of up to 16 (default), 1 = one voxel
- *                           per warp for supports of up to 32; both take the
- *                           same steps in the same order, and the supports
- *                           that outgrow them go on to the wider passes
  *   CSD_OPT_ICLS            amplitude-positivity QP kernel: 0 = the Gram
  *                           form (constraint values carried through
  *                           Gamma = W^T W; radial orders <= 6, the default),
@@ -306,8 +299,7 @@ enum csd_option {
   CSD_OPT_KKT_ITERATIONS = 3,
   CSD_OPT_TENSOR_WAIT_NS = 4,
   CSD_OPT_KKT_ROUNDS = 5,
-  CSD_OPT_POLISH = 6,
-  CSD_OPT_ICLS = 7
+  CSD_OPT_ICLS = 6
 };
 int csd_set_option(csd_handle* h, int32_t option, int64_t value);
 

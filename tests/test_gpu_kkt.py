@@ -213,29 +213,3 @@ def test_autotuned_support_identification(ph):
     both = auto["converged"] & fixed["converged"]
     assert both.mean() >= 0.99
     assert rel(auto["coef64"][both], fixed["coef64"][both]).max() <= 1e-6
-
-
-@pytest.mark.parametrize("k", [1, 32])
-def test_thread_and_warp_polish_take_the_same_steps(ph, k):
-    """The first polish pass one voxel per thread (supports up to 16, the
-    default) and one voxel per warp (up to 32) take the same steps in the same
-    order, so coefficients, iteration counts and certificates agree bit for
-    bit; with one support-identification iteration the starting supports are
-    wide and the voxels that outgrow 16 go on to the warp pass."""
-    from cs_dmri_b200 import _abi
-    kw = dict(alpha_mode="fixed", alpha=0.01)
-    with kkt_iterations(k):
-        a, ta = fit(ph, "mixed-kkt", **kw)
-        _abi.set_option(_abi.OPT_POLISH, 1)
-        try:
-            b, tb = fit(ph, "mixed-kkt", **kw)
-        finally:
-            _abi.set_option(_abi.OPT_POLISH, 0)
-    assert np.array_equal(a["coef64"], b["coef64"])
-    assert np.array_equal(a["iterations"], b["iterations"])
-    assert np.array_equal(a["converged"], b["converged"])
-    assert ta.kkt_overflow[0] >= tb.kkt_overflow[0] and tb.kkt_overflow[1] == 0
-    if k == 1:
-        assert ta.kkt_overflow[0] > 0
-    with pytest.raises(ValueError, match="invalid option"):
-        _abi.set_option(_abi.OPT_POLISH, 2)
