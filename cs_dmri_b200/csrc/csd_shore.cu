@@ -276,8 +276,9 @@ struct csd_handle {
   uint64_t icls_key = 0;
   int icls_m = 0, icls_m_pad = 0, icls_lmax = 0, icls_qmax = 0;
   DevBuf dirs, Cmat, Le, Wi, Q1, ovf;
-  // Gram form of the amplitude ICLS (active sets <= 32): W^T W, W^T, C = Y P
-  DevBuf icls_gam, icls_wt, icls_y, icls_pf, icls_jcol;
+  // Gram form of the amplitude ICLS (active sets <= 32): W^T W, G^-1 C^T,
+  // G^-1, C = Y P
+  DevBuf icls_gam, icls_ut, icls_ginv, icls_y, icls_pf, icls_jcol;
   bool icls_gram = false;  // the Gram-form kernel serves this table
   int icls_nsh = 0;
   int opt_icls = 0;        // 0 = Gram form where it applies, 1 = the Q1 form
@@ -593,11 +594,17 @@ void ensure_icls_setup(csd_handle* h, int radial_order, double zeta, double eps)
   h->icls_gram = h->icls_nsh <= 32 && m_pad == 32 * kIclsGramCpl && Kp <= 96 &&
                  csd::icls_gram_smem(h->icls_nsh, m_pad) <= static_cast<size_t>(h->smem_optin);
   if (h->icls_gram) {
-    const int64_t n_set = static_cast<int64_t>(m_pad) * m_pad + static_cast<int64_t>(m_pad) * Kp;
-    h->icls_gam.ensure(sizeof(double) * static_cast<size_t>(m_pad) * m_pad);
-    h->icls_wt.ensure(sizeof(double) * static_cast<size_t>(m_pad) * Kp);
-    csd::k_icls_gram_setup<<<static_cast<unsigned>((n_set + 255) / 256), 256, 0, st>>>(
-        h->Wi.as<double>(), K, Kp, m_pad, h->icls_gam.as<double>(), h->icls_wt.as<double>());
+    const int64_t n_gam = static_cast<int64_t>(m_pad) * m_pad;
+    h->icls_gam.ensure(sizeof(double) * static_cast<size_t>(n_gam));
+    csd::k_icls_gram_setup<<<static_cast<unsigned>((n_gam + 255) / 256), 256, 0, st>>>(
+        h->Wi.as<double>(), K, m_pad, h->icls_gam.as<double>());
+    CSD_LAUNCH();
+    h->icls_ut.ensure(sizeof(double) * static_cast<size_t>(m_pad) * Kp);
+    h->icls_ginv.ensure(sizeof(double) * static_cast<size_t>(Kp) * Kp);
+    CSD_CUDA(cudaMemsetAsync(h->icls_ginv.p, 0, sizeof(double) * static_cast<size_t>(Kp) * Kp, st));
+    csd::k_icls_gram_solves<<<(m_pad + K + 127) / 128, 128, 0, st>>>(h->Le.as<double>(), K, Kp, h->Wi.as<double>(),
+                                                                   m_pad, h->icls_ut.as<double>(),
+                                                                   h->icls_ginv.as<double>());
     CSD_LAUNCH();
     const int ny = h->icls_nsh * m_pad;
     h->icls_y.ensure(sizeof(double) * static_cast<size_t>(ny));
@@ -1437,9 +1444,9 @@ template <int RPL>
 void launch_icls_gram_t(csd_handle* h, const csd::IclsParams& p) {
   csd::IclsGramParams g{};
   g.B = p.B;
-  g.L = p.L;
+  g.Ginv = h->icls_ginv.as<double>();
   g.Gam = h->icls_gam.as<double>();
-  g.WT = h->icls_wt.as<double>();
+  g.UT = h->icls_ut.as<double>();
   g.Y = h->icls_y.as<double>();
   g.pf = h->icls_pf.as<double>();
   g.jcol = h->icls_jcol.as<int>();
@@ -2407,7 +2414,7 @@ void csd_destroy(csd_handle* h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   DevBuf* bufs[] = {&h->bvals, &h->bvecs, &h->M, &h->Mt, &h->G, &h->A, &h->gfrag, &h->mfrag, &h->mtfrag, &h->sst_v, &h->mom, &h->scal, &h->ok, &h->dirs, &h->Cmat, &h->Le, &h->Wi, &h->Q1, &h->ovf,
-                    &h->icls_gam, &h->icls_wt, &h->icls_y, &h->icls_pf, &h->icls_jcol,
+                    &h->icls_gam, &h->icls_ut, &h->icls_ginv, &h->icls_y, &h->icls_pf, &h->icls_jcol,
                     &h->data, &h->mask, &h->coeffs, &h->r2, &h->resid, &h->iters_map, &h->kind_map,
                     &h->alpha_map, &h->bic_map, &h->rss_map, &h->blk, &h->total, &h->vox, &h->B, &h->X, &h->sig,
                     &h->iters, &h->conv, &h->queue, &h->itotal, &h->resid_v, &h->nnz_v, &h->amax,

@@ -476,39 +476,63 @@ __global__ void __launch_bounds__(32 * kIclsWarps) k_icls(IclsParams p) {
 //   d1 = Q1^T w_p = R^-T Gamma[A, p]      (Q1 = W_A R^-1 is never formed),
 //   z . n_p = |v|^2 = Gamma[p, p] - |d1|^2,   r = R^-1 d1,
 //   v = w_p - W_A r,  so the constraint values s = W^T x~ move by
-//   t (Gamma[:, p] - Gamma[:, A] r) and x~ by t (w_p - W_A r).
-// A step therefore costs (q + 1) columns of Gamma instead of the K-wide
-// products with Q1, and the scan for the most violated constraint reads s
-// from registers instead of recomputing W^T x~ (m x K) every iteration.  The
-// first s = C x0 (x0 the unconstrained minimiser) comes from C = Y P: z0 = P x0
-// (one term per column) and s = Y z0, with Y (nsh x m) in shared memory.
-// The reference's multiplier rule is kept as is (a full step pushes t for
-// the new constraint), so drops follow its iteration path; the carried s
-// and x~ differ from recomputed ones by rounding only.  Active sets of up to
-// 32 are held one entry per lane (rank C = nsh <= 28 for lmax <= 6).
+//   t (Gamma[:, p] - Gamma[:, A] r) and x = L^-T x~ by t (u_p - U_A r),
+//   U = L^-T W = G^-1 C^T (once per table).
+// A step therefore costs (q + 1) columns of Gamma and of U^T instead of the
+// K-wide products with Q1, and the scan for the most violated constraint
+// reads s from registers instead of recomputing W^T x~ (m x K) every
+// iteration.  The unconstrained minimiser x0 = G^-1 b is one product with
+// the inverse (no per-voxel substitution), and the first s = C x0 comes from
+// C = Y P: z0 = P x0 (one term per column) and s = Y z0, with Y (nsh x m) in
+// shared memory.  The reference's multiplier rule is kept as is (a full step
+// pushes t for the new constraint), so drops follow its iteration path; the
+// carried s and x differ from recomputed ones by rounding only.  Active sets
+// of up to 32 are held one entry per lane (rank C = nsh <= 28 for lmax <= 6).
 
-__global__ void k_icls_gram_setup(const double* __restrict__ W, int K, int Kp, int m_pad, double* __restrict__ Gam,
-                                  double* __restrict__ WT) {
+__global__ void k_icls_gram_setup(const double* __restrict__ W, int K, int m_pad, double* __restrict__ Gam) {
   const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int64_t n2 = static_cast<int64_t>(m_pad) * m_pad;
-  if (idx < n2) {
-    const int c = static_cast<int>(idx / m_pad), q = static_cast<int>(idx % m_pad);
-    double a = 0.0;
-    for (int k = 0; k < K; ++k)
-      a = fma(W[static_cast<size_t>(k) * m_pad + c], W[static_cast<size_t>(k) * m_pad + q], a);
-    Gam[idx] = a;
-  } else if (idx < n2 + static_cast<int64_t>(m_pad) * Kp) {
-    const int64_t e = idx - n2;
-    const int c = static_cast<int>(e / Kp), k = static_cast<int>(e % Kp);
-    WT[e] = k < K ? W[static_cast<size_t>(k) * m_pad + c] : 0.0;
+  if (idx >= static_cast<int64_t>(m_pad) * m_pad) return;
+  const int c = static_cast<int>(idx / m_pad), q = static_cast<int>(idx % m_pad);
+  double a = 0.0;
+  for (int k = 0; k < K; ++k)
+    a = fma(W[static_cast<size_t>(k) * m_pad + c], W[static_cast<size_t>(k) * m_pad + q], a);
+  Gam[idx] = a;
+}
+
+// The Gram form's x-space operators, one thread per row: UT row c = L^-T w_c
+// = G^-1 c_c (c < m_pad; zero for the padding constraints), and row i of Ginv
+// = G^-1 e_i (i < K), by the factor's substitutions.  Columns K .. Kp-1 are 0.
+__global__ void k_icls_gram_solves(const double* __restrict__ L, int K, int Kp, const double* __restrict__ W,
+                                   int m_pad, double* __restrict__ UT, double* __restrict__ Ginv) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  double* z;
+  if (idx < m_pad) {
+    z = UT + static_cast<size_t>(idx) * Kp;
+    for (int r = 0; r < K; ++r) z[r] = W[static_cast<size_t>(r) * m_pad + idx];
+  } else if (idx < m_pad + K) {
+    const int i = idx - m_pad;
+    z = Ginv + static_cast<size_t>(i) * Kp;
+    for (int r = 0; r < K; ++r) {  // L y = e_i
+      double a = (r == i) ? 1.0 : 0.0;
+      for (int k = 0; k < r; ++k) a -= L[r * Kp + k] * z[k];
+      z[r] = a / L[r * Kp + r];
+    }
+  } else {
+    return;
   }
+  for (int r = K - 1; r >= 0; --r) {  // L^T z = y, in place
+    double a = z[r];
+    for (int k = r + 1; k < K; ++k) a -= L[k * Kp + r] * z[k];
+    z[r] = a / L[r * Kp + r];
+  }
+  for (int r = K; r < Kp; ++r) z[r] = 0.0;
 }
 
 struct IclsGramParams {
   const double* B;      // V x Kp: M^T s
-  const double* L;      // Kp x Kp: Cholesky factor of M^T M + eps I
+  const double* Ginv;   // Kp x Kp: (M^T M + eps I)^-1, symmetric
   const double* Gam;    // m_pad x m_pad: W^T W
-  const double* WT;     // m_pad x Kp: row c = w_c
+  const double* UT;     // m_pad x Kp: row c = u_c = L^-T w_c = G^-1 c_c
   const double* Y;      // nsh x m_pad: C = Y P
   const double* pf;     // K: the non-zero of column col of P ...
   const int* jcol;      // K: ... and its row
@@ -557,48 +581,26 @@ __global__ void __launch_bounds__(32 * kIclsGramWarps, 1) k_icls_gram(IclsGramPa
     if (vq >= static_cast<unsigned long long>(p.V)) break;
     const int64_t v = static_cast<int64_t>(vq);
 
-    // x~0 = L^-1 M^T s, then x0 = L^-T x~0 (icls.rs:271-273)
-    double xt[RPL], x0[RPL];
+    // x0 = G^-1 M^T s (icls.rs:271-273) as one product with the inverse
+    // (b staged in the warp's slice, G^-1 read by rows: coalesced over lanes)
+    for (int k = lane; k < K; k += 32) x0s[k] = p.B[v * Kp + k];
+    __syncwarp();
+    double xt[RPL];  // the iterate x, row lane + 32 c
 #pragma unroll
-    for (int c = 0; c < RPL; ++c) {
-      const int row = lane + 32 * c;
-      xt[c] = (row < K) ? p.B[v * Kp + row] : 0.0;
-    }
-    for (int i = 0; i < K; ++i) {
-      const int owner = i & 31, oc = i >> 5;
-      double xi = 0.0;
-#pragma unroll
-      for (int c = 0; c < RPL; ++c)
-        if (c == oc && lane == owner) xi = xt[c] / __ldg(p.L + i * Kp + i);
-      xi = __shfl_sync(kFull, xi, owner);
-#pragma unroll
-      for (int c = 0; c < RPL; ++c) {
-        const int row = lane + 32 * c;
-        if (row > i && row < K) xt[c] -= __ldg(p.L + row * Kp + i) * xi;
-        if (row == i) xt[c] = xi;
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < RPL; ++c) x0[c] = xt[c];
-    for (int i = K - 1; i >= 0; --i) {
-      const int owner = i & 31, oc = i >> 5;
-      double xi = 0.0;
+    for (int c = 0; c < RPL; ++c) xt[c] = 0.0;
+    for (int k = 0; k < K; ++k) {
+      const double bk = x0s[k];
+      const double* gk = p.Ginv + static_cast<size_t>(k) * Kp + lane;
 #pragma unroll
       for (int c = 0; c < RPL; ++c)
-        if (c == oc && lane == owner) xi = x0[c] / __ldg(p.L + i * Kp + i);
-      xi = __shfl_sync(kFull, xi, owner);
-#pragma unroll
-      for (int c = 0; c < RPL; ++c) {
-        const int row = lane + 32 * c;
-        if (row < i) x0[c] -= __ldg(p.L + i * Kp + row) * xi;
-        if (row == i) x0[c] = xi;
-      }
+        if (lane + 32 * c < K) xt[c] = fma(__ldg(gk + 32 * c), bk, xt[c]);
     }
+    __syncwarp();
     // s = C x0 = Y (P x0): z0[j] sums its columns in index order
 #pragma unroll
     for (int c = 0; c < RPL; ++c) {
       const int row = lane + 32 * c;
-      if (row < K) x0s[row] = x0[c];
+      if (row < K) x0s[row] = xt[c];
     }
     __syncwarp();
     if (lane < nsh) {
@@ -693,11 +695,11 @@ __global__ void __launch_bounds__(32 * kIclsGramWarps, 1) k_icls_gram(IclsGramPa
           break;
         }
         if (lane < q) u_i -= t * rr;
-        // s += t (Gamma[:, p] - Gamma[:, A] r), x~ += t (w_p - W_A r)
+        // s += t (Gamma[:, p] - Gamma[:, A] r), x += t (u_p - U_A r) (= L^-T of x~'s step)
         {
           double ds[CPL], dx[RPL];
           const double* gp = p.Gam + static_cast<size_t>(bestp) * mp + lane;
-          const double* wp = p.WT + static_cast<size_t>(bestp) * Kp + lane;
+          const double* wp = p.UT + static_cast<size_t>(bestp) * Kp + lane;
 #pragma unroll
           for (int c = 0; c < CPL; ++c) ds[c] = __ldg(gp + 32 * c);
 #pragma unroll
@@ -706,7 +708,7 @@ __global__ void __launch_bounds__(32 * kIclsGramWarps, 1) k_icls_gram(IclsGramPa
             const double ri = __shfl_sync(kFull, rr, i);
             const int ai = __shfl_sync(kFull, a_i, i);
             const double* ga = p.Gam + static_cast<size_t>(ai) * mp + lane;
-            const double* wa = p.WT + static_cast<size_t>(ai) * Kp + lane;
+            const double* wa = p.UT + static_cast<size_t>(ai) * Kp + lane;
 #pragma unroll
             for (int c = 0; c < CPL; ++c) ds[c] = fma(-ri, __ldg(ga + 32 * c), ds[c]);
 #pragma unroll
@@ -777,21 +779,6 @@ __global__ void __launch_bounds__(32 * kIclsGramWarps, 1) k_icls_gram(IclsGramPa
     }
     executed += static_cast<unsigned long long>(iters - 1);
 
-    // x = L^-T x~ (back substitution)
-    for (int i = K - 1; i >= 0; --i) {
-      const int owner = i & 31, oc = i >> 5;
-      double xi = 0.0;
-#pragma unroll
-      for (int c = 0; c < RPL; ++c)
-        if (c == oc && lane == owner) xi = xt[c] / __ldg(p.L + i * Kp + i);
-      xi = __shfl_sync(kFull, xi, owner);
-#pragma unroll
-      for (int c = 0; c < RPL; ++c) {
-        const int row = lane + 32 * c;
-        if (row < i) xt[c] -= __ldg(p.L + i * Kp + row) * xi;
-        if (row == i) xt[c] = xi;
-      }
-    }
 #pragma unroll
     for (int c = 0; c < RPL; ++c) {
       const int row = lane + 32 * c;
