@@ -2576,7 +2576,8 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
                            (fista_variant(h) == 3 || fista_variant(h) == 4);
     // A pageable output of the pipelined fit: the fit writes the handle's
     // page-locked output volume (in place and by slab copies, as for a
-    // page-locked output) and host threads copy it out afterwards.
+    // page-locked output); host threads then copy its masked rows out and
+    // zero the caller's other rows.
     float* host_out = out->coefficients;
     bool out_staged = false;
     if (pipelined) {
@@ -2634,8 +2635,18 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
     if (out_staged) {
       const auto t0 = std::chrono::steady_clock::now();
       const size_t row = sizeof(float) * static_cast<size_t>(K);
-      host_parallel(nvol, 4096, [&](int64_t lo, int64_t hi) {
-        std::memcpy(out->coefficients + lo * K, host_out + lo * K, row * static_cast<size_t>(hi - lo));
+      host_parallel(nvol, 4096, [&](int64_t lo, int64_t hi) {  // masked rows copied, the rest zeroed
+        int64_t i = lo;
+        while (i < hi) {
+          const bool in = mask[i] != 0;
+          int64_t e = i + 1;
+          while (e < hi && (mask[e] != 0) == in) ++e;
+          if (in)
+            std::memcpy(out->coefficients + i * K, host_out + i * K, row * static_cast<size_t>(e - i));
+          else
+            std::memset(out->coefficients + i * K, 0, row * static_cast<size_t>(e - i));
+          i = e;
+        }
       });
       h->timing.ms_host_copy_out =
           std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
