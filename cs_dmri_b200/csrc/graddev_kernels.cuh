@@ -27,6 +27,8 @@ namespace csd {
 
 constexpr int kGdChunk = 64;       // design rows per Gram chunk (one thread per row and value group)
 constexpr int kGdLanczos = 40;     // Lanczos steps (capped at K)
+constexpr int kGdLanczosKkt = 16;  // ... in the converged-optimum mode
+constexpr double kGdKktLipMargin = 1.05;  // its step: 1 / (1.05 L) from the 16-step estimate
 
 struct GraddevParams {
   const float* S;           // V x N signals
@@ -412,75 +414,82 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
     }
     __syncthreads();
 
-    // ---- 3. lambda_max(G) by Lanczos
+    // ---- 3. lambda_max(G) by Lanczos: `steps` steps, the largest Ritz value
+    // left in s_lmax (a lower bound of lambda_max, exact to ~1e-12 at 40)
     const int LDG = L.LDG;
-    const int m = min(K, kGdLanczos);
-    for (int i = tid; i < Kp; i += blockDim.x) {
-      lv[i] = (i < K) ? 1.0 + 0.5 * sin(1.7 * i + 0.3) : 0.0;  // fixed start vector
-      lv_prev[i] = 0.0;
-    }
-    {
-      const double e = (tid < K) ? lv[tid] : 0.0;  // K <= blockDim.x
-      const double inv = 1.0 / sqrt(gd_block_sum(e * e, red));
-      if (tid < K) lv[tid] *= inv;
-    }
-    __syncthreads();
-    int msteps = m;
-    double beta_prev = 0.0;
-    for (int j = 0; j < m; ++j) {
-      gd_gemv(G, LDG, K, lv, lw);
+    auto run_lanczos = [&](int steps) {
+      const int m = min(K, steps);
+      for (int i = tid; i < Kp; i += blockDim.x) {
+        lv[i] = (i < K) ? 1.0 + 0.5 * sin(1.7 * i + 0.3) : 0.0;  // fixed start vector
+        lv_prev[i] = 0.0;
+      }
+      {
+        const double e = (tid < K) ? lv[tid] : 0.0;  // K <= blockDim.x
+        const double inv = 1.0 / sqrt(gd_block_sum(e * e, red));
+        if (tid < K) lv[tid] *= inv;
+      }
       __syncthreads();
-      const double wi = (tid < K) ? lw[tid] : 0.0, vi = (tid < K) ? lv[tid] : 0.0;
-      const double al = gd_block_sum(wi * vi, red);
-      const double wn = (tid < K) ? wi - al * vi - beta_prev * lv_prev[tid] : 0.0;
-      const double bt = sqrt(gd_block_sum(wn * wn, red));
-      if (tid == 0) {
-        ta[j] = al;
-        tb[j] = bt;
+      int msteps = m;
+      double beta_prev = 0.0;
+      for (int j = 0; j < m; ++j) {
+        gd_gemv(G, LDG, K, lv, lw);
+        __syncthreads();
+        const double wi = (tid < K) ? lw[tid] : 0.0, vi = (tid < K) ? lv[tid] : 0.0;
+        const double al = gd_block_sum(wi * vi, red);
+        const double wn = (tid < K) ? wi - al * vi - beta_prev * lv_prev[tid] : 0.0;
+        const double bt = sqrt(gd_block_sum(wn * wn, red));
+        if (tid == 0) {
+          ta[j] = al;
+          tb[j] = bt;
+        }
+        if (!(bt > 1e-300 * fabs(al)) || j == m - 1) {  // every thread holds the same bt
+          msteps = j + 1;
+          break;
+        }
+        if (tid < K) {
+          lv_prev[tid] = vi;
+          lv[tid] = wn / bt;
+        }
+        beta_prev = bt;
+        __syncthreads();
       }
-      if (!(bt > 1e-300 * fabs(al)) || j == m - 1) {  // every thread holds the same bt
-        msteps = j + 1;
-        break;
-      }
-      if (tid < K) {
-        lv_prev[tid] = vi;
-        lv[tid] = wn / bt;
-      }
-      beta_prev = bt;
       __syncthreads();
-    }
-    __syncthreads();
-    {  // largest eigenvalue of the tridiagonal: multisection at one point per thread
-      double lo = 1e300, hi = -1e300;
-      for (int i = 0; i < msteps; ++i) {
-        const double r = (i > 0 ? fabs(tb[i - 1]) : 0.0) + (i < msteps - 1 ? fabs(tb[i]) : 0.0);
-        lo = fmin(lo, ta[i] - r);
-        hi = fmax(hi, ta[i] + r);
+      {  // largest eigenvalue of the tridiagonal: multisection at one point per thread
+        double lo = 1e300, hi = -1e300;
+        for (int i = 0; i < msteps; ++i) {
+          const double r = (i > 0 ? fabs(tb[i - 1]) : 0.0) + (i < msteps - 1 ? fabs(tb[i]) : 0.0);
+          lo = fmin(lo, ta[i] - r);
+          hi = fmax(hi, ta[i] + r);
+        }
+        const int P = blockDim.x;  // points lo + (hi - lo) (t + 1) / (P + 1)
+        for (int round = 0; round < 12 && hi - lo > 1e-16 * fmax(fabs(hi), fabs(lo)); ++round) {
+          if (tid == 0) s_first = P;
+          __syncthreads();
+          const double x = lo + (hi - lo) * (tid + 1) / (P + 1.0);
+          if (sturm_below(ta, tb, msteps, x) == msteps) atomicMin(&s_first, tid);  // x above every eigenvalue
+          __syncthreads();
+          const int first = s_first;  // the top eigenvalue lies in (x_{first-1}, x_first]
+          const double nlo = lo + (hi - lo) * first / (P + 1.0);
+          hi = lo + (hi - lo) * (first + 1) / (P + 1.0);
+          lo = nlo;
+          __syncthreads();
+        }
+        if (tid == 0) s_lmax = 0.5 * (lo + hi);
       }
-      const int P = blockDim.x;  // points lo + (hi - lo) (t + 1) / (P + 1)
-      for (int round = 0; round < 12 && hi - lo > 1e-16 * fmax(fabs(hi), fabs(lo)); ++round) {
-        if (tid == 0) s_first = P;
-        __syncthreads();
-        const double x = lo + (hi - lo) * (tid + 1) / (P + 1.0);
-        if (sturm_below(ta, tb, msteps, x) == msteps) atomicMin(&s_first, tid);  // x above every eigenvalue
-        __syncthreads();
-        const int first = s_first;  // the top eigenvalue lies in (x_{first-1}, x_first]
-        const double nlo = lo + (hi - lo) * first / (P + 1.0);
-        hi = lo + (hi - lo) * (first + 1) / (P + 1.0);
-        lo = nlo;
-        __syncthreads();
-      }
-      if (tid == 0) s_lmax = 0.5 * (lo + hi);
-    }
-    __syncthreads();
+      __syncthreads();
+    };
+    // the converged-optimum mode only needs a safe step for its support
+    // iterations (the polish certifies the minimiser whatever the path): fewer
+    // steps and a margin; a voxel it does not certify reruns the full count
+    run_lanczos(p.kkt ? kGdLanczosKkt : kGdLanczos);
     const double nv = static_cast<double>(n);
-    const double lip = (n > 0) ? fmax(s_lmax / nv, 2.220446049250313e-16) : 0.0;
+    double lip = (n > 0) ? fmax(s_lmax / nv, 2.220446049250313e-16) : 0.0;
 
     // ---- 4. FISTA (src/solver/fista.rs:70-143), Gram form
     const double n_inv = (n > 0) ? 1.0 / nv : 0.0;
-    const double step = (n > 0) ? 1.0 / lip : 0.0;
+    double step = (n > 0) ? 1.0 / (p.kkt ? lip * kGdKktLipMargin : lip) : 0.0;
     const double alpha_v = p.alpha_v ? p.alpha_v[v] : p.alpha;
-    const double thr = __dmul_rn(step, alpha_v);
+    double thr = __dmul_rn(step, alpha_v);
     // `max_it` iterations from zero, stopping early below `tol` (never with tol 0)
     auto run_fista = [&](int max_it, double tol, bool& converged) -> int {
       for (int i = tid; i < Kp; i += blockDim.x) {
@@ -586,6 +595,10 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
       kkt_val = s_lmax;
       __syncthreads();
       if (!cert && n > 0) {  // the reference FISTA from zero, reported uncertified
+        run_lanczos(kGdLanczos);  // the reference's step, from the full Lanczos count
+        lip = fmax(s_lmax / nv, 2.220446049250313e-16);
+        step = 1.0 / lip;
+        thr = __dmul_rn(step, alpha_v);
         bool conv_ref = false;
         it += run_fista(p.max_iter, p.tol, conv_ref);
       }

@@ -437,7 +437,10 @@ int csd_shore_rtop_adjoint_device(csd_handle* h, int32_t radial_order, double ze
  * iterations run in FP64 on the voxel's own Gram matrix, then one warp
  * polishes and certifies): converged = certified, and the call waits for its
  * work and reports the uncertified count and the polish rounds through
- * csd_last_timing. */
+ * csd_last_timing.  That mode's support iterations step by 1 / (1.05 L)
+ * from a 16-step Lanczos estimate of L_v (the value reported in
+ * d_lipschitz); a voxel left uncertified runs the full 40-step estimate and
+ * the reference FISTA. */
 int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signals, int64_t n_voxels,
                                  const csd_gtab* gtab, const csd_shore_spec* spec,
                                  const double* d_graddev, const uint8_t* d_keep,
