@@ -27,6 +27,7 @@ namespace csd {
 
 constexpr int kGdChunk = 64;       // design rows per Gram chunk (one thread per row and value group)
 constexpr int kGdLanczos = 40;     // Lanczos steps (capped at K)
+constexpr int kGdRcp = 17;         // reciprocals 1 / i, i < 17 (radial orders <= 16)
 constexpr int kGdLanczosKkt = 16;  // ... in the converged-optimum mode
 constexpr double kGdKktLipMargin = 1.05;  // its step: 1 / (1.05 L) from the 16-step estimate
 
@@ -182,6 +183,8 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
   __shared__ double s_lmax;
   __shared__ int s_first;
   __shared__ uint16_t gd_tri[kTriTable];  // (row, col) of a packed triangle, for the polish
+  __shared__ double gd_rcp[kGdRcp];       // 1 / i: the recurrences' divisors as products
+  for (int i = threadIdx.x; i < kGdRcp; i += blockDim.x) gd_rcp[i] = i > 0 ? 1.0 / i : 0.0;
   for (int e = threadIdx.x; e < kTriTable; e += blockDim.x) {
     const int r = tri_row(e);
     gd_tri[e] = static_cast<uint16_t>((r << 8) | (e - pk_row(r)));
@@ -306,9 +309,12 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
 
       // per-row values, one thread per row in each of three groups: radial
       // factors (group 0), cos / sin of m theta (group 1), associated
-      // Legendre values by the recurrence in l for each m (group 2); the
-      // operations are those of dev_shore_radial and dev_brainsuite_sh, so
-      // the entries equal the shared-design kernel's
+      // Legendre values by the recurrence in l for each m (group 2).  The
+      // formulas are those of dev_shore_radial and dev_brainsuite_sh, with
+      // the costly steps replaced: integer powers by products, the
+      // recurrences' divisions by reciprocal products, and cos / sin of
+      // m theta by rotation.  So the entries agree with the shared-design
+      // kernel's to a few units in the last place, not bit for bit.
       {
         const int t = tid % kGdChunk, grp = tid / kGdChunk;
         const double* gt = geo + 8 * t;
@@ -316,18 +322,42 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
         if (c0 + t >= n) {
           // past the last row: nothing to evaluate (the chunk entries are 0)
         } else if (grp == 0) {
-          double rp[8];
-          for (int l = 0; l <= R; l += 2) rp[l / 2] = pow(gt[5], static_cast<double>(l) / 2.0);
+          // u^(l/2) (l even) by products; the generalised Laguerre
+          // L_{n-l}^{(l+1/2)}(u) by its three-term recurrence with the
+          // divisor k + 1 taken as a product with 1 / (k + 1)
+          const double u = gt[5];
+          double rp[9];
+          rp[0] = 1.0;
+          for (int h = 1; h <= R / 2; ++h) rp[h] = rp[h - 1] * u;
           int j = 0;
           for (int nn = 0; nn <= R; ++nn)
             for (int l = 0; l <= nn; l += 2, ++j) {
-              const double lag = dev_gen_laguerre(nn - l, static_cast<double>(l) + 0.5, gt[5]);
+              const int deg = nn - l;
+              const double al = static_cast<double>(l) + 0.5;
+              double lag = 1.0;
+              if (deg >= 1) {
+                double lkm1 = 1.0, lk = 1.0 + al - u;
+                for (int k = 1; k < deg; ++k) {
+                  const double kf = k;
+                  const double lkp1 = ((2.0 * kf + 1.0 + al - u) * lk - (kf + al) * lkm1) * gd_rcp[k + 1];
+                  lkm1 = lk;
+                  lk = lkp1;
+                }
+                lag = lk;
+              }
               rad[t * NL + j] = kap[j] * lag * gt[6] * rp[l / 2];
             }
         } else if (grp == 1) {
+          // cos / sin of m theta by rotation from those of theta
+          double s1, c1;
+          sincos(gt[1], &s1, &c1);
+          double cm = c1, sm = s1;
           for (int mm = 1; mm <= R; ++mm) {
-            trg[t * L.NTR + mm - 1] = cos(static_cast<double>(mm) * gt[1]);
-            trg[t * L.NTR + R + mm - 1] = sin(static_cast<double>(mm) * gt[1]);
+            trg[t * L.NTR + mm - 1] = cm;
+            trg[t * L.NTR + R + mm - 1] = sm;
+            const double cn = fma(cm, c1, -sm * s1), sn = fma(sm, c1, cm * s1);
+            cm = cn;
+            sm = sn;
           }
         } else if (grp == 2) {
           const double x = gt[4];
@@ -347,7 +377,7 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
             if ((mm + 1) % 2 == 0) leg[t * L.NLM + ((mm + 1) / 2) * ((mm + 1) / 2) + mm] = pmmp1;
             for (int ll = mm + 2; ll <= R; ++ll) {
               const double llf = ll, mf = mm;
-              const double pll = ((2.0 * llf - 1.0) * x * pmmp1 - (llf + mf - 1.0) * pmm) / (llf - mf);
+              const double pll = ((2.0 * llf - 1.0) * x * pmmp1 - (llf + mf - 1.0) * pmm) * gd_rcp[ll - mm];
               pmm = pmmp1;
               pmmp1 = pll;
               if (ll % 2 == 0) leg[t * L.NLM + (ll / 2) * (ll / 2) + mm] = pll;
