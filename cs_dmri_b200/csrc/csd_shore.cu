@@ -297,6 +297,7 @@ struct csd_handle {
   // pipelined host-buffer fit: rhs stream + two compute streams, chunk events
   cudaStream_t pipe[4] = {nullptr, nullptr, nullptr, nullptr};  // rhs, two solve streams, output zero-fill
   cudaEvent_t pev[20] = {};
+  cudaEvent_t oev[15] = {};  // pipelined fit: chunk k's slab of the output is on the host
   DevBuf iota;
   // differentiable fit: adjoint solution w, overflow list and its count, RTOP constants
   DevBuf adjW, adjovf, adjstat, adjconst;
@@ -2109,7 +2110,8 @@ void gather_rows(const HostGather& hg, int64_t lo, int64_t hi) {
 
 FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_mask, int64_t nvol,
                           const HostGtab& g, const csd_shore_spec* spec, float* d_coeffs, float* host_coeffs,
-                          const HostGather* hg = nullptr) {
+                          const HostGather* hg = nullptr, float* user_out = nullptr,
+                          const uint8_t* host_mask = nullptr) {
   FitInfo info;
   h->sig_compact = nullptr;
   cudaStream_t st = h->stream;
@@ -2134,6 +2136,7 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
     CSD_CUDA(cudaMemcpyAsync(host_coeffs, d_coeffs, sizeof(float) * static_cast<size_t>(nvol) * K,
                              cudaMemcpyDeviceToHost, st));
     CSD_CUDA(cudaStreamSynchronize(st));
+    if (user_out) std::memset(user_out, 0, sizeof(float) * static_cast<size_t>(nvol) * K);
     return info;
   }
   const PipePlan plan = pipe_plan(h->num_sms);
@@ -2171,6 +2174,8 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   for (auto& p : h->pipe)
     if (!p) CSD_CUDA(cudaStreamCreateWithFlags(&p, cudaStreamNonBlocking));
   for (auto& e : h->pev)
+    if (!e) CSD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (auto& e : h->oev)
     if (!e) CSD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   CSD_CUDA(cudaStreamSynchronize(st));  // boundaries on the host; set-up done
   record(h, 2);
@@ -2290,6 +2295,33 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
       const int64_t lo = vb[k], hi = vb[k + 1];
       CSD_CUDA(cudaMemcpyAsync(host_coeffs + lo * K, d_coeffs + lo * K,
                                sizeof(float) * static_cast<size_t>(hi - lo) * K, cudaMemcpyDeviceToHost, ks));
+    }
+    CSD_CUDA(cudaEventRecord(h->oev[k], ks));  // chunk k's slab is on the host
+  }
+  if (user_out) {
+    // a caller's pageable output: each slab is copied out (masked rows;
+    // the others zeroed) as soon as it is on the host, so the copies of the
+    // first slabs overlap the later chunks' iterations
+    const size_t row = sizeof(float) * static_cast<size_t>(K);
+    for (int k = 0; k < C; ++k) {
+      CSD_CUDA(cudaEventSynchronize(h->oev[k]));
+      const auto t0 = std::chrono::steady_clock::now();
+      host_parallel(vb[k + 1] - vb[k], 4096, [&](int64_t a, int64_t b) {
+        int64_t i = vb[k] + a;
+        const int64_t end = vb[k] + b;
+        while (i < end) {
+          const bool in = host_mask[i] != 0;
+          int64_t j = i + 1;
+          while (j < end && (host_mask[j] != 0) == in) ++j;
+          if (in)
+            std::memcpy(user_out + i * K, host_coeffs + i * K, row * static_cast<size_t>(j - i));
+          else
+            std::memset(user_out + i * K, 0, row * static_cast<size_t>(j - i));
+          i = j;
+        }
+      });
+      h->timing.ms_host_copy_out +=
+          std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
   }
   if (d_out_host) CSD_CUDA(cudaStreamWaitEvent(st, h->pev[18], 0));
@@ -2435,6 +2467,8 @@ void csd_destroy(csd_handle* h) {
   if (h->order_ev) cudaEventDestroy(h->order_ev);
   for (auto& e : h->pev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : h->oev)
+    if (e) cudaEventDestroy(e);
   for (auto& e : h->kev)
     if (e) cudaEventDestroy(e);
   if (h->stage) cudaFreeHost(h->stage);
@@ -2576,8 +2610,8 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
                            (fista_variant(h) == 3 || fista_variant(h) == 4);
     // A pageable output of the pipelined fit: the fit writes the handle's
     // page-locked output volume (in place and by slab copies, as for a
-    // page-locked output); host threads then copy its masked rows out and
-    // zero the caller's other rows.
+    // page-locked output), and host threads copy each slab's masked rows out
+    // as soon as the slab is on the host and zero the caller's other rows.
     float* host_out = out->coefficients;
     bool out_staged = false;
     if (pipelined) {
@@ -2605,7 +2639,8 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
     }
     FitInfo info = pipelined
                        ? run_fit_pipelined(h, d_data, h->mask.as<uint8_t>(), nvol, g, spec, d.coeffs, host_out,
-                                           staged ? &hg : nullptr)
+                                           staged ? &hg : nullptr, out_staged ? out->coefficients : nullptr,
+                                           mask)
                        : run_fit(h, d_data, h->mask.as<uint8_t>(), nvol, g, spec, path_eps, d, on_host);
     if (!pipelined)
       CSD_CUDA(cudaMemcpyAsync(out->coefficients, d.coeffs, sizeof(float) * static_cast<size_t>(nvol) * K,
@@ -2632,25 +2667,6 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
     if (out->converged && info.V > 0)
       CSD_CUDA(cudaMemcpyAsync(out->converged, info.conv_final, info.V, cudaMemcpyDeviceToHost, st));
     CSD_CUDA(cudaStreamSynchronize(st));
-    if (out_staged) {
-      const auto t0 = std::chrono::steady_clock::now();
-      const size_t row = sizeof(float) * static_cast<size_t>(K);
-      host_parallel(nvol, 4096, [&](int64_t lo, int64_t hi) {  // masked rows copied, the rest zeroed
-        int64_t i = lo;
-        while (i < hi) {
-          const bool in = mask[i] != 0;
-          int64_t e = i + 1;
-          while (e < hi && (mask[e] != 0) == in) ++e;
-          if (in)
-            std::memcpy(out->coefficients + i * K, host_out + i * K, row * static_cast<size_t>(e - i));
-          else
-            std::memset(out->coefficients + i * K, 0, row * static_cast<size_t>(e - i));
-          i = e;
-        }
-      });
-      h->timing.ms_host_copy_out =
-          std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    }
     fill_scalars(g, info, spec, out);
     warnings += info.warnings;
     std::snprintf(out->warnings, sizeof out->warnings, "%s", warnings.c_str());
