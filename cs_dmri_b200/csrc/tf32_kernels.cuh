@@ -162,6 +162,7 @@ __global__ void __launch_bounds__(tf::THREADS, 2) k_fista_tf32(Tf32Params p) {
   unsigned char* sA = smem_tf;
   unsigned char* sB = sA + S::A_BYTES;
   __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar_b;  // the B operand's bulk copy
   __shared__ uint32_t tmem_slot;
   __shared__ int s_abort;
   __shared__ unsigned long long s_tile;
@@ -174,8 +175,6 @@ __global__ void __launch_bounds__(tf::THREADS, 2) k_fista_tf32(Tf32Params p) {
   const int j_lo = part * CPT;
 
   for (int i = tid; i < S::A_BYTES / 16; i += THREADS) reinterpret_cast<uint4*>(sA)[i] = make_uint4(0, 0, 0, 0);
-  for (int i = tid; i < S::B_BYTES / 16; i += THREADS)
-    reinterpret_cast<uint4*>(sB)[i] = reinterpret_cast<const uint4*>(p.gop)[i];
   for (int i = tid; i < min(p.iters, MOM_SMEM); i += THREADS) s_mom[i] = static_cast<float>(p.mom[i]);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
@@ -184,19 +183,43 @@ __global__ void __launch_bounds__(tf::THREADS, 2) k_fista_tf32(Tf32Params p) {
   }
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar_b)));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_abort = 0;
   }
   fence_before();
   __syncthreads();
   fence_after();
+  // B (the TF32 Gram operand, already in its shared-memory image in global
+  // memory) by one bulk copy on the copy engine; 16-byte aligned addresses
+  // and a size that is a multiple of 16 bytes, no multicast
+  static_assert(S::B_BYTES % 16 == 0 && S::A_BYTES % 16 == 0, "bulk copy granularity");
+  if (tid == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&mbar_b)),
+                 "r"(static_cast<uint32_t>(S::B_BYTES))
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(sB)),
+        "l"(p.gop), "r"(static_cast<uint32_t>(S::B_BYTES)), "r"(smem_u32(&mbar_b))
+        : "memory");
+    uint32_t done = 0;
+    const uint64_t t0 = globaltimer_ns();
+    while (!done && globaltimer_ns() - t0 < kWaitNs) done = try_wait(&mbar_b, 0);
+    if (!done) {  // give the copy a second bound to land before the CTA can leave
+      s_abort = 1;
+      const uint64_t t1 = globaltimer_ns();
+      while (!done && globaltimer_ns() - t1 < kWaitNs) done = try_wait(&mbar_b, 0);
+    }
+  }
+  __syncthreads();
   const uint32_t tbase = tmem_slot;
   const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
   const int64_t n_tiles = (p.n_work + TILE - 1) / TILE;
   uint32_t phase = 0;
   unsigned long long n_batches = 0;
 
-  while (true) {
+  while (!s_abort) {  // (set before the first tile only if the operand copy failed)
     __syncthreads();  // every thread has read the previous tile index
     if (tid == 0) s_tile = atomicAdd(p.queue, 1ull);
     __syncthreads();
