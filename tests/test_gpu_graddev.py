@@ -106,3 +106,19 @@ def test_certified_optimum_per_voxel_design(oracle, inputs, order):
         checked += 1
         assert np.linalg.norm(c[v] - want) <= 1e-6 * max(np.linalg.norm(want), 1e-300), v
     assert checked >= 0.9 * len(range(0, len(S), 2))
+
+
+def test_mixed_kkt_per_voxel_design_runs_the_certified_mode(inputs):
+    """precision "mixed-kkt" on per-voxel designs: each voxel has its own Gram
+    matrix, so there is no shared tensor-core operand and the support
+    iterations run in FP64.  The result is the "fp64-kkt" fit bit for bit;
+    precision "mixed" (the int8 path of the shared design) is refused."""
+    from cs_dmri_b200.graddev import shore_fit_graddev
+    S, bvals, bvecs, T, keep, big, small = inputs
+    kw = dict(alpha=0.01, radial_order=6, big_delta=big, small_delta=small)
+    a = shore_fit_graddev(S, bvals, bvecs, T, keep, precision="fp64-kkt", **kw)
+    b = shore_fit_graddev(S, bvals, bvecs, T, keep, precision="mixed-kkt", **kw)
+    assert np.array_equal(a["coefficients"].cpu().numpy(), b["coefficients"].cpu().numpy())
+    assert np.array_equal(a["iterations"].cpu().numpy(), b["iterations"].cpu().numpy())
+    with pytest.raises(Exception, match="precision fp64, fp64-kkt or mixed-kkt"):
+        shore_fit_graddev(S, bvals, bvecs, T, keep, precision="mixed", **kw)
