@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <map>
@@ -2096,15 +2097,65 @@ PipePlan pipe_plan(int num_sms) {
 struct HostGather {
   const float* data = nullptr;   // pageable (X, Y, Z, N) volume
   const uint8_t* mask = nullptr; // host mask
-  float* stage = nullptr;        // page-locked staging volume, same shape
+  float* stage = nullptr;        // page-locked staging: the volume's shape, or its masked rows in order
   int N = 0;
+  bool compact = false;          // stage holds the masked rows only (row j = j-th masked voxel)
 };
 
-void gather_rows(const HostGather& hg, int64_t lo, int64_t hi) {
+// The masked voxels of the volume range [lo, hi) in order, the j-th paired
+// with compact row c_lo + j, on host threads: each thread counts its range's
+// masked voxels first, so that it knows its first row.  on_row(v, row) for
+// every masked voxel, on_gap(v0, v1) for every run of unmasked ones.
+template <class Row, class Gap>
+static void masked_rows(const uint8_t* mask, int64_t lo, int64_t hi, int64_t c_lo, Row on_row, Gap on_gap) {
+  const int64_t n = hi - lo;
+  if (n <= 0) return;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int64_t T = std::min<int64_t>(std::min<unsigned>(hw, 32u), std::max<int64_t>(1, n / 4096));
+  std::vector<int64_t> first(static_cast<size_t>(T) + 1, 0);
+  auto each = [&](auto fn) {
+    std::vector<std::thread> pool;
+    for (int64_t t = 1; t < T; ++t) pool.emplace_back(fn, t, lo + n * t / T, lo + n * (t + 1) / T);
+    fn(int64_t{0}, lo, lo + n / T);
+    for (auto& th : pool) th.join();
+  };
+  each([&](int64_t t, int64_t a, int64_t b) {
+    int64_t c = 0;
+    for (int64_t v = a; v < b; ++v) c += mask[v] != 0;
+    first[static_cast<size_t>(t) + 1] = c;
+  });
+  for (int64_t t = 0; t < T; ++t) first[static_cast<size_t>(t) + 1] += first[static_cast<size_t>(t)];
+  each([&](int64_t t, int64_t a, int64_t b) {
+    int64_t row = c_lo + first[static_cast<size_t>(t)];
+    int64_t v = a;
+    while (v < b) {
+      if (mask[v]) {
+        on_row(v, row++);
+        ++v;
+      } else {
+        int64_t e = v + 1;
+        while (e < b && !mask[e]) ++e;
+        on_gap(v, e);
+        v = e;
+      }
+    }
+  });
+}
+
+// The masked rows of volume range [lo, hi) into the staging buffer; in the
+// compact layout the first of them goes to row c_lo.
+void gather_rows(const HostGather& hg, int64_t lo, int64_t hi, int64_t c_lo = 0) {
   const int N = hg.N;
+  const size_t row = sizeof(float) * static_cast<size_t>(N);
+  if (hg.compact) {
+    masked_rows(hg.mask, lo, hi, c_lo,
+                [&](int64_t v, int64_t r) { std::memcpy(hg.stage + r * N, hg.data + v * N, row); },
+                [](int64_t, int64_t) {});
+    return;
+  }
   host_parallel(hi - lo, 4096, [&](int64_t a, int64_t b) {
     for (int64_t v = lo + a; v < lo + b; ++v)
-      if (hg.mask[v]) std::memcpy(hg.stage + v * N, hg.data + v * N, sizeof(float) * N);
+      if (hg.mask[v]) std::memcpy(hg.stage + v * N, hg.data + v * N, row);
   });
 }
 
@@ -2133,8 +2184,9 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   info.V = V;
   if (V == 0) {
     for (int i : {2, 6, 7, 3}) record(h, i);
-    CSD_CUDA(cudaMemcpyAsync(host_coeffs, d_coeffs, sizeof(float) * static_cast<size_t>(nvol) * K,
-                             cudaMemcpyDeviceToHost, st));
+    if (!user_out)
+      CSD_CUDA(cudaMemcpyAsync(host_coeffs, d_coeffs, sizeof(float) * static_cast<size_t>(nvol) * K,
+                               cudaMemcpyDeviceToHost, st));
     CSD_CUDA(cudaStreamSynchronize(st));
     if (user_out) std::memset(user_out, 0, sizeof(float) * static_cast<size_t>(nvol) * K);
     return info;
@@ -2189,6 +2241,12 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
     cudaGetLastError();  // a pageable pointer may leave an error code behind
   }
   if (C < 2) d_out_host = nullptr;  // one chunk: a single copy back
+  // Compact host buffers (a staged pageable volume or output): the staging
+  // holds the masked rows in order, so the right-hand side reads row i of
+  // it for voxel position i, and the coefficients come back as rows in
+  // position order (V x K), which the host copies into the caller's volume.
+  const bool cin = hg && hg->compact, cout = user_out != nullptr;
+  const int64_t* rows_in = cin ? h->iota.as<int64_t>() : h->vox.as<int64_t>();
 
   const size_t rhs_smem = sizeof(double) * static_cast<size_t>(h->Np) * Kp + sizeof(float) * 8 * 8 * (h->Np + 4);
   CSD_CUDA(cudaFuncSetAttribute(csd::k_rhs_dmma<72>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2239,11 +2297,11 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
     const int64_t groups = (n + 7) / 8;
     const int rhs_grid = static_cast<int>(std::min<int64_t>(k == 0 ? h->num_sms : plan.rhs_ctas, (groups + 7) / 8));
     csd::k_rhs_dmma<72><<<std::max(rhs_grid, 1), 256, rhs_smem, rs>>>(
-        d_data, h->vox.as<int64_t>() + a, n, N, h->Np, h->mtfrag.as<double>(), h->B.as<double>() + a * Kp,
+        d_data, rows_in + a, n, N, h->Np, h->mtfrag.as<double>(), h->B.as<double>() + a * Kp,
         h->sig.as<float>() + a * N);
     CSD_LAUNCH();
     CSD_CUDA(cudaEventRecord(h->pev[k], rs));
-    if (k == C - 1 && d_out_host) {
+    if (k == C - 1 && d_out_host && !cout) {
       // zero-fill the last chunk's slab in the host volume once every row has been read
       const int64_t lo = vb[C - 1];
       CSD_CUDA(cudaStreamWaitEvent(h->pipe[3], h->pev[C - 1], 0));
@@ -2261,7 +2319,7 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
   for (int k = 0; k < C; ++k) {
     if (hg) {
       const auto t0 = std::chrono::steady_clock::now();
-      gather_rows(*hg, vb[k], vb[k + 1]);
+      gather_rows(*hg, vb[k], vb[k + 1], c0[k]);
       h->timing.ms_host_gather +=
           std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
       queue_rhs(k);
@@ -2284,47 +2342,38 @@ FitInfo run_fit_pipelined(csd_handle* h, const float* d_data, const uint8_t* d_m
     csd::EpilogueParams e = ep;
     e.list = h->iota.as<int64_t>() + a;
     e.n_work = n;
+    if (cout) e.vox = h->iota.as<int64_t>();  // rows in position order
     const bool direct = d_out_host && k == C - 1;
     if (direct) {
       e.coeffs = d_out_host;
-      CSD_CUDA(cudaStreamWaitEvent(ks, h->pev[18], 0));  // after the slab's zero-fill
+      if (!cout) CSD_CUDA(cudaStreamWaitEvent(ks, h->pev[18], 0));  // after the slab's zero-fill
     }
     launch_epilogue(h, e);
     h->stream = st;
     if (!direct) {
-      const int64_t lo = vb[k], hi = vb[k + 1];
+      const int64_t lo = cout ? c0[k] : vb[k], hi = cout ? c0[k + 1] : vb[k + 1];
       CSD_CUDA(cudaMemcpyAsync(host_coeffs + lo * K, d_coeffs + lo * K,
                                sizeof(float) * static_cast<size_t>(hi - lo) * K, cudaMemcpyDeviceToHost, ks));
     }
     CSD_CUDA(cudaEventRecord(h->oev[k], ks));  // chunk k's slab is on the host
   }
   if (user_out) {
-    // a caller's pageable output: each slab is copied out (masked rows;
-    // the others zeroed) as soon as it is on the host, so the copies of the
-    // first slabs overlap the later chunks' iterations
+    // a caller's pageable output: each chunk's rows are copied into the
+    // volume (the unmasked rows zeroed) as soon as they are on the host, so
+    // the copies of the first chunks overlap the later chunks' iterations
     const size_t row = sizeof(float) * static_cast<size_t>(K);
     for (int k = 0; k < C; ++k) {
       CSD_CUDA(cudaEventSynchronize(h->oev[k]));
       const auto t0 = std::chrono::steady_clock::now();
-      host_parallel(vb[k + 1] - vb[k], 4096, [&](int64_t a, int64_t b) {
-        int64_t i = vb[k] + a;
-        const int64_t end = vb[k] + b;
-        while (i < end) {
-          const bool in = host_mask[i] != 0;
-          int64_t j = i + 1;
-          while (j < end && (host_mask[j] != 0) == in) ++j;
-          if (in)
-            std::memcpy(user_out + i * K, host_coeffs + i * K, row * static_cast<size_t>(j - i));
-          else
-            std::memset(user_out + i * K, 0, row * static_cast<size_t>(j - i));
-          i = j;
-        }
-      });
+      masked_rows(
+          host_mask, vb[k], vb[k + 1], c0[k],
+          [&](int64_t v, int64_t r) { std::memcpy(user_out + v * K, host_coeffs + r * K, row); },
+          [&](int64_t v0, int64_t v1) { std::memset(user_out + v0 * K, 0, row * static_cast<size_t>(v1 - v0)); });
       h->timing.ms_host_copy_out +=
           std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
   }
-  if (d_out_host) CSD_CUDA(cudaStreamWaitEvent(st, h->pev[18], 0));
+  if (d_out_host && !cout) CSD_CUDA(cudaStreamWaitEvent(st, h->pev[18], 0));
   for (int j = 1; j <= 2; ++j) {
     CSD_CUDA(cudaEventRecord(h->pev[15 + j], h->pipe[j]));
     CSD_CUDA(cudaStreamWaitEvent(st, h->pev[15 + j], 0));
@@ -2561,14 +2610,35 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
     }
     h->timing.ms_host_gather = 0.f;
     h->timing.ms_host_copy_out = 0.f;
-    bool staged = false;
+    // Fixed-alpha FP64 L1 with nothing but the coefficients requested: the
+    // pipelined path (transfers overlap the fit) when the volume is on the host.
+    const bool pipe_ok = K == 72 && spec->regularization == CSD_REG_L1 && spec->alpha_mode == CSD_ALPHA_FIXED &&
+                         spec->precision == CSD_PRECISION_FP64 && spec->diagnostics == 0 && !out->coef64 &&
+                         !out->converged && spec->max_iter > 0 && (fista_variant(h) == 3 || fista_variant(h) == 4);
+    int64_t v_host = -1;  // masked voxels, counted on the host when a compact buffer is sized
+    auto masked_count = [&]() {
+      if (v_host < 0) {
+        std::atomic<int64_t> c{0};
+        host_parallel(nvol, 1 << 16, [&](int64_t a, int64_t b) {
+          int64_t k = 0;
+          for (int64_t v = a; v < b; ++v) k += mask[v] != 0;
+          c += k;
+        });
+        v_host = c.load();
+      }
+      return v_host;
+    };
+    bool staged = false, stage_compact = false;
     if (!on_host && h->dmma_rhs_possible(N, K)) {
       // A pageable volume: its masked rows are gathered on host threads into
-      // the handle's page-locked staging volume, which the device then reads
-      // in place like a page-locked input (masked rows only; the other rows
-      // of the staging volume are never read).  The pipelined fit gathers
-      // chunk by chunk (below); other fits gather everything first.
-      float* stage = ensure_pinned(h->stage, h->stage_bytes, sizeof(float) * static_cast<size_t>(nvol) * N);
+      // the handle's page-locked staging buffer, which the device then reads
+      // in place like a page-locked input.  For the pipelined fit the buffer
+      // holds only the masked rows, in order (gathered chunk by chunk,
+      // below); other fits use a buffer of the volume's shape (masked rows
+      // only written and read) and gather everything first.
+      stage_compact = pipe_ok;
+      const int64_t rows = stage_compact ? std::max<int64_t>(masked_count(), 1) : nvol;
+      float* stage = ensure_pinned(h->stage, h->stage_bytes, sizeof(float) * static_cast<size_t>(rows) * N);
       void* dp = nullptr;
       CSD_CUDA(cudaHostGetDevicePointer(&dp, stage, 0));
       d_data = static_cast<const float*>(dp);
@@ -2602,16 +2672,11 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
       h->kind_map.ensure(nvol);
       d.kind = h->kind_map.as<uint8_t>();
     }
-    // Fixed-alpha FP64 L1 of a page-locked volume with nothing but the
-    // coefficients requested: the pipelined path (transfers overlap the fit).
-    const bool pipelined = on_host && K == 72 && spec->regularization == CSD_REG_L1 &&
-                           spec->alpha_mode == CSD_ALPHA_FIXED && spec->precision == CSD_PRECISION_FP64 &&
-                           !diag && !out->coef64 && !out->converged && spec->max_iter > 0 &&
-                           (fista_variant(h) == 3 || fista_variant(h) == 4);
-    // A pageable output of the pipelined fit: the fit writes the handle's
-    // page-locked output volume (in place and by slab copies, as for a
-    // page-locked output), and host threads copy each slab's masked rows out
-    // as soon as the slab is on the host and zero the caller's other rows.
+    const bool pipelined = on_host && pipe_ok;
+    // A pageable output of the pipelined fit: the fit writes the masked
+    // voxels' coefficients in position order into the handle's page-locked
+    // buffer (V x K), and host threads copy each chunk's rows into the
+    // caller's volume as soon as they are on the host, zeroing the others.
     float* host_out = out->coefficients;
     bool out_staged = false;
     if (pipelined) {
@@ -2620,7 +2685,8 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
                               attr.type == cudaMemoryTypeHost && attr.devicePointer;
       cudaGetLastError();
       if (!pinned_out) {
-        host_out = ensure_pinned(h->ostage, h->ostage_bytes, sizeof(float) * static_cast<size_t>(nvol) * K);
+        host_out = ensure_pinned(h->ostage, h->ostage_bytes,
+                                 sizeof(float) * static_cast<size_t>(std::max<int64_t>(masked_count(), 1)) * K);
         out_staged = true;
       }
     }
@@ -2630,6 +2696,7 @@ int csd_shore_fit_volume(csd_handle* h, const float* data, const uint8_t* mask, 
       hg.mask = mask;
       hg.stage = h->stage;
       hg.N = N;
+      hg.compact = stage_compact;
       if (!pipelined) {
         const auto t0 = std::chrono::steady_clock::now();
         gather_rows(hg, 0, nvol);
