@@ -166,8 +166,8 @@ def select_alpha_hypergradient(data, bvals, bvecs, mask, *, big_delta=None, smal
                              radial_order=radial_order, zeta=zeta, holdout_fraction=holdout_fraction, seed=seed,
                              device=device)
     rows = np.flatnonzero(mask.ravel())  # masked voxels in x-y-z order
-    S = torch.from_numpy(np.ascontiguousarray(np.take(data.reshape(-1, N), rows, axis=0), dtype=np.float32))
-    S = S.to(sel.device)
+    flat = torch.from_numpy(np.ascontiguousarray(data.reshape(-1, N), dtype=np.float32))
+    S = flat.index_select(0, torch.from_numpy(rows)).to(sel.device)  # a gather on all host threads
     alpha, loss, loss0, _ = sel.run(S, alpha0=alpha0, steps=steps)
     coef = sel.full.fit(S, alpha).detach()
     K = coef.shape[1]
