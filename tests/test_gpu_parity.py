@@ -412,6 +412,29 @@ def test_pipelined_host_fit_matches_the_device_fit():
     np.testing.assert_array_equal(out2, pageable["coefficients"])
 
 
+def test_pageable_buffers_of_small_and_empty_masks():
+    """Pageable input and output on the pipelined path when the mask is
+    small (one chunk; given as non-0/1 bytes, which the wrapper maps to 0/1)
+    or empty: the staging holds the masked rows only, the caller's output is
+    filled completely (masked rows from the fit, the others zero), and the
+    result equals the device-buffer fit bit for bit."""
+    import torch
+    from cs_dmri_b200 import shore_fit, shore_fit_device
+    from cs_dmri_b200.phantom import make_phantom
+    ph = make_phantom((20, 18, 10), seed=8)
+    kw = dict(big_delta=ph.big_delta, small_delta=ph.small_delta, alpha_mode="fixed", alpha=0.01)
+    mask8 = ph.mask.astype(np.uint8) * 7  # any non-zero byte is inside
+    out = np.full(ph.data.shape[:3] + (72,), np.nan, np.float32)
+    shore_fit(ph.data, ph.bvals, ph.bvecs, mask8, coefficients_out=out, **kw)
+    dev, _ = shore_fit_device(torch.from_numpy(ph.data).cuda(), torch.from_numpy(ph.mask).cuda(), ph.bvals,
+                              ph.bvecs, **kw)
+    np.testing.assert_array_equal(out, dev.cpu().numpy())
+    empty = np.zeros(ph.mask.shape, bool)
+    out0 = np.full(ph.data.shape[:3] + (72,), np.nan, np.float32)
+    shore_fit(ph.data, ph.bvals, ph.bvecs, empty, coefficients_out=out0, **kw)
+    assert np.all(out0 == 0.0)
+
+
 def test_fista_autotuner_choice_changes_nothing():
     """The per-table autotuner picks k_fista_v3's warps per CTA (12 or 16)
     from a timed synthetic batch; both give bit-identical fits."""
