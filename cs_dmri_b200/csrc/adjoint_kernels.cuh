@@ -13,13 +13,14 @@
 //       grad_alpha = -n sign(c_S) . w_S.
 //
 //   L2 (src/solver/tikhonov.rs:26-76) solves H c = M^T s with
-//   H = M^T M + lambda_N N + lambda_L L, one factor H = L L^T for all voxels:
+//   H = M^T M + lambda_N N + lambda_L L, one matrix for all voxels:
 //       w = H^{-1} gc,  grad_s = M w,
 //       grad_lambda_N = -w . (N c),  grad_lambda_L = -w . (L c).
 //
-// The factorisations and solves run every sum in index order with separate
-// multiply and add (no fused multiply-add), as a sequential FP64 evaluation
-// does; grad_s = M w is a fixed-matrix apply (k_apply64).
+// The L1 factorisations and solves run every sum in index order with
+// separate multiply and add (no fused multiply-add), as a sequential FP64
+// evaluation does; the L2 adjoint's w = H^{-1} gc and grad_s = M w are
+// fixed-matrix applies (k_apply_dmma).
 #pragma once
 
 namespace csd {
@@ -193,66 +194,40 @@ __global__ void __launch_bounds__(256) k_l1_adjoint(AdjointParams p) {
   }
 }
 
-// L2 adjoint, one warp per voxel, the factor of H staged once per CTA with
-// a padded row stride: w = H^{-1} gc into W and the hyper-parameter
-// gradients.
+// L2 adjoint: w = H^{-1} gc is one fixed-matrix product per voxel (the
+// explicit inverse, built once per table and regularisation from the factor
+// by its own solves, applied on the FP64 tensor cores by k_apply_dmma), and
+// this kernel takes the hyper-parameter gradients from it, one warp per voxel:
+// grad_lambda_N = -sum_k w_k c_k (n(n+1))^2, grad_lambda_L = -sum_k w_k c_k
+// (l(l+1))^2 (the diagonal regularisation matrices of src/basis/shore.rs).
 template <int RPL>
-__global__ void __launch_bounds__(256) k_l2_adjoint(AdjointParams p) {
-  extern __shared__ __align__(16) double adj_smem[];
-  const int K = p.K, Kp = p.Kp, ld = K + 1;
-  double* sL = adj_smem;
-  for (int i = threadIdx.x; i < K * K; i += blockDim.x) sL[(i / K) * ld + (i % K)] = p.G[(i / K) * Kp + (i % K)];
-  __syncthreads();
+__global__ void __launch_bounds__(256) k_l2_hyper(const double* __restrict__ W, int64_t ldw,
+                                                  const double* __restrict__ X, int64_t ldx, int64_t V, int K,
+                                                  int radial_order, double* __restrict__ ghyper) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nw = blockDim.x >> 5;
-  for (int64_t v = static_cast<int64_t>(blockIdx.x) * nw + warp; v < p.V;
-       v += static_cast<int64_t>(gridDim.x) * nw) {
-    double r[RPL];
+  double wn[RPL], wl[RPL];  // this lane's regularisation weights
 #pragma unroll
-    for (int c = 0; c < RPL; ++c) {
-      const int row = lane + 32 * c;
-      r[c] = (row < K) ? p.GC[v * p.ldg + row] : 0.0;
+  for (int c = 0; c < RPL; ++c) {
+    const int row = lane + 32 * c;
+    wn[c] = wl[c] = 0.0;
+    if (row < K) {
+      int n = 0, l = 0, kk = 0;
+      col_to_nlk(radial_order, row, &n, &l, &kk);
+      const double nn = static_cast<double>(n * (n + 1)), ll = static_cast<double>(l * (l + 1));
+      wn[c] = nn * nn;
+      wl[c] = ll * ll;
     }
-    for (int i = 0; i < K; ++i) {
-      const int owner = i & 31, oc = i >> 5;
-      double yi = 0.0;
-#pragma unroll
-      for (int c = 0; c < RPL; ++c)
-        if (c == oc && lane == owner) yi = __ddiv_rn(r[c], sL[i * ld + i]);
-      yi = __shfl_sync(kFull, yi, owner);
-#pragma unroll
-      for (int c = 0; c < RPL; ++c) {
-        const int row = lane + 32 * c;
-        if (row > i && row < K) r[c] = __dsub_rn(r[c], __dmul_rn(sL[row * ld + i], yi));
-        if (row == i) r[c] = yi;
-      }
-    }
-    for (int i = K - 1; i >= 0; --i) {
-      const int owner = i & 31, oc = i >> 5;
-      double xi = 0.0;
-#pragma unroll
-      for (int c = 0; c < RPL; ++c)
-        if (c == oc && lane == owner) xi = __ddiv_rn(r[c], sL[i * ld + i]);
-      xi = __shfl_sync(kFull, xi, owner);
-#pragma unroll
-      for (int c = 0; c < RPL; ++c) {
-        const int row = lane + 32 * c;
-        if (row < i) r[c] = __dsub_rn(r[c], __dmul_rn(sL[i * ld + row], xi));
-        if (row == i) r[c] = xi;
-      }
-    }
+  }
+  for (int64_t v = static_cast<int64_t>(blockIdx.x) * nw + warp; v < V; v += static_cast<int64_t>(gridDim.x) * nw) {
     double dn = 0.0, dl = 0.0;
-    const double* x = p.X + v * p.ldx;
 #pragma unroll
     for (int c = 0; c < RPL; ++c) {
       const int row = lane + 32 * c;
       if (row < K) {
-        int n = 0, l = 0, kk = 0;
-        col_to_nlk(p.radial_order, row, &n, &l, &kk);
-        const double nn = static_cast<double>(n * (n + 1)), ll = static_cast<double>(l * (l + 1));
-        const double wc = __dmul_rn(r[c], x[row]);
-        dn = __dadd_rn(dn, __dmul_rn(wc, nn * nn));
-        dl = __dadd_rn(dl, __dmul_rn(wc, ll * ll));
+        const double wc = __dmul_rn(W[v * ldw + row], X[v * ldx + row]);
+        dn = __dadd_rn(dn, __dmul_rn(wc, wn[c]));
+        dl = __dadd_rn(dl, __dmul_rn(wc, wl[c]));
       }
     }
 #pragma unroll
@@ -260,16 +235,18 @@ __global__ void __launch_bounds__(256) k_l2_adjoint(AdjointParams p) {
       dn += __shfl_xor_sync(kFull, dn, o);
       dl += __shfl_xor_sync(kFull, dl, o);
     }
-#pragma unroll
-    for (int c = 0; c < RPL; ++c) {
-      const int row = lane + 32 * c;
-      if (row < Kp) p.W[v * Kp + row] = (row < K) ? r[c] : 0.0;
-    }
-    if (lane == 0 && p.ghyper) {
-      p.ghyper[2 * v] = -dn;
-      p.ghyper[2 * v + 1] = -dl;
+    if (lane == 0) {
+      ghyper[2 * v] = -dn;
+      ghyper[2 * v + 1] = -dl;
     }
   }
+}
+
+// Identity rows (K x Kp, zero padded): the right-hand sides whose solves give
+// the rows of H^{-1}.
+__global__ void k_identity_rows(double* __restrict__ I, int K, int Kp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < K * Kp) I[i] = ((i % Kp) == (i / Kp)) ? 1.0 : 0.0;
 }
 
 // out[v][r] = sum over k < cols of At[k * rows + r] in[v][k]: a fixed matrix
@@ -322,61 +299,114 @@ __global__ void __launch_bounds__(256) k_apply64(const double* __restrict__ At, 
 // order, frag[(mt * KT + kt) * 32 + lane] = A[8 mt + lane / 4][4 kt + lane % 4]
 // (zero padded; read from At), so each fragment is one conflict-free 256-byte
 // read.  A warp takes 8 voxels at a time: out^T (rows x 8) = A in^T, the
-// voxels' inputs as B fragments (loaded once per k-step and reused across a
-// chunk of kApplyMtc row tiles held as accumulators).
+// voxels' inputs as B fragments, reused across a chunk of kApplyMtc row tiles
+// held as accumulators.  The fragments come from global memory, so they are
+// fetched well ahead of their DMMAs: with KT <= kApplyKtr (inputs of up to 96
+// entries) a group's KT fragments sit in registers and serve every row
+// chunk, and the next group's are loaded while this one computes; longer
+// inputs stream through a ring of kApplyPf fragments.  Every tile accumulates
+// its k-steps in increasing order either way.
 constexpr int kApplyMtc = 12;
+constexpr int kApplyKtr = 24;
+constexpr int kApplyPf = 8;
 
+template <bool kRegs>
 __global__ void __launch_bounds__(256, 1) k_apply_dmma(const double* __restrict__ At, int rows, int cols,
                                                        const double* __restrict__ in, int64_t ldin, int64_t V,
                                                        double* __restrict__ out, float* __restrict__ out32,
                                                        int64_t ldout) {
   extern __shared__ __align__(16) double sA[];
   const int MT = (rows + 7) / 8, KT = (cols + 3) / 4;
-  for (int i = threadIdx.x; i < MT * KT * 32; i += blockDim.x) {
-    const int lane = i & 31, t = i >> 5, mt = t / KT, kt = t % KT;
-    const int r = 8 * mt + (lane >> 2), k = 4 * kt + (lane & 3);
-    sA[i] = (r < rows && k < cols) ? At[static_cast<size_t>(k) * rows + r] : 0.0;
+  const int n_frag = MT * KT * 32;
+  for (int i0 = threadIdx.x; i0 < n_frag; i0 += 8 * blockDim.x) {  // eight loads in flight per thread
+    double vals[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int i = i0 + u * blockDim.x;
+      const int lane = i & 31, t = i >> 5, mt = t / KT, kt = t % KT;
+      const int r = 8 * mt + (lane >> 2), k = 4 * kt + (lane & 3);
+      vals[u] = (i < n_frag && r < rows && k < cols) ? At[static_cast<size_t>(k) * rows + r] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (i0 + u * static_cast<int>(blockDim.x) < n_frag) sA[i0 + u * blockDim.x] = vals[u];
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, q = lane & 3;
   const int64_t groups = (V + 7) / 8;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
-  for (int64_t grp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp; grp < groups; grp += nwarps) {
-    const int64_t v0 = 8 * grp;
-    const int64_t vb = v0 + g;  // this lane's voxel in the B fragment
-    const bool vok = vb < V;
-    for (int mt0 = 0; mt0 < MT; mt0 += kApplyMtc) {
-      double d[kApplyMtc][2];
+  auto frag = [&](int64_t grp, int kt) -> double {  // this lane's B entry of k-step kt of a group
+    const int64_t vb = 8 * grp + g;
+    const int k = 4 * kt + q;
+    return (grp < groups && vb < V && k < cols) ? in[vb * ldin + k] : 0.0;
+  };
+  auto store = [&](int64_t v0, int mt0, const double (&d)[kApplyMtc][2]) {
 #pragma unroll
-      for (int j = 0; j < kApplyMtc; ++j) d[j][0] = d[j][1] = 0.0;
-      // B fragments two k-steps ahead, so a global load is in flight while
-      // the DMMAs of the current k-step issue
-      double bq[3];
+    for (int j = 0; j < kApplyMtc; ++j) {
+      const int r = 8 * (mt0 + j) + g;
+      if (mt0 + j >= MT || r >= rows) continue;
 #pragma unroll
-      for (int u = 0; u < 3; ++u) bq[u] = (vok && 4 * u + q < cols && u < KT) ? in[vb * ldin + 4 * u + q] : 0.0;
-      for (int kt = 0; kt < KT; ++kt) {
-        const double b = bq[0];
-        bq[0] = bq[1];
-        bq[1] = bq[2];
-        const int kn = 4 * (kt + 3) + q;
-        bq[2] = (vok && kn < cols) ? in[vb * ldin + kn] : 0.0;
-#pragma unroll
-        for (int j = 0; j < kApplyMtc; ++j)
-          if (mt0 + j < MT) dmma_m8n8k4(d[j][0], d[j][1], sA[((mt0 + j) * KT + kt) * 32 + lane], b);
+      for (int e = 0; e < 2; ++e) {
+        const int64_t vv = v0 + 2 * q + e;
+        if (vv < V) {
+          if (out) out[vv * ldout + r] = d[j][e];
+          if (out32) out32[vv * ldout + r] = static_cast<float>(d[j][e]);
+        }
       }
+    }
+  };
+  int64_t grp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp;
+  if constexpr (kRegs) {
+    double bn[kApplyKtr];
 #pragma unroll
-      for (int j = 0; j < kApplyMtc; ++j) {
-        const int r = 8 * (mt0 + j) + g;
-        if (mt0 + j >= MT || r >= rows) continue;
+    for (int kt = 0; kt < kApplyKtr; ++kt) bn[kt] = kt < KT ? frag(grp, kt) : 0.0;
+    for (; grp < groups; grp += nwarps) {
+      double bc[kApplyKtr];
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int64_t vv = v0 + 2 * q + e;
-          if (vv < V) {
-            if (out) out[vv * ldout + r] = d[j][e];
-            if (out32) out32[vv * ldout + r] = static_cast<float>(d[j][e]);
+      for (int kt = 0; kt < kApplyKtr; ++kt) {
+        bc[kt] = bn[kt];
+        bn[kt] = kt < KT ? frag(grp + nwarps, kt) : 0.0;  // the next group's, in flight meanwhile
+      }
+      for (int mt0 = 0; mt0 < MT; mt0 += kApplyMtc) {
+        double d[kApplyMtc][2];
+#pragma unroll
+        for (int j = 0; j < kApplyMtc; ++j) d[j][0] = d[j][1] = 0.0;
+#pragma unroll
+        for (int kt = 0; kt < kApplyKtr; ++kt) {
+          if (kt >= KT) break;
+#pragma unroll
+          for (int j = 0; j < kApplyMtc; ++j)
+            if (mt0 + j < MT) dmma_m8n8k4(d[j][0], d[j][1], sA[((mt0 + j) * KT + kt) * 32 + lane], bc[kt]);
+        }
+        store(8 * grp, mt0, d);
+      }
+    }
+  } else {
+    for (; grp < groups; grp += nwarps) {
+      for (int mt0 = 0; mt0 < MT; mt0 += kApplyMtc) {
+        double d[kApplyMtc][2];
+#pragma unroll
+        for (int j = 0; j < kApplyMtc; ++j) d[j][0] = d[j][1] = 0.0;
+        // slot u holds k-step kt0 + u; once its DMMAs have read it, it is
+        // refilled with k-step kt0 + u + kApplyPf (no register moves, which
+        // would wait for loads still in flight)
+        double bq[kApplyPf];
+#pragma unroll
+        for (int u = 0; u < kApplyPf; ++u) bq[u] = frag(grp, u);
+        for (int kt0 = 0; kt0 < KT; kt0 += kApplyPf) {
+#pragma unroll
+          for (int u = 0; u < kApplyPf; ++u) {
+            const int kt = kt0 + u;
+            if (kt < KT) {
+#pragma unroll
+              for (int j = 0; j < kApplyMtc; ++j)
+                if (mt0 + j < MT) dmma_m8n8k4(d[j][0], d[j][1], sA[((mt0 + j) * KT + kt) * 32 + lane], bq[u]);
+              bq[u] = frag(grp, kt + kApplyPf);
+            }
           }
         }
+        store(8 * grp, mt0, d);
       }
     }
   }

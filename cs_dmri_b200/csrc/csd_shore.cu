@@ -270,6 +270,9 @@ struct csd_handle {
   // mtfrag), so an L2 fit is the single product c = P s; built with the factor
   DevBuf pfrag, ptmp;
   bool pfrag_valid = false;
+  DevBuf hinv;                // H^{-1} of the current factor (L2 adjoint)
+  bool hinv_valid = false;
+  uint64_t hinv_key = 0;
   DevBuf mom;      // Nesterov momentum table (t_k - 1) / t_{k+1}
   int mom_len = 0;
   // amplitude-ICLS setup: constraint C (m x K), factor of M^T M + eps I, W = L^{-1} C^T
@@ -2503,7 +2506,7 @@ void csd_destroy(csd_handle* h) {
                     &h->pbest, &h->psel, &h->pact, &h->palpha_sel, &h->pit_sel, &h->pconv_sel,
                     &h->palpha_fb, &h->pit_fb, &h->pconv_fb, &h->pcode, &h->gdig, &h->gfexp, &h->flagged,
                     &h->mixstat, &h->pcoef, &h->pmat, &h->pout, &h->pgt, &h->pgv, &h->pdir, &h->pconst,
-                    &h->iota, &h->adjW, &h->adjovf, &h->adjstat, &h->adjconst,
+                    &h->iota, &h->adjW, &h->adjovf, &h->adjstat, &h->adjconst, &h->hinv,
                     &h->gdtab, &h->gdq, &h->tuneB, &h->tuneX, &h->tuneIt, &h->tuneConv, &h->tuneQ,
                     &h->schedY, &h->schedPend, &h->schedKey, &h->schedOrder, &h->schedCnt,
                     &h->schedD, &h->schedU, &h->schedN, &h->gtf32, &h->x32, &h->kktv, &h->kktovf,

@@ -130,20 +130,43 @@ void launch_l1_adjoint_t(csd_handle* h, const csd::AdjointParams& p0) {
   CSD_LAUNCH();
 }
 
+void launch_apply64(csd_handle* h, const double* At, int rows, int cols, const double* in, int64_t ldin, int64_t V,
+                    double* out, float* out32, int64_t ldout);
+
+// H^{-1} (K x K, row k = H^{-1} e_k) for the current factor, by the factor's
+// solves of the identity rows; kept until the factor changes.
+void ensure_hinv(csd_handle* h) {
+  if (h->hinv_valid && h->hinv_key == h->chol_key) return;
+  const int K = h->K, Kp = h->Kp;
+  cudaStream_t st = h->stream;
+  h->ptmp.ensure(2 * sizeof(double) * static_cast<size_t>(K) * Kp);
+  double* id = h->ptmp.as<double>();
+  double* rows = id + static_cast<size_t>(K) * Kp;
+  csd::k_identity_rows<<<(K * Kp + 255) / 256, 256, 0, st>>>(id, K, Kp);
+  CSD_LAUNCH();
+  launch_tikhonov(h, id, rows, K);
+  h->hinv.ensure(sizeof(double) * static_cast<size_t>(K) * K);
+  CSD_CUDA(cudaMemcpy2DAsync(h->hinv.p, sizeof(double) * K, rows, sizeof(double) * Kp, sizeof(double) * K, K,
+                             cudaMemcpyDeviceToDevice, st));
+  h->hinv_key = h->chol_key;
+  h->hinv_valid = true;
+}
+
+// L2 adjoint: w = H^{-1} gc (the rows of H^{-1} are its columns, so they are
+// the apply's transposed operand as they stand), then the hyper-parameter
+// gradients from w and c.
 template <int RPL>
 void launch_l2_adjoint_t(csd_handle* h, const csd::AdjointParams& p) {
-  const int warps = 8;
-  const size_t smem = sizeof(double) * ((static_cast<size_t>(p.K) * (p.K + 1) + 1) / 2 * 2);
-  if (smem > static_cast<size_t>(h->smem_optin))
-    throw Error{CSD_ERR_INVALID, "coefficient count too large for the L2 adjoint"};
-  CSD_CUDA(cudaFuncSetAttribute(csd::k_l2_adjoint<RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(smem)));
-  int per_sm = 0;
-  CSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, csd::k_l2_adjoint<RPL>, 32 * warps, smem));
-  const int64_t blocks = std::max<int64_t>(
-      1, std::min<int64_t>((p.V + warps - 1) / warps, static_cast<int64_t>(h->num_sms) * std::max(per_sm, 1)));
-  csd::k_l2_adjoint<RPL><<<static_cast<unsigned>(blocks), 32 * warps, smem, h->stream>>>(p);
-  CSD_LAUNCH();
+  ensure_hinv(h);
+  launch_apply64(h, h->hinv.as<double>(), p.K, p.K, p.GC, p.ldg, p.V, p.W, nullptr, p.Kp);
+  if (p.ghyper) {
+    const int warps = 8;
+    const int64_t blocks =
+        std::max<int64_t>(1, std::min<int64_t>((p.V + warps - 1) / warps, static_cast<int64_t>(h->num_sms) * 8));
+    csd::k_l2_hyper<RPL><<<static_cast<unsigned>(blocks), 32 * warps, 0, h->stream>>>(
+        p.W, p.Kp, p.X, p.ldx, p.V, p.K, p.radial_order, p.ghyper);
+    CSD_LAUNCH();
+  }
 }
 
 template <template <int> class F>
@@ -171,13 +194,18 @@ void launch_apply64(csd_handle* h, const double* At, int rows, int cols, const d
   // tensor-core path when the matrix fits in one CTA's shared memory
   const size_t dmma_smem = sizeof(double) * 32 * static_cast<size_t>((rows + 7) / 8) * ((cols + 3) / 4);
   if (dmma_smem <= static_cast<size_t>(h->smem_optin)) {
-    CSD_CUDA(cudaFuncSetAttribute(csd::k_apply_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(dmma_smem)));
     const int64_t groups = (V + 7) / 8;
     const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((groups + 7) / 8, h->num_sms));
-    csd::k_apply_dmma<<<static_cast<unsigned>(blocks), 256, dmma_smem, h->stream>>>(At, rows, cols, in, ldin, V,
-                                                                                    out, out32, ldout);
-    CSD_LAUNCH();
+    auto go = [&](auto kern) {
+      CSD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dmma_smem)));
+      kern<<<static_cast<unsigned>(blocks), 256, dmma_smem, h->stream>>>(At, rows, cols, in, ldin, V, out, out32,
+                                                                         ldout);
+      CSD_LAUNCH();
+    };
+    if ((cols + 3) / 4 <= csd::kApplyKtr)
+      go(csd::k_apply_dmma<true>);
+    else
+      go(csd::k_apply_dmma<false>);
     return;
   }
   const size_t per_warp = sizeof(double) * 8 * static_cast<size_t>(cols);

@@ -11,11 +11,12 @@
 // One persistent CTA per SM takes voxels from a queue.  Per voxel:
 //   1. kept rows, effective b and direction per row;
 //   2. G_v = M_v^T M_v on the FP64 tensor cores (DMMA m8n8k4): the geometry
-//      of every kept row first, then the design generated 64 rows at a time
-//      into shared memory (radial factors per
-//      (n, l) and SH values per (l, m), multiplied per column), each warp
-//      accumulating a fixed set of 8 x 8 tiles of the upper triangle in
-//      registers; b_v = M_v^T s_v alongside;
+//      of every kept row first, then 64 rows at a time in factored form in
+//      shared memory (radial factors per (n, l) and SH values per (l, k); a
+//      design entry is the product of one of each, formed as the DMMA
+//      operand fragment is loaded), each warp accumulating one rectangle or
+//      two triangles of 8 x 8 tiles of the upper triangle in registers
+//      (GramPlan); b_v = M_v^T s_v alongside;
 //   3. lambda_max(G_v) by Lanczos (a fixed number of steps, the largest Ritz
 //      value by multisection of the tridiagonal's Sturm count, one point per
 //      thread);
@@ -64,20 +65,25 @@ struct GraddevParams {
 };
 
 // Shared-memory plan (doubles unless noted), shared by host and device.
+// While G is built its region holds a chunk of kGdChunk design rows in
+// factored form: each entry of the design is the product of a radial factor
+// (one per (n, l)) and a real SH value (one per (l, k)), so a chunk keeps the
+// rows' NL radial factors (row stride RS, one more slot that holds 0 for the
+// padding columns) and NSH SH values (row stride YS); both strides are odd,
+// so the fragment loads of four consecutive rows fall in distinct banks.
 struct GdLayout {
-  int K, Kp, LDG, LDM, NL, NSH, NLM, NTR;
+  int K, Kp, LDG, NL, NSH, RS, YS;
   size_t g, vec, red, tri, tab, rows, colmap, total_bytes;
   __host__ __device__ GdLayout(int K_, int radial_order, int N) {
     K = K_;
     Kp = 8 * ((K + 7) / 8);
     LDG = K + (K & 1);   // even row stride of G: 16-byte rows, conflict-free 16-byte loads
-    LDM = Kp + 4;        // chunk row stride: conflict-free fragment loads
     NL = 0;
     for (int n = 0; n <= radial_order; ++n) NL += n / 2 + 1;
     NSH = (radial_order / 2 + 1) * (radial_order + 1);
-    NLM = (radial_order / 2 + 1) * (radial_order / 2 + 1);  // P_l^m, l even, 0 <= m <= l
-    NTR = 2 * radial_order;                                  // cos(m theta), sin(m theta), m = 1..order
-    const size_t chunk = static_cast<size_t>(kGdChunk) * (LDM + NL + NLM + NTR) + 8 * static_cast<size_t>(N);
+    RS = (NL + 1) | 1;
+    YS = NSH | 1;
+    const size_t chunk = static_cast<size_t>(kGdChunk) * (RS + YS) + 8 * static_cast<size_t>(N);
     const size_t gk = static_cast<size_t>(K) * LDG;
     const size_t gsize = gk > chunk ? gk : chunk;
     g = 0;
@@ -102,6 +108,20 @@ __device__ __forceinline__ double gd_block_sum(double a, double* red) {
   __syncthreads();
   double s = 0.0;
   for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += red[w];
+  return s;
+}
+
+// The same sum into slots no thread reads any more, so without the barrier
+// before the write: the caller separates the reads of an earlier sum into
+// `slots` from this write by a barrier of its own.
+__device__ __forceinline__ double gd_block_sum_fresh(double a, double* slots) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(kFull, a, o);
+  if (lane == 0) slots[warp] = a;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += slots[w];
   return s;
 }
 
@@ -137,6 +157,25 @@ __device__ __forceinline__ void gd_gemv(const double* G, int LDG, int K, const d
   }
 }
 
+// Work split of G's upper triangle of MT x MT tiles (8 x 8 each) between the
+// CTA's 8 warps.  The tile indices fall into NG groups of GS; a pair of
+// groups I < J is a GS x GS rectangle of tiles, a group I alone the triangle
+// of tiles (i, j), i <= j, inside it.  Warps 0 .. NR-1 take one rectangle
+// each, the others TPT triangles each.  Per k-step a warp then loads 2 GS
+// operand fragments (one per tile row or column it touches) for up to GS^2
+// products, where a list of independent tiles needs two loads per product.
+template <int MT>
+struct GramPlan {
+  static constexpr int GS = (MT > 9) ? 5 : 3;
+  static constexpr int NG = (MT + GS - 1) / GS;
+  static constexpr int NR = NG * (NG - 1) / 2;              // rectangles
+  static constexpr int TW = 8 - NR;                          // warps on triangles
+  static constexpr int TPT = (NG + TW - 1) / TW;             // triangles per such warp
+  static constexpr int TRI = GS * (GS + 1) / 2;              // tiles of one triangle
+  static constexpr int ACC = (GS * GS > TPT * TRI) ? GS * GS : TPT * TRI;
+  static_assert(NR <= 8 && TW >= 1 && TPT <= 2, "gram plan");
+};
+
 // Count of eigenvalues of the symmetric tridiagonal (a, b) below x (Sturm).
 __device__ __forceinline__ int sturm_below(const double* a, const double* b, int m, double x) {
   int c = 0;
@@ -152,17 +191,15 @@ __device__ __forceinline__ int sturm_below(const double* a, const double* b, int
 
 template <int MT>
 __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevParams p) {
-  constexpr int NT = MT * (MT + 1) / 2;  // upper-triangle tiles of G
-  constexpr int TPW = (NT + 7) / 8;      // tiles per warp
+  using GP = GramPlan<MT>;
+  constexpr int GS = GP::GS;
   extern __shared__ __align__(16) double gd_smem[];
   const GdLayout L(p.K, p.radial_order, p.N);
-  const int K = p.K, Kp = L.Kp, LDM = L.LDM, NL = L.NL, NSH = L.NSH, N = p.N;
+  const int K = p.K, Kp = L.Kp, NL = L.NL, NSH = L.NSH, RS = L.RS, YS = L.YS, N = p.N;
   double* G = gd_smem + L.g;
-  double* Mc = G;                                  // chunk: kGdChunk x LDM (aliases G while it is built)
-  double* rad = Mc + kGdChunk * LDM;               // kGdChunk x NL radial factors
-  double* leg = rad + kGdChunk * NL;               // kGdChunk x NLM associated Legendre values
-  double* trg = leg + kGdChunk * L.NLM;            // kGdChunk x NTR cos / sin of m theta
-  double* gall = trg + kGdChunk * L.NTR;           // N x 8 per kept row: r, theta, phi, signal, cos phi, u, exp(-u/2)
+  double* Rv = G;                                  // chunk: kGdChunk x RS radial factors (aliases G while it is built)
+  double* Yv = Rv + kGdChunk * RS;                 // kGdChunk x YS real SH values
+  double* gall = Yv + kGdChunk * YS;               // N x 8 per kept row: r, theta, phi, signal, cos phi, u, exp(-u/2)
   double* vb = gd_smem + L.vec;
   double* vx = vb + Kp;
   double* vy = vx + Kp;
@@ -176,8 +213,7 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
   double* kap = gd_smem + L.tab;                   // NL: kappa(zeta, n, l)
   double* shn = kap + NL;                          // NSH: SH normalisation of (l, k)
   int* rows = reinterpret_cast<int*>(gd_smem + L.rows);
-  int* col_map = reinterpret_cast<int*>(gd_smem + L.colmap);  // K: (radial block << 8) | SH entry
-  int* task_map = col_map + K;                                 // NL + NSH: (n or m) << 16 | l << 8 | k
+  int* col_map = reinterpret_cast<int*>(gd_smem + L.colmap);  // K: radial factor | SH entry << 16
   __shared__ int64_t s_v;
   __shared__ int s_n;
   __shared__ double s_lmax;
@@ -192,7 +228,7 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, q = lane & 3;
 
-  // column -> (radial block, SH entry) and the per-(n, l) / per-(l, k)
+  // column -> (radial factor, SH entry) and the per-(n, l) / per-(l, k)
   // constants, once per CTA (the same expressions as dev_shore_radial and
   // dev_brainsuite_sh evaluate per entry)
   for (int col = tid; col < K; col += blockDim.x) {
@@ -202,7 +238,7 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
     for (int nn = 0; nn < n; ++nn) nl += nn / 2 + 1;
     int lk = 0;
     for (int ll = 0; ll < l; ll += 2) lk += 2 * ll + 1;
-    col_map[col] = ((nl + l / 2) << 8) | (lk + k);
+    col_map[col] = (nl + l / 2) | ((lk + k) << 16);
   }
   for (int j = tid; j < NL + NSH; j += blockDim.x) {
     if (j < NL) {
@@ -212,7 +248,6 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
         ++nn;
       }
       kap[j] = dev_kappa(p.zeta, nn, 2 * rem);
-      task_map[j] = (nn << 16) | ((2 * rem) << 8);
     } else {
       int l = 0, rem = j - NL;
       while (rem >= 2 * l + 1) {
@@ -221,23 +256,36 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
       }
       const int m = (rem < l) ? l - rem : (rem == l ? 0 : rem - l);
       shn[j - NL] = sqrt((2.0 * l + 1.0) / (4.0 * CUDART_PI) * dev_factorial(l - m) / dev_factorial(l + m));
-      task_map[j] = (m << 16) | (l << 8) | rem;
     }
-  }
-  // this warp's tiles of the upper triangle, packed (mt << 8) | nt; nt >= MT
-  // marks an unused slot
-  int tile[TPW];
-#pragma unroll
-  for (int s = 0; s < TPW; ++s) {
-    const int tau = warp + 8 * s;
-    int mt = 0, rem = tau;
-    while (mt < MT && rem >= MT - mt) {
-      rem -= MT - mt;
-      ++mt;
-    }
-    tile[s] = (mt << 8) | (mt + rem);
   }
   __syncthreads();
+  // this warp's share of G's upper triangle (GramPlan): tile-index groups ga
+  // (and gb), and this lane's design column in each tile row / column it
+  // touches, as (radial factor | SH entry << 16); padding columns point at
+  // the chunk rows' zero slot
+  const bool is_rect = warp < GP::NR;
+  int ga = GP::NG, gb = GP::NG;  // NG: none
+  if (is_rect) {
+    int rem = warp;
+    ga = 0;
+    while (rem >= GP::NG - 1 - ga) {
+      rem -= GP::NG - 1 - ga;
+      ++ga;
+    }
+    gb = ga + 1 + rem;
+  } else {
+    ga = (warp - GP::NR) * GP::TPT;
+    if (GP::TPT == 2) gb = ga + 1;
+    if (ga > GP::NG) ga = GP::NG;
+    if (gb > GP::NG) gb = GP::NG;
+  }
+  int ca[GS], cb[GS];
+#pragma unroll
+  for (int i = 0; i < GS; ++i) {
+    const int c1 = 8 * (ga * GS + i) + g, c2 = 8 * (gb * GS + i) + g;
+    ca[i] = (ga < GP::NG && c1 < K) ? col_map[c1] : NL;
+    cb[i] = (gb < GP::NG && c2 < K) ? col_map[c2] : NL;
+  }
 
   unsigned long long executed = 0;
   while (true) {
@@ -301,67 +349,83 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
       gall[8 * r + 6] = exp(-u * 0.5);
     }
     __syncthreads();
-    double acc[TPW][2];  // this warp's tiles of G (declared after the geometry: fewer live registers there)
+    double acc[GP::ACC][2];  // this warp's tiles of G (declared after the geometry: fewer live registers there)
 #pragma unroll
-    for (int s = 0; s < TPW; ++s) acc[s][0] = acc[s][1] = 0.0;
+    for (int s = 0; s < GP::ACC; ++s) acc[s][0] = acc[s][1] = 0.0;
     for (int c0 = 0; c0 < n; c0 += kGdChunk) {
       const double* geo = gall + 8 * static_cast<size_t>(c0);
 
-      // per-row values, one thread per row in each of three groups: radial
-      // factors (group 0), cos / sin of m theta (group 1), associated
-      // Legendre values by the recurrence in l for each m (group 2).  The
-      // formulas are those of dev_shore_radial and dev_brainsuite_sh, with
-      // the costly steps replaced: integer powers by products, the
-      // recurrences' divisions by reciprocal products, and cos / sin of
-      // m theta by rotation.  So the entries agree with the shared-design
-      // kernel's to a few units in the last place, not bit for bit.
+      // the chunk's rows in factored form, one thread per row in each of four
+      // groups: radial factors for l = 0 and l >= 6 (group 0) and for
+      // l = 2, 4 (group 3); real SH values for even m (group 1) and odd m
+      // (group 2).  The formulas are those of dev_shore_radial and
+      // dev_brainsuite_sh, with the costly steps replaced: integer powers by
+      // products, the recurrences' divisions by reciprocal products, and
+      // cos / sin of m theta by rotation.  So the entries agree with the
+      // shared-design kernel's to a few units in the last place, not bit for
+      // bit.  Rows past the last kept one are zero.
       {
         const int t = tid % kGdChunk, grp = tid / kGdChunk;
         const double* gt = geo + 8 * t;
         const int R = p.radial_order;
+        double* Rt = Rv + t * RS;
+        double* Yt = Yv + t * YS;
         if (c0 + t >= n) {
-          // past the last row: nothing to evaluate (the chunk entries are 0)
-        } else if (grp == 0) {
-          // u^(l/2) (l even) by products; the generalised Laguerre
-          // L_{n-l}^{(l+1/2)}(u) by its three-term recurrence with the
-          // divisor k + 1 taken as a product with 1 / (k + 1)
+          if (grp == 0)
+            for (int j = 0; j < RS; ++j) Rt[j] = 0.0;
+          else if (grp == 1)
+            for (int j = 0; j < YS; ++j) Yt[j] = 0.0;
+        } else if (grp == 0 || grp == 3) {
+          // exp(-u/2) u^(l/2) L_{n-l}^{(l+1/2)}(u): the generalised Laguerre
+          // polynomials of every degree n - l from one three-term recurrence
+          // per l, with the divisor k + 1 taken as a product with 1 / (k + 1)
           const double u = gt[5];
-          double rp[9];
-          rp[0] = 1.0;
-          for (int h = 1; h <= R / 2; ++h) rp[h] = rp[h - 1] * u;
-          int j = 0;
-          for (int nn = 0; nn <= R; ++nn)
-            for (int l = 0; l <= nn; l += 2, ++j) {
-              const int deg = nn - l;
-              const double al = static_cast<double>(l) + 0.5;
-              double lag = 1.0;
-              if (deg >= 1) {
-                double lkm1 = 1.0, lk = 1.0 + al - u;
-                for (int k = 1; k < deg; ++k) {
-                  const double kf = k;
-                  const double lkp1 = ((2.0 * kf + 1.0 + al - u) * lk - (kf + al) * lkm1) * gd_rcp[k + 1];
-                  lkm1 = lk;
-                  lk = lkp1;
-                }
+          if (grp == 0) Rt[NL] = 0.0;  // the padding columns' factor
+          double upow = 1.0;
+          for (int l = 0; l <= R; l += 2) {
+            if (l > 0) upow *= u;  // u^(l/2) by products
+            if ((grp == 0) != (l == 0 || l >= 6)) continue;
+            const double al = static_cast<double>(l) + 0.5;
+            double lkm1 = 1.0, lk = 1.0 + al - u;
+            for (int deg = 0; l + deg <= R; ++deg) {
+              double lag;
+              if (deg == 0) {
+                lag = 1.0;
+              } else if (deg == 1) {
+                lag = lk;
+              } else {
+                const double kf = deg - 1;
+                const double lkp1 = ((2.0 * kf + 1.0 + al - u) * lk - (kf + al) * lkm1) * gd_rcp[deg];
+                lkm1 = lk;
+                lk = lkp1;
                 lag = lk;
               }
-              rad[t * NL + j] = kap[j] * lag * gt[6] * rp[l / 2];
+              const int nn = l + deg;
+              const int j = ((nn & 1) ? ((nn + 1) / 2) * ((nn + 1) / 2) : (nn / 2) * (nn / 2 + 1)) + l / 2;
+              Rt[j] = kap[j] * lag * gt[6] * upow;
             }
-        } else if (grp == 1) {
-          // cos / sin of m theta by rotation from those of theta
+          }
+        } else {
+          // P_l^m for l = m, m + 1, ..., R (dev_assoc_legendre's steps), times
+          // the SH normalisation and cos / sin of m theta (by rotation from
+          // those of theta)
+          const double x = gt[4];
           double s1, c1;
           sincos(gt[1], &s1, &c1);
-          double cm = c1, sm = s1;
-          for (int mm = 1; mm <= R; ++mm) {
-            trg[t * L.NTR + mm - 1] = cm;
-            trg[t * L.NTR + R + mm - 1] = sm;
-            const double cn = fma(cm, c1, -sm * s1), sn = fma(sm, c1, cm * s1);
-            cm = cn;
-            sm = sn;
-          }
-        } else if (grp == 2) {
-          const double x = gt[4];
-          for (int mm = 0; mm <= R; ++mm) {  // P_l^m for l = m, m + 1, ..., R (dev_assoc_legendre's steps)
+          double cm = 1.0, sm = 0.0;
+          const double s2 = sqrt(2.0);
+          for (int mm = 0; mm <= R; ++mm) {
+            if (mm > 0) {
+              if (mm == 1) {
+                cm = c1;
+                sm = s1;
+              } else {
+                const double cn = fma(cm, c1, -sm * s1), sn = fma(sm, c1, cm * s1);
+                cm = cn;
+                sm = sn;
+              }
+            }
+            if ((mm & 1) != (grp == 2 ? 1 : 0)) continue;
             double pmm = 1.0;
             if (mm > 0) {
               const double somx2 = sqrt(fmax((1.0 - x) * (1.0 + x), 0.0));
@@ -371,76 +435,101 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
                 fact += 2.0;
               }
             }
-            if (mm % 2 == 0) leg[t * L.NLM + (mm / 2) * (mm / 2) + mm] = pmm;
+            // the SH values of P_l^mm, l even: (l, l) for m = 0 (1 / sqrt(4 pi)
+            // at l = 0), (l, l - m) with cos and (l, l + m) with sin otherwise
+            auto emit = [&](int l, double P) {
+              const int lk = (l / 2) * (l - 1);
+              if (mm == 0) {
+                Yt[lk + l] = (l == 0) ? 1.0 / sqrt(4.0 * CUDART_PI) : shn[lk + l] * P;
+              } else {
+                const double plc = shn[lk + l - mm] * P;
+                Yt[lk + l - mm] = s2 * plc * cm;
+                const double pls = shn[lk + l + mm] * P;
+                Yt[lk + l + mm] = s2 * (((mm + 1) % 2 == 0) ? 1.0 : -1.0) * pls * sm;
+              }
+            };
+            if (mm % 2 == 0) emit(mm, pmm);
             if (mm + 1 > R) continue;
             double pmmp1 = x * (2.0 * mm + 1.0) * pmm;
-            if ((mm + 1) % 2 == 0) leg[t * L.NLM + ((mm + 1) / 2) * ((mm + 1) / 2) + mm] = pmmp1;
+            if ((mm + 1) % 2 == 0) emit(mm + 1, pmmp1);
             for (int ll = mm + 2; ll <= R; ++ll) {
               const double llf = ll, mf = mm;
               const double pll = ((2.0 * llf - 1.0) * x * pmmp1 - (llf + mf - 1.0) * pmm) * gd_rcp[ll - mm];
               pmm = pmmp1;
               pmmp1 = pll;
-              if (ll % 2 == 0) leg[t * L.NLM + (ll / 2) * (ll / 2) + mm] = pll;
+              if (ll % 2 == 0) emit(ll, pll);
             }
           }
         }
       }
       __syncthreads();
       const int rows_here = min(kGdChunk, n - c0);
-      for (int t = warp; t < kGdChunk; t += 8) {
-        for (int col = lane; col < Kp; col += 32) {
-          double val = 0.0;
-          if (col < K && t < rows_here) {
-            const int cm = col_map[col];
-            const int lk = cm & 0xff, tm = task_map[NL + lk];
-            const int m = tm >> 16, l = (tm >> 8) & 0xff, k = tm & 0xff;
-            double sh;
-            if (l == 0) {
-              sh = 1.0 / sqrt(4.0 * CUDART_PI);
-            } else {
-              const double pl = shn[lk] * leg[t * L.NLM + (l / 2) * (l / 2) + m];
-              const double s2 = sqrt(2.0);
-              if (k < l)
-                sh = s2 * pl * trg[t * L.NTR + m - 1];
-              else if (k == l)
-                sh = pl;
-              else
-                sh = s2 * (((m + 1) % 2 == 0) ? 1.0 : -1.0) * pl * trg[t * L.NTR + p.radial_order + m - 1];
-            }
-            val = rad[t * NL + (cm >> 8)] * sh;
-          }
-          Mc[t * LDM + col] = val;
-        }
-      }
-      __syncthreads();
       for (int col = tid; col < K; col += blockDim.x) {
+        const int cm = col_map[col], rj = cm & 0xffff, yj = cm >> 16;
         double a = vb[col];
-        for (int t = 0; t < rows_here; ++t) a = __dadd_rn(a, __dmul_rn(Mc[t * LDM + col], geo[8 * t + 3]));
+        for (int t = 0; t < rows_here; ++t)
+          a = __dadd_rn(a, __dmul_rn(Rv[t * RS + rj] * Yv[t * YS + yj], geo[8 * t + 3]));
         vb[col] = a;
       }
-#pragma unroll 1
-      for (int kk = 0; kk < (rows_here + 3) / 4; ++kk) {  // rows past n are zero
-        const double* rowp = Mc + (4 * kk + q) * LDM + g;
+      // this warp's tiles: the operand fragments of a k-step are design
+      // entries (rows 4 kk + q, this lane's columns), formed as radial factor
+      // x SH value; rows past n are zero
+#pragma unroll 2
+      for (int kk = 0; kk < (rows_here + 3) / 4; ++kk) {
+        const double* Rr = Rv + (4 * kk + q) * RS;
+        const double* Yr = Yv + (4 * kk + q) * YS;
+        double fa[GS], fb[GS];
 #pragma unroll
-        for (int s = 0; s < TPW; ++s)
-          if ((tile[s] & 0xff) < MT) dmma_m8n8k4(acc[s][0], acc[s][1], rowp[8 * (tile[s] >> 8)], rowp[8 * (tile[s] & 0xff)]);
+        for (int i = 0; i < GS; ++i) {
+          fa[i] = Rr[ca[i] & 0xffff] * Yr[ca[i] >> 16];
+          fb[i] = Rr[cb[i] & 0xffff] * Yr[cb[i] >> 16];
+        }
+        if (is_rect) {
+#pragma unroll
+          for (int i = 0; i < GS; ++i)
+#pragma unroll
+            for (int j = 0; j < GS; ++j)
+              if (gb * GS + j < MT) dmma_m8n8k4(acc[i * GS + j][0], acc[i * GS + j][1], fa[i], fb[j]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < GS; ++i)
+#pragma unroll
+            for (int j = i; j < GS; ++j) {
+              const int e = i * GS - i * (i - 1) / 2 + (j - i);  // (i, j) in the packed triangle
+              if (ga * GS + j < MT) dmma_m8n8k4(acc[e][0], acc[e][1], fa[i], fa[j]);
+              if (GP::TPT == 2 && gb * GS + j < MT)
+                dmma_m8n8k4(acc[GP::TRI + e][0], acc[GP::TRI + e][1], fb[i], fb[j]);
+            }
+        }
       }
       __syncthreads();
     }
     // G from the tiles (and the mirror of each off-diagonal tile)
-#pragma unroll
-    for (int s = 0; s < TPW; ++s) {
-      const int mt = tile[s] >> 8, nt = tile[s] & 0xff;
-      if (nt >= MT) continue;
-      const int i = 8 * mt + g;
+    auto put = [&](int mt, int nt, const double (&d)[2]) {
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
-        const int j = 8 * nt + 2 * q + e;
+        const int i = 8 * mt + g, j = 8 * nt + 2 * q + e;
         if (i < K && j < K) {
-          G[i * L.LDG + j] = acc[s][e];
-          if (mt != nt) G[j * L.LDG + i] = acc[s][e];  // a diagonal tile holds both halves itself
+          G[i * L.LDG + j] = d[e];
+          if (mt != nt) G[j * L.LDG + i] = d[e];  // a diagonal tile holds both halves itself
         }
       }
+    };
+    if (is_rect) {
+#pragma unroll
+      for (int i = 0; i < GS; ++i)
+#pragma unroll
+        for (int j = 0; j < GS; ++j)
+          if (ga * GS + i < MT && gb * GS + j < MT) put(ga * GS + i, gb * GS + j, acc[i * GS + j]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < GS; ++i)
+#pragma unroll
+        for (int j = i; j < GS; ++j) {
+          const int e = i * GS - i * (i - 1) / 2 + (j - i);
+          if (ga * GS + j < MT) put(ga * GS + i, ga * GS + j, acc[e]);
+          if (GP::TPT == 2 && gb * GS + j < MT) put(gb * GS + i, gb * GS + j, acc[GP::TRI + e]);
+        }
     }
     __syncthreads();
 
@@ -461,13 +550,16 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
       __syncthreads();
       int msteps = m;
       double beta_prev = 0.0;
+      // three barriers a step: w_i, v_i and v_prev_i are this thread's own
+      // entries (one row of the product per thread), the two sums use slots
+      // 0-7 and 8-15 of `red` (each read before the step's last barrier), and
+      // the last barrier orders the new v before the next step's product
       for (int j = 0; j < m; ++j) {
         gd_gemv(G, LDG, K, lv, lw);
-        __syncthreads();
         const double wi = (tid < K) ? lw[tid] : 0.0, vi = (tid < K) ? lv[tid] : 0.0;
-        const double al = gd_block_sum(wi * vi, red);
+        const double al = gd_block_sum_fresh(wi * vi, red);
         const double wn = (tid < K) ? wi - al * vi - beta_prev * lv_prev[tid] : 0.0;
-        const double bt = sqrt(gd_block_sum(wn * wn, red));
+        const double bt = sqrt(gd_block_sum_fresh(wn * wn, red + 8));
         if (tid == 0) {
           ta[j] = al;
           tb[j] = bt;
@@ -529,10 +621,14 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
       __syncthreads();
       int it = 0;
       converged = false;
+      // tol 0 (a fixed iteration count) needs no stopping test: no reductions
+      const bool check = tol > 0.0;
+      double mom_next = (max_it > 0) ? p.mom[0] : 0.0;
       while (n > 0 && it < max_it) {
+        const double mom = mom_next;
+        if (it + 1 < max_it) mom_next = p.mom[it + 1];  // in flight during the product
         gd_gemv(G, LDG, K, vy, vgy);
         __syncthreads();
-        const double mom = p.mom[it];
         double dx2 = 0.0, xn2 = 0.0;
         if (tid < K) {
           const int i = tid;
@@ -552,6 +648,11 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
           dx2 = __dmul_rn(d, d);
           xn2 = __dmul_rn(xn, xn);
         }
+        if (!check) {
+          ++it;
+          __syncthreads();  // the new y before the next product
+          continue;
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
           dx2 += __shfl_xor_sync(kFull, dx2, o);
@@ -569,12 +670,14 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
         }
         ++it;
         const double rel = sqrt(sdx) / fmax(sqrt(sxn), 1e-12);
-        __syncthreads();  // red and vy are rewritten next iteration
+        // no barrier here: red is next written after the next iteration's
+        // first barrier, which every thread reaches only once it has read it
         if (rel < tol) {
           converged = true;
           break;
         }
       }
+      __syncthreads();  // the polish reuses red and the vectors as scratch
       return it;
     };
     bool converged = false;
