@@ -795,7 +795,7 @@ def fwd_bwd_block(args, device: int, world: int) -> dict:
             out.update(block)
             out["solver"] = "L1 FISTA, alpha 0.01 (tol 1e-6), implicit differentiation on the support"
         else:
-            out["l2"] = dict(block, solver="Tikhonov, lambda_n = lambda_l = 0.05, transpose solve")
+            out["l2"] = dict(block, solver="Tikhonov, lambda_n = lambda_l = 0.05, adjoint as one product with H^-1")
     return out
 
 
