@@ -805,7 +805,10 @@ def graddev_block(args, device: int, world: int) -> dict:
     samples dropped, radial order 8 (K = 145), alpha 0.01: the reference's
     FISTA (`value`), and the certified optimum of each voxel's design
     (precision "fp64-kkt": 32 FISTA iterations, the polish on the voxel's own
-    Gram matrix, the KKT certificate).  CUDA events on the fit stream, max
+    Gram matrix, the KKT certificate), and its mixed-precision form
+    ("mixed-kkt": the Lanczos estimate and the support iterations in FP32 on
+    the hi plane of G_v, the polish in FP64 on hi + lo) with its error per
+    output (coefficients, RTOP, GFA) against the FP64 certified optimum.  CUDA events on the fit stream, max
     over ranks; min(steps, 3) timed steps (each builds 300k Gram matrices of
     145 x 145)."""
     import torch
@@ -836,6 +839,9 @@ def graddev_block(args, device: int, world: int) -> dict:
     it = float(out["iterations"].double().mean())
     ms_k, out_k = timed("fp64-kkt")
     t = _abi.last_timing(device)
+    ms_m, out_m = timed("mixed-kkt")
+    t_m = _abi.last_timing(device)
+    errors = graddev_output_errors(out_k["coefficients"], out_m["coefficients"], device)
     return {"metric": "per-voxel-design L1-fit voxels/s", "value": world * GRADDEV_VOXELS / (ms * 1e-3),
             "unit": "voxels/s", "ms_per_step": ms, "steps": steps,
             "workload": f"graddev300k: {GRADDEV_VOXELS} voxels, radial order 8 (K = 145), N = {S.shape[1]}, "
@@ -845,7 +851,47 @@ def graddev_block(args, device: int, world: int) -> dict:
                     "speedup_vs_reference_rule": ms / ms_k, "uncertified_voxels": t.kkt_uncertified,
                     "polish_rounds_per_voxel": t.kkt_rounds / GRADDEV_VOXELS,
                     "support_iterations": t.kkt_iterations,
-                    "certified_fraction": float(out_k["converged"].double().mean())}}
+                    "certified_fraction": float(out_k["converged"].double().mean())},
+            "mixed_kkt": {"value": world * GRADDEV_VOXELS / (ms_m * 1e-3), "ms_per_step": ms_m,
+                          "speedup_vs_reference_rule": ms / ms_m, "speedup_vs_fp64_kkt": ms_k / ms_m,
+                          "uncertified_voxels": t_m.kkt_uncertified,
+                          "certified_fraction": float(out_m["converged"].double().mean()),
+                          "dtype": "f32 Lanczos and support iterations, f64 polish and certificate",
+                          "error_vs_fp64_kkt": errors}}
+
+
+def graddev_output_errors(ref, got, device: int) -> dict:
+    """Per-output error of a per-voxel-design fit (radial order 8, zeta 700)
+    against an FP64 one: coefficients (per-voxel relative L2), RTOP (relative)
+    and GFA (absolute, on the 181-direction hemisphere)."""
+    import ctypes as C
+
+    import torch
+
+    from cs_dmri_b200 import _abi
+    from cs_dmri_b200._core import shore_odf_peaks
+
+    def stats(e):
+        e = np.asarray(e, np.float64)
+        e = e[np.isfinite(e)]
+        return {"median": float(np.median(e)), "p99": float(np.quantile(e, 0.99)), "max": float(e.max())}
+
+    a, b = ref.double().contiguous(), got.double().contiguous()
+    rel = (torch.linalg.norm(a - b, dim=1) / torch.linalg.norm(a, dim=1).clamp_min(1e-300)).cpu().numpy()
+    lib = _abi.load()
+    rt = []
+    for c in (a, b):
+        r = torch.empty(c.shape[0], dtype=torch.float64, device=c.device)
+        err = C.create_string_buffer(1024)
+        _abi.check(lib.csd_shore_rtop_device(_abi.handle(device), 8, 700.0, c.data_ptr(), c.shape[0], r.data_ptr(),
+                                             None, err, len(err)), err)
+        rt.append(r)
+    torch.cuda.synchronize(device)
+    ra, rb = rt[0].cpu().numpy(), rt[1].cpu().numpy()
+    rtop = np.abs(ra - rb) / np.maximum(np.abs(ra), 1e-300)
+    gfa = [shore_odf_peaks(c.cpu().numpy().astype(np.float32).reshape(-1, 1, 1, c.shape[1]), 8, 700.0,
+                           npeaks=1, device=device)["gfa"].ravel() for c in (a, b)]
+    return {"coefficients_rel_l2": stats(rel), "rtop_rel": stats(rtop), "gfa_abs": stats(np.abs(gfa[0] - gfa[1]))}
 
 
 def pipeline_block(ph, device: int, world: int) -> dict:

@@ -30,10 +30,12 @@ extern "C" int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signal
       throw Error{CSD_ERR_INVALID, "the per-voxel-design fit is built for radial orders 6 and 8"};
     if (spec->precision == CSD_PRECISION_MIXED)
       throw Error{CSD_ERR_INVALID, "the per-voxel-design fit takes precision fp64, fp64-kkt or mixed-kkt"};
-    // converged-optimum modes: the support-identification iterations run in
-    // FP64 here (each voxel has its own Gram matrix, so there is no shared
-    // tensor-core operand); the polish and certificate are those of the
-    // shared-design path
+    // converged-optimum modes: the polish and certificate are those of the
+    // shared-design path.  Each voxel has its own Gram matrix, so there is no
+    // shared tensor-core operand: "fp64-kkt" runs the support iterations in
+    // FP64, "mixed-kkt" keeps G_v as FP32 planes hi + lo and runs the Lanczos
+    // estimate and the support iterations in FP32 on hi (half the shared-memory
+    // traffic of the products), the polish in FP64 on hi + lo
     const bool kkt = spec->precision == CSD_PRECISION_MIXED_KKT || spec->precision == CSD_PRECISION_FP64_KKT;
     StreamScope scope(h, stream);
     HandleOrder call_order(h);
@@ -81,6 +83,7 @@ extern "C" int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signal
     p.n_rows = d_n_rows;
     p.iter_total = h->gdq.as<unsigned long long>() + 1;
     p.kkt = kkt ? 1 : 0;
+    p.mixed = spec->precision == CSD_PRECISION_MIXED_KKT ? 1 : 0;
     p.kkt_iters = kkt_iters;
     p.kkt_rounds = h->opt_kkt_rounds;
     p.kappa = kKktKappa;

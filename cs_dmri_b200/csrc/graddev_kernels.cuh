@@ -57,6 +57,10 @@ struct GraddevParams {
   // support, one warp polishes on G_v and certifies (polish_warp); a voxel it
   // cannot certify gets the reference FISTA from zero, uncertified
   int kkt;
+  // mixed != 0 (with kkt): G_v kept as FP32 planes hi + lo; the Lanczos
+  // estimate and the support iterations run in FP32 on hi, the polish and any
+  // fallback in FP64 on hi + lo
+  int mixed;
   int kkt_iters, kkt_rounds;
   double kappa;
   double* kkt_out;                   // V (nullable): largest KKT residual, NaN when uncertified
@@ -72,19 +76,24 @@ struct GraddevParams {
 // padding columns) and NSH SH values (row stride YS); both strides are odd,
 // so the fragment loads of four consecutive rows fall in distinct banks.
 struct GdLayout {
-  int K, Kp, LDG, NL, NSH, RS, YS;
+  int K, Kp, LDG, LDF, NL, NSH, RS, YS;
   size_t g, vec, red, tri, tab, rows, colmap, total_bytes;
   __host__ __device__ GdLayout(int K_, int radial_order, int N) {
     K = K_;
     Kp = 8 * ((K + 7) / 8);
     LDG = K + (K & 1);   // even row stride of G: 16-byte rows, conflict-free 16-byte loads
+    // row stride of the FP32 planes: 16-byte rows, an odd number of them, so
+    // that 8 rows' 16-byte loads at one column fall in distinct banks
+    LDF = 4 * ((K + 3) / 4);
+    if ((LDF / 4) % 2 == 0) LDF += 4;
     NL = 0;
     for (int n = 0; n <= radial_order; ++n) NL += n / 2 + 1;
     NSH = (radial_order / 2 + 1) * (radial_order + 1);
     RS = (NL + 1) | 1;
     YS = NSH | 1;
     const size_t chunk = static_cast<size_t>(kGdChunk) * (RS + YS) + 8 * static_cast<size_t>(N);
-    const size_t gk = static_cast<size_t>(K) * LDG;
+    const size_t gk64 = static_cast<size_t>(K) * LDG, gk32 = static_cast<size_t>(K) * LDF;  // gk32: two FP32 planes
+    const size_t gk = gk64 > gk32 ? gk64 : gk32;
     const size_t gsize = gk > chunk ? gk : chunk;
     g = 0;
     vec = (gsize + 1) & ~static_cast<size_t>(1);           // b, x, y, gy, v_prev, v, w: 7 * Kp
@@ -153,6 +162,52 @@ __device__ __forceinline__ void gd_gemv(const double* G, int LDG, int K, const d
       a1 = fma(g0.y, w0.y, a1);
     }
     if (K & 1) a2 = fma(G[static_cast<size_t>(i) * LDG + K - 1], v[K - 1], a2);
+    out[i] = (a0 + a1) + (a2 + a3);
+  }
+}
+
+// The same product with FP32 entries, vector and sums: G_v's hi plane (row
+// stride LDF), four entries per 16-byte load.
+__device__ __forceinline__ void gd_gemv32(const float* G, int LDF, int K, const float* v, float* out) {
+  for (int i = threadIdx.x; i < K; i += blockDim.x) {
+    const float4* gr = reinterpret_cast<const float4*>(G + static_cast<size_t>(i) * LDF);
+    const float4* v4 = reinterpret_cast<const float4*>(v);
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    const int h = K >> 2;
+#pragma unroll 4
+    for (int j = 0; j < h; ++j) {
+      const float4 g = gr[j], w = v4[j];
+      a0 = fmaf(g.x, w.x, a0);
+      a1 = fmaf(g.y, w.y, a1);
+      a2 = fmaf(g.z, w.z, a2);
+      a3 = fmaf(g.w, w.w, a3);
+    }
+    for (int j = 4 * h; j < K; ++j) a0 = fmaf(G[static_cast<size_t>(i) * LDF + j], v[j], a0);
+    out[i] = (a0 + a1) + (a2 + a3);
+  }
+}
+
+// The FP64 product with G_v rebuilt from its planes (hi + lo per entry).
+__device__ __forceinline__ void gd_gemv_hl(const float* Gh, const float* Gl, int LDF, int K, const double* v,
+                                           double* out) {
+  for (int i = threadIdx.x; i < K; i += blockDim.x) {
+    const float4* hr = reinterpret_cast<const float4*>(Gh + static_cast<size_t>(i) * LDF);
+    const float4* lr = reinterpret_cast<const float4*>(Gl + static_cast<size_t>(i) * LDF);
+    const double2* v2 = reinterpret_cast<const double2*>(v);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    const int h = K >> 2;
+    for (int j = 0; j < h; ++j) {
+      const float4 gh = hr[j], gl = lr[j];
+      const double2 w0 = v2[2 * j], w1 = v2[2 * j + 1];
+      a0 = fma(static_cast<double>(gh.x) + static_cast<double>(gl.x), w0.x, a0);
+      a1 = fma(static_cast<double>(gh.y) + static_cast<double>(gl.y), w0.y, a1);
+      a2 = fma(static_cast<double>(gh.z) + static_cast<double>(gl.z), w1.x, a2);
+      a3 = fma(static_cast<double>(gh.w) + static_cast<double>(gl.w), w1.y, a3);
+    }
+    for (int j = 4 * h; j < K; ++j) {
+      const size_t e = static_cast<size_t>(i) * LDF + j;
+      a0 = fma(static_cast<double>(Gh[e]) + static_cast<double>(Gl[e]), v[j], a0);
+    }
     out[i] = (a0 + a1) + (a2 + a3);
   }
 }
@@ -504,14 +559,30 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
       }
       __syncthreads();
     }
-    // G from the tiles (and the mirror of each off-diagonal tile)
+    // G from the tiles (and the mirror of each off-diagonal tile): FP64, or
+    // in the mixed mode the planes hi = fl32(G), lo = fl32(G - hi)
+    const bool mixed = p.mixed != 0;
+    const int LDF = L.LDF;
+    float* Ghi = reinterpret_cast<float*>(G);
+    float* Glo = Ghi + static_cast<size_t>(K) * LDF;
     auto put = [&](int mt, int nt, const double (&d)[2]) {
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int i = 8 * mt + g, j = 8 * nt + 2 * q + e;
         if (i < K && j < K) {
-          G[i * L.LDG + j] = d[e];
-          if (mt != nt) G[j * L.LDG + i] = d[e];  // a diagonal tile holds both halves itself
+          if (mixed) {
+            const float hi = __double2float_rn(d[e]);
+            const float lo = __double2float_rn(d[e] - static_cast<double>(hi));
+            Ghi[i * LDF + j] = hi;
+            Glo[i * LDF + j] = lo;
+            if (mt != nt) {
+              Ghi[j * LDF + i] = hi;
+              Glo[j * LDF + i] = lo;
+            }
+          } else {
+            G[i * L.LDG + j] = d[e];
+            if (mt != nt) G[j * L.LDG + i] = d[e];  // a diagonal tile holds both halves itself
+          }
         }
       }
     };
@@ -536,16 +607,37 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
     // ---- 3. lambda_max(G) by Lanczos: `steps` steps, the largest Ritz value
     // left in s_lmax (a lower bound of lambda_max, exact to ~1e-12 at 40)
     const int LDG = L.LDG;
-    auto run_lanczos = [&](int steps) {
+    // the FP64 product with G_v (from its planes in the mixed mode)
+    auto gemv64 = [&](const double* vin, double* vout) {
+      if (mixed)
+        gd_gemv_hl(Ghi, Glo, LDF, K, vin, vout);
+      else
+        gd_gemv(G, LDG, K, vin, vout);
+    };
+    // `lowp`: the vectors are FP32 (in the same slots) and the product uses
+    // G_v's hi plane; the sums and the tridiagonal stay FP64
+    auto run_lanczos = [&](int steps, bool lowp) {
       const int m = min(K, steps);
+      float* lv32 = reinterpret_cast<float*>(lv);
+      float* lvp32 = reinterpret_cast<float*>(lv_prev);
+      float* lw32 = reinterpret_cast<float*>(lw);
+      auto get = [&](const double* d, const float* f, int i) -> double {
+        return lowp ? static_cast<double>(f[i]) : d[i];
+      };
+      auto set = [&](double* d, float* f, int i, double x) {
+        if (lowp)
+          f[i] = static_cast<float>(x);
+        else
+          d[i] = x;
+      };
       for (int i = tid; i < Kp; i += blockDim.x) {
-        lv[i] = (i < K) ? 1.0 + 0.5 * sin(1.7 * i + 0.3) : 0.0;  // fixed start vector
-        lv_prev[i] = 0.0;
+        set(lv, lv32, i, (i < K) ? 1.0 + 0.5 * sin(1.7 * i + 0.3) : 0.0);  // fixed start vector
+        set(lv_prev, lvp32, i, 0.0);
       }
       {
-        const double e = (tid < K) ? lv[tid] : 0.0;  // K <= blockDim.x
+        const double e = (tid < K) ? get(lv, lv32, tid) : 0.0;  // K <= blockDim.x
         const double inv = 1.0 / sqrt(gd_block_sum(e * e, red));
-        if (tid < K) lv[tid] *= inv;
+        if (tid < K) set(lv, lv32, tid, get(lv, lv32, tid) * inv);
       }
       __syncthreads();
       int msteps = m;
@@ -555,10 +647,13 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
       // 0-7 and 8-15 of `red` (each read before the step's last barrier), and
       // the last barrier orders the new v before the next step's product
       for (int j = 0; j < m; ++j) {
-        gd_gemv(G, LDG, K, lv, lw);
-        const double wi = (tid < K) ? lw[tid] : 0.0, vi = (tid < K) ? lv[tid] : 0.0;
+        if (lowp)
+          gd_gemv32(Ghi, LDF, K, lv32, lw32);
+        else
+          gemv64(lv, lw);
+        const double wi = (tid < K) ? get(lw, lw32, tid) : 0.0, vi = (tid < K) ? get(lv, lv32, tid) : 0.0;
         const double al = gd_block_sum_fresh(wi * vi, red);
-        const double wn = (tid < K) ? wi - al * vi - beta_prev * lv_prev[tid] : 0.0;
+        const double wn = (tid < K) ? wi - al * vi - beta_prev * get(lv_prev, lvp32, tid) : 0.0;
         const double bt = sqrt(gd_block_sum_fresh(wn * wn, red + 8));
         if (tid == 0) {
           ta[j] = al;
@@ -569,8 +664,8 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
           break;
         }
         if (tid < K) {
-          lv_prev[tid] = vi;
-          lv[tid] = wn / bt;
+          set(lv_prev, lvp32, tid, vi);
+          set(lv, lv32, tid, wn / bt);
         }
         beta_prev = bt;
         __syncthreads();
@@ -603,7 +698,7 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
     // the converged-optimum mode only needs a safe step for its support
     // iterations (the polish certifies the minimiser whatever the path): fewer
     // steps and a margin; a voxel it does not certify reruns the full count
-    run_lanczos(p.kkt ? kGdLanczosKkt : kGdLanczos);
+    run_lanczos(p.kkt ? kGdLanczosKkt : kGdLanczos, mixed);
     const double nv = static_cast<double>(n);
     double lip = (n > 0) ? fmax(s_lmax / nv, 2.220446049250313e-16) : 0.0;
 
@@ -627,7 +722,7 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
       while (n > 0 && it < max_it) {
         const double mom = mom_next;
         if (it + 1 < max_it) mom_next = p.mom[it + 1];  // in flight during the product
-        gd_gemv(G, LDG, K, vy, vgy);
+        gemv64(vy, vgy);
         __syncthreads();
         double dx2 = 0.0, xn2 = 0.0;
         if (tid < K) {
@@ -680,8 +775,45 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
       __syncthreads();  // the polish reuses red and the vectors as scratch
       return it;
     };
+    // the mixed mode's support iterations: the same update in FP32 on G_v's
+    // hi plane, a fixed count, x_i and b_i in the registers of thread i and y
+    // in FP32 in y's slot; x is left in FP64 in vx for the polish
+    auto run_fista32 = [&](int iters) -> int {
+      float* y32 = reinterpret_cast<float*>(vy);
+      float* gy32 = reinterpret_cast<float*>(vgy);
+      const float step32 = static_cast<float>(step), thr32 = static_cast<float>(thr);
+      const float ninv32 = static_cast<float>(n_inv);
+      const float bi = (tid < K) ? static_cast<float>(vb[tid]) : 0.f;
+      float xi = 0.f;
+      for (int i = tid; i < Kp; i += blockDim.x) y32[i] = 0.f;
+      __syncthreads();
+      double mom_next = (iters > 0) ? p.mom[0] : 0.0;
+      for (int it = 0; n > 0 && it < iters; ++it) {
+        const float mom = static_cast<float>(mom_next);
+        if (it + 1 < iters) mom_next = p.mom[it + 1];
+        gd_gemv32(Ghi, LDF, K, y32, gy32);
+        __syncthreads();
+        if (tid < K) {
+          const float grad = (gy32[tid] - bi) * ninv32;
+          const float cand = y32[tid] - step32 * grad;
+          float sv = 0.f;
+          if (cand > thr32)
+            sv = cand - thr32;
+          else if (cand < -thr32)
+            sv = cand + thr32;
+          const float xn = p.non_negative ? fmaxf(sv, 0.f) : sv;
+          y32[tid] = xn + mom * (xn - xi);
+          xi = xn;
+        }
+        __syncthreads();  // the new y before the next product
+      }
+      for (int i = tid; i < Kp; i += blockDim.x) vx[i] = (i == tid && i < K) ? static_cast<double>(xi) : 0.0;
+      __syncthreads();
+      return n > 0 ? iters : 0;
+    };
     bool converged = false;
-    int it = run_fista(p.kkt ? p.kkt_iters : p.max_iter, p.kkt ? 0.0 : p.tol, converged);
+    int it = (p.kkt && mixed) ? run_fista32(p.kkt_iters)
+                              : run_fista(p.kkt ? p.kkt_iters : p.max_iter, p.kkt ? 0.0 : p.tol, converged);
     double kkt_val = 0.0;
     int rounds = 0;
     if (p.kkt) {
@@ -708,9 +840,11 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
         }
         __syncwarp();
         bool ovf = false;
-        const bool cert = polish_warp<RPL, 1>(G, LDG, K, Kp, cap, vb, fl, c, T, zw, zj, sidx, gd_tri, nv, n_inv,
-                                              alpha_v, p.non_negative, p.kappa, p.kkt_rounds, rounds, kkt_val,
-                                              ovf);
+        const bool cert =
+            mixed ? polish_warp<RPL, 1>(GramHiLo{Ghi, Glo, LDF}, K, Kp, cap, vb, fl, c, T, zw, zj, sidx, gd_tri, nv,
+                                        n_inv, alpha_v, p.non_negative, p.kappa, p.kkt_rounds, rounds, kkt_val, ovf)
+                  : polish_warp<RPL, 1>(GramDense{G, LDG}, K, Kp, cap, vb, fl, c, T, zw, zj, sidx, gd_tri, nv,
+                                        n_inv, alpha_v, p.non_negative, p.kappa, p.kkt_rounds, rounds, kkt_val, ovf);
         if (cert) {
 #pragma unroll
           for (int qq = 0; qq < RPL; ++qq)
@@ -728,7 +862,7 @@ __global__ void __launch_bounds__(256, (MT <= 9) ? 2 : 1) k_graddev_fit(GraddevP
       kkt_val = s_lmax;
       __syncthreads();
       if (!cert && n > 0) {  // the reference FISTA from zero, reported uncertified
-        run_lanczos(kGdLanczos);  // the reference's step, from the full Lanczos count
+        run_lanczos(kGdLanczos, false);  // the reference's step, from the full Lanczos count
         lip = fmax(s_lmax / nv, 2.220446049250313e-16);
         step = 1.0 / lip;
         thr = __dmul_rn(step, alpha_v);

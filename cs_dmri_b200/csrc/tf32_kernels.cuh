@@ -386,17 +386,34 @@ __device__ __forceinline__ void tri_entry(const uint16_t* tab, int e, int& r, in
   }
 }
 
+// Symmetric Gram matrix read by the polish: FP64 entries G[i * ld + j] in
+// global or shared memory ...
+struct GramDense {
+  const double* p;
+  int ld;
+  __device__ __forceinline__ double operator()(int i, int j) const { return p[i * ld + j]; }
+};
+// ... or two FP32 planes hi + lo with G = hi + lo to 48 bits (hi = fl32(G),
+// lo = fl32(G - hi)), each entry rebuilt in FP64.
+struct GramHiLo {
+  const float* hi;
+  const float* lo;
+  int ld;
+  __device__ __forceinline__ double operator()(int i, int j) const {
+    return static_cast<double>(hi[i * ld + j]) + static_cast<double>(lo[i * ld + j]);
+  }
+};
+
 // The active-set polish of one voxel by one warp (the method described at
-// k_l1_polish below).  G (entry (i, j) at G[i * ldg + j], symmetric) may be in
-// global or shared memory; bw (Kp doubles) holds b; fl (Kp ints) the signs of
+// k_l1_polish below).  G is a GramDense or GramHiLo; bw (Kp doubles) holds b; fl (Kp ints) the signs of
 // the starting support and c (coefficient j = lane + 32 q) the starting
 // point, both set by the caller; T, zw, zj, sidx are the warp's scratch (a
 // support of up to `cap`).  On return c holds the certified minimiser when
 // the voxel is certified; `round` counts the solves, `kkt_val` is the largest
 // KKT residual of a certified voxel, `overflowed` reports a support above
 // `cap` (the caller retries with more room).
-template <int RPL, int RPS>
-__device__ bool polish_warp(const double* G, int ldg, int K, int Kp, int cap, const double* bw, int* fl,
+template <int RPL, int RPS, class GM>
+__device__ bool polish_warp(const GM& G, int K, int Kp, int cap, const double* bw, int* fl,
                             double (&c)[RPL], double* T, double* zw, double* zj, int* sidx,
                             const uint16_t* tri_rc, double n, double n_inv, double alpha, int non_negative,
                             double kappa, int max_rounds, int& round, double& kkt_val, bool& overflowed) {
@@ -428,7 +445,7 @@ __device__ bool polish_warp(const double* G, int ldg, int K, int Kp, int cap, co
       for (int e = lane; e < pk_row(s); e += 32) {
         int i, k;
         tri_entry(tri_rc, e, i, k);
-        T[e] = G[sidx[i] * ldg + sidx[k]];
+        T[e] = G(sidx[i], sidx[k]);
       }
       // right-hand side b_S - n alpha sigma_S in registers: entry q = lane + 32 c
       double rv[RPS];
@@ -546,11 +563,11 @@ __device__ bool polish_warp(const double* G, int ldg, int K, int Kp, int cap, co
 #pragma unroll
       for (int q = 0; q < RPL; ++q) gq[q] = 0.0;
       for (int i = 0; i < s; ++i) {  // G symmetric: row S_i, columns j = lane + 32 q
-        const double* gi = G + sidx[i] * ldg;
+        const int si = sidx[i];
         const double zi = zw[i];
 #pragma unroll
         for (int q = 0; q < RPL; ++q)
-          if (lane + 32 * q < K) gq[q] = fma(gi[lane + 32 * q], zi, gq[q]);
+          if (lane + 32 * q < K) gq[q] = fma(G(si, lane + 32 * q), zi, gq[q]);
       }
 #pragma unroll
       for (int q = 0; q < RPL; ++q) {
@@ -670,7 +687,7 @@ __global__ void __launch_bounds__(256, 4) k_l1_polish(PolishParams p) {
     bool overflowed = false;
     double kkt_val = 0.0;
     int round = 0;
-    const bool certified = polish_warp<RPL, RPS>(p.G, Kp, K, Kp, cap, bw, fl, c, T, zw, zj, sidx, tri_rc, n, n_inv,
+    const bool certified = polish_warp<RPL, RPS>(GramDense{p.G, Kp}, K, Kp, cap, bw, fl, c, T, zw, zj, sidx, tri_rc, n, n_inv,
                                                  alpha, p.non_negative, p.kappa, p.rounds, round, kkt_val,
                                                  overflowed);
     rounds_sum += round;

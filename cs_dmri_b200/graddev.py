@@ -54,9 +54,13 @@ def shore_fit_graddev(signals, bvals, bvecs, graddev=None, sample_mask=None, *, 
     (None = all).  Inputs may be numpy arrays or CUDA tensors; outputs are
     CUDA tensors: ``coefficients`` (V, K) float64, ``iterations``,
     ``converged``, ``lipschitz`` (sigma_max(M_v)^2 / n_v) and ``n_samples``.
-    ``precision="fp64-kkt"`` (or "mixed-kkt") returns every voxel's
-    KKT-certified LASSO optimum on its own design instead of the reference
-    FISTA's stopped iterate; ``converged`` is then the certificate."""
+    ``precision="fp64-kkt"`` returns every voxel's KKT-certified LASSO
+    optimum on its own design instead of the reference FISTA's stopped
+    iterate; ``converged`` is then the certificate.  ``"mixed-kkt"`` returns
+    the same optimum with the Lanczos estimate and the support iterations in
+    FP32 (on the FP32 high part of each voxel's Gram matrix, held as high and
+    low FP32 parts) and the polish and certificate in FP64 (on the two parts
+    together, 48 bits of the matrix)."""
     import torch
 
     dev = torch.device("cuda", device)

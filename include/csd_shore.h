@@ -433,14 +433,18 @@ int csd_shore_rtop_adjoint_device(csd_handle* h, int32_t radial_order, double ze
  * coefficients (n_voxels, K) FP64, iterations, converged, and (nullable) L_v
  * and the kept sample count.  Asynchronous like the entry points above.
  * With precision FP64_KKT or MIXED_KKT each voxel's fit is its certified
- * LASSO optimum (as for csd_shore_fit_volume; the support-identification
- * iterations run in FP64 on the voxel's own Gram matrix, then one warp
- * polishes and certifies): converged = certified, and the call waits for its
- * work and reports the uncertified count and the polish rounds through
+ * LASSO optimum (as for csd_shore_fit_volume; support-identification
+ * iterations on the voxel's own Gram matrix, then one warp polishes and
+ * certifies): converged = certified, and the call waits for its work and
+ * reports the uncertified count and the polish rounds through
  * csd_last_timing.  That mode's support iterations step by 1 / (1.05 L)
  * from a 16-step Lanczos estimate of L_v (the value reported in
  * d_lipschitz); a voxel left uncertified runs the full 40-step estimate and
- * the reference FISTA. */
+ * the reference FISTA.  FP64_KKT runs everything in FP64.  MIXED_KKT keeps
+ * G_v as two FP32 parts hi = fl32(G), lo = fl32(G - hi) (48 bits of G in
+ * the space of the FP64 matrix) and runs the Lanczos estimate and the
+ * support iterations in FP32 on hi; the polish, the certificate and any
+ * uncertified voxel's FISTA run in FP64 on hi + lo. */
 int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signals, int64_t n_voxels,
                                  const csd_gtab* gtab, const csd_shore_spec* spec,
                                  const double* d_graddev, const uint8_t* d_keep,
