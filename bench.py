@@ -851,10 +851,14 @@ def graddev_block(args, device: int, world: int) -> dict:
                     "speedup_vs_reference_rule": ms / ms_k, "uncertified_voxels": t.kkt_uncertified,
                     "polish_rounds_per_voxel": t.kkt_rounds / GRADDEV_VOXELS,
                     "support_iterations": t.kkt_iterations,
+                    "autotune_ms_16_24_32_48": list(t.kkt_tune_ms),
                     "certified_fraction": float(out_k["converged"].double().mean())},
             "mixed_kkt": {"value": world * GRADDEV_VOXELS / (ms_m * 1e-3), "ms_per_step": ms_m,
                           "speedup_vs_reference_rule": ms / ms_m, "speedup_vs_fp64_kkt": ms_k / ms_m,
                           "uncertified_voxels": t_m.kkt_uncertified,
+                          "polish_rounds_per_voxel": t_m.kkt_rounds / GRADDEV_VOXELS,
+                          "support_iterations": t_m.kkt_iterations,
+                          "autotune_ms_16_24_32_48": list(t_m.kkt_tune_ms),
                           "certified_fraction": float(out_m["converged"].double().mean()),
                           "dtype": "f32 Lanczos and support iterations, f64 polish and certificate",
                           "error_vs_fp64_kkt": errors}}

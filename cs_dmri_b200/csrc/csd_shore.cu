@@ -329,6 +329,8 @@ struct csd_handle {
   // converged-optimum modes: the support-identification iteration count the
   // autotuner chose per (table, mode), and its candidates' batch times
   std::map<uint64_t, std::array<float, 5>> kkt_tune_cache;  // -> (iterations, ms at 16, 24, 32, 48)
+  // the same choice for the per-voxel-design fit, per (table, order, mode)
+  std::map<uint64_t, std::array<float, 5>> gd_tune_cache;
   int kkt_iters_used = 0;
   float kkt_tune_ms[4] = {0.f, 0.f, 0.f, 0.f};
   bool kkt_tuning = false;

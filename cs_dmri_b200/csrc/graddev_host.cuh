@@ -52,8 +52,8 @@ extern "C" int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signal
     CSD_CUDA(cudaMemcpyAsync(h->gdtab.p, g.bvals.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st));
     CSD_CUDA(cudaMemcpyAsync(h->gdtab.as<double>() + N, g.bvecs.data(), sizeof(double) * 3 * N,
                              cudaMemcpyHostToDevice, st));
-    const int kkt_iters = h->opt_kkt_iters > 0 ? h->opt_kkt_iters : 32;
-    ensure_mom(h, std::max(spec->max_iter, kkt_iters));
+    int kkt_iters = h->opt_kkt_iters > 0 ? h->opt_kkt_iters : 32;
+    ensure_mom(h, std::max(spec->max_iter, 48));
     h->gdq.ensure(4 * sizeof(unsigned long long));
     CSD_CUDA(cudaMemsetAsync(h->gdq.p, 0, 4 * sizeof(unsigned long long), st));
     csd::GraddevParams p{};
@@ -89,17 +89,75 @@ extern "C" int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signal
     p.kappa = kKktKappa;
     p.n_uncertified = h->gdq.as<unsigned long long>() + 2;
     p.round_total = h->gdq.as<unsigned long long>() + 3;
-    auto go = [&](auto kern) {
+    auto go = [&](auto kern, const csd::GraddevParams& q) {
       CSD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(lay.total_bytes)));
-      const int grid = static_cast<int>(std::min<int64_t>(h->num_sms, n_voxels));
-      kern<<<grid, 256, lay.total_bytes, st>>>(p);
+      const int grid = static_cast<int>(std::min<int64_t>(h->num_sms, q.V));
+      kern<<<grid, 256, lay.total_bytes, st>>>(q);
       CSD_LAUNCH();
     };
-    if (K == 72)
-      go(csd::k_graddev_fit<9>);
-    else
-      go(csd::k_graddev_fit<19>);
+    auto launch = [&](const csd::GraddevParams& q) {
+      if (K == 72)
+        go(csd::k_graddev_fit<9>, q);
+      else
+        go(csd::k_graddev_fit<19>, q);
+    };
+    // Autotuning of the certified modes' support-iteration count, once per
+    // (table, radial order, mode): the whole fit of a prefix of this call's
+    // own voxels (24 per SM: their deviation tensors and dropped samples are
+    // what sets the cost) with 16, 24, 32 and 48 iterations, untimed and then
+    // timed, and the fastest count serves this and later calls.  It runs only
+    // for calls of at least four such prefixes (a smaller call takes 32 until
+    // a larger one has tuned the table).  Every count ends at the certified
+    // optimum, so the choice changes the time, not the result.
+    float tune_ms[4] = {0.f, 0.f, 0.f, 0.f};
+    if (kkt && h->opt_kkt_iters <= 0) {
+      static constexpr int kCand[4] = {16, 24, 32, 48};
+      uint64_t key = 1469598103934665603ull;
+      key = fnv1a(key, g.bvals.data(), g.bvals.size() * sizeof(double));
+      key = fnv1a(key, g.bvecs.data(), g.bvecs.size() * sizeof(double));
+      const double sc[6] = {g.tau, g.b0, spec->zeta, static_cast<double>(spec->radial_order),
+                            static_cast<double>(spec->precision), static_cast<double>(spec->non_negative)};
+      key = fnv1a(key, sc, sizeof sc);
+      const int64_t Vt = 24 * static_cast<int64_t>(h->num_sms);
+      const auto hit = h->gd_tune_cache.find(key);
+      if (hit != h->gd_tune_cache.end()) {
+        kkt_iters = static_cast<int>(hit->second[0]);
+        for (int i = 0; i < 4; ++i) tune_ms[i] = hit->second[1 + i];
+      } else if (n_voxels >= 4 * Vt) {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        CSD_CUDA(cudaEventCreate(&e0));
+        CSD_CUDA(cudaEventCreate(&e1));
+        csd::GraddevParams q = p;
+        q.V = Vt;
+        float best = 0.f;
+        int best_k = 32;
+        for (int c = 0; c < 4; ++c) {
+          q.kkt_iters = kCand[c];
+          float ms = 0.f;
+          for (int pass = 0; pass < 2; ++pass) {
+            CSD_CUDA(cudaMemsetAsync(h->gdq.p, 0, 4 * sizeof(unsigned long long), st));
+            CSD_CUDA(cudaEventRecord(e0, st));
+            launch(q);
+            CSD_CUDA(cudaEventRecord(e1, st));
+            CSD_CUDA(cudaEventSynchronize(e1));
+            if (pass == 1 && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) ms = 0.f;
+          }
+          tune_ms[c] = ms;
+          if (ms > 0.f && (best == 0.f || ms < best)) {
+            best = ms;
+            best_k = kCand[c];
+          }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        kkt_iters = best_k;
+        h->gd_tune_cache[key] = {static_cast<float>(best_k), tune_ms[0], tune_ms[1], tune_ms[2], tune_ms[3]};
+        CSD_CUDA(cudaMemsetAsync(h->gdq.p, 0, 4 * sizeof(unsigned long long), st));
+      }
+    }
+    p.kkt_iters = kkt_iters;
+    launch(p);
     if (kkt) {  // the certificate counters (this mode waits for its work)
       unsigned long long c[2] = {0, 0};
       CSD_CUDA(cudaMemcpyAsync(c, h->gdq.as<unsigned long long>() + 2, sizeof c, cudaMemcpyDeviceToHost, st));
@@ -107,6 +165,7 @@ extern "C" int csd_shore_fit_graddev_device(csd_handle* h, const float* d_signal
       h->timing.kkt_uncertified = static_cast<int64_t>(c[0]);
       h->timing.kkt_rounds = c[1];
       h->timing.kkt_iterations = kkt_iters;
+      for (int i = 0; i < 4; ++i) h->timing.kkt_tune_ms[i] = tune_ms[i];
     }
   } catch (const Error& e) {
     set_err(err, err_len, e.msg);

@@ -130,3 +130,34 @@ def test_mixed_kkt_per_voxel_design_against_fp64_kkt(inputs, order):
     assert np.abs(la - lb).max() <= 1e-5 * la.max()
     with pytest.raises(Exception, match="precision fp64, fp64-kkt or mixed-kkt"):
         shore_fit_graddev(S, bvals, bvecs, T, keep, precision="mixed", **kw)
+
+
+def test_certified_support_iterations_autotuned():
+    """A certified per-voxel-design call of at least four tuning prefixes (24
+    voxels per SM each) picks the support-iteration count by timing 16, 24, 32
+    and 48 on its own first voxels, once per table, order and mode; a later
+    call takes the cached count.  The fit ends at the certified optimum
+    whatever the count: the same coefficients (1e-9) as a forced count of 32."""
+    import torch
+
+    from cs_dmri_b200 import _abi
+    from cs_dmri_b200.graddev import graddev_phantom, shore_fit_graddev
+    n = 4 * 24 * torch.cuda.get_device_properties(0).multi_processor_count + 16
+    S, bvals, bvecs, T, keep, big, small = graddev_phantom(n, seed=9)
+    kw = dict(alpha=0.01, radial_order=6, big_delta=big, small_delta=small, precision="mixed-kkt")
+    _abi.set_option(_abi.OPT_KKT_ITERATIONS, 32)
+    try:
+        forced = shore_fit_graddev(S, bvals, bvecs, T, keep, **kw)
+    finally:
+        _abi.set_option(_abi.OPT_KKT_ITERATIONS, 0)
+    tuned = shore_fit_graddev(S, bvals, bvecs, T, keep, **kw)
+    t = _abi.last_timing(0)
+    assert t.kkt_iterations in (16, 24, 32, 48) and min(t.kkt_tune_ms) > 0.0
+    assert t.kkt_uncertified == 0 and bool(tuned["converged"].all())
+    again = shore_fit_graddev(S, bvals, bvecs, T, keep, **kw)
+    t2 = _abi.last_timing(0)
+    assert t2.kkt_iterations == t.kkt_iterations and list(t2.kkt_tune_ms) == list(t.kkt_tune_ms)
+    a, b = forced["coefficients"].cpu().numpy(), tuned["coefficients"].cpu().numpy()
+    rel = np.linalg.norm(a - b, axis=1) / np.maximum(np.linalg.norm(a, axis=1), 1e-300)
+    assert rel.max() <= 1e-9, rel.max()
+    assert np.array_equal(b, again["coefficients"].cpu().numpy())
