@@ -29,8 +29,11 @@ namespace csd {
 constexpr int kGdChunk = 64;       // design rows per Gram chunk (one thread per row and value group)
 constexpr int kGdLanczos = 40;     // Lanczos steps (capped at K)
 constexpr int kGdRcp = 17;         // reciprocals 1 / i, i < 17 (radial orders <= 16)
-constexpr int kGdLanczosKkt = 16;  // ... in the converged-optimum mode
-constexpr double kGdKktLipMargin = 1.05;  // its step: 1 / (1.05 L) from the 16-step estimate
+// Lanczos steps in the converged-optimum modes, with the support iterations'
+// step 1 / (1.12 L) from that estimate: over sampled brain-phantom designs
+// the 10-step Ritz value stays within 1.048 of lambda_max (16 steps: 1.010)
+constexpr int kGdLanczosKkt = 10;
+constexpr double kGdKktLipMargin = 1.12;
 
 struct GraddevParams {
   const float* S;           // V x N signals

@@ -437,8 +437,8 @@ int csd_shore_rtop_adjoint_device(csd_handle* h, int32_t radial_order, double ze
  * iterations on the voxel's own Gram matrix, then one warp polishes and
  * certifies): converged = certified, and the call waits for its work and
  * reports the uncertified count and the polish rounds through
- * csd_last_timing.  That mode's support iterations step by 1 / (1.05 L)
- * from a 16-step Lanczos estimate of L_v (the value reported in
+ * csd_last_timing.  That mode's support iterations step by 1 / (1.12 L)
+ * from a 10-step Lanczos estimate of L_v (the value reported in
  * d_lipschitz); a voxel left uncertified runs the full 40-step estimate and
  * the reference FISTA.  FP64_KKT runs everything in FP64.  MIXED_KKT keeps
  * G_v as two FP32 parts hi = fl32(G), lo = fl32(G - hi) (48 bits of G in
