@@ -78,8 +78,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--profile-case", choices=["graddev2k", "diff50k", "peaks108k", "fista125k", "kkt64k",
-                                               "icls64k", "tikhonov64k"],
+    ap.add_argument("--profile-case", choices=["graddev2k", "graddev2k-mixed", "diff50k", "peaks108k", "fista125k",
+                                               "kkt64k", "icls64k", "tikhonov64k"],
                     help="run one small profiling workload instead of the benchmark")
     ap.add_argument("--workload", choices=["brain300k", "grid64k"], default="brain300k",
                     help="brain300k: the benchmark volume; grid64k: 40^3 fully masked (profiling case)")
@@ -943,6 +943,17 @@ def case_graddev2k() -> None:
     print("graddev2k: mean iterations", float(out["iterations"].double().mean()))
 
 
+def case_graddev2k_mixed() -> None:
+    import torch
+
+    from cs_dmri_b200.graddev import graddev_phantom, shore_fit_graddev
+    S, bvals, bvecs, T, keep, big, small = graddev_phantom(2000, seed=3)
+    out = shore_fit_graddev(S, bvals, bvecs, T, keep, alpha=0.01, radial_order=8, big_delta=big, small_delta=small,
+                            precision="mixed-kkt")
+    torch.cuda.synchronize()
+    print("graddev2k-mixed: certified fraction", float(out["converged"].double().mean()))
+
+
 def case_diff50k() -> None:
     import torch
 
@@ -1047,7 +1058,7 @@ def case_tikhonov64k() -> None:
     _case_grid64k("tikhonov64k", regularization="l2", lambda_n=0.05, lambda_l=0.05)
 
 
-PROFILE_CASES = {"graddev2k": case_graddev2k, "diff50k": case_diff50k, "peaks108k": case_peaks108k,
+PROFILE_CASES = {"graddev2k": case_graddev2k, "graddev2k-mixed": case_graddev2k_mixed, "diff50k": case_diff50k, "peaks108k": case_peaks108k,
                  "fista125k": case_fista125k, "kkt64k": case_kkt64k, "icls64k": case_icls64k,
                  "tikhonov64k": case_tikhonov64k}
 
